@@ -1,0 +1,332 @@
+"""Benchmark of the B200 ChFSI path (one JSON line on rank 0).
+
+Workload: the 64-atom Kleinman-Bylander cell (a = 20.52 bohr, Ecut 20 Ha,
+37,073 plane waves, 72^3 grid, 160 bands, 256 projectors, seed 0) in FP64.
+A step is one ChFSI iteration as the reference's diagonalize runs it: a
+degree-16 Chebyshev filter (17 H|psi> applies per band incl. the final one
+for Rayleigh-Ritz) followed by Rayleigh-Ritz.  Metric: H|psi> band-applies
+per second (n_bands x 17 per step).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference's algorithm on the host CPU (the C++
+oracle restatement; the reference crate itself cannot be built here) on a
+bounded sample of the same workload, with all host threads.
+For N > 1 (torchrun) every rank runs an independent replica of the workload
+(weak scaling, no collective on the data path); the value is the total over
+ranks divided by the slowest rank's time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "chemrust-scf_b200"))
+
+NDEG = 16
+CONFIG_INDEX = 1
+METRIC = "H|psi> band-applies/s (ChFSI iteration: degree-16 Chebyshev filter + Rayleigh-Ritz)"
+UNIT = "band-applies/s"
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "fallback": True}
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.3)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        mhz, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                mhz.append(float(f[0]))
+                mx = max(mx, float(f[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    import chfsi
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    s = chfsi.SyntheticSystem(config_index=CONFIG_INDEX, seed=rank)
+    ctx = chfsi.Context(s, device=local)
+    # V_eff of the first SCF step: V_loc + V_H + V_xc of the uniform density
+    rho0 = np.full(s.ng, s.n_elec / s.omega)
+    ctx.build_v_eff(rho0)
+    psi0 = s.psi0()
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=local)
+    nb = s.n_bands
+    applies_per_step = nb * (NDEG + 1)
+
+    # ---- device-resident timing: inputs already in HBM ---------------------
+    eig = ctx.diagonalize(NDEG)  # first step from the random start (untimed)
+    for _ in range(args.warmup):
+        eig = ctx.diagonalize(NDEG, eig)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = chfsi.launch_count()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            eig = ctx.diagonalize(NDEG, eig)
+        ev1.record(stream)
+        ev1.synchronize()
+    torch.cuda.synchronize()
+    launches = (chfsi.launch_count() - launches0) // max(1, args.steps)
+    ms = ev0.elapsed_time(ev1)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    ms_step = ms / args.steps
+    value = applies_per_step * args.steps * world / (ms * 1e-3)
+
+    # ---- roofline of the dominant kernel group: local H|psi> (3 FFT passes) -
+    x = torch.from_numpy(psi0).to(f"cuda:{local}")
+    y = torch.empty_like(x)
+    torch.cuda.synchronize()
+    for _ in range(3):
+        ctx.apply_h_local(x.data_ptr(), y.data_ptr(), nb)
+    reps = 10
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        ctx.apply_h_local(x.data_ptr(), y.data_ptr(), nb)
+    e1.record(stream)
+    e1.synchronize()
+    t_loc = e0.elapsed_time(e1) / reps * 1e-3
+    ncol, nz = s.info.n_columns, s.ngrid[2]
+    bytes_per_band = 16 * (4 * ncol * nz + 4 * s.n_pw)  # sticks x4, psi x2, kin-scaled psi, out
+    algo_bytes = bytes_per_band * nb
+    pk = peaks()
+    achieved = algo_bytes / t_loc / 1e9
+    roofline = {"kernel": "local H|psi> (z-sticks inverse, xy-planes x V, z-sticks forward)",
+                "bound": "hbm", "achieved": round(achieved, 1), "peak": pk["hbm_gbs"],
+                "unit": "GB/s", "frac": round(achieved / pk["hbm_gbs"], 4),
+                "traffic": None, "algorithmic_bytes_per_launch": algo_bytes,
+                "launch_ms": round(t_loc * 1e3, 4),
+                "peak_source": "measured" if not pk.get("fallback") else "fallback"}
+
+    # ---- end to end through the C ABI with pinned host buffers -------------
+    host_in = torch.from_numpy(psi0.copy()).pin_memory()
+    host_out = torch.empty_like(host_in).pin_memory()
+    hin, hout = host_in.numpy(), host_out.numpy()
+    for _ in range(2):
+        ctx.set_psi(hin)
+        eig = ctx.diagonalize(NDEG, eig)
+        _get_psi_into(ctx, hout)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(args.steps):
+        ctx.set_psi(hin)
+        eig = ctx.diagonalize(NDEG, eig)
+        _get_psi_into(ctx, hout)
+    t1.record(stream)
+    t1.synchronize()
+    ms_e2e = t0.elapsed_time(t1)
+    if dist:
+        t = torch.tensor([ms_e2e], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e_value = applies_per_step * args.steps * world / (ms_e2e * 1e-3)
+    psi_bytes = psi0.nbytes
+    e2e = {"value": round(e2e_value, 1), "unit": UNIT, "h2d_bytes_per_step": psi_bytes,
+           "d2h_bytes_per_step": psi_bytes + 8 * nb,
+           "api": "chfsi_set_psi + chfsi_diagonalize + chfsi_get_psi (pinned host buffers)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(s, seconds=args.cpu_seconds)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded 64-atom diamond cell; per-rank replica)",
+            "config": {"workload": "64-atom KB-projector cell, a=20.52 bohr, Ecut 20 Ha, "
+                                   "n_pw=%d, grid 72^3, 160 bands, 256 projectors, degree 16, FP64"
+                                   % s.n_pw,
+                       "n_pw": s.n_pw, "n_bands": nb, "ndeg": NDEG, "grid": list(s.ngrid),
+                       "n_proj": s.n_proj, "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "working set (psi 95 MB + beta 152 MB + sticks 250 MB) exceeds the 126 MB L2"},
+            "clocks": clk.summary(),
+            "e2e": e2e,
+            "gpu_launches": int(launches),
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    ctx.close()
+
+
+def _get_psi_into(ctx, out):
+    import ctypes as C
+    import chfsi
+    ctx._c(chfsi.lib().chfsi_get_psi(ctx.handle, out.ctypes.data_as(C.c_void_p)))
+
+
+def cpu_baseline(s, seconds=15.0, steps=1):
+    """Oracle (C++/OpenMP restatement) H|psi> band-applies/s on a bounded sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import oracle
+    o = oracle.Oracle.from_system(s)
+    rho0 = np.full(s.ng, s.n_elec / s.omega)
+    o.build_veff(rho0)
+    psi = s.psi0()
+    nb = 8
+    o.apply_h(psi[:nb])  # warm
+    done, t0 = 0, time.perf_counter()
+    while True:
+        o.apply_h(psi[:nb])
+        done += nb
+        el = time.perf_counter() - t0
+        if el >= seconds:
+            break
+    return {"value": round(done / el, 2), "unit": UNIT, "cores": oracle.lib().oracle_num_threads(),
+            "kind": "port",
+            "sample": "%d band-applies of full H|psi> (T + V_loc + V_NL) on the same 64-atom cell, "
+                      "%.1f s" % (done, el)}
+
+
+def run_reference(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import chfsi
+    import oracle
+    s = chfsi.SyntheticSystem(config_index=CONFIG_INDEX)
+    # sample: a 16-band slice of the workload, degree-16 filter (17 applies/band)
+    nb = 16
+    o = oracle.Oracle(s.ngrid, s.miller(), s.kinetic(), s.beta(), s.proj_offsets(), s.dmat(),
+                      s.psi0()[:nb], s.occupations()[:nb], s.vloc_g(), s.omega, s.gmax,
+                      s.e_ewald, s.n_atoms)
+    o.build_veff(np.full(s.ng, s.n_elec / s.omega))
+    for _ in range(args.warmup):
+        o.set_psi(s.psi0()[:nb])
+        o.chebyshev_filter(NDEG)
+    t = []
+    for _ in range(args.steps):
+        o.set_psi(s.psi0()[:nb])
+        t0 = time.perf_counter()
+        o.chebyshev_filter(NDEG)
+        t.append(time.perf_counter() - t0)
+    tot = sum(t)
+    value = nb * (NDEG + 1) * args.steps / tot
+    cores = oracle.lib().oracle_num_threads()
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 2), "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(tot / args.steps * 1e3, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded 64-atom diamond cell)",
+            "config": {"workload": "64-atom KB-projector cell, a=20.52 bohr, Ecut 20 Ha, "
+                                   "n_pw=%d, grid 72^3, 160 bands, 256 projectors, degree 16, FP64"
+                                   % s.n_pw, "parallelism": "host CPU"},
+            "cpu_baseline": {"value": round(value, 2), "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": "degree-16 Chebyshev filter of a 16-band slice per step"},
+            "e2e": {"value": round(value, 2), "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

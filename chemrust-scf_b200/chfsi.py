@@ -1,0 +1,460 @@
+"""ctypes binding of libchfsi_b200.so (include/chfsi.h).
+
+Python-side mirror of the chemrust-scf ChFSI interface (paths relative to
+that project):
+
+    Context.chebyshev_filter   src/eigensolver/chebyshev.rs:626   chebyshev_filter()
+    Context.rayleigh_ritz      src/eigensolver/rayleigh_ritz.rs:48 rayleigh_ritz()
+    Context.diagonalize        src/scf.rs:169 ScfIteration::diagonalize()
+    Context.apply_h            src/eigensolver/chebyshev.rs:371 apply_full_hamiltonian()
+    Context.construct_density  src/scf.rs:275 construct_density()
+    Context.build_v_eff        src/scf.rs:157 build_v_eff()
+    Context.run_scf            src/scf.rs:358 run_scf()
+
+Errors are raised as ChfsiError subclasses named after the crate's Error
+variants (src/types.rs:226-248).  There is no CPU fallback: every compute
+call goes to the CUDA library, and creating a context without a GPU raises
+NoDevice.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libchfsi_b200.so")
+
+OK, NOT_CONVERGED, NOT_IMPLEMENTED, CHEB_DIVERGED, RR_FAILED, CUDA_ERROR, BAD_INPUT, \
+    NO_DEVICE, OUT_OF_MEMORY, NUMERIC = 0, -1, -2, -3, -4, -5, -6, -7, -8, -9
+PREC_FP64, PREC_MIXED = 0, 1
+BOUND_HEURISTIC, BOUND_LANCZOS = 0, 1
+
+
+class ChfsiError(RuntimeError):
+    status = None
+
+
+class NotConverged(ChfsiError):
+    status = NOT_CONVERGED
+
+
+class NotImplementedErr(ChfsiError):
+    status = NOT_IMPLEMENTED
+
+
+class ChebyshevDiverged(ChfsiError):
+    status = CHEB_DIVERGED
+
+
+class RayleighRitzFailed(ChfsiError):
+    status = RR_FAILED
+
+
+class CudaError(ChfsiError):
+    status = CUDA_ERROR
+
+
+class BadInput(ChfsiError):
+    status = BAD_INPUT
+
+
+class NoDevice(ChfsiError):
+    status = NO_DEVICE
+
+
+class OutOfMemory(ChfsiError):
+    status = OUT_OF_MEMORY
+
+
+class NumericError(ChfsiError):
+    status = NUMERIC
+
+
+_ERRORS = {c.status: c for c in (NotConverged, NotImplementedErr, ChebyshevDiverged,
+                                  RayleighRitzFailed, CudaError, BadInput, NoDevice, OutOfMemory,
+                                  NumericError)}
+
+
+class SynthParams(C.Structure):
+    _fields_ = [("lattice", C.c_int), ("n_rep", C.c_int), ("a_conv", C.c_double),
+                ("jitter", C.c_double), ("z_val", C.c_double), ("rc_loc", C.c_double),
+                ("ecut", C.c_double), ("ngrid", C.c_int * 3), ("n_bands", C.c_int),
+                ("n_shell", C.c_int), ("rc_proj", C.c_double * 4), ("lmax", C.c_int),
+                ("d_min", C.c_double), ("d_max", C.c_double), ("uspp", C.c_int),
+                ("q_width", C.c_double), ("q_amp", C.c_double), ("kpt", C.c_double * 3),
+                ("seed", C.c_uint64)]
+
+
+class SystemInfo(C.Structure):
+    _fields_ = [("ngrid", C.c_int * 3), ("n_pw", C.c_int), ("n_bands", C.c_int),
+                ("n_occ", C.c_int), ("n_atoms", C.c_int), ("n_proj", C.c_int),
+                ("n_ions_with_proj", C.c_int), ("n_columns", C.c_int), ("omega", C.c_double),
+                ("n_elec", C.c_double), ("gmax", C.c_double), ("e_ewald", C.c_double),
+                ("lattice", C.c_double * 9)]
+
+
+class Dims(C.Structure):
+    _fields_ = [("ngrid", C.c_int * 3), ("n_pw", C.c_int), ("n_bands", C.c_int),
+                ("n_proj", C.c_int), ("n_ions", C.c_int)]
+
+
+class Config(C.Structure):
+    _fields_ = [("device", C.c_int), ("precision", C.c_int), ("bound_mode", C.c_int),
+                ("lanczos_steps", C.c_int), ("check_norms", C.c_int), ("reserved", C.c_int * 3)]
+
+
+class ScfParams(C.Structure):
+    _fields_ = [("ndeg", C.c_int), ("max_iter", C.c_int), ("tol_per_atom", C.c_double),
+                ("alpha", C.c_double), ("max_hist", C.c_int), ("first_passes", C.c_int),
+                ("kT", C.c_double)]
+
+
+class ScfResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("n_iter", C.c_int), ("e_total", C.c_double),
+                ("e_band", C.c_double), ("e_hartree", C.c_double), ("e_xc", C.c_double),
+                ("e_dc", C.c_double), ("e_entropy", C.c_double), ("mu", C.c_double),
+                ("seconds", C.c_double),
+                ("energies", C.POINTER(C.c_double)), ("eigenvalues", C.POINTER(C.c_double))]
+
+
+_lib = None
+
+
+def lib():
+    """Load libchfsi_b200.so (raises if the extension has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("libchfsi_b200.so is missing: run chemrust-scf_b200/build.py")
+    L = C.CDLL(LIB_PATH)
+    vp, i32p, dp = C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_double)
+    sig = {
+        "chfsi_synth_defaults": [C.c_int, C.POINTER(SynthParams)],
+        "chfsi_system_generate": [C.POINTER(SynthParams), C.POINTER(vp)],
+        "chfsi_system_get_info": [vp, C.POINTER(SystemInfo)],
+        "chfsi_system_get_miller": [vp, i32p],
+        "chfsi_system_get_kinetic": [vp, dp],
+        "chfsi_system_get_vloc_g": [vp, vp],
+        "chfsi_system_get_beta": [vp, vp],
+        "chfsi_system_get_proj_offsets": [vp, i32p],
+        "chfsi_system_get_dmat": [vp, vp],
+        "chfsi_system_get_qmat": [vp, vp],
+        "chfsi_system_get_psi0": [vp, vp],
+        "chfsi_system_get_occupations": [vp, dp],
+        "chfsi_system_get_positions": [vp, dp],
+        "chfsi_default_config": [C.POINTER(Config)],
+        "chfsi_create": [C.POINTER(Dims), C.POINTER(Config), C.POINTER(vp)],
+        "chfsi_create_from_system": [vp, C.POINTER(Config), C.POINTER(vp)],
+        "chfsi_set_basis": [vp, i32p, dp, C.c_double],
+        "chfsi_set_projectors": [vp, vp, i32p, vp],
+        "chfsi_set_veff": [vp, dp],
+        "chfsi_set_psi": [vp, vp],
+        "chfsi_get_psi": [vp, vp],
+        "chfsi_apply_h": [vp, vp, vp, C.c_int],
+        "chfsi_apply_h_local": [vp, vp, vp, C.c_int],
+        "chfsi_get_stream": [vp, C.POINTER(vp)],
+        "chfsi_chebyshev_filter": [vp, C.c_int, dp, C.c_int],
+        "chfsi_rayleigh_ritz": [vp, dp],
+        "chfsi_diagonalize": [vp, C.c_int, dp, C.c_int, dp],
+        "chfsi_get_bounds": [vp, dp],
+        "chfsi_get_filter_norms": [vp, dp, C.c_int],
+        "chfsi_psi_device_ptr": [vp, C.POINTER(vp)],
+        "chfsi_set_vloc_g": [vp, vp],
+        "chfsi_get_vloc": [vp, dp],
+        "chfsi_get_veff": [vp, dp],
+        "chfsi_set_cell": [vp, dp, C.c_double, C.c_int],
+        "chfsi_set_occupations": [vp, dp],
+        "chfsi_construct_density": [vp, dp],
+        "chfsi_build_veff": [vp, dp, dp],
+        "chfsi_get_density": [vp, dp],
+        "chfsi_scf_run": [vp, C.POINTER(ScfParams), C.POINTER(ScfResult)],
+    }
+    for name, args in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = C.c_int
+    L.chfsi_system_destroy.argtypes = [vp]
+    L.chfsi_system_destroy.restype = None
+    L.chfsi_destroy.argtypes = [vp]
+    L.chfsi_destroy.restype = None
+    L.chfsi_launch_count.argtypes = []
+    L.chfsi_launch_count.restype = C.c_longlong
+    L.chfsi_last_error.argtypes = [vp]
+    L.chfsi_last_error.restype = C.c_char_p
+    _lib = L
+    return L
+
+
+def launch_count():
+    """Kernels launched by the library since it was loaded."""
+    return int(lib().chfsi_launch_count())
+
+
+def _check(st, ctx=None):
+    if st == OK:
+        return
+    msg = lib().chfsi_last_error(ctx)
+    msg = msg.decode() if msg else ""
+    raise _ERRORS.get(st, ChfsiError)("chfsi status %d: %s" % (st, msg))
+
+
+def _ptr(a, ctype=None):
+    if ctype is None:
+        return a.ctypes.data_as(C.c_void_p)
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+# ---------------------------------------------------------------------------
+# Synthetic systems
+# ---------------------------------------------------------------------------
+class SyntheticSystem:
+    """Seeded synthetic plane-wave system (lattice, G-sphere, V_loc, projectors, psi0)."""
+
+    def __init__(self, params=None, config_index=None, **overrides):
+        L = lib()
+        if params is None:
+            params = SynthParams()
+            _check(L.chfsi_synth_defaults(0 if config_index is None else config_index,
+                                          C.byref(params)))
+        for k, v in overrides.items():
+            if k in ("ngrid", "rc_proj", "kpt"):
+                arr = getattr(params, k)
+                for i, x in enumerate(v):
+                    arr[i] = x
+            else:
+                setattr(params, k, v)
+        self.params = params
+        h = C.c_void_p()
+        _check(L.chfsi_system_generate(C.byref(params), C.byref(h)))
+        self.handle = h
+        info = SystemInfo()
+        _check(L.chfsi_system_get_info(h, C.byref(info)))
+        self.info = info
+        self.ngrid = tuple(info.ngrid)
+        self.n_pw, self.n_bands, self.n_occ = info.n_pw, info.n_bands, info.n_occ
+        self.n_atoms, self.n_proj, self.n_ions = info.n_atoms, info.n_proj, info.n_ions_with_proj
+        self.omega, self.n_elec, self.gmax, self.e_ewald = info.omega, info.n_elec, info.gmax, info.e_ewald
+        self.lattice = np.array(info.lattice[:]).reshape(3, 3)
+
+    def __del__(self):
+        if getattr(self, "handle", None) and _lib is not None:
+            _lib.chfsi_system_destroy(self.handle)
+            self.handle = None
+
+    def _get(self, fn, shape, dtype, ctype=None):
+        a = np.zeros(shape, dtype=dtype)
+        _check(getattr(lib(), fn)(self.handle, _ptr(a, ctype)))
+        return a
+
+    @property
+    def ng(self):
+        return int(np.prod(self.ngrid))
+
+    def miller(self):
+        return self._get("chfsi_system_get_miller", (self.n_pw, 3), np.int32, C.c_int32)
+
+    def kinetic(self):
+        return self._get("chfsi_system_get_kinetic", self.n_pw, np.float64, C.c_double)
+
+    def vloc_g(self):
+        return self._get("chfsi_system_get_vloc_g", self.ng, np.complex128)
+
+    def beta(self):
+        return self._get("chfsi_system_get_beta", (self.n_proj, self.n_pw), np.complex128)
+
+    def proj_offsets(self):
+        n = self.n_ions + 1 if self.n_ions else 0
+        return self._get("chfsi_system_get_proj_offsets", n, np.int32, C.c_int32)
+
+    def _blocks_len(self):
+        off = self.proj_offsets()
+        return int(sum((off[i + 1] - off[i]) ** 2 for i in range(len(off) - 1)))
+
+    def dmat(self):
+        return self._get("chfsi_system_get_dmat", self._blocks_len(), np.complex128)
+
+    def qmat(self):
+        return self._get("chfsi_system_get_qmat", self._blocks_len(), np.complex128)
+
+    def psi0(self):
+        return self._get("chfsi_system_get_psi0", (self.n_bands, self.n_pw), np.complex128)
+
+    def occupations(self):
+        return self._get("chfsi_system_get_occupations", self.n_bands, np.float64, C.c_double)
+
+    def positions(self):
+        return self._get("chfsi_system_get_positions", (self.n_atoms, 3), np.float64, C.c_double)
+
+
+# ---------------------------------------------------------------------------
+# Device context
+# ---------------------------------------------------------------------------
+class Context:
+    """Device-resident ChFSI state (one CUDA stream, all buffers on the GPU)."""
+
+    def __init__(self, system=None, dims=None, precision=PREC_FP64, bound_mode=BOUND_HEURISTIC,
+                 lanczos_steps=10, device=0):
+        L = lib()
+        cfg = Config()
+        _check(L.chfsi_default_config(C.byref(cfg)))
+        cfg.device, cfg.precision, cfg.bound_mode, cfg.lanczos_steps = \
+            device, precision, bound_mode, lanczos_steps
+        h = C.c_void_p()
+        if system is not None:
+            _check(L.chfsi_create_from_system(system.handle, C.byref(cfg), C.byref(h)))
+            self.ngrid, self.n_pw, self.n_bands = system.ngrid, system.n_pw, system.n_bands
+        else:
+            d = Dims()
+            for i in range(3):
+                d.ngrid[i] = dims["ngrid"][i]
+            d.n_pw, d.n_bands = dims["n_pw"], dims["n_bands"]
+            d.n_proj, d.n_ions = dims.get("n_proj", 0), dims.get("n_ions", 0)
+            _check(L.chfsi_create(C.byref(d), C.byref(cfg), C.byref(h)))
+            self.ngrid, self.n_pw, self.n_bands = tuple(dims["ngrid"]), d.n_pw, d.n_bands
+        self.handle = h
+        self.ng = int(np.prod(self.ngrid))
+
+    def close(self):
+        if getattr(self, "handle", None) and _lib is not None:
+            _lib.chfsi_destroy(self.handle)
+            self.handle = None
+
+    __del__ = close
+
+    def _c(self, st):
+        _check(st, self.handle)
+
+    # --- set-up -----------------------------------------------------------
+    def set_basis(self, miller, kinetic, gmax):
+        m = np.ascontiguousarray(miller, dtype=np.int32)
+        k = np.ascontiguousarray(kinetic, dtype=np.float64)
+        self._c(lib().chfsi_set_basis(self.handle, _ptr(m, C.c_int32), _ptr(k, C.c_double), gmax))
+
+    def set_projectors(self, beta, proj_offsets, dmat):
+        b = np.ascontiguousarray(beta, dtype=np.complex128)
+        o = np.ascontiguousarray(proj_offsets, dtype=np.int32)
+        d = np.ascontiguousarray(dmat, dtype=np.complex128)
+        self._c(lib().chfsi_set_projectors(self.handle, _ptr(b), _ptr(o, C.c_int32), _ptr(d)))
+
+    def set_veff(self, veff):
+        v = np.ascontiguousarray(veff, dtype=np.float64).ravel()
+        self._c(lib().chfsi_set_veff(self.handle, _ptr(v, C.c_double)))
+
+    def set_psi(self, psi):
+        p = np.ascontiguousarray(psi, dtype=np.complex128)
+        self._c(lib().chfsi_set_psi(self.handle, _ptr(p)))
+
+    def get_psi(self):
+        p = np.zeros((self.n_bands, self.n_pw), dtype=np.complex128)
+        self._c(lib().chfsi_get_psi(self.handle, _ptr(p)))
+        return p
+
+    def set_vloc_g(self, vloc_g):
+        v = np.ascontiguousarray(vloc_g, dtype=np.complex128)
+        self._c(lib().chfsi_set_vloc_g(self.handle, _ptr(v)))
+
+    def set_cell(self, lattice, e_ewald, n_atoms):
+        a = np.ascontiguousarray(lattice, dtype=np.float64).ravel()
+        self._c(lib().chfsi_set_cell(self.handle, _ptr(a, C.c_double), e_ewald, n_atoms))
+
+    def set_occupations(self, occ):
+        o = np.ascontiguousarray(occ, dtype=np.float64)
+        self._c(lib().chfsi_set_occupations(self.handle, _ptr(o, C.c_double)))
+
+    def get_vloc(self):
+        v = np.zeros(self.ng)
+        self._c(lib().chfsi_get_vloc(self.handle, _ptr(v, C.c_double)))
+        return v
+
+    def get_veff(self):
+        v = np.zeros(self.ng)
+        self._c(lib().chfsi_get_veff(self.handle, _ptr(v, C.c_double)))
+        return v
+
+    def psi_device_ptr(self):
+        p = C.c_void_p()
+        self._c(lib().chfsi_psi_device_ptr(self.handle, C.byref(p)))
+        return p.value
+
+    # --- hot path -----------------------------------------------------------
+    def apply_h(self, psi_dev_ptr, hpsi_dev_ptr, nb):
+        """H|psi> on device pointers (e.g. torch CUDA tensors' data_ptr())."""
+        self._c(lib().chfsi_apply_h(self.handle, C.c_void_p(psi_dev_ptr),
+                                    C.c_void_p(hpsi_dev_ptr), nb))
+
+    def apply_h_local(self, psi_dev_ptr, hpsi_dev_ptr, nb):
+        """T + V_loc only, on device pointers."""
+        self._c(lib().chfsi_apply_h_local(self.handle, C.c_void_p(psi_dev_ptr),
+                                          C.c_void_p(hpsi_dev_ptr), nb))
+
+    def stream(self):
+        """The context's cudaStream_t as an integer handle."""
+        p = C.c_void_p()
+        self._c(lib().chfsi_get_stream(self.handle, C.byref(p)))
+        return p.value or 0
+
+    def chebyshev_filter(self, ndeg, eigenvalues=None):
+        if eigenvalues is None:
+            self._c(lib().chfsi_chebyshev_filter(self.handle, ndeg, None, 0))
+        else:
+            e = np.ascontiguousarray(eigenvalues, dtype=np.float64)
+            self._c(lib().chfsi_chebyshev_filter(self.handle, ndeg, _ptr(e, C.c_double), len(e)))
+
+    def rayleigh_ritz(self):
+        w = np.zeros(self.n_bands)
+        self._c(lib().chfsi_rayleigh_ritz(self.handle, _ptr(w, C.c_double)))
+        return w
+
+    def diagonalize(self, ndeg, eigenvalues=None):
+        w = np.zeros(self.n_bands)
+        if eigenvalues is None:
+            self._c(lib().chfsi_diagonalize(self.handle, ndeg, None, 0, _ptr(w, C.c_double)))
+        else:
+            e = np.ascontiguousarray(eigenvalues, dtype=np.float64)
+            self._c(lib().chfsi_diagonalize(self.handle, ndeg, _ptr(e, C.c_double), len(e),
+                                            _ptr(w, C.c_double)))
+        return w
+
+    def bounds(self):
+        b = np.zeros(4)
+        self._c(lib().chfsi_get_bounds(self.handle, _ptr(b, C.c_double)))
+        return b
+
+    def filter_norms(self, ndeg):
+        n = np.zeros(ndeg + 1)
+        self._c(lib().chfsi_get_filter_norms(self.handle, _ptr(n, C.c_double), ndeg + 1))
+        return n
+
+    # --- SCF ---------------------------------------------------------------
+    def construct_density(self):
+        r = np.zeros(self.ng)
+        self._c(lib().chfsi_construct_density(self.handle, _ptr(r, C.c_double)))
+        return r
+
+    def build_v_eff(self, rho):
+        r = np.ascontiguousarray(rho, dtype=np.float64).ravel()
+        e2 = np.zeros(2)
+        self._c(lib().chfsi_build_veff(self.handle, _ptr(r, C.c_double), _ptr(e2, C.c_double)))
+        return e2
+
+    def get_density(self):
+        r = np.zeros(self.ng)
+        self._c(lib().chfsi_get_density(self.handle, _ptr(r, C.c_double)))
+        return r
+
+    def run_scf(self, ndeg, tol_per_atom=1e-6, max_iter=30, alpha=0.3, max_hist=6,
+                first_passes=4, kT=0.01, raise_not_converged=False):
+        p = ScfParams(ndeg, max_iter, tol_per_atom, alpha, max_hist, first_passes, kT)
+        energies = np.zeros(max_iter)
+        eigs = np.zeros(self.n_bands)
+        r = ScfResult()
+        r.energies = _ptr(energies, C.c_double)
+        r.eigenvalues = _ptr(eigs, C.c_double)
+        st = lib().chfsi_scf_run(self.handle, C.byref(p), C.byref(r))
+        if st not in (OK, NOT_CONVERGED) or (st == NOT_CONVERGED and raise_not_converged):
+            _check(st, self.handle)
+        return {"converged": st == OK, "n_iter": r.n_iter, "e_total": r.e_total,
+                "e_band": r.e_band, "e_hartree": r.e_hartree, "e_xc": r.e_xc, "e_dc": r.e_dc,
+                "e_entropy": r.e_entropy, "mu": r.mu,
+                "seconds": r.seconds, "energies": energies[:r.n_iter].copy(), "eigenvalues": eigs}

@@ -1,0 +1,1242 @@
+// chfsi_ctx: device-resident state of one ChFSI problem and the host-side
+// drivers of the filter, Rayleigh-Ritz and SCF steps (C ABI in chfsi.h).
+//
+// Reference correspondence (paths relative to the chemrust-scf project):
+//   chfsi_chebyshev_filter   src/eigensolver/chebyshev.rs:626-816
+//   chfsi_rayleigh_ritz      src/eigensolver/rayleigh_ritz.rs:48-245 with the
+//                            Cholesky-reduction math of subspace_diag.rs:229-391
+//   chfsi_diagonalize        src/scf.rs:169-265
+//   chfsi_scf_run            src/scf.rs:358-376 (+ intended bodies of the
+//                            todo!() transitions, plans/phase-2/PHASE_PLAN.md)
+// Every step runs on the device; the only host<->device traffic inside a
+// diagonalize is the eigenvalue / status read-back at its end (the
+// PcieAccount contract of src/scf.rs:238-251).
+#include "chfsi.h"
+#include "dense.hpp"
+#include "gemm.hpp"
+#include "kernels.hpp"
+#include "launch_count.hpp"
+#include "system.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+namespace chfsi {
+
+std::atomic<long long> g_launch_count{0};
+
+chfsi_status cuda_fail(cudaError_t e, const char* expr, const char* file, int line);
+
+namespace {
+
+thread_local std::string g_last_error;
+
+// ---------------------------------------------------------------- kernels
+__global__ void k_gather_rows(const double2* __restrict__ src, int ld_src,
+                              const int* __restrict__ perm, double2* __restrict__ dst, int n,
+                              int rows) {
+    const size_t tot = (size_t)rows * n;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < tot;
+         t += (size_t)gridDim.x * blockDim.x) {
+        const size_t b = t / n, i = t % n;
+        dst[t] = src[b * ld_src + perm[i]];
+    }
+}
+__global__ void k_scatter_rows(const double2* __restrict__ src, const int* __restrict__ perm,
+                               double2* __restrict__ dst, int ld_dst, int n, int rows) {
+    const size_t tot = (size_t)rows * n;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < tot;
+         t += (size_t)gridDim.x * blockDim.x) {
+        const size_t b = t / n, i = t % n;
+        dst[b * ld_dst + perm[i]] = src[t];
+    }
+}
+// cd[p][b] = sum_{j in ion(p)} D_ion[p - p0][j - p0] cp[j][b]
+__global__ void k_apply_dmat(const double2* __restrict__ cp, double2* __restrict__ cd, int np,
+                             int nb, const int* __restrict__ proj_ion, const int* __restrict__ poff,
+                             const int* __restrict__ doff, const double2* __restrict__ dmat) {
+    const size_t tot = (size_t)np * nb;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < tot;
+         t += (size_t)gridDim.x * blockDim.x) {
+        const int p = (int)(t / nb), b = (int)(t % nb);
+        const int ion = proj_ion[p];
+        const int p0 = poff[ion], ne = poff[ion + 1] - p0;
+        const double2* D = dmat + doff[ion] + (size_t)(p - p0) * ne;
+        double2 s = make_double2(0.0, 0.0);
+        for (int j = 0; j < ne; ++j) {
+            const double2 d = D[j], c = cp[(size_t)(p0 + j) * nb + b];
+            s.x += d.x * c.x - d.y * c.y;
+            s.y += d.x * c.y + d.y * c.x;
+        }
+        cd[t] = s;
+    }
+}
+__global__ void k_fill(double* x, size_t n, double v) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        x[i] = v;
+}
+
+int grid_for(size_t n) {
+    size_t b = (n + 255) / 256;
+    return (int)(b < 148 * 8 ? b : 148 * 8);
+}
+
+// Radices of an axis in DIF order: greedy 8, 4, 2, 3, 5.
+bool plan_axis(int n, AxisPlan& P) {
+    std::memset(&P, 0, sizeof(P));
+    P.n = n;
+    int m = n;
+    for (int r : {8, 4, 2, 3, 5}) {
+        while (m % r == 0) {
+            if (P.nst >= kMaxStages) return false;
+            P.r[P.nst++] = r;
+            m /= r;
+        }
+    }
+    return m == 1 && n >= 1;
+}
+
+// Position of frequency k after the in-place DIF (mixed-radix digit reversal).
+void digit_reversal(const AxisPlan& P, std::vector<int>& pos) {
+    const int n = P.n;
+    pos.assign(n, 0);
+    for (int k = 0; k < n; ++k) {
+        int p = 0, span = n, kk = k;
+        for (int t = 0; t < P.nst; ++t) {
+            const int r = P.r[t];
+            span /= r;
+            p += (kk % r) * span;
+            kk /= r;
+        }
+        pos[k] = p;
+    }
+}
+
+template <typename T> cudaError_t dalloc(T** p, size_t n) {
+    *p = nullptr;
+    if (n == 0) return cudaSuccess;
+    return cudaMalloc((void**)p, n * sizeof(T));
+}
+
+}  // namespace
+
+chfsi_status cuda_fail(cudaError_t e, const char* expr, const char* file, int line) {
+    char buf[512];
+    std::snprintf(buf, sizeof(buf), "CUDA error %s (%s) at %s:%d: %s", cudaGetErrorName(e),
+                  cudaGetErrorString(e), file, line, expr);
+    g_last_error = buf;
+    return e == cudaErrorMemoryAllocation ? CHFSI_ERR_OUT_OF_MEMORY : CHFSI_ERR_CUDA;
+}
+
+}  // namespace chfsi
+
+using namespace chfsi;
+
+struct chfsi_ctx {
+    chfsi_dims dims{};
+    chfsi_config cfg{};
+    int device = 0;
+    cudaStream_t st = nullptr;
+    std::string err;
+    int nx = 0, ny = 0, nz = 0, n_pw = 0, nb = 0, np = 0, nions = 0;
+    size_t ng = 0;
+    bool basis_set = false, veff_set = false, psi_set = false, proj_set = false;
+    bool have_vloc = false;
+    double kin_max = 0.0, omega = 0.0, n_elec = 0.0, e_ewald = 0.0, n_atoms = 1.0;
+    double recip[9] = {};
+    // geometry
+    HGeom geo{};
+    AxisPlan ax{}, ay{}, az{};
+    std::vector<int> dr[3];
+    int* d_col_start = nullptr; int* d_col_pos = nullptr; int* d_pw_col = nullptr;
+    int* d_pw_zpos = nullptr; int* d_xact = nullptr; int* d_idr[3] = {nullptr, nullptr, nullptr};
+    int* d_perm = nullptr; bool perm_identity = true;
+    double* d_kin = nullptr;
+    // potentials
+    double* d_veff = nullptr; double* d_vloc = nullptr; double* d_minmax = nullptr;
+    // projectors
+    double2* d_beta = nullptr; double2* d_dmat = nullptr;
+    int* d_proj_ion = nullptr; int* d_poff = nullptr; int* d_doff = nullptr;
+    double2* d_cp = nullptr; double2* d_cd = nullptr;
+    // wavefunctions
+    double2* d_psi = nullptr; double2* d_psi2 = nullptr; double2* d_hpsi = nullptr;
+    double2* d_nl = nullptr; double2* d_work = nullptr; double2* d_part = nullptr;
+    size_t part_elems = 0;
+    // Rayleigh-Ritz
+    double2* d_H = nullptr; double2* d_S = nullptr; double2* d_T1 = nullptr;
+    double2* d_T2 = nullptr; double2* d_V = nullptr;
+    double* d_eig = nullptr; double* d_eig_prev = nullptr; double* d_jac = nullptr;
+    int* d_flags = nullptr;  // [0] cholesky info, [1] norm-guard degree, [2] jacobi sweeps
+    int jac_max_sweeps = 40;
+    // filter
+    double* d_coef = nullptr; double* d_nsq = nullptr; int max_deg = 64;
+    double h_coef[6] = {};
+    std::vector<double> h_nsq;
+    int last_ndeg = 0;
+    // Lanczos
+    double2* d_lz_v = nullptr; double2* d_lz_v0 = nullptr; double2* d_lz_f = nullptr;
+    double2* d_lz_start = nullptr; double* d_lz = nullptr;
+    // density / SCF
+    double* d_occ = nullptr; std::vector<double> occ;
+    double* d_rho_in = nullptr; double* d_rho_out = nullptr; double* d_rho_next = nullptr;
+    double2* d_cgrid = nullptr; double* d_acc = nullptr;
+    double* d_hist = nullptr;  // 2 * kPulayMax * ng
+    double** d_hist_ptrs = nullptr;
+    double* d_dots = nullptr;
+    // pinned host scratch
+    double* h_pin = nullptr; size_t h_pin_n = 0;
+
+    chfsi_status fail(chfsi_status s, const std::string& m) {
+        err = m;
+        g_last_error = m;
+        return s;
+    }
+};
+
+#define CK(expr)                                                                   \
+    do {                                                                           \
+        cudaError_t _e = (expr);                                                   \
+        if (_e != cudaSuccess) {                                                   \
+            chfsi_status _s = cuda_fail(_e, #expr, __FILE__, __LINE__);            \
+            ctx->err = g_last_error;                                               \
+            return _s;                                                             \
+        }                                                                          \
+    } while (0)
+
+namespace {
+
+chfsi_status ensure_pinned(chfsi_ctx* ctx, size_t n) {
+    if (ctx->h_pin_n >= n) return CHFSI_OK;
+    if (ctx->h_pin) cudaFreeHost(ctx->h_pin);
+    ctx->h_pin = nullptr;
+    ctx->h_pin_n = 0;
+    CK(cudaMallocHost((void**)&ctx->h_pin, n * sizeof(double)));
+    ctx->h_pin_n = n;
+    return CHFSI_OK;
+}
+
+// ---------------------------------------------------------------- H|psi>
+// out = epilogue(H psi) for nb bands of psi (ld n_pw, context PW order).
+chfsi_status apply_h_dev(chfsi_ctx* ctx, const double2* psi, double2* out, int nb, int mode,
+                         double* norm_acc) {
+    Epilogue e{};
+    e.mode = mode;
+    e.kin = ctx->d_kin;
+    e.coef = ctx->d_coef;
+    e.nl = nullptr;
+    e.norm_acc = norm_acc;
+    e.inv_n = 1.0 / (double)ctx->ng;
+    if (ctx->np > 0) {
+        // C = beta^H psi, C <- D C, nl = beta C  (chebyshev.rs:416-500)
+        gemm_cn(ctx->d_beta, ctx->n_pw, psi, ctx->n_pw, ctx->np, nb, ctx->n_pw, ctx->d_part,
+                ctx->d_cp, ctx->st);
+        count_launch();
+        k_apply_dmat<<<grid_for((size_t)ctx->np * nb), 256, 0, ctx->st>>>(
+            ctx->d_cp, ctx->d_cd, ctx->np, nb, ctx->d_proj_ion, ctx->d_poff, ctx->d_doff,
+            ctx->d_dmat);
+        gemm_tn(ctx->d_cd, nb, ctx->d_beta, ctx->n_pw, ctx->d_nl, ctx->n_pw, nb, ctx->n_pw,
+                ctx->np, 1.0, 0.0, ctx->st);
+        e.nl = ctx->d_nl;
+    }
+    launch_zsticks_inverse<double2>(psi, ctx->n_pw, ctx->d_work, nb, ctx->geo, ctx->st);
+    launch_planes_vloc<double2>(ctx->d_work, ctx->d_veff, nb, ctx->geo, ctx->st);
+    launch_zsticks_forward<double2>(ctx->d_work, psi, ctx->n_pw, out, ctx->n_pw, nb, ctx->geo, e,
+                                    ctx->st);
+    CK(cudaGetLastError());
+    return CHFSI_OK;
+}
+
+// ---------------------------------------------------------------- bounds
+chfsi_status lanczos_bound(chfsi_ctx* ctx) {
+    const int k = std::max(2, std::min(ctx->cfg.lanczos_steps, 60));
+    const size_t n = ctx->n_pw;
+    CK(cudaMemsetAsync(ctx->d_lz, 0, sizeof(double) * 2 * k, ctx->st));
+    CK(cudaMemcpyAsync(ctx->d_lz_v, ctx->d_lz_start, n * sizeof(double2), cudaMemcpyDeviceToDevice,
+                       ctx->st));
+    double* fn0 = ctx->d_lz + 2 * k - 1;  // reuse last slot for |v0|^2 before the loop
+    sumsq(ctx->d_lz_v, n, fn0, ctx->st);
+    scale_by_rsqrt(ctx->d_lz_v, n, fn0, ctx->st);
+    CK(cudaMemsetAsync(fn0, 0, sizeof(double), ctx->st));
+    for (int j = 0; j < k; ++j) {
+        chfsi_status s = apply_h_dev(ctx, ctx->d_lz_v, ctx->d_lz_f, 1, kEpiApply, nullptr);
+        if (s) return s;
+        lanczos_a(ctx->d_lz_f, ctx->d_lz_v, ctx->d_lz_v0, j > 0 ? ctx->d_lz + k + j - 1 : nullptr,
+                  n, ctx->d_lz + j, ctx->st);
+        lanczos_b(ctx->d_lz_f, ctx->d_lz_v, ctx->d_lz + j, n, ctx->d_lz + k + j, ctx->st);
+        if (j < k - 1) lanczos_c(ctx->d_lz_f, ctx->d_lz_v, ctx->d_lz_v0, n, ctx->d_lz + k + j, ctx->st);
+    }
+    bounds(ctx->kin_max, ctx->d_minmax, nullptr, 0, ctx->d_lz, k, ctx->d_coef, ctx->st);
+    CK(cudaGetLastError());
+    return CHFSI_OK;
+}
+
+chfsi_status compute_bounds(chfsi_ctx* ctx, const double* eig_dev, int n_eig) {
+    if (ctx->cfg.bound_mode == CHFSI_BOUND_LANCZOS) {
+        chfsi_status s = lanczos_bound(ctx);
+        if (s) return s;
+        // the cut still comes from the previous eigenvalues
+        const int k = std::max(2, std::min(ctx->cfg.lanczos_steps, 60));
+        bounds(ctx->kin_max, ctx->d_minmax, eig_dev, n_eig, ctx->d_lz, k, ctx->d_coef, ctx->st);
+    } else {
+        bounds(ctx->kin_max, ctx->d_minmax, eig_dev, n_eig, nullptr, 0, ctx->d_coef, ctx->st);
+    }
+    CK(cudaGetLastError());
+    return CHFSI_OK;
+}
+
+// ---------------------------------------------------------------- filter
+chfsi_status filter_dev(chfsi_ctx* ctx, int ndeg, const double* eig_dev, int n_eig) {
+    if (ndeg < 0 || ndeg > ctx->max_deg) return ctx->fail(CHFSI_ERR_BAD_INPUT, "ndeg out of range");
+    chfsi_status s = compute_bounds(ctx, eig_dev, n_eig);
+    if (s) return s;
+    const size_t n = (size_t)ctx->nb * ctx->n_pw;
+    CK(cudaMemsetAsync(ctx->d_nsq, 0, sizeof(double) * (ndeg + 1), ctx->st));
+    sumsq(ctx->d_psi, n, ctx->d_nsq, ctx->st);
+    double2* A = ctx->d_psi;   // psi_{k-2}
+    double2* B = ctx->d_psi2;  // psi_{k-1}
+    if (ndeg >= 1) {
+        s = apply_h_dev(ctx, A, B, ctx->nb, kEpiChebFirst, ctx->d_nsq + 1);
+        if (s) return s;
+    }
+    for (int k = 2; k <= ndeg; ++k) {
+        // psi_k = 2 sigma(H) psi_{k-1} - psi_{k-2}, written over psi_{k-2}
+        s = apply_h_dev(ctx, B, A, ctx->nb, kEpiCheb, ctx->d_nsq + k);
+        if (s) return s;
+        std::swap(A, B);
+    }
+    double2* fin = ndeg >= 1 ? B : A;
+    double2* other = fin == ctx->d_psi ? ctx->d_psi2 : ctx->d_psi;
+    ctx->d_psi = fin;
+    ctx->d_psi2 = other;
+    s = apply_h_dev(ctx, ctx->d_psi, ctx->d_hpsi, ctx->nb, kEpiApply, nullptr);
+    if (s) return s;
+    norm_guard(ctx->d_nsq, ndeg, ctx->d_flags + 1, ctx->st);
+    ctx->last_ndeg = ndeg;
+    CK(cudaGetLastError());
+    return CHFSI_OK;
+}
+
+// ---------------------------------------------------------------- Rayleigh-Ritz
+chfsi_status rr_dev(chfsi_ctx* ctx) {
+    const int n = ctx->nb;
+    cudaStream_t st = ctx->st;
+    gemm_cn(ctx->d_psi, ctx->n_pw, ctx->d_hpsi, ctx->n_pw, n, n, ctx->n_pw, ctx->d_part, ctx->d_T1, st);
+    symmetrize(ctx->d_T1, ctx->d_H, n, st);
+    gemm_cn(ctx->d_psi, ctx->n_pw, ctx->d_psi, ctx->n_pw, n, n, ctx->n_pw, ctx->d_part, ctx->d_T1, st);
+    symmetrize(ctx->d_T1, ctx->d_S, n, st);
+    cholesky(ctx->d_S, n, ctx->d_flags + 0, st);                   // S -> L
+    tri_inv(ctx->d_S, ctx->d_T1, n, st);                            // T1 = L^-1
+    small_gemm(0, 0, ctx->d_T1, ctx->d_H, ctx->d_T2, n, st);        // T2 = Li H
+    small_gemm(0, 1, ctx->d_T2, ctx->d_T1, ctx->d_H, n, st);        // H = Li H Li^H
+    symmetrize(ctx->d_H, ctx->d_T2, n, st);                         // T2 = B
+    CK(jacobi(ctx->d_T2, ctx->d_V, n, ctx->jac_max_sweeps, 1e-26, ctx->d_jac, ctx->d_flags + 2, st));
+    sort_eig(ctx->d_T2, ctx->d_V, n, ctx->d_eig, ctx->d_H, st);     // H = U (sorted)
+    small_gemm(1, 0, ctx->d_T1, ctx->d_H, ctx->d_T2, n, st);        // T2 = Li^H U
+    gemm_tn(ctx->d_T2, n, ctx->d_psi, ctx->n_pw, ctx->d_psi2, ctx->n_pw, n, ctx->n_pw, n, 1.0, 0.0, st);
+    std::swap(ctx->d_psi, ctx->d_psi2);
+    CK(cudaGetLastError());
+    return CHFSI_OK;
+}
+
+// Read back eigenvalues, flags, bounds and norms; translate device flags into
+// the reference's error variants.
+chfsi_status finish_diag(chfsi_ctx* ctx, double* eig_out, bool have_rr) {
+    const int n = ctx->nb;
+    chfsi_status s = ensure_pinned(ctx, (size_t)n + 16 + ctx->max_deg + 1);
+    if (s) return s;
+    double* h = ctx->h_pin;
+    CK(cudaMemcpyAsync(h, ctx->d_eig, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(h + n, ctx->d_coef, sizeof(double) * 6, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(h + n + 6, ctx->d_flags, sizeof(int) * 4, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(h + n + 8, ctx->d_nsq, sizeof(double) * (ctx->last_ndeg + 1),
+                       cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    std::memcpy(ctx->h_coef, h + n, sizeof(double) * 6);
+    int flags[4];
+    std::memcpy(flags, h + n + 6, sizeof(flags));
+    ctx->h_nsq.assign(h + n + 8, h + n + 8 + ctx->last_ndeg + 1);
+    if (flags[1] != 0) {
+        char buf[256];
+        int k = flags[1];
+        double np_ = std::sqrt(ctx->h_nsq[k - 1]), nc = std::sqrt(ctx->h_nsq[k]);
+        std::snprintf(buf, sizeof(buf),
+                      "Chebyshev filtering diverged: norm grew %.2ex at iteration %d", nc / np_, k);
+        return ctx->fail(CHFSI_ERR_CHEB_DIVERGED, buf);
+    }
+    if (have_rr) {
+        if (flags[0] != 0) {
+            char buf[128];
+            std::snprintf(buf, sizeof(buf), "Rayleigh-Ritz failed: info=%d (overlap not positive definite)", flags[0]);
+            return ctx->fail(CHFSI_ERR_RR_FAILED, buf);
+        }
+        if (flags[2] >= ctx->jac_max_sweeps) {
+            return ctx->fail(CHFSI_ERR_RR_FAILED, "Rayleigh-Ritz failed: eigensolver did not converge");
+        }
+        for (int i = 0; i < n; ++i)
+            if (!std::isfinite(h[i])) return ctx->fail(CHFSI_ERR_NUMERIC, "non-finite eigenvalue");
+        if (eig_out) std::memcpy(eig_out, h, sizeof(double) * n);
+    }
+    return CHFSI_OK;
+}
+
+// ---------------------------------------------------------------- potentials
+void grid_fft3(chfsi_ctx* ctx, double2* g, bool forward) {
+    launch_axis_fft<double2>(g, ctx->nx, ctx->ny, ctx->nz, 0, forward, ctx->ax, ctx->st);
+    launch_axis_fft<double2>(g, ctx->nx, ctx->ny, ctx->nz, 1, forward, ctx->ay, ctx->st);
+    launch_axis_fft<double2>(g, ctx->nx, ctx->ny, ctx->nz, 2, forward, ctx->az, ctx->st);
+}
+
+GridRecip grid_recip(chfsi_ctx* ctx) {
+    GridRecip gr{};
+    gr.nx = ctx->nx; gr.ny = ctx->ny; gr.nz = ctx->nz;
+    gr.idr_x = ctx->d_idr[0]; gr.idr_y = ctx->d_idr[1]; gr.idr_z = ctx->d_idr[2];
+    std::memcpy(gr.b, ctx->recip, sizeof(gr.b));
+    return gr;
+}
+
+// veff = vloc + V_H[rho] + V_xc[rho]; acc[0] += E_H[rho], acc[1] += E_xc[rho]
+chfsi_status build_veff_dev(chfsi_ctx* ctx, const double* rho, double* acc) {
+    launch_real_to_complex(rho, ctx->d_cgrid, ctx->ng, ctx->st);
+    grid_fft3(ctx, ctx->d_cgrid, true);
+    launch_hartree_gspace(ctx->d_cgrid, grid_recip(ctx), ctx->omega, acc + 0, ctx->st);
+    grid_fft3(ctx, ctx->d_cgrid, false);
+    launch_assemble_veff(ctx->d_vloc, ctx->d_cgrid, rho, ctx->d_veff, ctx->ng,
+                         ctx->omega / (double)ctx->ng, acc + 1, ctx->st);
+    minmax(ctx->d_veff, ctx->ng, ctx->d_minmax, ctx->st);
+    CK(cudaGetLastError());
+    return CHFSI_OK;
+}
+
+chfsi_status density_dev(chfsi_ctx* ctx, double* rho) {
+    int nocc = 0;
+    for (int b = 0; b < ctx->nb; ++b)
+        if (ctx->occ[b] != 0.0) nocc = b + 1;
+    CK(cudaMemsetAsync(rho, 0, sizeof(double) * ctx->ng, ctx->st));
+    if (nocc == 0) return CHFSI_OK;
+    launch_zsticks_inverse<double2>(ctx->d_psi, ctx->n_pw, ctx->d_work, nocc, ctx->geo, ctx->st);
+    launch_planes_density<double2>(ctx->d_work, ctx->d_occ, nocc, 1.0 / ctx->omega, rho, ctx->geo,
+                                   ctx->st);
+    CK(cudaGetLastError());
+    return CHFSI_OK;
+}
+
+chfsi_status alloc_all(chfsi_ctx* ctx) {
+    const size_t nbpw = (size_t)ctx->nb * ctx->n_pw;
+    CK(dalloc(&ctx->d_kin, ctx->n_pw));
+    CK(dalloc(&ctx->d_perm, ctx->n_pw));
+    CK(dalloc(&ctx->d_pw_col, ctx->n_pw));
+    CK(dalloc(&ctx->d_pw_zpos, ctx->n_pw));
+    CK(dalloc(&ctx->d_veff, ctx->ng));
+    CK(dalloc(&ctx->d_vloc, ctx->ng));
+    CK(dalloc(&ctx->d_minmax, 2));
+    CK(dalloc(&ctx->d_psi, nbpw));
+    CK(dalloc(&ctx->d_psi2, nbpw));
+    CK(dalloc(&ctx->d_hpsi, nbpw));
+    if (ctx->np > 0) {
+        CK(dalloc(&ctx->d_nl, nbpw));
+        CK(dalloc(&ctx->d_beta, (size_t)ctx->np * ctx->n_pw));
+        CK(dalloc(&ctx->d_cp, (size_t)ctx->np * ctx->nb));
+        CK(dalloc(&ctx->d_cd, (size_t)ctx->np * ctx->nb));
+        CK(dalloc(&ctx->d_proj_ion, ctx->np));
+        CK(dalloc(&ctx->d_poff, ctx->nions + 1));
+        CK(dalloc(&ctx->d_doff, ctx->nions));
+    }
+    const size_t nn = (size_t)ctx->nb * ctx->nb;
+    CK(dalloc(&ctx->d_H, nn)); CK(dalloc(&ctx->d_S, nn)); CK(dalloc(&ctx->d_T1, nn));
+    CK(dalloc(&ctx->d_T2, nn)); CK(dalloc(&ctx->d_V, nn));
+    CK(dalloc(&ctx->d_eig, ctx->nb)); CK(dalloc(&ctx->d_eig_prev, ctx->nb));
+    CK(dalloc(&ctx->d_jac, jacobi_scratch_doubles(ctx->nb, ctx->jac_max_sweeps)));
+    CK(dalloc(&ctx->d_flags, 8));
+    CK(cudaMemset(ctx->d_flags, 0, 8 * sizeof(int)));
+    CK(dalloc(&ctx->d_coef, 8));
+    CK(dalloc(&ctx->d_nsq, ctx->max_deg + 2));
+    CK(dalloc(&ctx->d_lz_v, ctx->n_pw)); CK(dalloc(&ctx->d_lz_v0, ctx->n_pw));
+    CK(dalloc(&ctx->d_lz_f, ctx->n_pw)); CK(dalloc(&ctx->d_lz_start, ctx->n_pw));
+    CK(dalloc(&ctx->d_lz, 2 * 64));
+    CK(dalloc(&ctx->d_occ, ctx->nb));
+    CK(dalloc(&ctx->d_rho_in, ctx->ng)); CK(dalloc(&ctx->d_rho_out, ctx->ng));
+    CK(dalloc(&ctx->d_rho_next, ctx->ng));
+    CK(dalloc(&ctx->d_cgrid, ctx->ng));
+    CK(dalloc(&ctx->d_acc, 8));
+    CK(dalloc(&ctx->d_hist, 2 * (size_t)kPulayMax * ctx->ng));
+    CK(dalloc(&ctx->d_hist_ptrs, 2 * kPulayMax));
+    CK(dalloc(&ctx->d_dots, kPulayMax));
+    // split-K partials: max over the GEMMs that use them
+    // (any band count 1..nb may reach the projector GEMM through chfsi_apply_h)
+    size_t pe = splitk_partial_elems(ctx->nb, ctx->nb, ctx->n_pw);
+    if (ctx->np > 0)
+        for (int n = 1; n <= ctx->nb; ++n)
+            pe = std::max(pe, splitk_partial_elems(ctx->np, n, ctx->n_pw));
+    ctx->part_elems = pe;
+    CK(dalloc(&ctx->d_part, pe));
+    // Lanczos start vector: SplitMix64(0x5EED) uniform pairs in [-1/2, 1/2)
+    {
+        std::vector<double2> v(ctx->n_pw);
+        uint64_t s = 0x5EEDULL;
+        auto next = [&s]() {
+            uint64_t z = (s += 0x9E3779B97F4A7C15ULL);
+            z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+            z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+            return z ^ (z >> 31);
+        };
+        for (int g = 0; g < ctx->n_pw; ++g) {
+            double re = (double)(next() >> 11) * (1.0 / 9007199254740992.0) - 0.5;
+            double im = (double)(next() >> 11) * (1.0 / 9007199254740992.0) - 0.5;
+            v[g] = make_double2(re, im);
+        }
+        CK(cudaMemcpy(ctx->d_lz_start, v.data(), v.size() * sizeof(double2), cudaMemcpyHostToDevice));
+    }
+    std::vector<double*> hp(2 * kPulayMax);
+    for (int i = 0; i < 2 * kPulayMax; ++i) hp[i] = ctx->d_hist + (size_t)i * ctx->ng;
+    CK(cudaMemcpy(ctx->d_hist_ptrs, hp.data(), hp.size() * sizeof(double*), cudaMemcpyHostToDevice));
+    ctx->occ.assign(ctx->nb, 0.0);
+    CK(cudaMemset(ctx->d_occ, 0, sizeof(double) * ctx->nb));
+    CK(cudaMemset(ctx->d_vloc, 0, sizeof(double) * ctx->ng));
+    return CHFSI_OK;
+}
+
+void free_all(chfsi_ctx* ctx) {
+    void* ptrs[] = {ctx->d_col_start, ctx->d_col_pos, ctx->d_pw_col, ctx->d_pw_zpos, ctx->d_xact,
+                    ctx->d_idr[0], ctx->d_idr[1], ctx->d_idr[2], ctx->d_perm, ctx->d_kin,
+                    ctx->d_veff, ctx->d_vloc, ctx->d_minmax, ctx->d_beta, ctx->d_dmat,
+                    ctx->d_proj_ion, ctx->d_poff, ctx->d_doff, ctx->d_cp, ctx->d_cd, ctx->d_psi,
+                    ctx->d_psi2, ctx->d_hpsi, ctx->d_nl, ctx->d_work, ctx->d_part, ctx->d_H,
+                    ctx->d_S, ctx->d_T1, ctx->d_T2, ctx->d_V, ctx->d_eig, ctx->d_eig_prev,
+                    ctx->d_jac, ctx->d_flags, ctx->d_coef, ctx->d_nsq, ctx->d_lz_v, ctx->d_lz_v0,
+                    ctx->d_lz_f, ctx->d_lz_start, ctx->d_lz, ctx->d_occ, ctx->d_rho_in,
+                    ctx->d_rho_out, ctx->d_rho_next, ctx->d_cgrid, ctx->d_acc, ctx->d_hist,
+                    ctx->d_hist_ptrs, ctx->d_dots};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (ctx->h_pin) cudaFreeHost(ctx->h_pin);
+    if (ctx->st) cudaStreamDestroy(ctx->st);
+}
+
+}  // namespace
+
+// ============================================================== C ABI
+extern "C" {
+
+chfsi_status chfsi_default_config(chfsi_config* c) {
+    if (!c) return CHFSI_ERR_BAD_INPUT;
+    std::memset(c, 0, sizeof(*c));
+    c->device = 0;
+    c->precision = CHFSI_PREC_FP64;
+    c->bound_mode = CHFSI_BOUND_HEURISTIC;
+    c->lanczos_steps = 10;
+    c->check_norms = 1;
+    return CHFSI_OK;
+}
+
+const char* chfsi_last_error(const chfsi_ctx* ctx) {
+    if (ctx && !ctx->err.empty()) return ctx->err.c_str();
+    return g_last_error.c_str();
+}
+
+chfsi_status chfsi_create(const chfsi_dims* dims, const chfsi_config* cfg, chfsi_ctx** out) {
+    if (!dims || !out) return CHFSI_ERR_BAD_INPUT;
+    *out = nullptr;
+    if (dims->n_pw <= 0 || dims->n_bands <= 0 || dims->n_bands > dims->n_pw || dims->n_proj < 0 ||
+        (dims->n_proj > 0 && dims->n_ions <= 0))
+        return CHFSI_ERR_BAD_INPUT;
+    for (int d = 0; d < 3; ++d)
+        if (dims->ngrid[d] <= 0 || dims->ngrid[d] > 256) return CHFSI_ERR_BAD_INPUT;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        g_last_error = "no CUDA device visible";
+        return CHFSI_ERR_NO_DEVICE;
+    }
+    chfsi_ctx* ctx = new (std::nothrow) chfsi_ctx();
+    if (!ctx) return CHFSI_ERR_OUT_OF_MEMORY;
+    ctx->dims = *dims;
+    if (cfg) ctx->cfg = *cfg; else chfsi_default_config(&ctx->cfg);
+    if (ctx->cfg.precision != CHFSI_PREC_FP64) {
+        delete ctx;
+        g_last_error = "mixed precision is not available in this build";
+        return CHFSI_ERR_NOT_IMPLEMENTED;
+    }
+    ctx->device = ctx->cfg.device;
+    chfsi_status s = CHFSI_OK;
+    auto bail = [&](chfsi_status e) { free_all(ctx); delete ctx; return e; };
+    if (cudaSetDevice(ctx->device) != cudaSuccess) { g_last_error = "cudaSetDevice failed"; return bail(CHFSI_ERR_CUDA); }
+    if (cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess) return bail(CHFSI_ERR_CUDA);
+    ctx->nx = dims->ngrid[0]; ctx->ny = dims->ngrid[1]; ctx->nz = dims->ngrid[2];
+    ctx->ng = (size_t)ctx->nx * ctx->ny * ctx->nz;
+    ctx->n_pw = dims->n_pw; ctx->nb = dims->n_bands; ctx->np = dims->n_proj; ctx->nions = dims->n_ions;
+    if (!plan_axis(ctx->nx, ctx->ax) || !plan_axis(ctx->ny, ctx->ay) || !plan_axis(ctx->nz, ctx->az)) {
+        g_last_error = "FFT grid dimensions must be 2,3,5-smooth";
+        return bail(CHFSI_ERR_BAD_INPUT);
+    }
+    digit_reversal(ctx->ax, ctx->dr[0]);
+    digit_reversal(ctx->ay, ctx->dr[1]);
+    digit_reversal(ctx->az, ctx->dr[2]);
+    s = alloc_all(ctx);
+    if (s) return bail(s);
+    // inverse digit reversal tables (position -> frequency) for the potential kernels
+    for (int d = 0; d < 3; ++d) {
+        const std::vector<int>& p = ctx->dr[d];
+        std::vector<int> inv(p.size());
+        for (size_t k = 0; k < p.size(); ++k) inv[p[k]] = (int)k;
+        if (cudaMalloc((void**)&ctx->d_idr[d], inv.size() * sizeof(int)) != cudaSuccess) return bail(CHFSI_ERR_OUT_OF_MEMORY);
+        cudaMemcpy(ctx->d_idr[d], inv.data(), inv.size() * sizeof(int), cudaMemcpyHostToDevice);
+    }
+    *out = ctx;
+    return CHFSI_OK;
+}
+
+void chfsi_destroy(chfsi_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->st) cudaStreamSynchronize(ctx->st);
+    free_all(ctx);
+    delete ctx;
+}
+
+chfsi_status chfsi_set_basis(chfsi_ctx* ctx, const int32_t* miller, const double* kinetic,
+                             double gmax) {
+    if (!ctx || !miller || !kinetic) return CHFSI_ERR_BAD_INPUT;
+    cudaSetDevice(ctx->device);
+    const int n = ctx->n_pw, nx = ctx->nx, ny = ctx->ny, nz = ctx->nz;
+    auto wrap = [](int h, int m) { return h >= 0 ? h : h + m; };
+    std::vector<int> ix(n), iy(n), iz(n);
+    for (int g = 0; g < n; ++g) {
+        int h = miller[3 * g], k = miller[3 * g + 1], l = miller[3 * g + 2];
+        if (std::abs(2 * h) >= nx + (nx & 1) || std::abs(2 * k) >= ny + (ny & 1) ||
+            std::abs(2 * l) >= nz + (nz & 1))
+            return ctx->fail(CHFSI_ERR_BAD_INPUT, "Miller index outside the FFT grid");
+        ix[g] = wrap(h, nx); iy[g] = wrap(k, ny); iz[g] = wrap(l, nz);
+    }
+    // internal order: by column (iy, ix), then l ascending
+    std::vector<int> perm(n);
+    for (int g = 0; g < n; ++g) perm[g] = g;
+    std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) {
+        int ca = iy[a] * nx + ix[a], cb = iy[b] * nx + ix[b];
+        if (ca != cb) return ca < cb;
+        return miller[3 * a + 2] < miller[3 * b + 2];
+    });
+    ctx->perm_identity = true;
+    for (int g = 0; g < n; ++g)
+        if (perm[g] != g) { ctx->perm_identity = false; break; }
+    std::vector<int> col_start, col_pos, pw_col(n), pw_zpos(n), xact;
+    std::vector<double> kin(n);
+    std::vector<char> xused(nx, 0);
+    int last = -1;
+    for (int i = 0; i < n; ++i) {
+        const int g = perm[i];
+        const int c = iy[g] * nx + ix[g];
+        if (c != last) {
+            col_start.push_back(i);
+            const int px = ctx->dr[0][ix[g]], py = ctx->dr[1][iy[g]];
+            col_pos.push_back(py * (nx | 1) + px);
+            xused[px] = 1;
+            last = c;
+        } else if (i > 0 && miller[3 * g + 2] == miller[3 * perm[i - 1] + 2]) {
+            return ctx->fail(CHFSI_ERR_BAD_INPUT, "duplicate plane wave");
+        }
+        pw_col[i] = (int)col_start.size() - 1;
+        pw_zpos[i] = ctx->dr[2][iz[g]];
+        kin[i] = kinetic[g];
+    }
+    const int ncol = (int)col_start.size();
+    col_start.push_back(n);
+    for (int x = 0; x < nx; ++x)
+        if (xused[x]) xact.push_back(x);
+    double kmax = 0.0;
+    for (int g = 0; g < n; ++g) kmax = std::max(kmax, kinetic[g]);
+    // kinetic bound of the reference: 1/2 Gmax^2 (chebyshev.rs:232)
+    ctx->kin_max = gmax > 0.0 ? 0.5 * gmax * gmax : kmax;
+    if (ctx->d_col_start) cudaFree(ctx->d_col_start);
+    if (ctx->d_col_pos) cudaFree(ctx->d_col_pos);
+    if (ctx->d_xact) cudaFree(ctx->d_xact);
+    if (ctx->d_work) cudaFree(ctx->d_work);
+    ctx->d_col_start = ctx->d_col_pos = ctx->d_xact = nullptr;
+    ctx->d_work = nullptr;
+    CK(dalloc(&ctx->d_col_start, ncol + 1));
+    CK(dalloc(&ctx->d_col_pos, ncol));
+    CK(dalloc(&ctx->d_xact, xact.size()));
+    CK(dalloc(&ctx->d_work, (size_t)ctx->nb * nz * ncol));
+    CK(cudaMemcpy(ctx->d_col_start, col_start.data(), sizeof(int) * (ncol + 1), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_col_pos, col_pos.data(), sizeof(int) * ncol, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_xact, xact.data(), sizeof(int) * xact.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_pw_col, pw_col.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_pw_zpos, pw_zpos.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_kin, kin.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_perm, perm.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    HGeom& g = ctx->geo;
+    g.nx = nx; g.ny = ny; g.nz = nz; g.n_pw = n; g.ncol = ncol;
+    g.lsz = nz | 1; g.lsx = nx | 1; g.nxact = (int)xact.size();
+    g.col_start = ctx->d_col_start; g.col_pos = ctx->d_col_pos; g.pw_col = ctx->d_pw_col;
+    g.pw_zpos = ctx->d_pw_zpos; g.xact = ctx->d_xact;
+    g.ax = ctx->ax; g.ay = ctx->ay; g.az = ctx->az;
+    if (planes_smem_bytes(g, sizeof(double2)) > 227 * 1024)
+        return ctx->fail(CHFSI_ERR_BAD_INPUT, "xy plane does not fit in shared memory");
+    if ((size_t)nx * ny > kDensityPlanePoints)
+        return ctx->fail(CHFSI_ERR_BAD_INPUT, "xy plane too large for the density kernel");
+    ctx->basis_set = true;
+    return CHFSI_OK;
+}
+
+chfsi_status chfsi_set_projectors(chfsi_ctx* ctx, const chfsi_c128* beta,
+                                  const int32_t* proj_offsets, const chfsi_c128* dmat) {
+    if (!ctx || !ctx->basis_set) return CHFSI_ERR_BAD_INPUT;
+    if (ctx->np == 0) return CHFSI_OK;
+    if (!beta || !proj_offsets || !dmat) return CHFSI_ERR_BAD_INPUT;
+    cudaSetDevice(ctx->device);
+    const int ni = ctx->nions;
+    if (proj_offsets[0] != 0 || proj_offsets[ni] != ctx->np)
+        return ctx->fail(CHFSI_ERR_BAD_INPUT, "projector offsets do not cover n_proj");
+    std::vector<int> pion(ctx->np), doff(ni);
+    size_t dt = 0;
+    for (int i = 0; i < ni; ++i) {
+        const int ne = proj_offsets[i + 1] - proj_offsets[i];
+        if (ne <= 0) return ctx->fail(CHFSI_ERR_BAD_INPUT, "empty projector block");
+        for (int p = proj_offsets[i]; p < proj_offsets[i + 1]; ++p) pion[p] = i;
+        doff[i] = (int)dt;
+        dt += (size_t)ne * ne;
+    }
+    if (ctx->d_dmat) cudaFree(ctx->d_dmat);
+    ctx->d_dmat = nullptr;
+    CK(dalloc(&ctx->d_dmat, dt));
+    CK(cudaMemcpy(ctx->d_dmat, dmat, dt * sizeof(double2), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_proj_ion, pion.data(), sizeof(int) * ctx->np, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_poff, proj_offsets, sizeof(int) * (ni + 1), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_doff, doff.data(), sizeof(int) * ni, cudaMemcpyHostToDevice));
+    const size_t nbeta = (size_t)ctx->np * ctx->n_pw;
+    if (ctx->perm_identity) {
+        CK(cudaMemcpy(ctx->d_beta, beta, nbeta * sizeof(double2), cudaMemcpyHostToDevice));
+    } else {
+        // stage in the hpsi buffer when it is large enough, else in a temporary
+        double2* stage = nullptr;
+        CK(cudaMalloc((void**)&stage, nbeta * sizeof(double2)));
+        cudaMemcpy(stage, beta, nbeta * sizeof(double2), cudaMemcpyHostToDevice);
+        count_launch();
+        k_gather_rows<<<grid_for(nbeta), 256, 0, ctx->st>>>(stage, ctx->n_pw, ctx->d_perm,
+                                                           ctx->d_beta, ctx->n_pw, ctx->np);
+        cudaStreamSynchronize(ctx->st);
+        cudaFree(stage);
+        CK(cudaGetLastError());
+    }
+    ctx->proj_set = true;
+    return CHFSI_OK;
+}
+
+chfsi_status chfsi_set_veff(chfsi_ctx* ctx, const double* veff) {
+    if (!ctx || !veff) return CHFSI_ERR_BAD_INPUT;
+    cudaSetDevice(ctx->device);
+    CK(cudaMemcpyAsync(ctx->d_veff, veff, ctx->ng * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+    minmax(ctx->d_veff, ctx->ng, ctx->d_minmax, ctx->st);
+    CK(cudaGetLastError());
+    ctx->veff_set = true;
+    return CHFSI_OK;
+}
+
+chfsi_status chfsi_set_psi(chfsi_ctx* ctx, const chfsi_c128* psi) {
+    if (!ctx || !psi || !ctx->basis_set) return CHFSI_ERR_BAD_INPUT;
+    cudaSetDevice(ctx->device);
+    const size_t n = (size_t)ctx->nb * ctx->n_pw;
+    if (ctx->perm_identity) {
+        CK(cudaMemcpyAsync(ctx->d_psi, psi, n * sizeof(double2), cudaMemcpyHostToDevice, ctx->st));
+    } else {
+        CK(cudaMemcpyAsync(ctx->d_psi2, psi, n * sizeof(double2), cudaMemcpyHostToDevice, ctx->st));
+        count_launch();
+        k_gather_rows<<<grid_for(n), 256, 0, ctx->st>>>(ctx->d_psi2, ctx->n_pw, ctx->d_perm,
+                                                       ctx->d_psi, ctx->n_pw, ctx->nb);
+        CK(cudaGetLastError());
+    }
+    ctx->psi_set = true;
+    return CHFSI_OK;
+}
+
+chfsi_status chfsi_get_psi(chfsi_ctx* ctx, chfsi_c128* psi) {
+    if (!ctx || !psi) return CHFSI_ERR_BAD_INPUT;
+    cudaSetDevice(ctx->device);
+    const size_t n = (size_t)ctx->nb * ctx->n_pw;
+    if (ctx->perm_identity) {
+        CK(cudaMemcpyAsync(psi, ctx->d_psi, n * sizeof(double2), cudaMemcpyDeviceToHost, ctx->st));
+    } else {
+        count_launch();
+        k_scatter_rows<<<grid_for(n), 256, 0, ctx->st>>>(ctx->d_psi, ctx->d_perm, ctx->d_psi2,
+                                                        ctx->n_pw, ctx->n_pw, ctx->nb);
+        CK(cudaMemcpyAsync(psi, ctx->d_psi2, n * sizeof(double2), cudaMemcpyDeviceToHost, ctx->st));
+    }
+    CK(cudaStreamSynchronize(ctx->st));
+    return CHFSI_OK;
+}
+
+chfsi_status chfsi_psi_device_ptr(chfsi_ctx* ctx, chfsi_c128** out) {
+    if (!ctx || !out) return CHFSI_ERR_BAD_INPUT;
+    *out = reinterpret_cast<chfsi_c128*>(ctx->d_psi);
+    return CHFSI_OK;
+}
+
+static chfsi_status ready(chfsi_ctx* ctx) {
+    if (!ctx) return CHFSI_ERR_BAD_INPUT;
+    if (!ctx->basis_set) return ctx->fail(CHFSI_ERR_BAD_INPUT, "basis not set");
+    if (!ctx->veff_set) return ctx->fail(CHFSI_ERR_BAD_INPUT, "V_eff not set");
+    if (ctx->np > 0 && !ctx->proj_set) return ctx->fail(CHFSI_ERR_BAD_INPUT, "projectors not set");
+    cudaSetDevice(ctx->device);
+    return CHFSI_OK;
+}
+
+chfsi_status chfsi_apply_h_local(chfsi_ctx* ctx, const chfsi_c128* psi_dev, chfsi_c128* hpsi_dev,
+                                 int nb) {
+    chfsi_status s = ready(ctx);
+    if (s) return s;
+    if (!psi_dev || !hpsi_dev || nb <= 0 || nb > ctx->nb) return CHFSI_ERR_BAD_INPUT;
+    const int np = ctx->np;
+    ctx->np = 0;  // local part only: T + V_loc
+    s = apply_h_dev(ctx, reinterpret_cast<const double2*>(psi_dev),
+                    reinterpret_cast<double2*>(hpsi_dev), nb, kEpiApply, nullptr);
+    ctx->np = np;
+    if (s) return s;
+    CK(cudaStreamSynchronize(ctx->st));
+    return CHFSI_OK;
+}
+
+chfsi_status chfsi_get_stream(chfsi_ctx* ctx, void** out) {
+    if (!ctx || !out) return CHFSI_ERR_BAD_INPUT;
+    *out = (void*)ctx->st;
+    return CHFSI_OK;
+}
+
+long long chfsi_launch_count(void) { return g_launch_count.load(); }
+
+chfsi_status chfsi_apply_h(chfsi_ctx* ctx, const chfsi_c128* psi_dev, chfsi_c128* hpsi_dev, int nb) {
+    chfsi_status s = ready(ctx);
+    if (s) return s;
+    if (!psi_dev || !hpsi_dev || nb <= 0 || nb > ctx->nb) return CHFSI_ERR_BAD_INPUT;
+    s = apply_h_dev(ctx, reinterpret_cast<const double2*>(psi_dev),
+                    reinterpret_cast<double2*>(hpsi_dev), nb, kEpiApply, nullptr);
+    if (s) return s;
+    CK(cudaStreamSynchronize(ctx->st));
+    return CHFSI_OK;
+}
+
+static chfsi_status upload_eig(chfsi_ctx* ctx, const double* eig_prev, int n_eig,
+                               const double** dev) {
+    *dev = nullptr;
+    if (!eig_prev || n_eig <= 0) return CHFSI_OK;
+    if (n_eig > ctx->nb) return CHFSI_ERR_BAD_INPUT;
+    CK(cudaMemcpyAsync(ctx->d_eig_prev, eig_prev, sizeof(double) * n_eig, cudaMemcpyHostToDevice,
+                       ctx->st));
+    *dev = ctx->d_eig_prev;
+    return CHFSI_OK;
+}
+
+chfsi_status chfsi_chebyshev_filter(chfsi_ctx* ctx, int ndeg, const double* eig_prev, int n_eig) {
+    chfsi_status s = ready(ctx);
+    if (s) return s;
+    if (!ctx->psi_set) return ctx->fail(CHFSI_ERR_BAD_INPUT, "psi not set");
+    const double* ed = nullptr;
+    s = upload_eig(ctx, eig_prev, n_eig, &ed);
+    if (s) return s;
+    s = filter_dev(ctx, ndeg, ed, ed ? n_eig : 0);
+    if (s) return s;
+    return finish_diag(ctx, nullptr, false);
+}
+
+chfsi_status chfsi_rayleigh_ritz(chfsi_ctx* ctx, double* eig_out) {
+    chfsi_status s = ready(ctx);
+    if (s) return s;
+    s = rr_dev(ctx);
+    if (s) return s;
+    return finish_diag(ctx, eig_out, true);
+}
+
+chfsi_status chfsi_diagonalize(chfsi_ctx* ctx, int ndeg, const double* eig_prev, int n_eig,
+                               double* eig_out) {
+    chfsi_status s = ready(ctx);
+    if (s) return s;
+    if (!ctx->psi_set) return ctx->fail(CHFSI_ERR_BAD_INPUT, "psi not set");
+    const double* ed = nullptr;
+    s = upload_eig(ctx, eig_prev, n_eig, &ed);
+    if (s) return s;
+    s = filter_dev(ctx, ndeg, ed, ed ? n_eig : 0);
+    if (s) return s;
+    s = rr_dev(ctx);
+    if (s) return s;
+    return finish_diag(ctx, eig_out, true);
+}
+
+chfsi_status chfsi_get_bounds(chfsi_ctx* ctx, double* out4) {
+    if (!ctx || !out4) return CHFSI_ERR_BAD_INPUT;
+    for (int i = 0; i < 4; ++i) out4[i] = ctx->h_coef[i];
+    return CHFSI_OK;
+}
+
+chfsi_status chfsi_get_filter_norms(chfsi_ctx* ctx, double* out, int n) {
+    if (!ctx || !out) return CHFSI_ERR_BAD_INPUT;
+    for (int i = 0; i < n && i < (int)ctx->h_nsq.size(); ++i) out[i] = std::sqrt(ctx->h_nsq[i]);
+    return CHFSI_OK;
+}
+
+chfsi_status chfsi_create_from_system(const chfsi_system* sys, const chfsi_config* cfg,
+                                      chfsi_ctx** out) {
+    if (!sys || !out) return CHFSI_ERR_BAD_INPUT;
+    const System& s = *reinterpret_cast<const System*>(sys);
+    chfsi_dims d{};
+    for (int i = 0; i < 3; ++i) d.ngrid[i] = s.ngrid[i];
+    d.n_pw = s.n_pw; d.n_bands = s.n_bands; d.n_proj = s.n_proj; d.n_ions = s.n_ions_proj;
+    chfsi_ctx* ctx = nullptr;
+    chfsi_status st = chfsi_create(&d, cfg, &ctx);
+    if (st) return st;
+    auto bail = [&](chfsi_status e) { chfsi_destroy(ctx); return e; };
+    if ((st = chfsi_set_basis(ctx, s.miller.data(), s.kinetic.data(), s.gmax))) return bail(st);
+    if (s.n_proj > 0 &&
+        (st = chfsi_set_projectors(ctx, reinterpret_cast<const chfsi_c128*>(s.beta.data()),
+                                   s.proj_offsets.data(),
+                                   reinterpret_cast<const chfsi_c128*>(s.dmat.data()))))
+        return bail(st);
+    if ((st = chfsi_set_psi(ctx, reinterpret_cast<const chfsi_c128*>(s.psi0.data())))) return bail(st);
+    if ((st = chfsi_set_occupations(ctx, s.occ.data()))) return bail(st);
+    if ((st = chfsi_set_vloc_g(ctx, reinterpret_cast<const chfsi_c128*>(s.vloc_g.data())))) return bail(st);
+    double lat[9];
+    std::memcpy(lat, s.lattice, sizeof(lat));
+    if ((st = chfsi_set_cell(ctx, lat, s.e_ewald, s.n_atoms))) return bail(st);
+    // a usable V_eff before the first SCF step: V_loc alone
+    std::vector<double> v(ctx->ng);
+    cudaMemcpy(v.data(), ctx->d_vloc, sizeof(double) * ctx->ng, cudaMemcpyDeviceToHost);
+    if ((st = chfsi_set_veff(ctx, v.data()))) return bail(st);
+    *out = ctx;
+    return CHFSI_OK;
+}
+
+// ---------------------------------------------------------------- SCF pieces
+chfsi_status chfsi_set_occupations(chfsi_ctx* ctx, const double* occ) {
+    if (!ctx || !occ) return CHFSI_ERR_BAD_INPUT;
+    cudaSetDevice(ctx->device);
+    ctx->occ.assign(occ, occ + ctx->nb);
+    ctx->n_elec = 0.0;
+    for (double f : ctx->occ) ctx->n_elec += f;
+    CK(cudaMemcpy(ctx->d_occ, occ, sizeof(double) * ctx->nb, cudaMemcpyHostToDevice));
+    return CHFSI_OK;
+}
+
+chfsi_status chfsi_set_cell(chfsi_ctx* ctx, const double* lattice, double e_ewald, int n_atoms) {
+    if (!ctx || !lattice || n_atoms <= 0) return CHFSI_ERR_BAD_INPUT;
+    const double* a = lattice;
+    const double vol = a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) +
+                       a[2] * (a[3] * a[7] - a[4] * a[6]);
+    if (!(std::fabs(vol) > 0.0)) return CHFSI_ERR_BAD_INPUT;
+    ctx->omega = std::fabs(vol);
+    // b_i = 2 pi (a_j x a_k) / vol
+    const double tp = 2.0 * 3.14159265358979323846 / vol;
+    auto cross = [](const double* u, const double* v, double* w) {
+        w[0] = u[1] * v[2] - u[2] * v[1];
+        w[1] = u[2] * v[0] - u[0] * v[2];
+        w[2] = u[0] * v[1] - u[1] * v[0];
+    };
+    cross(a + 3, a + 6, ctx->recip + 0);
+    cross(a + 6, a + 0, ctx->recip + 3);
+    cross(a + 0, a + 3, ctx->recip + 6);
+    for (int i = 0; i < 9; ++i) ctx->recip[i] *= tp;
+    ctx->e_ewald = e_ewald;
+    ctx->n_atoms = n_atoms;
+    return CHFSI_OK;
+}
+
+chfsi_status chfsi_set_vloc_g(chfsi_ctx* ctx, const chfsi_c128* vloc_g) {
+    if (!ctx || !vloc_g) return CHFSI_ERR_BAD_INPUT;
+    cudaSetDevice(ctx->device);
+    // natural G order -> digit-reversed layout, then inverse transform
+    std::vector<double2> h(ctx->ng);
+    const double2* src = reinterpret_cast<const double2*>(vloc_g);
+    for (int iz = 0; iz < ctx->nz; ++iz)
+        for (int iy = 0; iy < ctx->ny; ++iy)
+            for (int ix = 0; ix < ctx->nx; ++ix) {
+                const size_t from = ix + (size_t)ctx->nx * (iy + (size_t)ctx->ny * iz);
+                const size_t to = ctx->dr[0][ix] +
+                                  (size_t)ctx->nx * (ctx->dr[1][iy] + (size_t)ctx->ny * ctx->dr[2][iz]);
+                h[to] = src[from];
+            }
+    CK(cudaMemcpy(ctx->d_cgrid, h.data(), sizeof(double2) * ctx->ng, cudaMemcpyHostToDevice));
+    grid_fft3(ctx, ctx->d_cgrid, false);
+    launch_take_real(ctx->d_cgrid, ctx->d_vloc, ctx->ng, ctx->st);
+    CK(cudaStreamSynchronize(ctx->st));
+    CK(cudaGetLastError());
+    ctx->have_vloc = true;
+    return CHFSI_OK;
+}
+
+chfsi_status chfsi_get_vloc(chfsi_ctx* ctx, double* out) {
+    if (!ctx || !out) return CHFSI_ERR_BAD_INPUT;
+    cudaSetDevice(ctx->device);
+    CK(cudaMemcpy(out, ctx->d_vloc, sizeof(double) * ctx->ng, cudaMemcpyDeviceToHost));
+    return CHFSI_OK;
+}
+
+chfsi_status chfsi_get_veff(chfsi_ctx* ctx, double* out) {
+    if (!ctx || !out) return CHFSI_ERR_BAD_INPUT;
+    cudaSetDevice(ctx->device);
+    CK(cudaStreamSynchronize(ctx->st));
+    CK(cudaMemcpy(out, ctx->d_veff, sizeof(double) * ctx->ng, cudaMemcpyDeviceToHost));
+    return CHFSI_OK;
+}
+
+chfsi_status chfsi_construct_density(chfsi_ctx* ctx, double* rho_out) {
+    if (!ctx || !ctx->basis_set) return CHFSI_ERR_BAD_INPUT;
+    if (ctx->omega <= 0.0) return ctx->fail(CHFSI_ERR_BAD_INPUT, "cell not set");
+    cudaSetDevice(ctx->device);
+    chfsi_status s = density_dev(ctx, ctx->d_rho_out);
+    if (s) return s;
+    if (rho_out) {
+        CK(cudaMemcpyAsync(rho_out, ctx->d_rho_out, sizeof(double) * ctx->ng, cudaMemcpyDeviceToHost, ctx->st));
+    }
+    CK(cudaStreamSynchronize(ctx->st));
+    return CHFSI_OK;
+}
+
+chfsi_status chfsi_build_veff(chfsi_ctx* ctx, const double* rho, double* e2) {
+    if (!ctx || !rho) return CHFSI_ERR_BAD_INPUT;
+    if (!ctx->have_vloc || ctx->omega <= 0.0) return ctx->fail(CHFSI_ERR_BAD_INPUT, "V_loc / cell not set");
+    cudaSetDevice(ctx->device);
+    CK(cudaMemcpyAsync(ctx->d_rho_in, rho, sizeof(double) * ctx->ng, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemsetAsync(ctx->d_acc, 0, sizeof(double) * 8, ctx->st));
+    chfsi_status s = build_veff_dev(ctx, ctx->d_rho_in, ctx->d_acc);
+    if (s) return s;
+    double acc[2];
+    CK(cudaMemcpyAsync(acc, ctx->d_acc, sizeof(acc), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    ctx->veff_set = true;
+    if (e2) { e2[0] = acc[0]; e2[1] = acc[1]; }
+    return CHFSI_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ SCF loop
+namespace {
+
+struct PulayState {
+    int m = 0;            // entries in history
+    int head = 0;         // ring slot of the oldest entry
+    double M[kPulayMax][kPulayMax] = {};
+};
+
+// Fermi-Dirac occupations f_i = 2 / (1 + exp((e_i - mu)/kT)), mu by
+// bisection on sum f = n_elec (the occupation step planned for
+// construct_density, PROJECT_ROOT_PLAN.md:582-589; SmearingParams
+// src/types.rs:204-211).  kT <= 0: aufbau.  Returns -kT S.
+double fermi_occupations(const double* e, int n, double n_elec, double kT, double* f, double* mu_out) {
+    if (kT <= 0.0) {
+        double left = n_elec;
+        for (int i = 0; i < n; ++i) {
+            f[i] = std::min(2.0, std::max(0.0, left));
+            left -= f[i];
+        }
+        if (mu_out) *mu_out = 0.0;
+        return 0.0;
+    }
+    double lo = e[0], hi = e[0];
+    for (int i = 0; i < n; ++i) { lo = std::min(lo, e[i]); hi = std::max(hi, e[i]); }
+    lo -= 40.0 * kT + 1.0;
+    hi += 40.0 * kT + 1.0;
+    auto count = [&](double mu) {
+        double s = 0.0;
+        for (int i = 0; i < n; ++i) {
+            const double x = std::min(700.0, std::max(-700.0, (e[i] - mu) / kT));
+            s += 2.0 / (1.0 + std::exp(x));
+        }
+        return s;
+    };
+    for (int it = 0; it < 200; ++it) {
+        const double mid = 0.5 * (lo + hi);
+        if (count(mid) < n_elec) lo = mid; else hi = mid;
+    }
+    const double mu = 0.5 * (lo + hi);
+    double ts = 0.0;
+    for (int i = 0; i < n; ++i) {
+        const double x = std::min(700.0, std::max(-700.0, (e[i] - mu) / kT));
+        f[i] = 2.0 / (1.0 + std::exp(x));
+        const double ft = 0.5 * f[i];
+        if (ft > 1e-300 && ft < 1.0 - 1e-16)
+            ts += -2.0 * (ft * std::log(ft) + (1.0 - ft) * std::log(1.0 - ft));
+    }
+    if (mu_out) *mu_out = mu;
+    return -kT * ts;
+}
+
+// Solve the bordered Pulay system; returns false if singular.
+bool pulay_coefficients(int m, const double M[kPulayMax][kPulayMax], double* c) {
+    const int n = m + 1;
+    double A[kPulayMax + 1][kPulayMax + 2];
+    for (int i = 0; i < m; ++i) {
+        for (int j = 0; j < m; ++j) A[i][j] = M[i][j];
+        A[i][m] = 1.0;
+        A[i][n] = 0.0;
+    }
+    for (int j = 0; j < m; ++j) A[m][j] = 1.0;
+    A[m][m] = 0.0;
+    A[m][n] = 1.0;
+    for (int col = 0; col < n; ++col) {
+        int piv = col;
+        for (int r = col + 1; r < n; ++r)
+            if (std::fabs(A[r][col]) > std::fabs(A[piv][col])) piv = r;
+        if (piv != col)
+            for (int k = 0; k <= n; ++k) std::swap(A[col][k], A[piv][k]);
+        const double d = A[col][col];
+        if (d == 0.0) return false;
+        for (int r = col + 1; r < n; ++r) {
+            const double f = A[r][col] / d;
+            for (int k = col; k <= n; ++k) A[r][k] -= f * A[col][k];
+        }
+    }
+    double x[kPulayMax + 1];
+    for (int i = n - 1; i >= 0; --i) {
+        double s = A[i][n];
+        for (int k = i + 1; k < n; ++k) s -= A[i][k] * x[k];
+        x[i] = s / A[i][i];
+    }
+    for (int i = 0; i < m; ++i) c[i] = x[i];
+    return true;
+}
+
+}  // namespace
+
+extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
+                                      chfsi_scf_result* r) {
+    if (!ctx || !p || !r) return CHFSI_ERR_BAD_INPUT;
+    if (!ctx->basis_set || !ctx->psi_set || !ctx->have_vloc || ctx->omega <= 0.0)
+        return ctx->fail(CHFSI_ERR_BAD_INPUT, "context not fully initialised");
+    if (ctx->np > 0 && !ctx->proj_set) return ctx->fail(CHFSI_ERR_BAD_INPUT, "projectors not set");
+    if (p->max_hist < 1 || p->max_hist > kPulayMax || p->max_iter < 1 || p->ndeg < 0)
+        return CHFSI_ERR_BAD_INPUT;
+    cudaSetDevice(ctx->device);
+    double* r_energies = r->energies;
+    double* r_eigs = r->eigenvalues;
+    std::memset(r, 0, sizeof(*r));
+    r->energies = r_energies;
+    r->eigenvalues = r_eigs;
+    const size_t ng = ctx->ng;
+    const double dv = ctx->omega / (double)ng;
+    cudaStream_t st = ctx->st;
+    const double n_elec = ctx->n_elec;
+    count_launch();
+    k_fill<<<grid_for(ng), 256, 0, st>>>(ctx->d_rho_in, ng, n_elec / ctx->omega);
+    PulayState ps;
+    chfsi_status s = ensure_pinned(ctx, (size_t)ctx->nb + 64 + ctx->max_deg);
+    if (s) return s;
+    std::vector<double> eig(ctx->nb);
+    bool have_eig = false;
+    double e_prev = 0.0;
+    chfsi_status status = CHFSI_NOT_CONVERGED;
+    cudaEvent_t t0, t1;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    cudaEventRecord(t0, st);
+    int it;
+    for (it = 1; it <= p->max_iter; ++it) {
+        // build_v_eff (scf.rs:157)
+        CK(cudaMemsetAsync(ctx->d_acc, 0, sizeof(double) * 8, st));
+        s = build_veff_dev(ctx, ctx->d_rho_in, ctx->d_acc);
+        if (s) { status = s; break; }
+        ctx->veff_set = true;
+        // diagonalize (scf.rs:169)
+        const int passes = it == 1 ? std::max(1, p->first_passes) : 1;
+        for (int q = 0; q < passes; ++q) {
+            s = filter_dev(ctx, p->ndeg, have_eig ? ctx->d_eig : nullptr, have_eig ? ctx->nb : 0);
+            if (!s) s = rr_dev(ctx);
+            if (!s) s = finish_diag(ctx, eig.data(), true);
+            if (s) break;
+            have_eig = true;
+        }
+        if (s) { status = s; break; }
+        // occupations from the new eigenvalues, then construct_density (scf.rs:275)
+        double mu = 0.0;
+        const double e_ts = fermi_occupations(eig.data(), ctx->nb, n_elec, p->kT, ctx->occ.data(), &mu);
+        CK(cudaMemcpyAsync(ctx->d_occ, ctx->occ.data(), sizeof(double) * ctx->nb, cudaMemcpyHostToDevice, st));
+        s = density_dev(ctx, ctx->d_rho_out);
+        if (s) { status = s; break; }
+        // energy of rho_out: E_H, E_xc, double counting
+        CK(cudaMemsetAsync(ctx->d_acc, 0, sizeof(double) * 8, st));
+        launch_real_to_complex(ctx->d_rho_out, ctx->d_cgrid, ng, st);
+        grid_fft3(ctx, ctx->d_cgrid, true);
+        launch_hartree_gspace(ctx->d_cgrid, grid_recip(ctx), ctx->omega, ctx->d_acc + 0, st);
+        launch_energy_terms(ctx->d_rho_out, ctx->d_veff, ctx->d_vloc, ng, dv, ctx->d_acc + 1,
+                            ctx->d_acc + 2, st);
+        CK(cudaGetLastError());
+        double acc[3];
+        CK(cudaMemcpyAsync(acc, ctx->d_acc, sizeof(acc), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        double eband = 0.0;
+        for (int b = 0; b < ctx->nb; ++b) eband += ctx->occ[b] * eig[b];
+        const double etot = eband - acc[2] + acc[0] + acc[1] + ctx->e_ewald + e_ts;
+        r->e_entropy = e_ts;
+        r->mu = mu;
+        if (r->energies) r->energies[it - 1] = etot;
+        r->e_band = eband; r->e_hartree = acc[0]; r->e_xc = acc[1]; r->e_dc = acc[2];
+        r->e_total = etot;
+        r->n_iter = it;
+        // check (scf.rs:328): |dE| per atom below tolerance
+        if (it > 1 && std::fabs(etot - e_prev) / ctx->n_atoms < p->tol_per_atom) {
+            status = CHFSI_OK;
+            e_prev = etot;
+            break;
+        }
+        e_prev = etot;
+        // mix (mixing.rs:24): Pulay over (rho_in, rho_out - rho_in)
+        if (ps.m == p->max_hist) {
+            // drop the oldest entry
+            for (int i = 0; i + 1 < ps.m; ++i)
+                for (int j = 0; j + 1 < ps.m; ++j) ps.M[i][j] = ps.M[i + 1][j + 1];
+            ps.head = (ps.head + 1) % kPulayMax;
+            --ps.m;
+        }
+        const int slot = (ps.head + ps.m) % kPulayMax;
+        double* hr = ctx->d_hist + (size_t)slot * ng;
+        double* hres = ctx->d_hist + (size_t)(kPulayMax + slot) * ng;
+        pulay_push(ctx->d_rho_in, ctx->d_rho_out, hr, hres, ng, st);
+        ++ps.m;
+        // ordered pointer lists (oldest first): residual pointers for dots,
+        // then the combine needs both lists
+        std::vector<double*> lr(ps.m), lres(ps.m);
+        for (int i = 0; i < ps.m; ++i) {
+            const int sl = (ps.head + i) % kPulayMax;
+            lr[i] = ctx->d_hist + (size_t)sl * ng;
+            lres[i] = ctx->d_hist + (size_t)(kPulayMax + sl) * ng;
+        }
+        CK(cudaMemcpyAsync(ctx->d_hist_ptrs, lres.data(), sizeof(double*) * ps.m, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ctx->d_hist_ptrs + kPulayMax, lr.data(), sizeof(double*) * ps.m, cudaMemcpyHostToDevice, st));
+        CK(cudaMemsetAsync(ctx->d_dots, 0, sizeof(double) * kPulayMax, st));
+        dots(hres, ctx->d_hist_ptrs, ps.m, ng, ctx->d_dots, st);
+        double dd[kPulayMax];
+        CK(cudaMemcpyAsync(dd, ctx->d_dots, sizeof(double) * ps.m, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        const int nw = ps.m - 1;
+        for (int j = 0; j < ps.m; ++j) { ps.M[nw][j] = dd[j]; ps.M[j][nw] = dd[j]; }
+        double c[kPulayMax] = {};
+        if (ps.m == 1 || !pulay_coefficients(ps.m, ps.M, c)) {
+            for (int j = 0; j < ps.m; ++j) c[j] = 0.0;
+            c[ps.m - 1] = 1.0;
+        }
+        pulay_combine(ctx->d_hist_ptrs + kPulayMax, ctx->d_hist_ptrs, ps.m, c, p->alpha, ng,
+                      ctx->d_rho_next, st);
+        std::swap(ctx->d_rho_in, ctx->d_rho_next);
+        CK(cudaGetLastError());
+    }
+    cudaEventRecord(t1, st);
+    cudaEventSynchronize(t1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, t0, t1);
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    r->seconds = ms * 1e-3;
+    r->status = status;
+    if (r->eigenvalues) std::memcpy(r->eigenvalues, eig.data(), sizeof(double) * ctx->nb);
+    return status;
+}
+
+extern "C" chfsi_status chfsi_get_density(chfsi_ctx* ctx, double* rho) {
+    if (!ctx || !rho) return CHFSI_ERR_BAD_INPUT;
+    cudaSetDevice(ctx->device);
+    CK(cudaStreamSynchronize(ctx->st));
+    CK(cudaMemcpy(rho, ctx->d_rho_out, sizeof(double) * ctx->ng, cudaMemcpyDeviceToHost));
+    return CHFSI_OK;
+}

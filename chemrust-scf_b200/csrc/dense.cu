@@ -1,0 +1,586 @@
+// Small dense FP64 kernels of the Rayleigh-Ritz step and the scalar
+// plumbing of the filter (bounds, norm guard, Lanczos), all on the device so
+// the ChFSI iteration needs no host round trip until the eigenvalues return.
+//
+// Rayleigh-Ritz follows the Cholesky reduction of the reference's CPU
+// path (src/eigensolver/subspace_diag.rs:229-391):
+//   S = L L^H (right-looking Cholesky, info = failing column as ZPOTRF),
+//   Li = L^-1, B = Li H Li^H (Hermitian-symmetrised),
+//   B U = U diag(w) by parallel cyclic Jacobi (cooperative launch,
+//   round-robin pair ordering, rows then columns per step),
+//   V = Li^H U; psi <- psi V (caller).
+// It replaces cuSOLVER ZHEGVD itype 1 (src/device/solver.rs:47-95).
+#include "dense.hpp"
+#include "launch_count.hpp"
+
+#include <cooperative_groups.h>
+
+namespace cg = cooperative_groups;
+
+namespace chfsi {
+
+namespace {
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double block_sum(double v, double* red) {
+    v = warp_sum(v);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) red[w] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+        s = warp_sum(s);
+    }
+    return s;
+}
+
+__global__ void k_symmetrize(const double2* __restrict__ in, double2* __restrict__ out, int n) {
+    const size_t nn = (size_t)n * n;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < nn;
+         t += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(t / n), j = (int)(t % n);
+        const double2 a = in[(size_t)i * n + j], b = in[(size_t)j * n + i];
+        out[t] = make_double2(0.5 * (a.x + b.x), 0.5 * (a.y - b.y));
+    }
+}
+
+// Right-looking Cholesky of a Hermitian positive-definite matrix in place
+// (lower triangle = L, upper zeroed).  info = 0 or the failing column + 1.
+__global__ void __launch_bounds__(1024) k_cholesky(double2* A, int n, int* info) {
+    __shared__ double ljj;
+    __shared__ int fail;
+    if (threadIdx.x == 0) fail = 0;
+    __syncthreads();
+    for (int j = 0; j < n; ++j) {
+        if (threadIdx.x == 0) {
+            const double d = A[(size_t)j * n + j].x;
+            if (!(d > 0.0)) { fail = j + 1; }
+            else {
+                ljj = sqrt(d);
+                A[(size_t)j * n + j] = make_double2(ljj, 0.0);
+            }
+        }
+        __syncthreads();
+        if (fail) break;
+        const double inv = 1.0 / ljj;
+        for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) {
+            double2& a = A[(size_t)i * n + j];
+            a = make_double2(a.x * inv, a.y * inv);
+        }
+        __syncthreads();
+        // trailing update of the lower triangle: A[i][k] -= L[i][j] conj(L[k][j]), j < k <= i
+        const int m = n - j - 1;
+        const size_t tri = (size_t)m * (m + 1) / 2;
+        for (size_t t = threadIdx.x; t < tri; t += blockDim.x) {
+            // map t -> (ii, kk) with 0 <= kk <= ii < m
+            int ii = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+            while ((size_t)(ii + 1) * (ii + 2) / 2 <= t) ++ii;
+            while ((size_t)ii * (ii + 1) / 2 > t) --ii;
+            const int kk = (int)(t - (size_t)ii * (ii + 1) / 2);
+            const int i = j + 1 + ii, k = j + 1 + kk;
+            const double2 lij = A[(size_t)i * n + j], lkj = A[(size_t)k * n + j];
+            double2& a = A[(size_t)i * n + k];
+            a.x -= lij.x * lkj.x + lij.y * lkj.y;
+            a.y -= lij.y * lkj.x - lij.x * lkj.y;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *info = fail;
+    if (fail) return;
+    for (size_t t = threadIdx.x; t < (size_t)n * n; t += blockDim.x) {
+        const int i = (int)(t / n), k = (int)(t % n);
+        if (k > i) A[t] = make_double2(0.0, 0.0);
+    }
+}
+
+// X = L^-1 by forward substitution, one column per thread.
+__global__ void k_tri_inv(const double2* __restrict__ L, double2* __restrict__ X, int n) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    for (int i = 0; i < c; ++i) X[(size_t)i * n + c] = make_double2(0.0, 0.0);
+    for (int i = c; i < n; ++i) {
+        double2 s = make_double2(i == c ? 1.0 : 0.0, 0.0);
+        for (int k = c; k < i; ++k) {
+            const double2 l = L[(size_t)i * n + k], x = X[(size_t)k * n + c];
+            s.x -= l.x * x.x - l.y * x.y;
+            s.y -= l.x * x.y + l.y * x.x;
+        }
+        const double2 d = L[(size_t)i * n + i];  // real diagonal
+        X[(size_t)i * n + c] = make_double2(s.x / d.x, s.y / d.x);
+    }
+}
+
+// C = op(A) op(B), n x n row-major; op 0 = N, 1 = conjugate transpose.
+template <int OPA, int OPB>
+__global__ void __launch_bounds__(256)
+k_small_gemm(const double2* __restrict__ A, const double2* __restrict__ B, double2* __restrict__ C,
+             int n) {
+    __shared__ double2 As[16][17], Bs[16][17];
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const int i = blockIdx.y * 16 + ty, j = blockIdx.x * 16 + tx;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int k0 = 0; k0 < n; k0 += 16) {
+        {
+            const int r = blockIdx.y * 16 + ty, k = k0 + tx;
+            double2 v = make_double2(0.0, 0.0);
+            if (r < n && k < n) {
+                if (OPA == 0) v = A[(size_t)r * n + k];
+                else { v = A[(size_t)k * n + r]; v.y = -v.y; }
+            }
+            As[ty][tx] = v;
+            const int kb = k0 + ty, cc = blockIdx.x * 16 + tx;
+            double2 w = make_double2(0.0, 0.0);
+            if (kb < n && cc < n) {
+                if (OPB == 0) w = B[(size_t)kb * n + cc];
+                else { w = B[(size_t)cc * n + kb]; w.y = -w.y; }
+            }
+            Bs[ty][tx] = w;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            const double2 a = As[ty][k], b = Bs[k][tx];
+            acc.x = fma(a.x, b.x, acc.x);
+            acc.x = fma(-a.y, b.y, acc.x);
+            acc.y = fma(a.x, b.y, acc.y);
+            acc.y = fma(a.y, b.x, acc.y);
+        }
+        __syncthreads();
+    }
+    if (i < n && j < n) C[(size_t)i * n + j] = acc;
+}
+
+// Parallel cyclic Jacobi for a Hermitian n x n matrix (row-major, in place).
+// On exit diag(A) holds the eigenvalues and V the eigenvectors (columns).
+// scratch: [0] |A|_F^2, [1 + s] off-diagonal |A|^2 after sweep s; rot: 4 doubles per pair.
+__global__ void __launch_bounds__(256)
+k_jacobi(double2* A, double2* V, int n, int max_sweeps, double tol2, double* scratch,
+         double* rot, int* sweeps_out) {
+    cg::grid_group grid = cg::this_grid();
+    __shared__ double red[32];
+    const int lane = threadIdx.x & 31;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const size_t nn = (size_t)n * n;
+    const size_t gtid = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    const size_t gstride = (size_t)gridDim.x * blockDim.x;
+    for (size_t t = gtid; t < nn; t += gstride)
+        V[t] = make_double2((t / n) == (t % n) ? 1.0 : 0.0, 0.0);
+    double tot = 0.0;
+    for (size_t t = gtid; t < nn; t += gstride) tot += A[t].x * A[t].x + A[t].y * A[t].y;
+    tot = block_sum(tot, red);
+    if (threadIdx.x == 0) atomicAdd(&scratch[0], tot);
+    grid.sync();
+    const double total = scratch[0];
+    const int m = n + (n & 1);
+    const int npairs = m / 2;
+    int sweep = 0;
+    for (; sweep < max_sweeps; ++sweep) {
+        for (int s = 0; s < m - 1; ++s) {
+            // ---- phase 1: rotation parameters + row update (rows p, q)
+            for (int pi = gw; pi < npairs; pi += nwarps) {
+                int a = pi == 0 ? 0 : 1 + ((pi - 1 + s) % (m - 1));
+                int b = 1 + ((m - 2 - pi + s) % (m - 1));
+                int p = min(a, b), q = max(a, b);
+                double c = 1.0, sn = 0.0, phr = 1.0, phi = 0.0;
+                const bool live = q < n;
+                if (live) {
+                    const double2 apq = A[(size_t)p * n + q];
+                    const double app = A[(size_t)p * n + p].x, aqq = A[(size_t)q * n + q].x;
+                    const double bm = hypot(apq.x, apq.y);
+                    if (bm > 1e-300 && bm > 1e-18 * sqrt(fabs(app * aqq))) {
+                        phr = apq.x / bm;
+                        phi = apq.y / bm;
+                        const double tau = (aqq - app) / (2.0 * bm);
+                        const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+                        c = 1.0 / sqrt(1.0 + t * t);
+                        sn = t * c;
+                    }
+                }
+                __syncwarp();
+                if (lane == 0) {
+                    rot[4 * pi + 0] = c; rot[4 * pi + 1] = sn;
+                    rot[4 * pi + 2] = phr; rot[4 * pi + 3] = phi;
+                }
+                if (live && sn != 0.0) {
+                    // conj(g_qp) = -s ph, conj(g_qq) = c ph ; row' = G^H row
+                    for (int k = lane; k < n; k += 32) {
+                        const double2 apk = A[(size_t)p * n + k], aqk = A[(size_t)q * n + k];
+                        // ph * aqk
+                        const double2 pa = make_double2(phr * aqk.x - phi * aqk.y, phr * aqk.y + phi * aqk.x);
+                        A[(size_t)p * n + k] = make_double2(c * apk.x - sn * pa.x, c * apk.y - sn * pa.y);
+                        A[(size_t)q * n + k] = make_double2(sn * apk.x + c * pa.x, sn * apk.y + c * pa.y);
+                    }
+                }
+            }
+            grid.sync();
+            // ---- phase 2: column update (columns p, q) of A and V
+            for (int pi = gw; pi < npairs; pi += nwarps) {
+                int a = pi == 0 ? 0 : 1 + ((pi - 1 + s) % (m - 1));
+                int b = 1 + ((m - 2 - pi + s) % (m - 1));
+                int p = min(a, b), q = max(a, b);
+                if (q >= n) continue;
+                const double c = rot[4 * pi + 0], sn = rot[4 * pi + 1];
+                const double phr = rot[4 * pi + 2], phi = rot[4 * pi + 3];
+                if (sn == 0.0) continue;
+                // g_qp = -s conj(ph), g_qq = c conj(ph); col' = col G
+                for (int k = lane; k < n; k += 32) {
+                    const double2 akp = A[(size_t)k * n + p], akq = A[(size_t)k * n + q];
+                    const double2 qc = make_double2(phr * akq.x + phi * akq.y, phr * akq.y - phi * akq.x);
+                    A[(size_t)k * n + p] = make_double2(c * akp.x - sn * qc.x, c * akp.y - sn * qc.y);
+                    A[(size_t)k * n + q] = make_double2(sn * akp.x + c * qc.x, sn * akp.y + c * qc.y);
+                    const double2 vkp = V[(size_t)k * n + p], vkq = V[(size_t)k * n + q];
+                    const double2 vc = make_double2(phr * vkq.x + phi * vkq.y, phr * vkq.y - phi * vkq.x);
+                    V[(size_t)k * n + p] = make_double2(c * vkp.x - sn * vc.x, c * vkp.y - sn * vc.y);
+                    V[(size_t)k * n + q] = make_double2(sn * vkp.x + c * vc.x, sn * vkp.y + c * vc.y);
+                }
+                __syncwarp();
+                if (lane == 0) {
+                    A[(size_t)p * n + q] = make_double2(0.0, 0.0);
+                    A[(size_t)q * n + p] = make_double2(0.0, 0.0);
+                    A[(size_t)p * n + p].y = 0.0;
+                    A[(size_t)q * n + q].y = 0.0;
+                }
+            }
+            grid.sync();
+        }
+        double off = 0.0;
+        for (size_t t = gtid; t < nn; t += gstride)
+            if ((t / n) != (t % n)) off += A[t].x * A[t].x + A[t].y * A[t].y;
+        off = block_sum(off, red);
+        if (threadIdx.x == 0) atomicAdd(&scratch[1 + sweep], off);
+        grid.sync();
+        if (scratch[1 + sweep] <= tol2 * total) { ++sweep; break; }
+    }
+    if (gtid == 0) *sweeps_out = sweep;
+}
+
+// Sort eigenvalues ascending (stable by index) and permute eigenvector columns.
+__global__ void __launch_bounds__(1024)
+k_sort_eig(const double2* __restrict__ A, const double2* __restrict__ V, int n,
+           double* __restrict__ w_out, double2* __restrict__ U) {
+    extern __shared__ int perm_smem[];
+    int* dest = perm_smem;  // dest[i] = rank of eigenvalue i
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double wi = A[(size_t)i * n + i].x;
+        int r = 0;
+        for (int j = 0; j < n; ++j) {
+            const double wj = A[(size_t)j * n + j].x;
+            r += (wj < wi) || (wj == wi && j < i);
+        }
+        dest[i] = r;
+        w_out[r] = wi;
+    }
+    __syncthreads();
+    for (size_t t = threadIdx.x; t < (size_t)n * n; t += blockDim.x) {
+        const int row = (int)(t / n), i = (int)(t % n);
+        U[(size_t)row * n + dest[i]] = V[t];
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_minmax(const double* __restrict__ v, size_t n, double* out) {
+    __shared__ double smin[32], smax[32];
+    double lo = 1e300, hi = -1e300;
+    for (size_t i = threadIdx.x; i < n; i += blockDim.x) {
+        lo = fmin(lo, v[i]);
+        hi = fmax(hi, v[i]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if ((threadIdx.x & 31) == 0) { smin[threadIdx.x >> 5] = lo; smax[threadIdx.x >> 5] = hi; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) { lo = fmin(lo, smin[w]); hi = fmax(hi, smax[w]); }
+        out[0] = lo;
+        out[1] = hi;
+    }
+}
+
+__global__ void __launch_bounds__(256)
+k_sumsq(const double2* __restrict__ x, size_t n, double* acc) {
+    __shared__ double red[32];
+    double s = 0.0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        s += x[i].x * x[i].x + x[i].y * x[i].y;
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) atomicAdd(acc, s);
+}
+
+// Largest eigenvalue of the Lanczos tridiagonal by Sturm bisection.
+__device__ double tridiag_max(const double* d, const double* e, int k) {
+    double lo = 1e300, hi = -1e300;
+    for (int i = 0; i < k; ++i) {
+        const double r = (i > 0 ? fabs(e[i - 1]) : 0.0) + (i < k - 1 ? fabs(e[i]) : 0.0);
+        lo = fmin(lo, d[i] - r);
+        hi = fmax(hi, d[i] + r);
+    }
+    for (int it = 0; it < 200; ++it) {
+        const double mid = 0.5 * (lo + hi);
+        if (mid <= lo || mid >= hi) break;
+        int c = 0;
+        double q = d[0] - mid;
+        if (q < 0) ++c;
+        for (int i = 1; i < k; ++i) {
+            const double qq = q == 0.0 ? 1e-300 : q;
+            q = d[i] - mid - e[i - 1] * e[i - 1] / qq;
+            if (q < 0) ++c;
+        }
+        if (c >= k) hi = mid; else lo = mid;
+    }
+    return hi;
+}
+
+// Spectral bounds (src/eigensolver/chebyshev.rs:225-254).  coef[0..5] =
+// lambda_max, eps_cut, center c, half-width e, 1/e, -c/e.  lanczos: k alphas
+// followed by k squared residual norms |f_j|^2 (null: kinetic + potential-
+// range bound); the Lanczos bound is lambda_max(T_k) + |f_k| (Zhou 2010).
+__global__ void k_bounds(double kin_max, const double* __restrict__ minmax,
+                         const double* __restrict__ eig, int n_eig, const double* lanczos, int k,
+                         double* coef) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double lm;
+    if (lanczos) {
+        double e[64];
+        for (int i = 0; i < k - 1 && i < 64; ++i) e[i] = sqrt(lanczos[k + i]);
+        lm = tridiag_max(lanczos, e, k) + sqrt(lanczos[2 * k - 1]);
+    } else {
+        lm = kin_max + (minmax[1] - minmax[0]);
+    }
+    double cut;
+    if (!eig || n_eig == 0) cut = lm / 3.0;
+    else {
+        const double e0 = eig[0], el = eig[n_eig - 1];
+        cut = fmin(el + 0.2 * (el - e0), lm * 0.95);
+    }
+    const double c = (lm + cut) / 2.0, e = (lm - cut) / 2.0;
+    coef[0] = lm; coef[1] = cut; coef[2] = c; coef[3] = e;
+    coef[4] = 1.0 / e;
+    coef[5] = -c / e;
+}
+
+// 10x norm-growth guard over the squared norms of one filter
+// (src/eigensolver/chebyshev.rs:552-563), checked for k >= 2 as the
+// reference does; status[0] = first failing degree (0 = none).
+__global__ void k_norm_guard(const double* __restrict__ nsq, int ndeg, int* status) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    int fail = 0;
+    for (int k = 2; k <= ndeg && !fail; ++k) {
+        const double prev = sqrt(nsq[k - 1]), cur = sqrt(nsq[k]);
+        const double growth = prev > 0.0 ? cur / prev : 1.0;
+        if (growth > 10.0 || !(cur == cur)) fail = k;
+    }
+    status[0] = fail;
+}
+
+// ---- Lanczos helpers (vectors of n complex, scalars on device)
+__global__ void k_scale_by_rsqrt(double2* v, size_t n, const double* nsq) {
+    const double s = 1.0 / sqrt(*nsq);
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        v[i] = make_double2(v[i].x * s, v[i].y * s);
+}
+// f -= beta v0 (if beta_sq); alpha_acc += Re<v, f>
+__global__ void __launch_bounds__(256)
+k_lanczos_a(double2* f, const double2* v, const double2* v0, const double* beta_sq, size_t n,
+            double* alpha_acc) {
+    __shared__ double red[32];
+    const double bt = beta_sq ? sqrt(*beta_sq) : 0.0;
+    double s = 0.0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        double2 x = f[i];
+        if (beta_sq) { x.x -= bt * v0[i].x; x.y -= bt * v0[i].y; f[i] = x; }
+        s += v[i].x * x.x + v[i].y * x.y;
+    }
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) atomicAdd(alpha_acc, s);
+}
+// f -= alpha v; fn_acc += |f|^2
+__global__ void __launch_bounds__(256)
+k_lanczos_b(double2* f, const double2* v, const double* alpha, size_t n, double* fn_acc) {
+    __shared__ double red[32];
+    const double a = *alpha;
+    double s = 0.0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        double2 x = f[i];
+        x.x -= a * v[i].x;
+        x.y -= a * v[i].y;
+        f[i] = x;
+        s += x.x * x.x + x.y * x.y;
+    }
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) atomicAdd(fn_acc, s);
+}
+// v0 = v; v = f / sqrt(fn)
+__global__ void k_lanczos_c(const double2* f, double2* v, double2* v0, size_t n, const double* fn) {
+    const double s = 1.0 / sqrt(*fn);
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        v0[i] = v[i];
+        v[i] = make_double2(f[i].x * s, f[i].y * s);
+    }
+}
+// beta[j] = sqrt(fn)
+__global__ void k_lanczos_store_beta(const double* fn, double* beta) {
+    if (threadIdx.x == 0) *beta = sqrt(*fn);
+}
+
+// ---- Pulay helpers
+__global__ void k_pulay_push(const double* rin, const double* rout, double* hr, double* hres,
+                             size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        hr[i] = rin[i];
+        hres[i] = rout[i] - rin[i];
+    }
+}
+__global__ void __launch_bounds__(256)
+k_dots(const double* __restrict__ x, const double* const* ys, int m, size_t n, double* out) {
+    __shared__ double red[32];
+    double acc[kPulayMax];
+    for (int j = 0; j < kPulayMax; ++j) acc[j] = 0.0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const double xi = x[i];
+#pragma unroll
+        for (int j = 0; j < kPulayMax; ++j)
+            if (j < m) acc[j] += xi * ys[j][i];
+    }
+    for (int j = 0; j < m; ++j) {
+        const double s = block_sum(acc[j], red);
+        if (threadIdx.x == 0) atomicAdd(&out[j], s);
+    }
+}
+struct PulayCoef { double c[kPulayMax]; };
+__global__ void k_pulay_combine(const double* const* hr, const double* const* hres, int m,
+                                PulayCoef pc, double alpha, size_t n, double* out) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int j = 0; j < m; ++j) s += pc.c[j] * (hr[j][i] + alpha * hres[j][i]);
+        out[i] = s;
+    }
+}
+
+int grid_for(size_t n) {
+    size_t b = (n + 255) / 256;
+    return (int)(b < 148 * 8 ? b : 148 * 8);
+}
+
+}  // namespace
+
+void symmetrize(const double2* in, double2* out, int n, cudaStream_t st) {
+    count_launch();
+    k_symmetrize<<<grid_for((size_t)n * n), 256, 0, st>>>(in, out, n);
+}
+void cholesky(double2* A, int n, int* info, cudaStream_t st) {
+    count_launch();
+    k_cholesky<<<1, 1024, 0, st>>>(A, n, info);
+}
+void tri_inv(const double2* L, double2* X, int n, cudaStream_t st) {
+    count_launch();
+    k_tri_inv<<<(n + 63) / 64, 64, 0, st>>>(L, X, n);
+}
+void small_gemm(int opa, int opb, const double2* A, const double2* B, double2* C, int n,
+                cudaStream_t st) {
+    count_launch();
+    dim3 grid((n + 15) / 16, (n + 15) / 16);
+    if (opa == 0 && opb == 0) k_small_gemm<0, 0><<<grid, 256, 0, st>>>(A, B, C, n);
+    else if (opa == 0 && opb == 1) k_small_gemm<0, 1><<<grid, 256, 0, st>>>(A, B, C, n);
+    else if (opa == 1 && opb == 0) k_small_gemm<1, 0><<<grid, 256, 0, st>>>(A, B, C, n);
+    else k_small_gemm<1, 1><<<grid, 256, 0, st>>>(A, B, C, n);
+}
+size_t jacobi_scratch_doubles(int n, int max_sweeps) {
+    return 1 + (size_t)max_sweeps + 4 * (size_t)((n + 1) / 2 + 1);
+}
+cudaError_t jacobi(double2* A, double2* V, int n, int max_sweeps, double tol2, double* scratch,
+                   int* sweeps_out, cudaStream_t st) {
+    count_launch();
+    cudaMemsetAsync(scratch, 0, sizeof(double) * (1 + max_sweeps), st);
+    double* rot = scratch + 1 + max_sweeps;
+    const int npairs = (n + 1) / 2;
+    const int warps_per_block = 8;
+    int blocks = (npairs + warps_per_block - 1) / warps_per_block;
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_jacobi, 256, 0);
+    if (per_sm < 1) per_sm = 1;
+    if (blocks > sms * per_sm) blocks = sms * per_sm;
+    if (blocks < 1) blocks = 1;
+    void* args[] = {&A, &V, &n, &max_sweeps, &tol2, &scratch, &rot, &sweeps_out};
+    return cudaLaunchCooperativeKernel((const void*)k_jacobi, dim3(blocks), dim3(256), args, 0, st);
+}
+void sort_eig(const double2* A, const double2* V, int n, double* w, double2* U, cudaStream_t st) {
+    count_launch();
+    k_sort_eig<<<1, 1024, sizeof(int) * n, st>>>(A, V, n, w, U);
+}
+void minmax(const double* v, size_t n, double* out, cudaStream_t st) {
+    count_launch();
+    k_minmax<<<1, 1024, 0, st>>>(v, n, out);
+}
+void sumsq(const double2* x, size_t n, double* acc, cudaStream_t st) {
+    count_launch();
+    k_sumsq<<<grid_for(n), 256, 0, st>>>(x, n, acc);
+}
+void bounds(double kin_max, const double* minmax_dev, const double* eig_dev, int n_eig,
+            const double* lanczos, int k, double* coef, cudaStream_t st) {
+    count_launch();
+    k_bounds<<<1, 32, 0, st>>>(kin_max, minmax_dev, eig_dev, n_eig, lanczos, k, coef);
+}
+void norm_guard(const double* nsq, int ndeg, int* status, cudaStream_t st) {
+    count_launch();
+    k_norm_guard<<<1, 32, 0, st>>>(nsq, ndeg, status);
+}
+void scale_by_rsqrt(double2* v, size_t n, const double* nsq, cudaStream_t st) {
+    count_launch();
+    k_scale_by_rsqrt<<<grid_for(n), 256, 0, st>>>(v, n, nsq);
+}
+void lanczos_a(double2* f, const double2* v, const double2* v0, const double* beta_sq, size_t n,
+               double* alpha_acc, cudaStream_t st) {
+    count_launch();
+    k_lanczos_a<<<grid_for(n), 256, 0, st>>>(f, v, v0, beta_sq, n, alpha_acc);
+}
+void lanczos_b(double2* f, const double2* v, const double* alpha, size_t n, double* fn_acc,
+               cudaStream_t st) {
+    count_launch();
+    k_lanczos_b<<<grid_for(n), 256, 0, st>>>(f, v, alpha, n, fn_acc);
+}
+void lanczos_c(const double2* f, double2* v, double2* v0, size_t n, const double* fn,
+               cudaStream_t st) {
+    count_launch();
+    k_lanczos_c<<<grid_for(n), 256, 0, st>>>(f, v, v0, n, fn);
+}
+void lanczos_store_beta(const double* fn, double* beta, cudaStream_t st) {
+    count_launch();
+    k_lanczos_store_beta<<<1, 32, 0, st>>>(fn, beta);
+}
+void pulay_push(const double* rin, const double* rout, double* hr, double* hres, size_t n,
+                cudaStream_t st) {
+    count_launch();
+    k_pulay_push<<<grid_for(n), 256, 0, st>>>(rin, rout, hr, hres, n);
+}
+void dots(const double* x, const double* const* ys, int m, size_t n, double* out, cudaStream_t st) {
+    count_launch();
+    k_dots<<<grid_for(n), 256, 0, st>>>(x, ys, m, n, out);
+}
+void pulay_combine(const double* const* hr, const double* const* hres, int m, const double* c,
+                   double alpha, size_t n, double* out, cudaStream_t st) {
+    count_launch();
+    PulayCoef pc{};
+    for (int j = 0; j < m && j < kPulayMax; ++j) pc.c[j] = c[j];
+    k_pulay_combine<<<grid_for(n), 256, 0, st>>>(hr, hres, m, pc, alpha, n, out);
+}
+
+}  // namespace chfsi

@@ -1,0 +1,199 @@
+// Shared-memory mixed-radix FFT line engine.
+//
+// A CTA transforms a set of lines that live in shared memory.  Line l starts
+// at smem offset base(l) and its elements are es apart.  Transforms are
+// in place and unnormalised:
+//   forward (DIF, sign -1): natural order in  -> digit-reversed order out
+//   inverse (DIT, sign +1): digit-reversed in -> natural order out
+// so a forward / pointwise-multiply / inverse sequence never needs an
+// explicit permutation; the digit-reversal map only enters where plane
+// waves are scattered into or gathered from a grid (host-built tables).
+//
+// For N = r0 r1 ... r_{s-1}, the DIF stage t with block size B and span
+// S = B / r_t maps, for every block b0 and n1 < S,
+//   x_j = a[b0 + n1 + j S],  y_m = sum_j x_j w_r^{-jm},  a[b0 + n1 + m S] = y_m w_B^{-n1 m}
+// and the DIT runs the stages in reverse order with the twiddle applied
+// before the butterfly (the transpose of the DIF, hence F P^T).
+#pragma once
+
+#include "common.cuh"
+
+namespace chfsi {
+
+constexpr int kMaxStages = 10;
+
+struct AxisPlan {
+    int n;
+    int nst;
+    int r[kMaxStages];  // radices in DIF order
+};
+
+// r-point DFT in registers, exponent sign SIGN (+1 or -1).
+template <typename C> __device__ __forceinline__ void dft2(C* x) {
+    C a = x[0], b = x[1];
+    x[0] = cadd(a, b);
+    x[1] = csub(a, b);
+}
+
+template <int SIGN, typename C> __device__ __forceinline__ void dft3(C* x) {
+    using R = typename RealOf<C>::type;
+    const R h = (R)0.86602540378443864676;  // sin(2 pi / 3)
+    C t1 = cadd(x[1], x[2]);
+    C t2 = csub(x[1], x[2]);
+    C y0 = cadd(x[0], t1);
+    C m = mk(x[0].x - (R)0.5 * t1.x, x[0].y - (R)0.5 * t1.y);
+    C u = cmul_i<SIGN>(cscale(t2, h));
+    x[0] = y0;
+    x[1] = cadd(m, u);
+    x[2] = csub(m, u);
+}
+template <int SIGN, typename C> __device__ __forceinline__ void dft4(C* x) {
+    C a = cadd(x[0], x[2]), b = csub(x[0], x[2]);
+    C c = cadd(x[1], x[3]), d = cmul_i<SIGN>(csub(x[1], x[3]));
+    x[0] = cadd(a, c);
+    x[2] = csub(a, c);
+    x[1] = cadd(b, d);
+    x[3] = csub(b, d);
+}
+template <int SIGN, typename C> __device__ __forceinline__ void dft5(C* x) {
+    using R = typename RealOf<C>::type;
+    const R c1 = (R)0.30901699437494742410, c2 = (R)-0.80901699437494742410;
+    const R s1 = (R)0.95105651629515357212, s2 = (R)0.58778525229247312917;
+    C a1 = cadd(x[1], x[4]), b1 = csub(x[1], x[4]);
+    C a2 = cadd(x[2], x[3]), b2 = csub(x[2], x[3]);
+    C y0 = cadd(x[0], cadd(a1, a2));
+    C t1 = mk(x[0].x + c1 * a1.x + c2 * a2.x, x[0].y + c1 * a1.y + c2 * a2.y);
+    C t2 = mk(x[0].x + c2 * a1.x + c1 * a2.x, x[0].y + c2 * a1.y + c1 * a2.y);
+    C u1 = cmul_i<SIGN>(mk(s1 * b1.x + s2 * b2.x, s1 * b1.y + s2 * b2.y));
+    C u2 = cmul_i<SIGN>(mk(s2 * b1.x - s1 * b2.x, s2 * b1.y - s1 * b2.y));
+    x[0] = y0;
+    x[1] = cadd(t1, u1);
+    x[4] = csub(t1, u1);
+    x[2] = cadd(t2, u2);
+    x[3] = csub(t2, u2);
+}
+// radix 8 = 2 x 4 split: x_j, j = 4 a + b  -> DFT over a (size 2), twiddle, DFT over b (size 4)
+template <int SIGN, typename C> __device__ __forceinline__ void dft8(C* x) {
+    using R = typename RealOf<C>::type;
+    const R r2 = (R)0.70710678118654752440;
+    // stage 1: four radix-2 butterflies on (x_b, x_{b+4})
+    C u[8];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+        u[b] = cadd(x[b], x[b + 4]);
+        u[b + 4] = csub(x[b], x[b + 4]);
+    }
+    // twiddle w8^{SIGN * b} on the odd half
+    u[5] = mk(r2 * (u[5].x - (R)SIGN * u[5].y), r2 * (u[5].y + (R)SIGN * u[5].x));
+    u[6] = cmul_i<SIGN>(u[6]);
+    u[7] = mk(r2 * (-u[7].x - (R)SIGN * u[7].y), r2 * (-u[7].y + (R)SIGN * u[7].x));
+    C e[4] = {u[0], u[1], u[2], u[3]}, o[4] = {u[4], u[5], u[6], u[7]};
+    dft4<SIGN>(e);
+    dft4<SIGN>(o);
+    // output index k = 2 k' + a
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        x[2 * k] = e[k];
+        x[2 * k + 1] = o[k];
+    }
+}
+
+template <int R, int SIGN, typename C> __device__ __forceinline__ void dft_r(C* x) {
+    if constexpr (R == 2) dft2(x);
+    else if constexpr (R == 3) dft3<SIGN>(x);
+    else if constexpr (R == 4) dft4<SIGN>(x);
+    else if constexpr (R == 5) dft5<SIGN>(x);
+    else if constexpr (R == 8) dft8<SIGN>(x);
+}
+
+// One DIF (FWD=true, sign -1) or DIT (FWD=false, sign +1) stage of radix R
+// over nlines lines.  tw[j] = exp(+2 pi i j / n).
+template <int R, bool FWD, typename C, class LineBase>
+__device__ __forceinline__ void fft_stage(C* s, int nlines, LineBase lb, int es, int n, int B,
+                                          const C* tw) {
+    const int S = B / R;
+    const int nb = n / R;
+    const int step = n / B;
+    const int total = nlines * nb;
+    for (int u = threadIdx.x; u < total; u += blockDim.x) {
+        const int l = u / nb;
+        const int v = u - l * nb;
+        const int blk = v / S;
+        const int n1 = v - blk * S;
+        C* p = s + lb(l) + (blk * B + n1) * es;
+        const int se = S * es;
+        C x[R];
+#pragma unroll
+        for (int j = 0; j < R; ++j) x[j] = p[j * se];
+        const int e = step * n1;
+        if (FWD) {
+            dft_r<R, -1>(x);
+#pragma unroll
+            for (int m = 1; m < R; ++m) x[m] = cmulc(tw[e * m], x[m]);
+        } else {
+#pragma unroll
+            for (int m = 1; m < R; ++m) x[m] = cmul(tw[e * m], x[m]);
+            dft_r<R, 1>(x);
+        }
+#pragma unroll
+        for (int m = 0; m < R; ++m) p[m * se] = x[m];
+    }
+}
+
+template <bool FWD, typename C, class LineBase>
+__device__ __forceinline__ void fft_dispatch(int r, C* s, int nlines, LineBase lb, int es, int n,
+                                             int B, const C* tw) {
+    switch (r) {
+    case 2: fft_stage<2, FWD>(s, nlines, lb, es, n, B, tw); break;
+    case 3: fft_stage<3, FWD>(s, nlines, lb, es, n, B, tw); break;
+    case 4: fft_stage<4, FWD>(s, nlines, lb, es, n, B, tw); break;
+    case 5: fft_stage<5, FWD>(s, nlines, lb, es, n, B, tw); break;
+    case 8: fft_stage<8, FWD>(s, nlines, lb, es, n, B, tw); break;
+    default: break;
+    }
+}
+
+// Forward transform (DIF, sign -1) of nlines lines; ends with __syncthreads.
+template <typename C, class LineBase>
+__device__ __forceinline__ void fft_forward(C* s, int nlines, LineBase lb, int es,
+                                            const AxisPlan& P, const C* tw) {
+    int B = P.n;
+    for (int t = 0; t < P.nst; ++t) {
+        fft_dispatch<true>(P.r[t], s, nlines, lb, es, P.n, B, tw);
+        __syncthreads();
+        B /= P.r[t];
+    }
+}
+
+// Inverse transform (DIT, sign +1); ends with __syncthreads.
+template <typename C, class LineBase>
+__device__ __forceinline__ void fft_inverse(C* s, int nlines, LineBase lb, int es,
+                                            const AxisPlan& P, const C* tw) {
+    int S = 1;
+    for (int t = P.nst - 1; t >= 0; --t) {
+        const int B = S * P.r[t];
+        fft_dispatch<false>(P.r[t], s, nlines, lb, es, P.n, B, tw);
+        __syncthreads();
+        S = B;
+    }
+}
+
+struct LinesStrided {
+    int ls;
+    __device__ __forceinline__ int operator()(int l) const { return l * ls; }
+};
+struct LinesListed {
+    const int* list;
+    __device__ __forceinline__ int operator()(int l) const { return list[l]; }
+};
+
+// tw[j] = exp(+2 pi i j / n), computed in FP64 then rounded to C.
+template <typename C> __device__ __forceinline__ void load_twiddles(C* tw, int n) {
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        double sn, cs;
+        sincospi(2.0 * (double)j / (double)n, &sn, &cs);
+        tw[j] = to_c(make_double2(cs, sn), C{});
+    }
+}
+
+}  // namespace chfsi

@@ -1,0 +1,496 @@
+// Local Hamiltonian H_loc|psi> = T psi + FFT^-1[V(r) FFT[psi]] on the
+// G-sphere, as three pruned passes over a band batch (role of the reference's
+// init_kinetic / zero / scatter / cuFFT Z2Z / veff_multiply / cuFFT /
+// gather_add_kinetic sequence, src/eigensolver/chebyshev.rs:279-365):
+//
+//   pass 1  z-sticks:  scatter the sphere coefficients of a group of (x,y)
+//           columns into smem z-lines, inverse FFT along z, write the sticks
+//           plane-major: work[b][z][column]
+//   pass 2  xy-planes: unpack one z-plane (only the columns that carry
+//           plane waves), inverse FFT along y (active x lines only) and x,
+//           multiply by V(r), forward FFT along x and y (active x lines),
+//           pack the columns back in place
+//   pass 3  z-sticks:  forward FFT along z, gather the sphere, add the
+//           kinetic and non-local terms and run the Chebyshev-recurrence
+//           epilogue, reducing |psi_k|^2 for the norm guard
+//
+// HBM traffic per band: 4 x (ncol x nz) complex words plus the sphere
+// vectors, versus ~14 N^3 words for the unpruned zero/scatter/FFT/multiply/
+// FFT/gather sequence.
+#include "kernels.hpp"
+#include "launch_count.hpp"
+
+#include <cstdio>
+
+namespace chfsi {
+
+namespace {
+
+template <typename C> __device__ __forceinline__ C czero() {
+    using R = typename RealOf<C>::type;
+    return mk((R)0, (R)0);
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Block-wide sum; result valid in thread 0.  red needs blockDim/32 doubles.
+__device__ __forceinline__ double block_sum(double v, double* red) {
+    v = warp_sum(v);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) red[w] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+        s = warp_sum(s);
+    }
+    return s;
+}
+
+template <typename C> __host__ __device__ __forceinline__ size_t align16(size_t n) {
+    return (n * sizeof(C) + 15) & ~(size_t)15;
+}
+
+// ---------------------------------------------------------------- pass 1
+template <typename C>
+__global__ void __launch_bounds__(256)
+k_zsticks_inverse(const C* __restrict__ psi, int ldp, C* __restrict__ work, HGeom g) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* tw = reinterpret_cast<C*>(smem_raw);
+    C* lines = reinterpret_cast<C*>(smem_raw + align16<C>(g.nz));
+    const int b = blockIdx.y;
+    const int c0 = blockIdx.x * kColsPerBlock;
+    const int c1 = min(c0 + kColsPerBlock, g.ncol);
+    const int nl = c1 - c0;
+    load_twiddles(tw, g.nz);
+    for (int i = threadIdx.x; i < kColsPerBlock * g.lsz; i += blockDim.x) lines[i] = czero<C>();
+    __syncthreads();
+    const int g0 = g.col_start[c0], g1 = g.col_start[c1];
+    const C* pb = psi + (size_t)b * ldp;
+    for (int q = g0 + threadIdx.x; q < g1; q += blockDim.x)
+        lines[(g.pw_col[q] - c0) * g.lsz + g.pw_zpos[q]] = pb[q];
+    __syncthreads();
+    fft_inverse(lines, nl, LinesStrided{g.lsz}, 1, g.az, tw);
+    C* wb = work + (size_t)b * g.nz * g.ncol;
+    for (int u = threadIdx.x; u < g.nz * kColsPerBlock; u += blockDim.x) {
+        const int z = u / kColsPerBlock, cl = u - z * kColsPerBlock;
+        if (cl < nl) wb[(size_t)z * g.ncol + c0 + cl] = lines[cl * g.lsz + z];
+    }
+}
+
+// ---------------------------------------------------------------- pass 2
+template <typename C>
+__global__ void __launch_bounds__(512)
+k_planes_vloc(C* __restrict__ work, const double* __restrict__ veff, HGeom g) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* twx = reinterpret_cast<C*>(smem_raw);
+    C* twy = reinterpret_cast<C*>(smem_raw + align16<C>(g.nx));
+    C* plane = reinterpret_cast<C*>(smem_raw + align16<C>(g.nx) + align16<C>(g.ny));
+    int* xl = reinterpret_cast<int*>(plane + (size_t)g.ny * g.lsx);
+    const int z = blockIdx.x, b = blockIdx.y;
+    load_twiddles(twx, g.nx);
+    load_twiddles(twy, g.ny);
+    for (int i = threadIdx.x; i < g.nxact; i += blockDim.x) xl[i] = g.xact[i];
+    for (int i = threadIdx.x; i < g.ny * g.lsx; i += blockDim.x) plane[i] = czero<C>();
+    __syncthreads();
+    C* wp = work + ((size_t)b * g.nz + z) * g.ncol;
+    for (int c = threadIdx.x; c < g.ncol; c += blockDim.x) plane[g.col_pos[c]] = wp[c];
+    __syncthreads();
+    fft_inverse(plane, g.nxact, LinesListed{xl}, g.lsx, g.ay, twy);
+    fft_inverse(plane, g.ny, LinesStrided{g.lsx}, 1, g.ax, twx);
+    const double* vz = veff + (size_t)z * g.nx * g.ny;
+    using R = typename RealOf<C>::type;
+    for (int i = threadIdx.x; i < g.nx * g.ny; i += blockDim.x) {
+        const int y = i / g.nx, x = i - y * g.nx;
+        C& v = plane[y * g.lsx + x];
+        v = cscale(v, (R)vz[i]);
+    }
+    __syncthreads();
+    fft_forward(plane, g.ny, LinesStrided{g.lsx}, 1, g.ax, twx);
+    fft_forward(plane, g.nxact, LinesListed{xl}, g.lsx, g.ay, twy);
+    for (int c = threadIdx.x; c < g.ncol; c += blockDim.x) wp[c] = plane[g.col_pos[c]];
+}
+
+// ---------------------------------------------------------------- pass 3
+template <typename C, int MODE>
+__global__ void __launch_bounds__(256)
+k_zsticks_forward(const C* __restrict__ work, const C* __restrict__ psi, int ldp, C* out, int ldo,
+                  HGeom g, Epilogue e) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* tw = reinterpret_cast<C*>(smem_raw);
+    C* lines = reinterpret_cast<C*>(smem_raw + align16<C>(g.nz));
+    __shared__ double red[32];
+    using R = typename RealOf<C>::type;
+    const int b = blockIdx.y;
+    const int c0 = blockIdx.x * kColsPerBlock;
+    const int c1 = min(c0 + kColsPerBlock, g.ncol);
+    const int nl = c1 - c0;
+    load_twiddles(tw, g.nz);
+    const C* wb = work + (size_t)b * g.nz * g.ncol;
+    for (int u = threadIdx.x; u < g.nz * kColsPerBlock; u += blockDim.x) {
+        const int z = u / kColsPerBlock, cl = u - z * kColsPerBlock;
+        lines[cl * g.lsz + z] = cl < nl ? wb[(size_t)z * g.ncol + c0 + cl] : czero<C>();
+    }
+    __syncthreads();
+    fft_forward(lines, nl, LinesStrided{g.lsz}, 1, g.az, tw);
+    const int g0 = g.col_start[c0], g1 = g.col_start[c1];
+    const C* pb = psi + (size_t)b * ldp;
+    C* ob = out + (size_t)b * ldo;
+    const C* nlb = e.nl ? reinterpret_cast<const C*>(e.nl) + (size_t)b * ldp : nullptr;
+    R ie = 0, nc = 0;
+    if (MODE != kEpiApply) {
+        ie = (R)e.coef[4];
+        nc = (R)e.coef[5];
+    }
+    const R inv_n = (R)e.inv_n;
+    double nacc = 0.0;
+    for (int q = g0 + threadIdx.x; q < g1; q += blockDim.x) {
+        const C v = lines[(g.pw_col[q] - c0) * g.lsz + g.pw_zpos[q]];
+        const C p = pb[q];
+        const R k = (R)e.kin[q];
+        C h = mk(p.x * k, p.y * k);
+        h = mk(h.x + v.x * inv_n, h.y + v.y * inv_n);
+        if (nlb) h = cadd(h, nlb[q]);
+        if (MODE == kEpiApply) {
+            ob[q] = h;
+        } else {
+            C s = mk(h.x * ie + nc * p.x, h.y * ie + nc * p.y);
+            C o;
+            if (MODE == kEpiChebFirst) o = s;
+            else {
+                const C prev = ob[q];
+                o = mk((R)2 * s.x - prev.x, (R)2 * s.y - prev.y);
+            }
+            ob[q] = o;
+            nacc += (double)o.x * (double)o.x + (double)o.y * (double)o.y;
+        }
+    }
+    if (MODE != kEpiApply && e.norm_acc) {
+        double s = block_sum(nacc, red);
+        if (threadIdx.x == 0) atomicAdd(e.norm_acc, s);
+    }
+}
+
+// ------------------------------------------------------ density (pass 2')
+template <typename C, int MAXPT>
+__global__ void __launch_bounds__(512)
+k_planes_density(const C* __restrict__ work, const double* __restrict__ occ, int nb, int bpg,
+                 double scale, double* rho, HGeom g) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* twx = reinterpret_cast<C*>(smem_raw);
+    C* twy = reinterpret_cast<C*>(smem_raw + align16<C>(g.nx));
+    C* plane = reinterpret_cast<C*>(smem_raw + align16<C>(g.nx) + align16<C>(g.ny));
+    int* xl = reinterpret_cast<int*>(plane + (size_t)g.ny * g.lsx);
+    const int z = blockIdx.x;
+    const int b0 = blockIdx.y * bpg, b1 = min(b0 + bpg, nb);
+    load_twiddles(twx, g.nx);
+    load_twiddles(twy, g.ny);
+    for (int i = threadIdx.x; i < g.nxact; i += blockDim.x) xl[i] = g.xact[i];
+    double acc[MAXPT];
+#pragma unroll
+    for (int k = 0; k < MAXPT; ++k) acc[k] = 0.0;
+    const int npl = g.nx * g.ny;
+    for (int b = b0; b < b1; ++b) {
+        const double f = occ[b] * scale;
+        if (f == 0.0) continue;
+        for (int i = threadIdx.x; i < g.ny * g.lsx; i += blockDim.x) plane[i] = czero<C>();
+        __syncthreads();
+        const C* wp = work + ((size_t)b * g.nz + z) * g.ncol;
+        for (int c = threadIdx.x; c < g.ncol; c += blockDim.x) plane[g.col_pos[c]] = wp[c];
+        __syncthreads();
+        fft_inverse(plane, g.nxact, LinesListed{xl}, g.lsx, g.ay, twy);
+        fft_inverse(plane, g.ny, LinesStrided{g.lsx}, 1, g.ax, twx);
+#pragma unroll
+        for (int k = 0; k < MAXPT; ++k) {
+            const int i = threadIdx.x + k * blockDim.x;
+            if (i < npl) {
+                const int y = i / g.nx, x = i - y * g.nx;
+                const C v = plane[y * g.lsx + x];
+                acc[k] += f * ((double)v.x * v.x + (double)v.y * v.y);
+            }
+        }
+        __syncthreads();
+    }
+    double* rz = rho + (size_t)z * npl;
+#pragma unroll
+    for (int k = 0; k < MAXPT; ++k) {
+        const int i = threadIdx.x + k * blockDim.x;
+        if (i < npl) atomicAdd(&rz[i], acc[k]);
+    }
+}
+
+// ------------------------------------------------------ full-grid axis FFT
+template <typename C, bool FWD>
+__global__ void __launch_bounds__(256)
+k_axis_fft(C* data, int nx, int ny, int nz, int axis, AxisPlan P, int lb) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = P.n;
+    const int ls = n | 1;
+    C* tw = reinterpret_cast<C*>(smem_raw);
+    C* lines = reinterpret_cast<C*>(smem_raw + align16<C>(n));
+    load_twiddles(tw, n);
+    // line-batch decomposition
+    size_t base;      // offset of element 0 of line 0 of the batch
+    size_t lstride;   // offset between consecutive lines of the batch
+    size_t estride;   // offset between consecutive elements of a line
+    int nl;
+    if (axis == 0) {
+        const int nlines = ny * nz;
+        const int l0 = blockIdx.x * lb;
+        nl = min(lb, nlines - l0);
+        base = (size_t)l0 * nx; lstride = nx; estride = 1;
+    } else {
+        const int nxb = (nx + lb - 1) / lb;
+        const int x0 = (blockIdx.x % nxb) * lb;
+        const int other = blockIdx.x / nxb;  // z for axis 1, y for axis 2
+        nl = min(lb, nx - x0);
+        lstride = 1;
+        if (axis == 1) { base = (size_t)other * nx * ny + x0; estride = nx; }
+        else { base = (size_t)other * nx + x0; estride = (size_t)nx * ny; }
+    }
+    for (int u = threadIdx.x; u < lb * n; u += blockDim.x) {
+        int l, j;
+        if (axis == 0) { l = u / n; j = u - l * n; }
+        else { j = u / lb; l = u - j * lb; }
+        lines[l * ls + j] = l < nl ? data[base + l * lstride + j * estride] : czero<C>();
+    }
+    __syncthreads();
+    if (FWD) fft_forward(lines, nl, LinesStrided{ls}, 1, P, tw);
+    else fft_inverse(lines, nl, LinesStrided{ls}, 1, P, tw);
+    for (int u = threadIdx.x; u < lb * n; u += blockDim.x) {
+        int l, j;
+        if (axis == 0) { l = u / n; j = u - l * n; }
+        else { j = u / lb; l = u - j * lb; }
+        if (l < nl) data[base + l * lstride + j * estride] = lines[l * ls + j];
+    }
+}
+
+// ------------------------------------------------------ potential kernels
+__device__ __forceinline__ void lda_pz(double rho, double& exc, double& vxc) {
+    // Perdew-Zunger 1981 parametrisation of Ceperley-Alder, unpolarised.
+    if (rho < 1e-30) { exc = 0.0; vxc = 0.0; return; }
+    const double rs = cbrt(3.0 / (4.0 * 3.14159265358979323846 * rho));
+    const double ex = -0.4581652932831429 / rs;
+    const double vx = 4.0 / 3.0 * ex;
+    double ec, vc;
+    if (rs >= 1.0) {
+        const double gm = -0.1423, b1 = 1.0529, b2 = 0.3334;
+        const double sr = sqrt(rs);
+        const double den = 1.0 + b1 * sr + b2 * rs;
+        ec = gm / den;
+        vc = ec * (1.0 + 7.0 / 6.0 * b1 * sr + 4.0 / 3.0 * b2 * rs) / den;
+    } else {
+        const double A = 0.0311, B = -0.048, Cc = 0.0020, D = -0.0116;
+        const double lr = log(rs);
+        ec = A * lr + B + Cc * rs * lr + D * rs;
+        vc = A * lr + (B - A / 3.0) + 2.0 / 3.0 * Cc * rs * lr + (2.0 * D - Cc) / 3.0 * rs;
+    }
+    exc = ex + ec;
+    vxc = vx + vc;
+}
+
+__global__ void k_real_to_complex(const double* r, double2* c, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        c[i] = make_double2(r[i], 0.0);
+}
+
+__global__ void k_take_real(const double2* c, double* r, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        r[i] = c[i].x;
+}
+
+__global__ void __launch_bounds__(256)
+k_hartree_gspace(double2* c, GridRecip gr, double omega, double* eh_acc) {
+    __shared__ double red[32];
+    const size_t n = (size_t)gr.nx * gr.ny * gr.nz;
+    const double inv_n = 1.0 / (double)n;
+    const double four_pi = 4.0 * 3.14159265358979323846;
+    double eh = 0.0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const int ix = (int)(i % gr.nx);
+        const int iy = (int)((i / gr.nx) % gr.ny);
+        const int iz = (int)(i / ((size_t)gr.nx * gr.ny));
+        int h = gr.idr_x[ix], k = gr.idr_y[iy], l = gr.idr_z[iz];
+        if (h >= (gr.nx + 1) / 2) h -= gr.nx;
+        if (k >= (gr.ny + 1) / 2) k -= gr.ny;
+        if (l >= (gr.nz + 1) / 2) l -= gr.nz;
+        const double gx = h * gr.b[0] + k * gr.b[3] + l * gr.b[6];
+        const double gy = h * gr.b[1] + k * gr.b[4] + l * gr.b[7];
+        const double gz = h * gr.b[2] + k * gr.b[5] + l * gr.b[8];
+        const double g2 = gx * gx + gy * gy + gz * gz;
+        if (h == 0 && k == 0 && l == 0) { c[i] = make_double2(0.0, 0.0); continue; }
+        const double2 rg = make_double2(c[i].x * inv_n, c[i].y * inv_n);
+        eh += 0.5 * omega * four_pi * (rg.x * rg.x + rg.y * rg.y) / g2;
+        c[i] = make_double2(four_pi * rg.x / g2, four_pi * rg.y / g2);
+    }
+    double s = block_sum(eh, red);
+    if (threadIdx.x == 0) atomicAdd(eh_acc, s);
+}
+
+__global__ void __launch_bounds__(256)
+k_assemble_veff(const double* vloc, const double2* vh, const double* rho, double* veff, size_t n,
+                double dv, double* exc_acc) {
+    __shared__ double red[32];
+    double e = 0.0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        double ex, vx;
+        const double r = rho[i];
+        lda_pz(r > 0.0 ? r : 0.0, ex, vx);
+        veff[i] = vloc[i] + vh[i].x + vx;
+        e += r * ex;
+    }
+    double s = block_sum(e, red);
+    if (threadIdx.x == 0 && exc_acc) atomicAdd(exc_acc, s * dv);
+}
+
+__global__ void __launch_bounds__(256)
+k_energy_terms(const double* rho_out, const double* veff, const double* vloc, size_t n, double dv,
+               double* exc_acc, double* dc_acc) {
+    __shared__ double red[32];
+    double e = 0.0, d = 0.0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        double ex, vx;
+        const double r = rho_out[i];
+        lda_pz(r > 0.0 ? r : 0.0, ex, vx);
+        e += r * ex;
+        d += (veff[i] - vloc[i]) * r;
+    }
+    double s = block_sum(e, red);
+    if (threadIdx.x == 0) atomicAdd(exc_acc, s * dv);
+    s = block_sum(d, red);
+    if (threadIdx.x == 0) atomicAdd(dc_acc, s * dv);
+}
+
+// Opt a kernel into more than 48 KB of dynamic shared memory (once per
+// kernel and size class).
+template <typename K> void allow_smem(K kernel, size_t bytes) {
+    if (bytes > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+int grid_for(size_t n, int threads) {
+    size_t b = (n + threads - 1) / threads;
+    return (int)(b < 148 * 8 ? b : 148 * 8);
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ launchers
+template <typename C>
+void launch_zsticks_inverse(const C* psi, int ldp, C* work, int nb, const HGeom& g,
+                            cudaStream_t st) {
+    count_launch();
+    dim3 grid((g.ncol + kColsPerBlock - 1) / kColsPerBlock, nb);
+    size_t sm = align16<C>(g.nz) + (size_t)kColsPerBlock * g.lsz * sizeof(C);
+    allow_smem(k_zsticks_inverse<C>, sm);
+    k_zsticks_inverse<C><<<grid, 256, sm, st>>>(psi, ldp, work, g);
+}
+
+size_t planes_smem_bytes(const HGeom& g, size_t csize) {
+    auto a16 = [](size_t b) { return (b + 15) & ~(size_t)15; };
+    return a16(g.nx * csize) + a16(g.ny * csize) + (size_t)g.ny * g.lsx * csize +
+           (size_t)g.nxact * sizeof(int);
+}
+
+template <typename C>
+void launch_planes_vloc(C* work, const double* veff, int nb, const HGeom& g, cudaStream_t st) {
+    count_launch();
+    dim3 grid(g.nz, nb);
+    size_t sm = planes_smem_bytes(g, sizeof(C));
+    allow_smem(k_planes_vloc<C>, sm);
+    k_planes_vloc<C><<<grid, 512, sm, st>>>(work, veff, g);
+}
+
+template <typename C>
+void launch_zsticks_forward(const C* work, const C* psi, int ldp, C* out, int ldo, int nb,
+                            const HGeom& g, const Epilogue& e, cudaStream_t st) {
+    count_launch();
+    dim3 grid((g.ncol + kColsPerBlock - 1) / kColsPerBlock, nb);
+    size_t sm = align16<C>(g.nz) + (size_t)kColsPerBlock * g.lsz * sizeof(C);
+    allow_smem(k_zsticks_forward<C, kEpiApply>, sm);
+    allow_smem(k_zsticks_forward<C, kEpiChebFirst>, sm);
+    allow_smem(k_zsticks_forward<C, kEpiCheb>, sm);
+    switch (e.mode) {
+    case kEpiApply: k_zsticks_forward<C, kEpiApply><<<grid, 256, sm, st>>>(work, psi, ldp, out, ldo, g, e); break;
+    case kEpiChebFirst: k_zsticks_forward<C, kEpiChebFirst><<<grid, 256, sm, st>>>(work, psi, ldp, out, ldo, g, e); break;
+    default: k_zsticks_forward<C, kEpiCheb><<<grid, 256, sm, st>>>(work, psi, ldp, out, ldo, g, e); break;
+    }
+}
+
+template <typename C>
+void launch_planes_density(const C* work, const double* occ, int nb, double scale, double* rho,
+                           const HGeom& g, cudaStream_t st) {
+    count_launch();
+    int groups = (2 * 148 + g.nz - 1) / g.nz;
+    if (groups > nb) groups = nb;
+    if (groups < 1) groups = 1;
+    const int bpg = (nb + groups - 1) / groups;
+    groups = (nb + bpg - 1) / bpg;
+    dim3 grid(g.nz, groups);
+    size_t sm = planes_smem_bytes(g, sizeof(C));
+    allow_smem(k_planes_density<C, 24>, sm);
+    k_planes_density<C, 24><<<grid, 512, sm, st>>>(work, occ, nb, bpg, scale, rho, g);
+}
+
+template <typename C>
+void launch_axis_fft(C* data, int nx, int ny, int nz, int axis, bool forward, const AxisPlan& P,
+                     cudaStream_t st) {
+    count_launch();
+    const int lb = 16;
+    int blocks;
+    if (axis == 0) blocks = (ny * nz + lb - 1) / lb;
+    else blocks = ((nx + lb - 1) / lb) * (axis == 1 ? nz : ny);
+    size_t sm = align16<C>(P.n) + (size_t)lb * (P.n | 1) * sizeof(C);
+    allow_smem(k_axis_fft<C, true>, sm);
+    allow_smem(k_axis_fft<C, false>, sm);
+    if (forward) k_axis_fft<C, true><<<blocks, 256, sm, st>>>(data, nx, ny, nz, axis, P, lb);
+    else k_axis_fft<C, false><<<blocks, 256, sm, st>>>(data, nx, ny, nz, axis, P, lb);
+}
+
+void launch_real_to_complex(const double* r, double2* c, size_t n, cudaStream_t st) {
+    count_launch();
+    k_real_to_complex<<<grid_for(n, 256), 256, 0, st>>>(r, c, n);
+}
+void launch_take_real(const double2* c, double* r, size_t n, cudaStream_t st) {
+    count_launch();
+    k_take_real<<<grid_for(n, 256), 256, 0, st>>>(c, r, n);
+}
+void launch_hartree_gspace(double2* c, const GridRecip& gr, double omega, double* eh_acc,
+                           cudaStream_t st) {
+    count_launch();
+    size_t n = (size_t)gr.nx * gr.ny * gr.nz;
+    k_hartree_gspace<<<grid_for(n, 256), 256, 0, st>>>(c, gr, omega, eh_acc);
+}
+void launch_assemble_veff(const double* vloc, const double2* vh, const double* rho, double* veff,
+                          size_t n, double dv, double* exc_acc, cudaStream_t st) {
+    count_launch();
+    k_assemble_veff<<<grid_for(n, 256), 256, 0, st>>>(vloc, vh, rho, veff, n, dv, exc_acc);
+}
+void launch_energy_terms(const double* rho_out, const double* veff, const double* vloc, size_t n,
+                         double dv, double* exc_acc, double* dc_acc, cudaStream_t st) {
+    count_launch();
+    k_energy_terms<<<grid_for(n, 256), 256, 0, st>>>(rho_out, veff, vloc, n, dv, exc_acc, dc_acc);
+}
+
+#define CHFSI_INST(C)                                                                        \
+    template void launch_zsticks_inverse<C>(const C*, int, C*, int, const HGeom&, cudaStream_t); \
+    template void launch_planes_vloc<C>(C*, const double*, int, const HGeom&, cudaStream_t);     \
+    template void launch_zsticks_forward<C>(const C*, const C*, int, C*, int, int, const HGeom&, \
+                                            const Epilogue&, cudaStream_t);                      \
+    template void launch_planes_density<C>(const C*, const double*, int, double, double*,        \
+                                           const HGeom&, cudaStream_t);                          \
+    template void launch_axis_fft<C>(C*, int, int, int, int, bool, const AxisPlan&, cudaStream_t);
+CHFSI_INST(double2)
+CHFSI_INST(float2)
+#undef CHFSI_INST
+
+}  // namespace chfsi

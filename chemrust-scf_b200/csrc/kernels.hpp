@@ -1,0 +1,85 @@
+// Launch interfaces of the device kernels (host side).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+
+#include "fft_engine.cuh"
+
+namespace chfsi {
+
+// Geometry of the pruned plane-wave <-> grid transforms.
+struct HGeom {
+    int nx, ny, nz;
+    int n_pw, ncol;
+    int lsz;     // smem line stride of z-sticks (odd)
+    int lsx;     // smem row stride of an xy plane (odd)
+    int nxact;   // x positions (digit-reversed) that carry columns
+    const int* col_start;  // ncol + 1: plane-wave range per column
+    const int* col_pos;    // ncol: py * lsx + px, digit-reversed plane offset
+    const int* pw_col;     // n_pw: column of each plane wave
+    const int* pw_zpos;    // n_pw: digit-reversed z position
+    const int* xact;       // nxact: digit-reversed x positions
+    AxisPlan ax, ay, az;
+};
+
+// Pass-3 epilogue: what to do with (H psi)_g once it is assembled.
+enum EpiMode { kEpiApply = 0, kEpiChebFirst = 1, kEpiCheb = 2 };
+
+struct Epilogue {
+    int mode;
+    const double* kin;     // n_pw
+    const double* coef;    // device: [.., .., c, e, 1/e, -c/e]
+    const void* nl;        // non-local contribution (same type as psi), ld n_pw; may be null
+    double* norm_acc;      // += sum |out|^2 (may be null)
+    double inv_n;          // 1 / N^3
+};
+
+constexpr int kColsPerBlock = 32;
+// density accumulation keeps 24 plane points per thread x 512 threads
+constexpr size_t kDensityPlanePoints = 24 * 512;
+
+// psi (nb x n_pw, ld ldp) -> work (nb x nz x ncol): scatter + inverse z.
+template <typename C>
+void launch_zsticks_inverse(const C* psi, int ldp, C* work, int nb, const HGeom& g,
+                            cudaStream_t st);
+// work planes: inverse y, inverse x, x V(r), forward x, forward y (in place).
+template <typename C>
+void launch_planes_vloc(C* work, const double* veff, int nb, const HGeom& g, cudaStream_t st);
+// work -> out: forward z + gather + kinetic + non-local + epilogue.
+template <typename C>
+void launch_zsticks_forward(const C* work, const C* psi, int ldp, C* out, int ldo, int nb,
+                            const HGeom& g, const Epilogue& e, cudaStream_t st);
+// density: rho[r] += sum_b occ[b] |psi_b(r)|^2 * scale from inverse-z work.
+template <typename C>
+void launch_planes_density(const C* work, const double* occ, int nb, double scale, double* rho,
+                           const HGeom& g, cudaStream_t st);
+size_t planes_smem_bytes(const HGeom& g, size_t csize);
+
+// Full-grid 1D transforms along one axis (0 = x, 1 = y, 2 = z) of a
+// complex grid [nz][ny][nx].
+template <typename C>
+void launch_axis_fft(C* data, int nx, int ny, int nz, int axis, bool forward, const AxisPlan& P,
+                     cudaStream_t st);
+
+// Potential helpers on the full grid.
+struct GridRecip {
+    int nx, ny, nz;
+    const int* idr_x; const int* idr_y; const int* idr_z;  // digit-reversed pos -> frequency
+    double b[9];       // reciprocal lattice rows b1, b2, b3
+};
+void launch_real_to_complex(const double* r, double2* c, size_t n, cudaStream_t st);
+// In G space (digit-reversed layout): c <- 4 pi c / (N^3 G^2), G = 0 -> 0;
+// eh_acc += 1/2 Omega 4 pi |c / N^3|^2 / G^2 (before scaling).
+void launch_hartree_gspace(double2* c, const GridRecip& gr, double omega, double* eh_acc,
+                           cudaStream_t st);
+// veff = vloc + Re(vh) + vxc(rho);  exc_acc += sum rho eps_xc * dv.
+void launch_assemble_veff(const double* vloc, const double2* vh, const double* rho, double* veff,
+                          size_t n, double dv, double* exc_acc, cudaStream_t st);
+// exc_acc += sum rho eps_xc(rho) dv;  dc_acc += sum (veff - vloc) rho_out dv
+void launch_energy_terms(const double* rho_out, const double* veff, const double* vloc, size_t n,
+                         double dv, double* exc_acc, double* dc_acc, cudaStream_t st);
+void launch_take_real(const double2* c, double* r, size_t n, cudaStream_t st);
+
+}  // namespace chfsi

@@ -1,0 +1,263 @@
+/*
+ * chfsi.h — C ABI of the B200 (sm_100a) Chebyshev-filtered subspace iteration
+ * (ChFSI) SCF path.
+ *
+ * The entry points replace, one for one, the crate-internal Rust contracts of
+ * the reference crate chemrust-scf (paths relative to that project):
+ *
+ *   chfsi_chebyshev_filter   src/eigensolver/chebyshev.rs:626-816  chebyshev_filter()
+ *   chfsi_rayleigh_ritz      src/eigensolver/rayleigh_ritz.rs:48-245 rayleigh_ritz()
+ *   chfsi_diagonalize        src/scf.rs:169-265  ScfIteration<_, VEffBuilt>::diagonalize()
+ *   chfsi_apply_h            src/eigensolver/chebyshev.rs:371-403 apply_full_hamiltonian()
+ *   chfsi_set_veff           src/scf.rs:188-195 (V_eff upload + min/max fold)
+ *   chfsi_set_basis          src/scf.rs:387-401 pw_coords_to_fft_indices()
+ *   chfsi_set_projectors     src/eigensolver/vnl_data.rs:25-89 VnlBatchData::precompute()
+ *   chfsi_construct_density  src/scf.rs:275-279 construct_density() (todo!() in the reference)
+ *   chfsi_build_veff         src/scf.rs:157-159 build_v_eff()       (todo!() in the reference)
+ *   (Pulay step of chfsi_scf_run) src/mixing.rs:24-27 DensityHistory::mix (todo!() there)
+ *   chfsi_scf_run            src/scf.rs:358-376 run_scf(); shape of the planned
+ *                            scf_run() C ABI (PROJECT_ROOT_PLAN.md:957-1018)
+ *   chfsi_create / _destroy  planned scf_context_create/_destroy (PROJECT_ROOT_PLAN.md:860-1029)
+ *
+ * Conventions (identical to the reference's):
+ *   - complex numbers are interleaved (re, im) doubles (CudaComplex = double2,
+ *     src/device/mod.rs:27);
+ *   - wavefunctions are band-major ("ColumnDistributed"): psi[b * n_pw + g]
+ *     (src/layout.rs:25-26, chebyshev.rs:104-106);
+ *   - the FFT grid is stored [ngz][ngy][ngx] with linear index
+ *     ix + ngx * (iy + ngy * iz); negative Miller indices wrap to n + h
+ *     (src/scf.rs:382-401);
+ *   - both FFT directions are unnormalised; H|psi> applies 1/N^3 at the gather
+ *     (chebyshev.rs:126-142, 654);
+ *   - eigenvalues are returned ascending (subspace_diag.rs:335-363).
+ *
+ * Ownership: a context owns all of its device memory and one CUDA stream.
+ * Calls on one context are not re-entrant.  Host arrays passed in are copied;
+ * device pointers passed to chfsi_apply_h stay owned by the caller.
+ * Errors are returned as chfsi_status (mirror of the crate's Error enum,
+ * src/types.rs:226-248); chfsi_last_error() gives the message.
+ */
+#ifndef CHFSI_H
+#define CHFSI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Status codes: mirror of src/types.rs:226-248 Error, plus the planned     */
+/* scf_run convention (0 converged, -1 not converged, < -1 error).          */
+/* ------------------------------------------------------------------------ */
+typedef enum chfsi_status {
+    CHFSI_OK                  = 0,
+    CHFSI_NOT_CONVERGED       = -1,  /* scf_run hit max iterations           */
+    CHFSI_ERR_NOT_IMPLEMENTED = -2,  /* Error::NotImplemented                */
+    CHFSI_ERR_CHEB_DIVERGED   = -3,  /* Error::ChebyshevDiverged             */
+    CHFSI_ERR_RR_FAILED       = -4,  /* Error::RayleighRitzFailed{info}      */
+    CHFSI_ERR_CUDA            = -5,  /* Error::Cuda                          */
+    CHFSI_ERR_BAD_INPUT       = -6,  /* shape / pointer / range violation    */
+    CHFSI_ERR_NO_DEVICE       = -7,  /* no CUDA device visible               */
+    CHFSI_ERR_OUT_OF_MEMORY   = -8,
+    CHFSI_ERR_NUMERIC         = -9   /* NaN/Inf detected on device           */
+} chfsi_status;
+
+typedef struct chfsi_c128 { double re, im; } chfsi_c128;
+
+/* Precision of the filter (the Rayleigh-Ritz eigensolve is always FP64). */
+enum { CHFSI_PREC_FP64 = 0, CHFSI_PREC_MIXED = 1 };
+/* Upper spectral bound used by the filter. */
+enum {
+    CHFSI_BOUND_HEURISTIC = 0, /* chebyshev.rs:225-254: 1/2 Gmax^2 + (maxV - minV) */
+    CHFSI_BOUND_LANCZOS   = 1  /* k-step Lanczos: lambda_max(T_k) + |f_k| (Zhou 2010) */
+};
+/* Density mixer. */
+enum { CHFSI_MIX_PULAY = 0, CHFSI_MIX_LINEAR = 1 };
+
+/* ------------------------------------------------------------------------ */
+/* Synthetic systems (the seeded inputs of the benchmark configurations).   */
+/* The reference obtains these from chemrust-hamiltonian-core (absent);     */
+/* here they come from analytic formulas, deterministic in the seed.        */
+/* ------------------------------------------------------------------------ */
+enum { CHFSI_LATTICE_DIAMOND = 0, CHFSI_LATTICE_SC = 1, CHFSI_LATTICE_BCC = 2 };
+
+typedef struct chfsi_synth_params {
+    int      lattice;        /* CHFSI_LATTICE_*                                   */
+    int      n_rep;          /* conventional cells per axis                       */
+    double   a_conv;         /* conventional cubic cell edge (bohr)               */
+    double   jitter;         /* uniform +-jitter per Cartesian component (bohr)   */
+    double   z_val;          /* valence charge per atom                           */
+    double   rc_loc;         /* V_loc(G) = -4 pi Z/(Omega G^2) exp(-G^2 rc^2/4)   */
+    double   ecut;           /* plane-wave cutoff (Ha): 1/2 |G+k|^2 <= ecut        */
+    int      ngrid[3];       /* FFT grid; 0 = smallest 2,3,5-smooth >= 4 m + 1     */
+    int      n_bands;        /* 0 = 1.25 x occupied, rounded up                   */
+    int      n_shell;        /* radial projector shells per atom (0: local only)  */
+    double   rc_proj[4];     /* beta_l(r) = r^l exp(-r^2/rc^2) per shell           */
+    int      lmax;           /* projectors for l = 0..lmax (lmax <= 1)            */
+    double   d_min, d_max;   /* D_ll ~ U[d_min, d_max] (Ha) per atom, shell, l    */
+    int      uspp;           /* 1: augmentation charges q_ij (S = 1 + b q b^H)    */
+    double   q_width;        /* Gaussian width of Q_ij(r) (bohr)                  */
+    double   q_amp;          /* A_ij ~ U[-q_amp, q_amp]                           */
+    double   kpt[3];         /* k in reduced (fractional) coordinates             */
+    uint64_t seed;
+} chfsi_synth_params;
+
+typedef struct chfsi_system chfsi_system;
+
+typedef struct chfsi_system_info {
+    int    ngrid[3];
+    int    n_pw;
+    int    n_bands;
+    int    n_occ;           /* bands with occupation 2                          */
+    int    n_atoms;
+    int    n_proj;          /* total projectors over all atoms                  */
+    int    n_ions_with_proj;
+    int    n_columns;       /* (x,y) columns that hold plane waves              */
+    double omega;           /* cell volume (bohr^3)                             */
+    double n_elec;
+    double gmax;            /* max |G+k| over the plane-wave sphere             */
+    double e_ewald;         /* ion-ion energy of point charges (Ha)             */
+    double lattice[9];      /* rows a1, a2, a3 (bohr)                           */
+} chfsi_system_info;
+
+chfsi_status chfsi_synth_defaults(int config_index, chfsi_synth_params* out);
+chfsi_status chfsi_system_generate(const chfsi_synth_params* p, chfsi_system** out);
+void         chfsi_system_destroy(chfsi_system* s);
+chfsi_status chfsi_system_get_info(const chfsi_system* s, chfsi_system_info* out);
+/* Miller indices (n_pw x 3), sorted by (iy, ix) column then iz. */
+chfsi_status chfsi_system_get_miller(const chfsi_system* s, int32_t* out);
+/* 1/2 |G+k|^2 per plane wave (n_pw). */
+chfsi_status chfsi_system_get_kinetic(const chfsi_system* s, double* out);
+/* V_loc(G) * S(G) on the full FFT grid (ngz*ngy*ngx, grid order). */
+chfsi_status chfsi_system_get_vloc_g(const chfsi_system* s, chfsi_c128* out);
+/* Projectors beta_p(G+k), row-major (n_proj x n_pw), grouped by ion. */
+chfsi_status chfsi_system_get_beta(const chfsi_system* s, chfsi_c128* out);
+/* proj_offsets[n_ions_with_proj + 1]: first projector of each ion. */
+chfsi_status chfsi_system_get_proj_offsets(const chfsi_system* s, int32_t* out);
+/* Per-ion D blocks (ne_i x ne_i, row-major), concatenated over ions. */
+chfsi_status chfsi_system_get_dmat(const chfsi_system* s, chfsi_c128* out);
+/* Per-ion q blocks (same layout as D); zero when the system is not USPP. */
+chfsi_status chfsi_system_get_qmat(const chfsi_system* s, chfsi_c128* out);
+/* Initial wavefunctions: complex Gaussian, band-major (n_bands x n_pw). */
+chfsi_status chfsi_system_get_psi0(const chfsi_system* s, chfsi_c128* out);
+/* Occupations (n_bands). */
+chfsi_status chfsi_system_get_occupations(const chfsi_system* s, double* out);
+/* Atom positions (n_atoms x 3, Cartesian bohr). */
+chfsi_status chfsi_system_get_positions(const chfsi_system* s, double* out);
+
+/* ------------------------------------------------------------------------ */
+/* Context (device state).                                                  */
+/* ------------------------------------------------------------------------ */
+typedef struct chfsi_ctx chfsi_ctx;
+
+typedef struct chfsi_dims {
+    int ngrid[3];           /* ngx, ngy, ngz                                    */
+    int n_pw;
+    int n_bands;
+    int n_proj;             /* 0: local Hamiltonian only                        */
+    int n_ions;             /* ions carrying projectors                         */
+} chfsi_dims;
+
+typedef struct chfsi_config {
+    int    device;          /* CUDA ordinal                                     */
+    int    precision;       /* CHFSI_PREC_*                                     */
+    int    bound_mode;      /* CHFSI_BOUND_*                                    */
+    int    lanczos_steps;   /* k for CHFSI_BOUND_LANCZOS (default 10)          */
+    int    check_norms;     /* 1: 10x norm-growth guard (chebyshev.rs:552-563) */
+    int    reserved[3];
+} chfsi_config;
+
+chfsi_status chfsi_default_config(chfsi_config* out);
+chfsi_status chfsi_create(const chfsi_dims* dims, const chfsi_config* cfg, chfsi_ctx** out);
+void         chfsi_destroy(chfsi_ctx* ctx);
+const char*  chfsi_last_error(const chfsi_ctx* ctx);
+/* Convenience: create a context and upload every array of a synthetic system. */
+chfsi_status chfsi_create_from_system(const chfsi_system* s, const chfsi_config* cfg,
+                                      chfsi_ctx** out);
+
+chfsi_status chfsi_set_basis(chfsi_ctx* ctx, const int32_t* miller, const double* kinetic,
+                             double gmax);
+chfsi_status chfsi_set_projectors(chfsi_ctx* ctx, const chfsi_c128* beta,
+                                  const int32_t* proj_offsets, const chfsi_c128* dmat);
+chfsi_status chfsi_set_veff(chfsi_ctx* ctx, const double* veff);
+chfsi_status chfsi_set_psi(chfsi_ctx* ctx, const chfsi_c128* psi);
+chfsi_status chfsi_get_psi(chfsi_ctx* ctx, chfsi_c128* psi);
+/* H|psi> for nb bands; psi_dev/hpsi_dev are DEVICE pointers in the
+ * context's plane-wave order (the order given to chfsi_set_basis). */
+chfsi_status chfsi_apply_h(chfsi_ctx* ctx, const chfsi_c128* psi_dev, chfsi_c128* hpsi_dev,
+                           int nb);
+/* Chebyshev filter of the context's psi in place; leaves H|psi_filtered> on
+ * the device for chfsi_rayleigh_ritz.  eig_prev may be NULL (first SCF step). */
+chfsi_status chfsi_chebyshev_filter(chfsi_ctx* ctx, int ndeg, const double* eig_prev,
+                                    int n_eig);
+/* Rayleigh-Ritz on the filtered psi: psi <- psi V, eigenvalues ascending. */
+chfsi_status chfsi_rayleigh_ritz(chfsi_ctx* ctx, double* eig_out);
+/* Filter + Rayleigh-Ritz (one ChFSI iteration). */
+chfsi_status chfsi_diagonalize(chfsi_ctx* ctx, int ndeg, const double* eig_prev, int n_eig,
+                               double* eig_out);
+/* Spectral bounds used by the last filter: {lambda_max, eps_cut, center, half_width}. */
+chfsi_status chfsi_get_bounds(chfsi_ctx* ctx, double* out4);
+/* Frobenius norms |psi_k| per filter degree k = 0..ndeg of the last filter. */
+chfsi_status chfsi_get_filter_norms(chfsi_ctx* ctx, double* out, int n);
+
+/* Local part only, T + V_loc (apply_v_loc_hamiltonian, chebyshev.rs:279-365). */
+chfsi_status chfsi_apply_h_local(chfsi_ctx* ctx, const chfsi_c128* psi_dev,
+                                 chfsi_c128* hpsi_dev, int nb);
+
+/* Device pointer of the context's psi (n_bands x n_pw, context PW order). */
+chfsi_status chfsi_psi_device_ptr(chfsi_ctx* ctx, chfsi_c128** out);
+/* The context's CUDA stream (cudaStream_t), for event timing by the caller. */
+chfsi_status chfsi_get_stream(chfsi_ctx* ctx, void** out);
+/* Kernels launched by this library since load (all contexts). */
+long long    chfsi_launch_count(void);
+
+
+/* ------------------------------------------------------------------------ */
+/* SCF pieces: V_loc, cell, occupations, density, V_eff, full SCF loop.     */
+/* ------------------------------------------------------------------------ */
+/* V_loc(G) S(G) on the full grid (natural grid order), transformed to V_loc(r). */
+chfsi_status chfsi_set_vloc_g(chfsi_ctx* ctx, const chfsi_c128* vloc_g);
+chfsi_status chfsi_get_vloc(chfsi_ctx* ctx, double* out);
+chfsi_status chfsi_get_veff(chfsi_ctx* ctx, double* out);
+/* lattice rows a1, a2, a3 (bohr), ion-ion energy and atom count (for dE/atom). */
+chfsi_status chfsi_set_cell(chfsi_ctx* ctx, const double* lattice, double e_ewald, int n_atoms);
+chfsi_status chfsi_set_occupations(chfsi_ctx* ctx, const double* occ);
+/* rho(r) = sum_b f_b |psi_b(r)|^2 / Omega of the context's psi (construct_density). */
+chfsi_status chfsi_construct_density(chfsi_ctx* ctx, double* rho_out);
+/* V_eff = V_loc + V_H[rho] + V_xc^LDA-PZ[rho] (build_v_eff); e2 = {E_H, E_xc} or NULL. */
+chfsi_status chfsi_build_veff(chfsi_ctx* ctx, const double* rho, double* e2);
+/* Density of the last chfsi_construct_density / chfsi_scf_run step. */
+chfsi_status chfsi_get_density(chfsi_ctx* ctx, double* rho);
+
+typedef struct chfsi_scf_params {
+    int    ndeg;          /* Chebyshev degree                                   */
+    int    max_iter;      /* SCF iterations at most                             */
+    double tol_per_atom;  /* converged when |E_i - E_{i-1}| / n_atoms < tol (Ha) */
+    double alpha;         /* Pulay mixing parameter                             */
+    int    max_hist;      /* Pulay history length, 1..8 (1 = linear mixing)     */
+    int    first_passes;  /* filter + Rayleigh-Ritz passes in the first step    */
+    double kT;            /* Fermi-Dirac smearing (Ha); <= 0: fixed aufbau occupations */
+} chfsi_scf_params;
+
+typedef struct chfsi_scf_result {
+    int     status;       /* CHFSI_OK (converged), CHFSI_NOT_CONVERGED or error */
+    int     n_iter;
+    double  e_total;      /* free energy: sum f eps - int (V_H+V_xc)[in] rho_out
+                             + E_H + E_xc + E_ion-ion - kT S                    */
+    double  e_band, e_hartree, e_xc, e_dc, e_entropy, mu;
+    double  seconds;      /* device time of the whole loop                      */
+    double* energies;     /* caller array of max_iter entries, or NULL          */
+    double* eigenvalues;  /* caller array of n_bands entries, or NULL           */
+} chfsi_scf_result;
+
+/* Full SCF from a uniform density: build_v_eff -> diagonalize -> density ->
+ * energy -> check -> Pulay mix (run_scf, src/scf.rs:358-376).  Returns
+ * CHFSI_OK when converged, CHFSI_NOT_CONVERGED after max_iter. */
+chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p, chfsi_scf_result* r);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CHFSI_H */

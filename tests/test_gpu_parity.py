@@ -1,0 +1,189 @@
+"""Parity of the CUDA path (through the C ABI) against the CPU oracle.
+
+FP64 tolerances: H|psi> 1e-12 relative; filtered psi 1e-10 relative;
+eigenvalues and energies 1e-10 Ha (north-star bar for the plain FP64 method).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module")
+def sys0(chfsi):
+    return chfsi.SyntheticSystem(config_index=0)
+
+
+@pytest.fixture(scope="module")
+def sys1s(chfsi):
+    # config-1 physics (64 atoms, KB projectors) with fewer bands: fast parity case
+    return chfsi.SyntheticSystem(config_index=1, n_bands=132)
+
+
+def rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def gpu_apply(chfsi, ctx, psi):
+    x = torch.from_numpy(np.ascontiguousarray(psi)).cuda()
+    y = torch.empty_like(x)
+    ctx.apply_h(x.data_ptr(), y.data_ptr(), psi.shape[0])
+    torch.cuda.synchronize()
+    return y.cpu().numpy()
+
+
+@pytest.mark.parametrize("which", ["sys0", "sys1s"])
+def test_apply_h_parity(chfsi, oracle, which, request):
+    s = request.getfixturevalue(which)
+    ctx = chfsi.Context(s)
+    o = oracle.Oracle.from_system(s)
+    v = o.vloc_r() + 0.05 * np.sin(np.arange(s.ng) * 1e-3)
+    ctx.set_veff(v)
+    o.set_veff(v)
+    psi = s.psi0()[:8]
+    h_gpu = gpu_apply(chfsi, ctx, psi)
+    h_cpu = o.apply_h(psi)
+    assert rel(h_gpu, h_cpu) < 1e-12
+
+
+def test_vloc_parity(chfsi, oracle, sys0):
+    ctx = chfsi.Context(sys0)
+    o = oracle.Oracle.from_system(sys0)
+    np.testing.assert_allclose(ctx.get_vloc(), o.vloc_r(), atol=1e-12)
+
+
+def test_filter_parity(chfsi, oracle, sys0):
+    ctx = chfsi.Context(sys0)
+    o = oracle.Oracle.from_system(sys0)
+    v = o.vloc_r()
+    ctx.set_veff(v)
+    o.set_veff(v)
+    ctx.chebyshev_filter(12)
+    st, _ = o.chebyshev_filter(12)
+    assert st == 0
+    np.testing.assert_allclose(ctx.bounds(), o.bounds(), rtol=1e-13)
+    np.testing.assert_allclose(ctx.filter_norms(12), o.norms(), rtol=1e-11)
+    assert rel(ctx.get_psi(), o.get_psi()) < 1e-10
+
+
+@pytest.mark.parametrize("which,ndeg,passes", [("sys0", 12, 3), ("sys1s", 16, 2)])
+def test_diagonalize_eigenvalue_parity(chfsi, oracle, which, ndeg, passes, request):
+    s = request.getfixturevalue(which)
+    ctx = chfsi.Context(s)
+    o = oracle.Oracle.from_system(s)
+    v = o.vloc_r()
+    ctx.set_veff(v)
+    o.set_veff(v)
+    wg = wc = None
+    for _ in range(passes):
+        wg = ctx.diagonalize(ndeg, wg)
+        wc = o.diagonalize(ndeg, wc)
+        np.testing.assert_allclose(wg, wc, atol=1e-10, rtol=0)
+
+
+def test_golden_cfg0_first_iteration(chfsi, sys0):
+    g = json.load(open(os.path.join(ROOT, "tests", "golden", "cfg0_oracle.json")))
+    ctx = chfsi.Context(sys0)
+    ctx.set_veff(ctx.get_vloc())
+    w = ctx.diagonalize(12)
+    np.testing.assert_allclose(w, g["eig_iter1"], atol=1e-10, rtol=0)
+    for _ in range(2):
+        w = ctx.diagonalize(12, w)
+    np.testing.assert_allclose(w, g["eig_iter3"], atol=1e-10, rtol=0)
+
+
+def test_density_and_veff_parity(chfsi, oracle, sys0):
+    ctx = chfsi.Context(sys0)
+    o = oracle.Oracle.from_system(sys0)
+    v = o.vloc_r()
+    ctx.set_veff(v)
+    o.set_veff(v)
+    w = ctx.diagonalize(12)
+    o.diagonalize(12)
+    ctx.set_occupations(sys0.occupations())
+    rg = ctx.construct_density()
+    rc = o.density()
+    assert rel(rg, rc) < 1e-11
+    assert abs(rg.sum() * sys0.omega / sys0.ng - 32.0) < 1e-9
+    ctx.build_v_eff(rc)
+    o.build_veff(rc)
+    np.testing.assert_allclose(ctx.get_veff(), o.get_veff(), atol=1e-11)
+
+
+def test_scf_energy_parity(chfsi, oracle, sys0):
+    ctx = chfsi.Context(sys0)
+    o = oracle.Oracle.from_system(sys0)
+    rg = ctx.run_scf(12, max_iter=6, kT=0.01)
+    rc = o.run_scf(12, max_iter=6, kT=0.01)
+    np.testing.assert_allclose(rg["energies"], rc["energies"], atol=1e-9, rtol=0)
+    np.testing.assert_allclose(rg["eigenvalues"], rc["eigenvalues"], atol=1e-9, rtol=0)
+
+
+def test_scf_converges_cfg0(chfsi, oracle, sys0):
+    g = json.load(open(os.path.join(ROOT, "tests", "golden", "cfg0_oracle.json")))
+    ctx = chfsi.Context(sys0)
+    r = ctx.run_scf(12, max_iter=40, kT=0.01)
+    assert r["converged"]
+    np.testing.assert_allclose(r["energies"][:3], g["scf_energies_3"], atol=1e-9)
+
+
+def test_lanczos_bound_parity(chfsi, oracle, sys1s):
+    ctx = chfsi.Context(sys1s, bound_mode=chfsi.BOUND_LANCZOS, lanczos_steps=10)
+    o = oracle.Oracle.from_system(sys1s)
+    o.set_bound_mode(1, 10)
+    v = o.vloc_r()
+    ctx.set_veff(v)
+    o.set_veff(v)
+    ctx.chebyshev_filter(4)
+    o.chebyshev_filter(4)
+    np.testing.assert_allclose(ctx.bounds(), o.bounds(), rtol=1e-10)
+
+
+def test_shuffled_plane_wave_order(chfsi, oracle, sys0):
+    """The boundary accepts any plane-wave order (pw_coords_to_fft_indices)."""
+    rng = np.random.default_rng(5)
+    perm = rng.permutation(sys0.n_pw)
+    mil = sys0.miller()[perm]
+    kin = sys0.kinetic()[perm]
+    psi = sys0.psi0()[:, perm]
+    ctx = chfsi.Context(dims={"ngrid": sys0.ngrid, "n_pw": sys0.n_pw, "n_bands": sys0.n_bands})
+    ctx.set_basis(mil, kin, sys0.gmax)
+    ref = chfsi.Context(sys0)
+    v = ref.get_vloc()
+    ctx.set_veff(v)
+    ref.set_veff(v)
+    ctx.set_psi(psi)
+    np.testing.assert_array_equal(ctx.get_psi(), psi)
+    w1 = ctx.diagonalize(12)
+    w2 = ref.diagonalize(12)
+    np.testing.assert_allclose(w1, w2, atol=1e-10)
+
+
+def test_rr_failure_is_reported(chfsi, sys0):
+    ctx = chfsi.Context(sys0)
+    ctx.set_veff(ctx.get_vloc())
+    psi = sys0.psi0()
+    psi[1] = psi[0]  # rank-deficient subspace -> S_sub not positive definite
+    ctx.set_psi(psi)
+    with pytest.raises(chfsi.RayleighRitzFailed):
+        ctx.diagonalize(0)
+
+
+def test_norm_guard_reports_divergence(chfsi, sys0):
+    """chebyshev.rs:552-563: growth > 10x between degrees is ChebyshevDiverged.
+
+    Previous eigenvalues far above the spectrum push the cut to 0.95 lambda_max
+    (chebyshev.rs:243-249), so the whole occupied spectrum sits far below the
+    filter interval and |psi_k| grows by ~2|sigma| per degree.
+    """
+    ctx = chfsi.Context(sys0)
+    ctx.set_veff(ctx.get_vloc())
+    with pytest.raises(chfsi.ChebyshevDiverged):
+        ctx.chebyshev_filter(6, eigenvalues=np.linspace(0.0, 1e4, sys0.n_bands))

@@ -1,0 +1,214 @@
+"""Pins the CPU oracle to the reference's known-answer tests and to independent
+numpy / scipy restatements (no GPU needed)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+GOLD = os.path.join(ROOT, "tests", "golden")
+
+
+def ka():
+    return json.load(open(os.path.join(GOLD, "reference_known_answers.json")))
+
+
+def test_rr_4x4_known_eigenvalues(oracle):
+    # subspace_diag.rs:535-590 (generalised RR via Cholesky reduction)
+    c = ka()["rr_4x4"]
+    w, v = oracle.hegv(np.diag(c["h_diag"]).astype(complex), np.diag(c["s_diag"]).astype(complex))
+    np.testing.assert_allclose(w, c["expected"], atol=c["tol"], rtol=0)
+    # eigenvectors are S-orthonormal
+    S = np.diag(c["s_diag"])
+    np.testing.assert_allclose(v.conj().T @ S @ v, np.eye(4), atol=1e-12)
+
+
+def test_zhegvd_known_eigenvalues(oracle):
+    # solver.rs:113-163
+    c = ka()["zhegvd_4x4"]
+    w, _ = oracle.hegv(np.diag(c["a_diag"]).astype(complex), np.eye(4, dtype=complex))
+    np.testing.assert_allclose(w, c["expected"], atol=c["tol"], rtol=0)
+
+
+def test_fft_forward_inverse_identity(oracle):
+    # fft.rs:239-281: 8^3, input[i] = (i, 2i) for i < 10, forward then inverse = N^3 x
+    c = ka()["fft_8cubed_identity"]
+    n = c["n"]
+    x = np.zeros(n[0] * n[1] * n[2], complex)
+    for i in range(c["nonzero"]):
+        x[i] = i + 2j * i
+    g = x.reshape(n[2], n[1], n[0])
+    y = oracle.fft3d(oracle.fft3d(g, -1), +1).ravel() / np.prod(n)
+    assert np.abs(y - x).max() < c["tol"]
+
+
+@pytest.mark.parametrize("shape", [(8, 8, 8), (40, 40, 40), (12, 10, 15), (9, 6, 5)])
+def test_fft_matches_numpy(oracle, shape):
+    rng = np.random.default_rng(3)
+    g = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    np.testing.assert_allclose(oracle.fft3d(g, -1), np.fft.fftn(g), atol=1e-9 * np.sqrt(g.size))
+    np.testing.assert_allclose(oracle.fft3d(g, +1), np.fft.ifftn(g) * g.size,
+                               atol=1e-9 * np.sqrt(g.size))
+
+
+def test_lcg_matches_reference_sequence():
+    c = ka()["lcg_seed42"]
+    s, out = 42, []
+    for _ in range(8):
+        s = (s * 25214903917 + 11) & 0xFFFFFFFFFFFF
+        out.append(s / 281474976710656.0)
+    np.testing.assert_array_equal(out, c["first8"])
+
+
+def lcg_matrix(seed, rows, cols):
+    s = seed
+    out = np.zeros((rows, cols), complex)
+    for i in range(rows):
+        for j in range(cols):
+            s = (s * 25214903917 + 11) & 0xFFFFFFFFFFFF
+            re = s / 281474976710656.0 - 0.5
+            s = (s * 25214903917 + 11) & 0xFFFFFFFFFFFF
+            im = s / 281474976710656.0 - 0.5
+            out[i, j] = re + 1j * im
+    return out
+
+
+def test_hegv_matches_scipy(oracle):
+    scipy_linalg = pytest.importorskip("scipy.linalg")
+    psi = lcg_matrix(42, 12, 40)
+    hp = lcg_matrix(7, 40, 40)
+    hp = hp + hp.conj().T
+    H = psi.conj() @ hp @ psi.T
+    S = psi.conj() @ psi.T
+    w, v = oracle.hegv(H, S)
+    ws = scipy_linalg.eigh(H, S, eigvals_only=True)
+    np.testing.assert_allclose(w, ws, atol=1e-10 * np.abs(ws).max())
+    # S-orthonormality after rotation (subspace_diag.rs:681-865, < 1e-10)
+    np.testing.assert_allclose(v.conj().T @ S @ v, np.eye(12), atol=1e-10)
+    np.testing.assert_allclose(v.conj().T @ H @ v, np.diag(w), atol=1e-9)
+
+
+def test_hegv_rejects_indefinite_overlap(oracle):
+    with pytest.raises(RuntimeError):
+        oracle.hegv(np.eye(3, dtype=complex), np.diag([1.0, -1.0, 1.0]).astype(complex))
+
+
+def numpy_apply_h(s, o, psi, veff):
+    """Independent H|psi> with numpy FFTs (chebyshev.rs:279-365, 416-500)."""
+    nx, ny, nz = s.ngrid
+    mil = s.miller()
+    kin = s.kinetic()
+    out = np.empty_like(psi)
+    V = veff.reshape(nz, ny, nx)
+    for b in range(psi.shape[0]):
+        g = np.zeros((nz, ny, nx), complex)
+        g[mil[:, 2] % nz, mil[:, 1] % ny, mil[:, 0] % nx] = psi[b]
+        r = np.fft.ifftn(g) * g.size
+        back = np.fft.fftn(r * V)
+        out[b] = kin * psi[b] + back[mil[:, 2] % nz, mil[:, 1] % ny, mil[:, 0] % nx] / g.size
+    if s.n_proj:
+        beta = s.beta()
+        off = s.proj_offsets()
+        dm = s.dmat()
+        D = np.zeros((s.n_proj, s.n_proj), complex)
+        pos = 0
+        for i in range(len(off) - 1):
+            ne = off[i + 1] - off[i]
+            D[off[i]:off[i + 1], off[i]:off[i + 1]] = dm[pos:pos + ne * ne].reshape(ne, ne)
+            pos += ne * ne
+        out += (beta.T @ (D @ (beta.conj() @ psi.T))).T
+    return out
+
+
+def small_system(chfsi, cfg=1):
+    return chfsi.SyntheticSystem(config_index=cfg, n_rep=1, ecut=5.0, ngrid=[0, 0, 0], n_bands=20)
+
+
+@pytest.mark.parametrize("cfg", [0, 1])
+def test_oracle_apply_h_matches_numpy(chfsi, oracle, cfg):
+    s = small_system(chfsi, cfg)
+    o = oracle.Oracle.from_system(s)
+    v = o.vloc_r() + 0.1 * np.cos(np.arange(s.ng) * 0.001)
+    o.set_veff(v)
+    psi = s.psi0()
+    np.testing.assert_allclose(o.apply_h(psi), numpy_apply_h(s, o, psi, v), atol=1e-11)
+
+
+def test_vloc_r_is_inverse_fft_of_vloc_g(chfsi, oracle, cfg0):
+    o = oracle.Oracle.from_system(cfg0)
+    nx, ny, nz = cfg0.ngrid
+    ref = (np.fft.ifftn(cfg0.vloc_g().reshape(nz, ny, nx)) * cfg0.ng).real.ravel()
+    np.testing.assert_allclose(o.vloc_r(), ref, atol=1e-12)
+
+
+def test_filter_matches_numpy_recurrence(chfsi, oracle):
+    s = small_system(chfsi, 1)
+    o = oracle.Oracle.from_system(s)
+    v = o.vloc_r()
+    o.set_veff(v)
+    psi = s.psi0()
+    st, _ = o.chebyshev_filter(6)
+    assert st == 0
+    lm, cut, c, e = o.bounds()
+    kin_max = 0.5 * s.gmax ** 2
+    assert lm == pytest.approx(kin_max + v.max() - v.min(), rel=1e-14)
+    assert cut == pytest.approx(lm / 3, rel=1e-14)
+    a = psi
+    h = numpy_apply_h(s, o, a, v)
+    b = h / e - c / e * a
+    for _ in range(2, 7):
+        h = numpy_apply_h(s, o, b, v)
+        a, b = b, 2 * (h / e - c / e * b) - a
+    scale = np.abs(b).max()
+    np.testing.assert_allclose(o.get_psi(), b, atol=1e-11 * scale)
+    np.testing.assert_allclose(o.get_hpsi(), numpy_apply_h(s, o, b, v), atol=1e-10 * scale)
+
+
+def test_rr_eigenvalues_match_dense_diagonalisation(chfsi, oracle):
+    """After enough filter passes the Ritz values equal the lowest eigenvalues of H."""
+    scipy_linalg = pytest.importorskip("scipy.linalg")
+    s = small_system(chfsi, 1)
+    o = oracle.Oracle.from_system(s)
+    v = o.vloc_r()
+    o.set_veff(v)
+    w = o.diagonalize(10)
+    for _ in range(25):
+        w = o.diagonalize(10, w)
+    Hd = numpy_apply_h(s, o, np.eye(s.n_pw, dtype=complex), v)  # rows = H e_g
+    Hd = Hd.T
+    ev = scipy_linalg.eigh(0.5 * (Hd + Hd.conj().T), eigvals_only=True)[: s.n_bands]
+    np.testing.assert_allclose(w[:16], ev[:16], atol=1e-8)
+
+
+def test_lanczos_bound_is_an_upper_bound(chfsi, oracle):
+    scipy_linalg = pytest.importorskip("scipy.linalg")
+    s = small_system(chfsi, 1)
+    o = oracle.Oracle.from_system(s)
+    v = o.vloc_r()
+    o.set_veff(v)
+    o.set_bound_mode(1, 10)
+    o.chebyshev_filter(2)
+    lm = o.bounds()[0]
+    Hd = numpy_apply_h(s, o, np.eye(s.n_pw, dtype=complex), v).T
+    emax = scipy_linalg.eigh(0.5 * (Hd + Hd.conj().T), eigvals_only=True)[-1]
+    assert emax <= lm <= emax * 1.5
+
+
+def test_fermi_occupations(oracle):
+    e = np.linspace(-1, 1, 21)
+    f, ts = oracle.fermi(e, 16.0, 0.01)
+    assert abs(f.sum() - 16.0) < 1e-10 and np.all(np.diff(f) <= 0)
+    assert ts <= 0
+    f0, ts0 = oracle.fermi(e, 16.0, 0.0)
+    assert np.all(f0[:8] == 2) and np.all(f0[8:] == 0) and ts0 == 0
+
+
+def test_cfg0_golden_regression(chfsi, oracle, cfg0):
+    g = json.load(open(os.path.join(GOLD, "cfg0_oracle.json")))
+    o = oracle.Oracle.from_system(cfg0)
+    o.set_veff(o.vloc_r())
+    w = o.diagonalize(12)
+    np.testing.assert_allclose(w, g["eig_iter1"], atol=1e-10)
+    np.testing.assert_allclose(o.bounds(), g["bounds_iter1"], rtol=1e-13)
