@@ -154,6 +154,8 @@ def lib():
         "chfsi_apply_h": [vp, vp, vp, C.c_int],
         "chfsi_apply_h_local": [vp, vp, vp, C.c_int],
         "chfsi_get_stream": [vp, C.POINTER(vp)],
+        "chfsi_zgemm_cn": [vp, C.c_int, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp],
+        "chfsi_zgemm_cn_bf16x3": [vp, C.c_int, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp],
         "chfsi_chebyshev_filter": [vp, C.c_int, dp, C.c_int],
         "chfsi_rayleigh_ritz": [vp, dp],
         "chfsi_diagonalize": [vp, C.c_int, dp, C.c_int, dp],
@@ -184,6 +186,18 @@ def lib():
     L.chfsi_last_error.restype = C.c_char_p
     _lib = L
     return L
+
+
+def zgemm_cn(a_dev, lda, b_dev, ldb, m, n, k, c_dev, stream=0):
+    """C[m][n] = sum_k conj(A[m][k]) B[n][k] on device pointers (blocks until done)."""
+    _check(lib().chfsi_zgemm_cn(C.c_void_p(a_dev), lda, C.c_void_p(b_dev), ldb, m, n, k,
+                                C.c_void_p(c_dev), C.c_void_p(stream)))
+
+
+def zgemm_cn_bf16x3(a_dev, lda, b_dev, ldb, m, n, k, c_dev, stream=0):
+    """Same product on tcgen05 tensor cores, BF16 3-way split, FP32 accumulation."""
+    _check(lib().chfsi_zgemm_cn_bf16x3(C.c_void_p(a_dev), lda, C.c_void_p(b_dev), ldb, m, n, k,
+                                       C.c_void_p(c_dev), C.c_void_p(stream)))
 
 
 def launch_count():

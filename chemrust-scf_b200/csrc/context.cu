@@ -14,6 +14,7 @@
 #include "chfsi.h"
 #include "dense.hpp"
 #include "gemm.hpp"
+#include "gemm_tc.hpp"
 #include "kernels.hpp"
 #include "launch_count.hpp"
 #include "system.hpp"
@@ -1238,5 +1239,71 @@ extern "C" chfsi_status chfsi_get_density(chfsi_ctx* ctx, double* rho) {
     cudaSetDevice(ctx->device);
     CK(cudaStreamSynchronize(ctx->st));
     CK(cudaMemcpy(rho, ctx->d_rho_out, sizeof(double) * ctx->ng, cudaMemcpyDeviceToHost));
+    return CHFSI_OK;
+}
+
+// C[m][n] = sum_k conj(A[m][k]) B[n][k] on device pointers (row-major,
+// leading dimensions lda, ldb; C dense m x n) — the op::C ZGEMM of the
+// reference's BlasHandle::gemm_c64 (src/device/blas.rs:79-102) as used for
+// beta^H psi and the subspace matrices.  Split-K partials go to stream-
+// ordered scratch (cudaMallocAsync / cudaFreeAsync on `stream`).
+extern "C" chfsi_status chfsi_zgemm_cn(const chfsi_c128* a_dev, int lda, const chfsi_c128* b_dev,
+                                       int ldb, int m, int n, int k, chfsi_c128* c_dev,
+                                       void* stream) {
+    if (!a_dev || !b_dev || !c_dev || m <= 0 || n <= 0 || k <= 0 || lda < k || ldb < k)
+        return CHFSI_ERR_BAD_INPUT;
+    cudaStream_t st = (cudaStream_t)stream;
+    double2* part = nullptr;
+    const size_t pe = splitk_partial_elems(m, n, k);
+    cudaError_t e = cudaMallocAsync((void**)&part, pe * sizeof(double2), st);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMallocAsync", __FILE__, __LINE__);
+    gemm_cn(reinterpret_cast<const double2*>(a_dev), lda, reinterpret_cast<const double2*>(b_dev),
+            ldb, m, n, k, part, reinterpret_cast<double2*>(c_dev), st);
+    e = cudaGetLastError();
+    cudaFreeAsync(part, st);
+    if (e != cudaSuccess) return cuda_fail(e, "gemm_cn", __FILE__, __LINE__);
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize", __FILE__, __LINE__);
+    return CHFSI_OK;
+}
+
+// Mixed-precision variant of chfsi_zgemm_cn: tcgen05 BF16 3-way split
+// products with FP32 accumulation (partials summed in FP64).  Plane and
+// partial scratch are stream-ordered allocations on `stream`.
+extern "C" chfsi_status chfsi_zgemm_cn_bf16x3(const chfsi_c128* a_dev, int lda,
+                                              const chfsi_c128* b_dev, int ldb, int m, int n,
+                                              int k, chfsi_c128* c_dev, void* stream) {
+    if (!a_dev || !b_dev || !c_dev || m <= 0 || n <= 0 || k <= 0 || lda < k || ldb < k)
+        return CHFSI_ERR_BAD_INPUT;
+    cudaStream_t st = (cudaStream_t)stream;
+    const int kp = tc_kpad(k);
+    TcPlanes pa, pb;
+    pa.rows_alloc = tc_rows_alloc(2 * m, true, n);
+    pb.rows_alloc = tc_rows_alloc(n, false, n);
+    const size_t na = (size_t)pa.rows_alloc * kp, nbe = (size_t)pb.rows_alloc * kp;
+    char* buf = nullptr;
+    const size_t part_f = tc_partial_floats(m, n, k);
+    const size_t bytes = 3 * (na + nbe) * 2 + part_f * 4 + 256;
+    cudaError_t e = cudaMallocAsync((void**)&buf, bytes, st);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMallocAsync", __FILE__, __LINE__);
+    cudaMemsetAsync(buf, 0, 3 * (na + nbe) * 2 + 256, st);
+    for (int i = 0; i < 3; ++i) {
+        pa.p[i] = buf + (size_t)i * na * 2;
+        pb.p[i] = buf + 3 * na * 2 + (size_t)i * nbe * 2;
+    }
+    int* err = (int*)(buf + 3 * (na + nbe) * 2);
+    float* part = (float*)(buf + 3 * (na + nbe) * 2 + 256);
+    tc_pack<double2>(reinterpret_cast<const double2*>(a_dev), lda, m, k, true, false, pa, st);
+    tc_pack<double2>(reinterpret_cast<const double2*>(b_dev), ldb, n, k, false, false, pb, st);
+    e = tc_gemm(pa, pb, m, n, k, kTcOutPartial, c_dev, n, part, err, st);
+    int herr = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaFreeAsync(buf, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(e, "tc_gemm", __FILE__, __LINE__);
+    if (herr) {
+        g_last_error = "tensor-core GEMM pipeline wait timed out";
+        return CHFSI_ERR_CUDA;
+    }
     return CHFSI_OK;
 }

@@ -1,0 +1,471 @@
+// tcgen05 (5th-generation tensor core) complex GEMM in BF16 3-way split
+// precision with FP32 accumulation in TMEM, operands fed by TMA.
+//
+// Complex product C[m][n] = sum_k conj(A[m][k]) B[n][k] as one real GEMM:
+//   A'' (2M x 2K): row 2m = (a_re, a_im) pairs, row 2m+1 = (-a_im, a_re) pairs
+//   B'  ( N x 2K): row n  = (b_re, b_im) pairs (the interleaved complex row)
+//   C''[2m][n] = Re C[m][n],  C''[2m+1][n] = Im C[m][n]
+// Each real operand x is split x = x1 + x2 + x3 (bf16, x2 = bf16(x - x1), ...)
+// and the six leading products (3,1) (2,2) (1,3) (2,1) (1,2) (1,1) are
+// accumulated into one TMEM tile (small terms first): relative error at the
+// FP32 level with BF16 tensor-core throughput.
+//
+// Kernel structure (one CTA per 128 x BN output tile and K range):
+//   warp 0 lane 0: TMA producer, 4-stage ring of {A 128x64, B BNx64} bf16
+//                  tiles with 128-byte swizzle, mbarrier complete_tx
+//   warp 1 lane 0: MMA issuer, 4 x tcgen05.mma (M128 x N BN x K16) per
+//                  stage, tcgen05.commit frees the stage
+//   all 4 warps  : epilogue, tcgen05.ld 32 lanes x 16 columns per step
+// Every wait is bounded; on timeout the kernel records the failure in an
+// error word and skips the remaining work instead of spinning forever.
+#include "gemm_tc.hpp"
+#include "launch_count.hpp"
+
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cudaTypedefs.h>
+
+#include <cstring>
+#include <mutex>
+
+namespace chfsi {
+
+namespace {
+
+constexpr int kBM = 128;
+constexpr int kBK = 64;          // one 128-byte swizzle atom of bf16
+constexpr int kStages = 4;
+constexpr int kThreads = 128;
+constexpr long long kSpinLimit = 1LL << 28;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+// Bounded parity wait; returns false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    const uint32_t a = smem_u32(bar);
+    for (long long i = 0; i < kSpinLimit; ++i) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* smem_dst, const CUtensorMap* map, uint64_t* bar,
+                                            int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%3, %4}], [%2];" ::"r"(smem_u32(smem_dst)),
+        "l"((uint64_t)map), "r"(smem_u32(bar)), "r"(x), "r"(y)
+        : "memory");
+}
+
+// K-major, 128-byte swizzled operand tile: rows of 64 bf16 (128 B), 8-row
+// groups 1024 B apart (SBO), start address advanced 32 B per K=16 step.
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)1 << 16;                 // leading byte offset (unused for SW128 K-major)
+    d |= (uint64_t)(1024 >> 4) << 32;        // stride byte offset
+    d |= (uint64_t)1 << 46;                  // descriptor version (sm_100)
+    d |= (uint64_t)2 << 61;                  // 128-byte swizzle
+    return d;
+}
+
+// kind::f16 instruction descriptor: BF16 x BF16 -> F32, K-major A and B.
+__host__ __device__ constexpr uint32_t idesc_bf16(int m, int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) |
+           ((uint32_t)(m >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc,
+                                          uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t* r) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+        "%12, %13, %14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+          "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+struct TcMaps {
+    CUtensorMap a[3];
+    CUtensorMap b[3];
+};
+
+// out modes
+enum { kOutPartialF32 = 0, kOutComplexF32 = 1, kOutComplexF64 = 2 };
+
+template <int MODE>
+__global__ void __launch_bounds__(kThreads, 1)
+k_umma_split3(const __grid_constant__ TcMaps maps, int M2, int N, int bn, int ktiles_total,
+              int ktiles_per_split, void* out, long long ldo, int* err) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    // 1024-byte aligned stage ring
+    unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    const int a_bytes = kBM * kBK * 2;
+    const int b_bytes = bn * kBK * 2;
+    unsigned char* sa = base;
+    unsigned char* sb = base + kStages * a_bytes;
+    uint64_t* full = (uint64_t*)(sb + kStages * b_bytes);
+    uint64_t* empty = full + kStages;
+    uint64_t* done = empty + kStages;
+    uint32_t* tmem_slot = (uint32_t*)(done + 1);
+    int* abort_flag = (int*)(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * bn;
+    const int kt0 = blockIdx.z * ktiles_per_split;
+    const int kt1 = min(ktiles_total, kt0 + ktiles_per_split);
+    const int nk = kt1 - kt0;
+    const int iters = 6 * (nk > 0 ? nk : 0);
+    // (a plane, b plane) pairs, smallest terms first
+    const int pa[6] = {2, 1, 0, 1, 0, 0};
+    const int pb[6] = {0, 1, 2, 0, 1, 0};
+    int ncols = 32;
+    while (ncols < bn) ncols <<= 1;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(done, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(tmem_slot)),
+                     "r"(ncols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0 && iters > 0) {
+        // ---- TMA producer
+        for (int it = 0; it < iters; ++it) {
+            const int s = it % kStages;
+            const uint32_t ph = (it / kStages) & 1;
+            if (it >= kStages && !mbar_wait(&empty[s], ph ^ 1)) {
+                atomicExch(err, 1);
+                *(volatile int*)abort_flag = 1;
+                break;
+            }
+            if (*(volatile int*)abort_flag) break;
+            const int t = it / nk, kk = it - t * nk;
+            const int kx = (kt0 + kk) * kBK;
+            mbar_expect_tx(&full[s], a_bytes + b_bytes);
+            tma_load_2d(sa + s * a_bytes, &maps.a[pa[t]], &full[s], kx, m0);
+            tma_load_2d(sb + s * b_bytes, &maps.b[pb[t]], &full[s], kx, n0);
+        }
+    } else if (warp == 1 && lane == 0 && iters > 0) {
+        // ---- MMA issuer
+        const uint32_t idesc = idesc_bf16(kBM, bn);
+        bool ok = true;
+        for (int it = 0; it < iters; ++it) {
+            const int s = it % kStages;
+            const uint32_t ph = (it / kStages) & 1;
+            if (!mbar_wait(&full[s], ph)) {
+                atomicExch(err, 2);
+                *(volatile int*)abort_flag = 1;
+                ok = false;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint64_t da = umma_desc_sw128(smem_u32(sa + s * a_bytes));
+            const uint64_t db = umma_desc_sw128(smem_u32(sb + s * b_bytes));
+#pragma unroll
+            for (int k = 0; k < kBK / 16; ++k)
+                umma_bf16(tmem, da + 2 * k, db + 2 * k, idesc, (it > 0 || k > 0) ? 1u : 0u);
+            umma_commit(&empty[s]);
+        }
+        (void)ok;
+        umma_commit(done);
+    }
+    __syncwarp();
+    // ---- epilogue: every warp reads its 32 TMEM lanes
+    bool have = iters > 0;
+    if (have) {
+        if (!mbar_wait(done, 0)) {
+            atomicExch(err, 3);
+            have = false;
+        }
+    }
+    have = __all_sync(0xffffffffu, have);  // tcgen05.ld is warp-collective
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const int row = m0 + warp * 32 + lane;
+    for (int c0 = 0; c0 < bn; c0 += 16) {
+        uint32_t r[16];
+        if (have) {
+            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, r);
+        } else {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) r[j] = 0u;
+        }
+        if (MODE == kOutPartialF32) {
+            float* o = (float*)out + (long long)blockIdx.z * ldo * M2;
+            if (row < M2) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const int col = n0 + c0 + j;
+                    if (col < N) o[(long long)row * ldo + col] = __uint_as_float(r[j]);
+                }
+            }
+        } else {
+            // rows 2m (real) and 2m+1 (imaginary) sit in adjacent lanes
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const float v = __uint_as_float(r[j]);
+                const float w = __shfl_down_sync(0xffffffffu, v, 1);
+                const int col = n0 + c0 + j;
+                if ((lane & 1) == 0 && row + 1 < M2 + 1 && row < M2 && col < N) {
+                    const long long m = row >> 1;
+                    if (MODE == kOutComplexF32)
+                        ((float2*)out)[m * ldo + col] = make_float2(v, w);
+                    else
+                        ((double2*)out)[m * ldo + col] = make_double2((double)v, (double)w);
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 1) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
+    }
+}
+
+// ---- operand packing: complex rows -> three bf16 planes (split 1 + 2 + 3)
+__device__ __forceinline__ void split3(float v, __nv_bfloat16& h1, __nv_bfloat16& h2,
+                                       __nv_bfloat16& h3) {
+    h1 = __float2bfloat16_rn(v);
+    const float r1 = v - __bfloat162float(h1);
+    h2 = __float2bfloat16_rn(r1);
+    const float r2 = r1 - __bfloat162float(h2);
+    h3 = __float2bfloat16_rn(r2);
+}
+
+template <typename CIn, bool DOUBLED, bool CONJ_T>
+__global__ void k_pack3(const CIn* __restrict__ x, long long ldx, int rows, int K, int kp,
+                        __nv_bfloat16* __restrict__ p0, __nv_bfloat16* __restrict__ p1,
+                        __nv_bfloat16* __restrict__ p2) {
+    // DOUBLED: output rows 2r, 2r+1 per input row (conj-first operand)
+    // CONJ_T:  input element (r, k) is read as conj(x[k][r]) (transposed source)
+    const long long kc = kp / 2;  // complex columns incl. padding
+    const long long tot = (long long)rows * kc;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(t / kc), k = (int)(t % kc);
+        float re = 0.f, im = 0.f;
+        if (k < K) {
+            if (CONJ_T) {
+                const CIn v = x[(long long)k * ldx + r];
+                re = (float)v.x;
+                im = -(float)v.y;
+            } else {
+                const CIn v = x[(long long)r * ldx + k];
+                re = (float)v.x;
+                im = (float)v.y;
+            }
+        }
+        __nv_bfloat16 a1, a2, a3, b1, b2, b3;
+        split3(re, a1, a2, a3);
+        split3(im, b1, b2, b3);
+        if (DOUBLED) {
+            const long long o0 = (2LL * r) * kp + 2 * k, o1 = (2LL * r + 1) * kp + 2 * k;
+            p0[o0] = a1; p0[o0 + 1] = b1; p1[o0] = a2; p1[o0 + 1] = b2; p2[o0] = a3; p2[o0 + 1] = b3;
+            const __nv_bfloat16 z = __float2bfloat16_rn(0.f);
+            // (-im, re)
+            p0[o1] = __hsub(z, b1); p0[o1 + 1] = a1;
+            p1[o1] = __hsub(z, b2); p1[o1 + 1] = a2;
+            p2[o1] = __hsub(z, b3); p2[o1 + 1] = a3;
+        } else {
+            const long long o = (long long)r * kp + 2 * k;
+            p0[o] = a1; p0[o + 1] = b1; p1[o] = a2; p1[o + 1] = b2; p2[o] = a3; p2[o + 1] = b3;
+        }
+    }
+}
+
+// sum of split-K partials -> complex (rows 2m, 2m+1 -> re, im), FP64 output
+__global__ void k_reduce_tc(const float* __restrict__ part, int splits, int M, int N,
+                            double2* __restrict__ out) {
+    const long long mn = (long long)M * N;
+    const long long stride = 2LL * M * N;  // one partial = (2M) x N
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < mn;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long m = t / N, n = t % N;
+        double re = 0.0, im = 0.0;
+        for (int s = 0; s < splits; ++s) {
+            re += part[s * stride + (2 * m) * N + n];
+            im += part[s * stride + (2 * m + 1) * N + n];
+        }
+        out[t] = make_double2(re, im);
+    }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    });
+    return fn;
+}
+
+bool make_map(CUtensorMap* m, const void* ptr, int rows, int kp, int box_rows) {
+    auto enc = get_encode();
+    if (!enc || rows < box_rows) return false;
+    cuuint64_t dims[2] = {(cuuint64_t)kp, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)kp * 2};
+    cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)box_rows};
+    cuuint32_t es[2] = {1, 1};
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr), dims, strides,
+                     box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+int pick_bn(int n) {
+    const int tiles = (n + 255) / 256;
+    int bn = (n + tiles - 1) / tiles;
+    bn = (bn + 15) / 16 * 16;
+    return bn < 16 ? 16 : (bn > 256 ? 256 : bn);
+}
+
+size_t smem_bytes(int bn) {
+    return 1024 + (size_t)kStages * (kBM * kBK * 2 + bn * kBK * 2) + (2 * kStages + 1) * 8 + 16;
+}
+
+int grid_for(long long n) {
+    long long b = (n + 255) / 256;
+    return (int)(b < 148 * 8 ? b : 148 * 8);
+}
+
+}  // namespace
+
+int tc_kpad(int K) { return ((2 * K + kBK - 1) / kBK) * kBK; }
+
+size_t tc_partial_floats(int M, int N, int K) {
+    const int kp = tc_kpad(K);
+    const int ktiles = kp / kBK;
+    const int mt = (2 * M + kBM - 1) / kBM, nt = (N + pick_bn(N) - 1) / pick_bn(N);
+    int splits = (148 + mt * nt - 1) / (mt * nt);
+    if (splits > ktiles) splits = ktiles;
+    if (splits < 1) splits = 1;
+    return (size_t)splits * 2 * M * N;
+}
+
+template <typename CIn>
+void tc_pack(const CIn* x, long long ldx, int rows, int K, bool doubled, bool conj_transposed,
+             TcPlanes& planes, cudaStream_t st) {
+    count_launch();
+    const int kp = tc_kpad(K);
+    __nv_bfloat16* p0 = (__nv_bfloat16*)planes.p[0];
+    __nv_bfloat16* p1 = (__nv_bfloat16*)planes.p[1];
+    __nv_bfloat16* p2 = (__nv_bfloat16*)planes.p[2];
+    const long long tot = (long long)rows * (kp / 2);
+    const int g = grid_for(tot);
+    if (doubled) {
+        if (conj_transposed) k_pack3<CIn, true, true><<<g, 256, 0, st>>>(x, ldx, rows, K, kp, p0, p1, p2);
+        else k_pack3<CIn, true, false><<<g, 256, 0, st>>>(x, ldx, rows, K, kp, p0, p1, p2);
+    } else {
+        if (conj_transposed) k_pack3<CIn, false, true><<<g, 256, 0, st>>>(x, ldx, rows, K, kp, p0, p1, p2);
+        else k_pack3<CIn, false, false><<<g, 256, 0, st>>>(x, ldx, rows, K, kp, p0, p1, p2);
+    }
+    planes.rows = doubled ? 2 * rows : rows;
+    planes.kp = kp;
+}
+
+int tc_rows_alloc(int rows, bool a_operand, int n_for_b) {
+    const int box = a_operand ? kBM : pick_bn(n_for_b);
+    return rows < box ? box : rows;
+}
+
+cudaError_t tc_gemm(const TcPlanes& a, const TcPlanes& b, int M, int N, int K, int out_mode,
+                    void* out, long long ldo, float* part, int* err, cudaStream_t st) {
+    if (a.kp != tc_kpad(K) || b.kp != a.kp || a.rows != 2 * M || b.rows != N)
+        return cudaErrorInvalidValue;
+    const int bn = pick_bn(N);
+    if (a.rows_alloc < kBM || b.rows_alloc < bn) return cudaErrorInvalidValue;
+    TcMaps maps;
+    for (int i = 0; i < 3; ++i) {
+        if (!make_map(&maps.a[i], a.p[i], a.rows_alloc, a.kp, kBM)) return cudaErrorInvalidValue;
+        if (!make_map(&maps.b[i], b.p[i], b.rows_alloc, b.kp, bn)) return cudaErrorInvalidValue;
+    }
+    const int ktiles = a.kp / kBK;
+    const int mt = (2 * M + kBM - 1) / kBM, nt = (N + bn - 1) / bn;
+    int splits = 1;
+    if (out_mode == kTcOutPartial) {
+        splits = (148 + mt * nt - 1) / (mt * nt);
+        if (splits > ktiles) splits = ktiles;
+        if (splits < 1) splits = 1;
+    }
+    const int kps = (ktiles + splits - 1) / splits;
+    splits = (ktiles + kps - 1) / kps;
+    dim3 grid(mt, nt, splits);
+    const size_t sm = smem_bytes(bn);
+    count_launch();
+    if (out_mode == kTcOutPartial) {
+        cudaFuncSetAttribute(k_umma_split3<kOutPartialF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_umma_split3<kOutPartialF32><<<grid, kThreads, sm, st>>>(maps, 2 * M, N, bn, ktiles, kps,
+                                                                  part, N, err);
+        count_launch();
+        k_reduce_tc<<<grid_for((long long)M * N), 256, 0, st>>>(part, splits, M, N, (double2*)out);
+    } else if (out_mode == kTcOutComplexF32) {
+        cudaFuncSetAttribute(k_umma_split3<kOutComplexF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_umma_split3<kOutComplexF32><<<grid, kThreads, sm, st>>>(maps, 2 * M, N, bn, ktiles, kps,
+                                                                  out, ldo, err);
+    } else {
+        cudaFuncSetAttribute(k_umma_split3<kOutComplexF64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_umma_split3<kOutComplexF64><<<grid, kThreads, sm, st>>>(maps, 2 * M, N, bn, ktiles, kps,
+                                                                  out, ldo, err);
+    }
+    return cudaGetLastError();
+}
+
+template void tc_pack<double2>(const double2*, long long, int, int, bool, bool, TcPlanes&, cudaStream_t);
+template void tc_pack<float2>(const float2*, long long, int, int, bool, bool, TcPlanes&, cudaStream_t);
+
+}  // namespace chfsi

@@ -213,6 +213,17 @@ chfsi_status chfsi_get_stream(chfsi_ctx* ctx, void** out);
 /* Kernels launched by this library since load (all contexts). */
 long long    chfsi_launch_count(void);
 
+/* C[m][n] = sum_k conj(A[m][k]) B[n][k] on DEVICE pointers (row-major; C is
+ * m x n dense), on `stream` (cudaStream_t, 0 = legacy default).  The op::C
+ * ZGEMM of BlasHandle::gemm_c64 (src/device/blas.rs:79-102) that forms
+ * beta^H psi, psi^H psi and psi^H H psi.  Blocks until done. */
+chfsi_status chfsi_zgemm_cn(const chfsi_c128* a_dev, int lda, const chfsi_c128* b_dev, int ldb,
+                            int m, int n, int k, chfsi_c128* c_dev, void* stream);
+/* Same product on the tcgen05 tensor cores in BF16 3-way split precision
+ * with FP32 accumulation (the mixed-precision projector / overlap GEMM). */
+chfsi_status chfsi_zgemm_cn_bf16x3(const chfsi_c128* a_dev, int lda, const chfsi_c128* b_dev,
+                                   int ldb, int m, int n, int k, chfsi_c128* c_dev, void* stream);
+
 
 /* ------------------------------------------------------------------------ */
 /* SCF pieces: V_loc, cell, occupations, density, V_eff, full SCF loop.     */
