@@ -156,6 +156,7 @@ def lib():
         "chfsi_get_stream": [vp, C.POINTER(vp)],
         "chfsi_zgemm_cn": [vp, C.c_int, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp],
         "chfsi_zgemm_cn_bf16x3": [vp, C.c_int, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp],
+        "chfsi_zgemm_cn_noalloc": [vp, C.c_int, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp],
         "chfsi_chebyshev_filter": [vp, C.c_int, dp, C.c_int],
         "chfsi_rayleigh_ritz": [vp, dp],
         "chfsi_diagonalize": [vp, C.c_int, dp, C.c_int, dp],
@@ -192,6 +193,12 @@ def zgemm_cn(a_dev, lda, b_dev, ldb, m, n, k, c_dev, stream=0):
     """C[m][n] = sum_k conj(A[m][k]) B[n][k] on device pointers (blocks until done)."""
     _check(lib().chfsi_zgemm_cn(C.c_void_p(a_dev), lda, C.c_void_p(b_dev), ldb, m, n, k,
                                 C.c_void_p(c_dev), C.c_void_p(stream)))
+
+
+def zgemm_cn_noalloc(a_dev, lda, b_dev, ldb, m, n, k, c_dev, stream=0):
+    """zgemm_cn without device allocation (static 4 MiB scratch; m * n <= 262144)."""
+    _check(lib().chfsi_zgemm_cn_noalloc(C.c_void_p(a_dev), lda, C.c_void_p(b_dev), ldb, m, n, k,
+                                        C.c_void_p(c_dev), C.c_void_p(stream)))
 
 
 def zgemm_cn_bf16x3(a_dev, lda, b_dev, ldb, m, n, k, c_dev, stream=0):

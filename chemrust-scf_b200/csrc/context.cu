@@ -127,6 +127,8 @@ template <typename T> cudaError_t dalloc(T** p, size_t n) {
 
 }  // namespace
 
+void set_last_error(const char* msg) { g_last_error = msg; }
+
 chfsi_status cuda_fail(cudaError_t e, const char* expr, const char* file, int line) {
     char buf[512];
     std::snprintf(buf, sizeof(buf), "CUDA error %s (%s) at %s:%d: %s", cudaGetErrorName(e),

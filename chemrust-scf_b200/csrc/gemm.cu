@@ -205,3 +205,26 @@ void gemm_tn(const double2* W, int ldw, const double2* X, int ldx, double2* O, i
 }
 
 }  // namespace chfsi
+
+namespace chfsi {
+
+// gemm_cn with the split count capped at max_splits (>= 1); partials need
+// min(splitk_count, max_splits) * M * N elements of `part`.
+void gemm_cn_capped(const double2* A, int lda, const double2* B, int ldb, int M, int N, int K,
+                    int max_splits, double2* part, double2* out, cudaStream_t st) {
+    count_launch(2);
+    int splits = splitk_count(M, N, K);
+    if (splits > max_splits) splits = max_splits;
+    if (splits < 1) splits = 1;
+    int kchunk = (K + splits - 1) / splits;
+    kchunk = (kchunk + BK - 1) / BK * BK;
+    const int used = (K + kchunk - 1) / kchunk;
+    dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN, used);
+    k_gemm_cn_splitk<<<grid, 256, 0, st>>>(A, lda, B, ldb, M, N, K, kchunk, part);
+    const size_t mn = (size_t)M * N;
+    int blocks = (int)((mn + 255) / 256);
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    k_reduce_partials<<<blocks, 256, 0, st>>>(part, used, mn, out);
+}
+
+}  // namespace chfsi

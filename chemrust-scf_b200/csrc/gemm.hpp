@@ -11,6 +11,9 @@ namespace chfsi {
 void gemm_cn(const double2* A, int lda, const double2* B, int ldb, int M, int N, int K,
              double2* part, double2* out, cudaStream_t st);
 int splitk_count(int M, int N, int K);
+// same product with at most max_splits K-splits (partials: splits * M * N elements)
+void gemm_cn_capped(const double2* A, int lda, const double2* B, int ldb, int M, int N, int K,
+                    int max_splits, double2* part, double2* out, cudaStream_t st);
 size_t splitk_partial_elems(int M, int N, int K);
 
 // O[m][n] = alpha sum_k W[k][m] X[k][n] + beta O[m][n]

@@ -219,6 +219,18 @@ long long    chfsi_launch_count(void);
  * beta^H psi, psi^H psi and psi^H H psi.  Blocks until done. */
 chfsi_status chfsi_zgemm_cn(const chfsi_c128* a_dev, int lda, const chfsi_c128* b_dev, int ldb,
                             int m, int n, int k, chfsi_c128* c_dev, void* stream);
+/* Same product with no device allocation, for callers that cannot call
+ * cudaMalloc (a host code that gives the whole GPU to its own memory pool, or
+ * a latency-critical caller for which cudaMalloc/cudaFree would synchronise
+ * the device).  No counterpart in the reference.  Split-K partials use one
+ * static device array of CHFSI_NOALLOC_SCRATCH_BYTES per GPU (held until the
+ * process exits); m * n must not exceed CHFSI_NOALLOC_SCRATCH_BYTES / 16
+ * (262144), otherwise CHFSI_ERR_BAD_INPUT.  The first call on a device sets
+ * up the array's device address (make it before any stream capture).  Calls
+ * share the array: calls that overlap on the GPU race.  Blocks until done. */
+#define CHFSI_NOALLOC_SCRATCH_BYTES (4u * 1024u * 1024u)
+chfsi_status chfsi_zgemm_cn_noalloc(const chfsi_c128* a_dev, int lda, const chfsi_c128* b_dev,
+                                    int ldb, int m, int n, int k, chfsi_c128* c_dev, void* stream);
 /* Same product on the tcgen05 tensor cores in BF16 3-way split precision
  * with FP32 accumulation (the mixed-precision projector / overlap GEMM). */
 chfsi_status chfsi_zgemm_cn_bf16x3(const chfsi_c128* a_dev, int lda, const chfsi_c128* b_dev,
