@@ -212,6 +212,52 @@ def run_ours(args):
            "d2h_bytes_per_step": psi_bytes + 8 * nb,
            "api": "chfsi_set_psi + chfsi_diagonalize + chfsi_get_psi (pinned host buffers)"}
 
+    # ---- mixed precision: FP32 filter, tcgen05 BF16x3 GEMMs, FP64 RR eigensolve
+    mixed = None
+    if not args.fp64_only:
+        mctx = chfsi.Context(s, device=local, precision=chfsi.PREC_MIXED)
+        mctx.build_v_eff(rho0)
+        mstream = torch.cuda.ExternalStream(mctx.stream(), device=local)
+        meig = mctx.diagonalize(NDEG)
+        for _ in range(args.warmup):
+            meig = mctx.diagonalize(NDEG, meig)
+        torch.cuda.synchronize()
+        m0 = torch.cuda.Event(enable_timing=True)
+        m1 = torch.cuda.Event(enable_timing=True)
+        m0.record(mstream)
+        for _ in range(args.steps):
+            meig = mctx.diagonalize(NDEG, meig)
+        m1.record(mstream)
+        m1.synchronize()
+        mms = m0.elapsed_time(m1)
+        if dist:
+            t = torch.tensor([mms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            mms = float(t.item())
+        mixed = {"value": round(applies_per_step * args.steps * world / (mms * 1e-3), 1),
+                 "unit": UNIT, "ms_per_step": round(mms / args.steps, 3),
+                 "dtype": "f32 filter, bf16x3 tcgen05 GEMMs (fp32 accumulate), f64 eigensolve"}
+        mctx.close()
+        if not args.no_scf:
+            res = {}
+            for name, prec in (("fp64", chfsi.PREC_FP64), ("mixed", chfsi.PREC_MIXED)):
+                sctx = chfsi.Context(s, device=local, precision=prec)
+                r = sctx.run_scf(NDEG, tol_per_atom=1e-6, max_iter=60, kT=0.01)
+                res[name] = r
+                sctx.close()
+            f, m = res["fp64"], res["mixed"]
+            mixed["time_to_scf"] = {
+                "criterion": "|dE| < 1e-6 Ha/atom (Fermi-Dirac kT = 0.01 Ha, Pulay 0.3/6)",
+                "fp64_s": round(f["seconds"], 4), "fp64_iterations": f["n_iter"],
+                "mixed_s": round(m["seconds"], 4), "mixed_iterations": m["n_iter"],
+                "mixed_iterations_in_mixed_precision": m["n_iter_mixed"],
+                "speedup": round(f["seconds"] / m["seconds"], 3) if m["seconds"] > 0 else None,
+                "converged": [bool(f["converged"]), bool(m["converged"])],
+                "energy_diff_per_atom_Ha": abs(f["e_total"] - m["e_total"]) / s.n_atoms,
+                "max_occupied_eigenvalue_diff_Ha":
+                    float(np.abs(f["eigenvalues"][:s.n_occ] - m["eigenvalues"][:s.n_occ]).max()),
+            }
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(s, seconds=args.cpu_seconds)
@@ -233,6 +279,7 @@ def run_ours(args):
             "gpu_launches": int(launches),
             "roofline": roofline,
             "cpu_baseline": cpu,
+            "mixed_precision": mixed,
         }
         print(json.dumps(line))
     if dist:
@@ -321,6 +368,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fp64-only", action="store_true", help="skip the mixed-precision lines")
+    ap.add_argument("--no-scf", action="store_true", help="skip the time-to-SCF comparison")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -106,11 +106,12 @@ class Config(C.Structure):
 class ScfParams(C.Structure):
     _fields_ = [("ndeg", C.c_int), ("max_iter", C.c_int), ("tol_per_atom", C.c_double),
                 ("alpha", C.c_double), ("max_hist", C.c_int), ("first_passes", C.c_int),
-                ("kT", C.c_double)]
+                ("kT", C.c_double), ("fp64_switch_per_atom", C.c_double)]
 
 
 class ScfResult(C.Structure):
-    _fields_ = [("status", C.c_int), ("n_iter", C.c_int), ("e_total", C.c_double),
+    _fields_ = [("status", C.c_int), ("n_iter", C.c_int), ("n_iter_mixed", C.c_int),
+                ("e_total", C.c_double),
                 ("e_band", C.c_double), ("e_hartree", C.c_double), ("e_xc", C.c_double),
                 ("e_dc", C.c_double), ("e_entropy", C.c_double), ("mu", C.c_double),
                 ("seconds", C.c_double),
@@ -149,6 +150,8 @@ def lib():
         "chfsi_set_basis": [vp, i32p, dp, C.c_double],
         "chfsi_set_projectors": [vp, vp, i32p, vp],
         "chfsi_set_veff": [vp, dp],
+        "chfsi_set_qmat": [vp, vp],
+        "chfsi_get_s_min": [vp, dp],
         "chfsi_set_psi": [vp, vp],
         "chfsi_get_psi": [vp, vp],
         "chfsi_apply_h": [vp, vp, vp, C.c_int],
@@ -358,6 +361,16 @@ class Context:
         d = np.ascontiguousarray(dmat, dtype=np.complex128)
         self._c(lib().chfsi_set_projectors(self.handle, _ptr(b), _ptr(o, C.c_int32), _ptr(d)))
 
+    def set_qmat(self, qmat):
+        """Ultrasoft overlap S = 1 + beta q beta^H (generalised problem)."""
+        q = np.ascontiguousarray(qmat, dtype=np.complex128)
+        self._c(lib().chfsi_set_qmat(self.handle, _ptr(q)))
+
+    def s_min(self):
+        v = C.c_double()
+        self._c(lib().chfsi_get_s_min(self.handle, C.byref(v)))
+        return v.value
+
     def set_veff(self, veff):
         v = np.ascontiguousarray(veff, dtype=np.float64).ravel()
         self._c(lib().chfsi_set_veff(self.handle, _ptr(v, C.c_double)))
@@ -465,8 +478,9 @@ class Context:
         return r
 
     def run_scf(self, ndeg, tol_per_atom=1e-6, max_iter=30, alpha=0.3, max_hist=6,
-                first_passes=4, kT=0.01, raise_not_converged=False):
-        p = ScfParams(ndeg, max_iter, tol_per_atom, alpha, max_hist, first_passes, kT)
+                first_passes=4, kT=0.01, fp64_switch_per_atom=1e-4, raise_not_converged=False):
+        p = ScfParams(ndeg, max_iter, tol_per_atom, alpha, max_hist, first_passes, kT,
+                      fp64_switch_per_atom)
         energies = np.zeros(max_iter)
         eigs = np.zeros(self.n_bands)
         r = ScfResult()
@@ -475,7 +489,8 @@ class Context:
         st = lib().chfsi_scf_run(self.handle, C.byref(p), C.byref(r))
         if st not in (OK, NOT_CONVERGED) or (st == NOT_CONVERGED and raise_not_converged):
             _check(st, self.handle)
-        return {"converged": st == OK, "n_iter": r.n_iter, "e_total": r.e_total,
+        return {"converged": st == OK, "n_iter": r.n_iter, "n_iter_mixed": r.n_iter_mixed,
+                "e_total": r.e_total,
                 "e_band": r.e_band, "e_hartree": r.e_hartree, "e_xc": r.e_xc, "e_dc": r.e_dc,
                 "e_entropy": r.e_entropy, "mu": r.mu,
                 "seconds": r.seconds, "energies": energies[:r.n_iter].copy(), "eigenvalues": eigs}

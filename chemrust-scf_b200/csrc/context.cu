@@ -15,12 +15,14 @@
 #include "dense.hpp"
 #include "gemm.hpp"
 #include "gemm_tc.hpp"
+#include "fft_plan.hpp"
 #include "kernels.hpp"
 #include "launch_count.hpp"
 #include "system.hpp"
 
 #include <algorithm>
 #include <cmath>
+#include <complex>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -32,6 +34,7 @@ namespace chfsi {
 std::atomic<long long> g_launch_count{0};
 
 chfsi_status cuda_fail(cudaError_t e, const char* expr, const char* file, int line);
+bool invert_complex(std::vector<std::complex<double>>& a, int n);
 
 namespace {
 
@@ -83,24 +86,76 @@ __global__ void k_fill(double* x, size_t n, double v) {
         x[i] = v;
 }
 
+__global__ void k_f64_to_f32(const double2* __restrict__ a, float2* __restrict__ b, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        b[i] = make_float2((float)a[i].x, (float)a[i].y);
+}
+__global__ void k_f32_to_f64(const float2* __restrict__ a, double2* __restrict__ b, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        b[i] = make_double2((double)a[i].x, (double)a[i].y);
+}
+__global__ void __launch_bounds__(256) k_sumsq32(const float2* __restrict__ x, size_t n, double* acc) {
+    __shared__ double red[8];
+    double s = 0.0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        s += (double)x[i].x * x[i].x + (double)x[i].y * x[i].y;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < 8; ++w) t += red[w];
+        atomicAdd(acc, t);
+    }
+}
+
+__global__ void k_conj(const double2* __restrict__ a, double2* __restrict__ b, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        b[i] = make_double2(a[i].x, -a[i].y);
+}
+
+// Chebyshev step of the generalised problem: y = S^-1 H x = hx - corr, then
+// the recurrence epilogue of the local pass (first degree / later degrees).
+__global__ void __launch_bounds__(256)
+k_cheb_combine(const double2* __restrict__ hx, const double2* __restrict__ corr,
+               const double2* __restrict__ x, double2* out, size_t n, const double* coef, int mode,
+               double* norm_acc) {
+    __shared__ double red[8];
+    const double ie = coef[4], nc = coef[5];
+    double acc = 0.0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const double2 h = make_double2(hx[i].x - corr[i].x, hx[i].y - corr[i].y);
+        const double2 p = x[i];
+        const double2 s = make_double2(h.x * ie + nc * p.x, h.y * ie + nc * p.y);
+        double2 o;
+        if (mode == 1) o = s;
+        else {
+            const double2 prev = out[i];
+            o = make_double2(2.0 * s.x - prev.x, 2.0 * s.y - prev.y);
+        }
+        out[i] = o;
+        acc += o.x * o.x + o.y * o.y;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0 && norm_acc) {
+        double t = 0.0;
+        for (int w = 0; w < 8; ++w) t += red[w];
+        atomicAdd(norm_acc, t);
+    }
+}
+
 int grid_for(size_t n) {
     size_t b = (n + 255) / 256;
     return (int)(b < 148 * 8 ? b : 148 * 8);
-}
-
-// Radices of an axis in DIF order: greedy 8, 4, 2, 3, 5.
-bool plan_axis(int n, AxisPlan& P) {
-    std::memset(&P, 0, sizeof(P));
-    P.n = n;
-    int m = n;
-    for (int r : {8, 4, 2, 3, 5}) {
-        while (m % r == 0) {
-            if (P.nst >= kMaxStages) return false;
-            P.r[P.nst++] = r;
-            m /= r;
-        }
-    }
-    return m == 1 && n >= 1;
 }
 
 // Position of frequency k after the in-place DIF (mixed-radix digit reversal).
@@ -192,6 +247,22 @@ struct chfsi_ctx {
     double* d_hist = nullptr;  // 2 * kPulayMax * ng
     double** d_hist_ptrs = nullptr;
     double* d_dots = nullptr;
+    // ultrasoft overlap S = 1 + beta q beta^H
+    bool uspp = false;
+    double s_min = 1.0;
+    double2* d_qmat = nullptr;   // per-ion q blocks (layout of D)
+    double2* d_sinvT = nullptr;  // M^T, M = q (1 + B q)^-1, S^-1 = 1 - beta M beta^H
+    double2* d_cq = nullptr;     // n_proj x n_bands scratch
+    double2* d_sx = nullptr;     // n_bands x n_pw scratch
+    // mixed precision (FP32 filter, tcgen05 BF16x3 GEMMs)
+    bool mixed = false;          // configured precision
+    bool mixed_active = false;   // current filter precision (SCF may switch to FP64)
+    float2* d_psi32a = nullptr; float2* d_psi32b = nullptr; float2* d_psi32 = nullptr;
+    float2* d_hpsi32 = nullptr; float2* d_nl32 = nullptr; float2* d_work32 = nullptr;
+    void* d_planes = nullptr;    // all bf16 plane storage
+    TcPlanes tp_beta_a, tp_betaT_b, tp_psi_b, tp_psi_a, tp_hpsi_b, tp_small_a, tp_psiT_b;
+    float* d_tc_part = nullptr; int* d_tc_err = nullptr;
+    bool beta_planes_ready = false;
     // pinned host scratch
     double* h_pin = nullptr; size_t h_pin_n = 0;
 
@@ -255,6 +326,28 @@ chfsi_status apply_h_dev(chfsi_ctx* ctx, const double2* psi, double2* out, int n
     return CHFSI_OK;
 }
 
+// One filter operator application: H x, or S^-1 H x for the generalised
+// (ultrasoft) problem, where S^-1 = 1 - beta M beta^H is applied to H x by
+// three GEMMs and the recurrence epilogue runs in k_cheb_combine.
+chfsi_status apply_op_dev(chfsi_ctx* ctx, const double2* x, double2* out, int nb, int mode,
+                          double* norm_acc) {
+    if (!ctx->uspp || mode == kEpiApply) return apply_h_dev(ctx, x, out, nb, mode, norm_acc);
+    chfsi_status s = apply_h_dev(ctx, x, ctx->d_hpsi, nb, kEpiApply, nullptr);
+    if (s) return s;
+    cudaStream_t st = ctx->st;
+    gemm_cn(ctx->d_beta, ctx->n_pw, ctx->d_hpsi, ctx->n_pw, ctx->np, nb, ctx->n_pw, ctx->d_part,
+            ctx->d_cp, st);
+    gemm_tn(ctx->d_sinvT, ctx->np, ctx->d_cp, nb, ctx->d_cq, nb, ctx->np, nb, ctx->np, 1.0, 0.0, st);
+    gemm_tn(ctx->d_cq, nb, ctx->d_beta, ctx->n_pw, ctx->d_sx, ctx->n_pw, nb, ctx->n_pw, ctx->np, 1.0,
+            0.0, st);
+    const size_t n = (size_t)nb * ctx->n_pw;
+    count_launch();
+    k_cheb_combine<<<grid_for(n), 256, 0, st>>>(ctx->d_hpsi, ctx->d_sx, x, out, n, ctx->d_coef,
+                                                 mode == kEpiChebFirst ? 1 : 2, norm_acc);
+    CK(cudaGetLastError());
+    return CHFSI_OK;
+}
+
 // ---------------------------------------------------------------- bounds
 chfsi_status lanczos_bound(chfsi_ctx* ctx) {
     const int k = std::max(2, std::min(ctx->cfg.lanczos_steps, 60));
@@ -274,7 +367,8 @@ chfsi_status lanczos_bound(chfsi_ctx* ctx) {
         lanczos_b(ctx->d_lz_f, ctx->d_lz_v, ctx->d_lz + j, n, ctx->d_lz + k + j, ctx->st);
         if (j < k - 1) lanczos_c(ctx->d_lz_f, ctx->d_lz_v, ctx->d_lz_v0, n, ctx->d_lz + k + j, ctx->st);
     }
-    bounds(ctx->kin_max, ctx->d_minmax, nullptr, 0, ctx->d_lz, k, ctx->d_coef, ctx->st);
+    bounds(ctx->kin_max, ctx->d_minmax, nullptr, 0, ctx->d_lz, k, 1.0 / ctx->s_min, ctx->d_coef,
+           ctx->st);
     CK(cudaGetLastError());
     return CHFSI_OK;
 }
@@ -285,9 +379,11 @@ chfsi_status compute_bounds(chfsi_ctx* ctx, const double* eig_dev, int n_eig) {
         if (s) return s;
         // the cut still comes from the previous eigenvalues
         const int k = std::max(2, std::min(ctx->cfg.lanczos_steps, 60));
-        bounds(ctx->kin_max, ctx->d_minmax, eig_dev, n_eig, ctx->d_lz, k, ctx->d_coef, ctx->st);
+        bounds(ctx->kin_max, ctx->d_minmax, eig_dev, n_eig, ctx->d_lz, k, 1.0 / ctx->s_min,
+               ctx->d_coef, ctx->st);
     } else {
-        bounds(ctx->kin_max, ctx->d_minmax, eig_dev, n_eig, nullptr, 0, ctx->d_coef, ctx->st);
+        bounds(ctx->kin_max, ctx->d_minmax, eig_dev, n_eig, nullptr, 0, 1.0 / ctx->s_min, ctx->d_coef,
+               ctx->st);
     }
     CK(cudaGetLastError());
     return CHFSI_OK;
@@ -304,12 +400,12 @@ chfsi_status filter_dev(chfsi_ctx* ctx, int ndeg, const double* eig_dev, int n_e
     double2* A = ctx->d_psi;   // psi_{k-2}
     double2* B = ctx->d_psi2;  // psi_{k-1}
     if (ndeg >= 1) {
-        s = apply_h_dev(ctx, A, B, ctx->nb, kEpiChebFirst, ctx->d_nsq + 1);
+        s = apply_op_dev(ctx, A, B, ctx->nb, kEpiChebFirst, ctx->d_nsq + 1);
         if (s) return s;
     }
     for (int k = 2; k <= ndeg; ++k) {
         // psi_k = 2 sigma(H) psi_{k-1} - psi_{k-2}, written over psi_{k-2}
-        s = apply_h_dev(ctx, B, A, ctx->nb, kEpiCheb, ctx->d_nsq + k);
+        s = apply_op_dev(ctx, B, A, ctx->nb, kEpiCheb, ctx->d_nsq + k);
         if (s) return s;
         std::swap(A, B);
     }
@@ -332,6 +428,17 @@ chfsi_status rr_dev(chfsi_ctx* ctx) {
     gemm_cn(ctx->d_psi, ctx->n_pw, ctx->d_hpsi, ctx->n_pw, n, n, ctx->n_pw, ctx->d_part, ctx->d_T1, st);
     symmetrize(ctx->d_T1, ctx->d_H, n, st);
     gemm_cn(ctx->d_psi, ctx->n_pw, ctx->d_psi, ctx->n_pw, n, n, ctx->n_pw, ctx->d_part, ctx->d_T1, st);
+    if (ctx->uspp) {
+        // S_sub = psi^H psi + C^H q C with C = beta^H psi
+        gemm_cn(ctx->d_beta, ctx->n_pw, ctx->d_psi, ctx->n_pw, ctx->np, n, ctx->n_pw, ctx->d_part,
+                ctx->d_cp, st);
+        count_launch();
+        k_apply_dmat<<<grid_for((size_t)ctx->np * n), 256, 0, st>>>(
+            ctx->d_cp, ctx->d_cd, ctx->np, n, ctx->d_proj_ion, ctx->d_poff, ctx->d_doff, ctx->d_qmat);
+        count_launch();
+        k_conj<<<grid_for((size_t)ctx->np * n), 256, 0, st>>>(ctx->d_cp, ctx->d_cq, (size_t)ctx->np * n);
+        gemm_tn(ctx->d_cq, n, ctx->d_cd, n, ctx->d_T1, n, n, n, ctx->np, 1.0, 1.0, st);
+    }
     symmetrize(ctx->d_T1, ctx->d_S, n, st);
     cholesky(ctx->d_S, n, ctx->d_flags + 0, st);                   // S -> L
     tri_inv(ctx->d_S, ctx->d_T1, n, st);                            // T1 = L^-1
@@ -347,6 +454,177 @@ chfsi_status rr_dev(chfsi_ctx* ctx) {
     return CHFSI_OK;
 }
 
+// ---------------------------------------------------------------- mixed precision
+// FP32 filter with the projector GEMMs on tcgen05 (BF16 3-way split, FP32
+// accumulation in TMEM); Rayleigh-Ritz overlap / subspace matrices and the
+// psi V rotation on tcgen05, Cholesky and eigensolve in FP64.
+
+chfsi_status alloc_mixed(chfsi_ctx* ctx, int ncol) {
+    const int nb = ctx->nb, np = ctx->np, npw = ctx->n_pw;
+    const size_t nbpw = (size_t)nb * npw;
+    CK(dalloc(&ctx->d_psi32a, nbpw));
+    CK(dalloc(&ctx->d_psi32b, nbpw));
+    CK(dalloc(&ctx->d_hpsi32, nbpw));
+    if (np > 0) CK(dalloc(&ctx->d_nl32, nbpw));
+    CK(dalloc(&ctx->d_work32, (size_t)nb * ctx->nz * ncol));
+    struct Spec { TcPlanes* t; int rows_alloc; int kp; };
+    const int kp_pw = tc_kpad(npw);
+    std::vector<Spec> specs = {
+        {&ctx->tp_psi_b, tc_rows_alloc(nb, false, nb), kp_pw},
+        {&ctx->tp_psi_a, tc_rows_alloc(2 * nb, true, 0), kp_pw},
+        {&ctx->tp_hpsi_b, tc_rows_alloc(nb, false, nb), kp_pw},
+        {&ctx->tp_small_a, tc_rows_alloc(2 * nb, true, 0), std::max(tc_kpad(std::max(np, 1)), tc_kpad(nb))},
+        {&ctx->tp_psiT_b, tc_rows_alloc(npw, false, npw), tc_kpad(nb)},
+    };
+    if (np > 0) {
+        specs.push_back({&ctx->tp_beta_a, tc_rows_alloc(2 * np, true, 0), kp_pw});
+        specs.push_back({&ctx->tp_betaT_b, tc_rows_alloc(npw, false, npw), tc_kpad(np)});
+    }
+    size_t total = 0;
+    for (auto& s : specs) total += 3 * (size_t)s.rows_alloc * s.kp;
+    CK(cudaMalloc(&ctx->d_planes, total * 2));
+    CK(cudaMemset(ctx->d_planes, 0, total * 2));
+    char* p = (char*)ctx->d_planes;
+    for (auto& s : specs) {
+        for (int i = 0; i < 3; ++i) {
+            s.t->p[i] = p;
+            p += (size_t)s.rows_alloc * s.kp * 2;
+        }
+        s.t->rows_alloc = s.rows_alloc;
+        s.t->kp = s.kp;
+    }
+    size_t pf = tc_partial_floats(nb, nb, npw);
+    if (np > 0) pf = std::max(pf, tc_partial_floats(np, nb, npw));
+    CK(dalloc(&ctx->d_tc_part, pf));
+    CK(dalloc(&ctx->d_tc_err, 4));
+    CK(cudaMemset(ctx->d_tc_err, 0, 4 * sizeof(int)));
+    return CHFSI_OK;
+}
+
+chfsi_status pack_beta_planes(chfsi_ctx* ctx) {
+    if (!ctx->mixed || ctx->np == 0) return CHFSI_OK;
+    // beta^H psi: A operand = beta rows (doubled); back-projection: B operand = beta^T
+    tc_pack<double2>(ctx->d_beta, ctx->n_pw, ctx->np, ctx->n_pw, true, kSrcPlain, ctx->tp_beta_a, ctx->st);
+    tc_pack<double2>(ctx->d_beta, ctx->n_pw, ctx->n_pw, ctx->np, false, kSrcT, ctx->tp_betaT_b, ctx->st);
+    CK(cudaGetLastError());
+    ctx->beta_planes_ready = true;
+    return CHFSI_OK;
+}
+
+chfsi_status apply_h_dev32(chfsi_ctx* ctx, const float2* psi, float2* out, int nb, int mode,
+                           double* norm_acc) {
+    Epilogue e{};
+    e.mode = mode;
+    e.kin = ctx->d_kin;
+    e.coef = ctx->d_coef;
+    e.nl = nullptr;
+    e.norm_acc = norm_acc;
+    e.inv_n = 1.0 / (double)ctx->ng;
+    cudaStream_t st = ctx->st;
+    if (ctx->np > 0) {
+        // C = beta^H psi (tcgen05), C <- D C (FP64), nl = beta C (tcgen05, FP32 out)
+        tc_pack<float2>(psi, ctx->n_pw, nb, ctx->n_pw, false, kSrcPlain, ctx->tp_psi_b, st);
+        CK(tc_gemm(ctx->tp_beta_a, ctx->tp_psi_b, ctx->np, nb, ctx->n_pw, kTcOutPartial, ctx->d_cp,
+                   nb, ctx->d_tc_part, ctx->d_tc_err, st));
+        count_launch();
+        k_apply_dmat<<<grid_for((size_t)ctx->np * nb), 256, 0, st>>>(
+            ctx->d_cp, ctx->d_cd, ctx->np, nb, ctx->d_proj_ion, ctx->d_poff, ctx->d_doff, ctx->d_dmat);
+        tc_pack<double2>(ctx->d_cd, nb, nb, ctx->np, true, kSrcConjT, ctx->tp_small_a, st);
+        CK(tc_gemm(ctx->tp_small_a, ctx->tp_betaT_b, nb, ctx->n_pw, ctx->np, kTcOutComplexF32,
+                   ctx->d_nl32, ctx->n_pw, nullptr, ctx->d_tc_err, st));
+        e.nl = ctx->d_nl32;
+    }
+    launch_zsticks_inverse<float2>(psi, ctx->n_pw, ctx->d_work32, nb, ctx->geo, st);
+    launch_planes_vloc<float2>(ctx->d_work32, ctx->d_veff, nb, ctx->geo, st);
+    launch_zsticks_forward<float2>(ctx->d_work32, psi, ctx->n_pw, out, ctx->n_pw, nb, ctx->geo, e, st);
+    CK(cudaGetLastError());
+    return CHFSI_OK;
+}
+
+chfsi_status filter_dev32(chfsi_ctx* ctx, int ndeg, const double* eig_dev, int n_eig) {
+    if (ndeg < 0 || ndeg > ctx->max_deg) return ctx->fail(CHFSI_ERR_BAD_INPUT, "ndeg out of range");
+    if (ctx->np > 0 && !ctx->beta_planes_ready) {
+        chfsi_status s = pack_beta_planes(ctx);
+        if (s) return s;
+    }
+    chfsi_status s = compute_bounds(ctx, eig_dev, n_eig);
+    if (s) return s;
+    const size_t n = (size_t)ctx->nb * ctx->n_pw;
+    cudaStream_t st = ctx->st;
+    count_launch();
+    k_f64_to_f32<<<grid_for(n), 256, 0, st>>>(ctx->d_psi, ctx->d_psi32a, n);
+    CK(cudaMemsetAsync(ctx->d_nsq, 0, sizeof(double) * (ndeg + 1), st));
+    count_launch();
+    k_sumsq32<<<grid_for(n), 256, 0, st>>>(ctx->d_psi32a, n, ctx->d_nsq);
+    float2* A = ctx->d_psi32a;
+    float2* B = ctx->d_psi32b;
+    if (ndeg >= 1) {
+        s = apply_h_dev32(ctx, A, B, ctx->nb, kEpiChebFirst, ctx->d_nsq + 1);
+        if (s) return s;
+    }
+    for (int k = 2; k <= ndeg; ++k) {
+        s = apply_h_dev32(ctx, B, A, ctx->nb, kEpiCheb, ctx->d_nsq + k);
+        if (s) return s;
+        std::swap(A, B);
+    }
+    float2* fin = ndeg >= 1 ? B : A;
+    ctx->d_psi32 = fin;
+    s = apply_h_dev32(ctx, fin, ctx->d_hpsi32, ctx->nb, kEpiApply, nullptr);
+    if (s) return s;
+    // keep the FP64 master copy consistent with the filtered subspace
+    count_launch();
+    k_f32_to_f64<<<grid_for(n), 256, 0, st>>>(fin, ctx->d_psi, n);
+    norm_guard(ctx->d_nsq, ndeg, ctx->d_flags + 1, st);
+    ctx->last_ndeg = ndeg;
+    CK(cudaGetLastError());
+    return CHFSI_OK;
+}
+
+chfsi_status rr_dev32(chfsi_ctx* ctx) {
+    const int n = ctx->nb, npw = ctx->n_pw;
+    cudaStream_t st = ctx->st;
+    const float2* psi = ctx->d_psi32;
+    tc_pack<float2>(psi, npw, n, npw, true, kSrcPlain, ctx->tp_psi_a, st);
+    tc_pack<float2>(psi, npw, n, npw, false, kSrcPlain, ctx->tp_psi_b, st);
+    tc_pack<float2>(ctx->d_hpsi32, npw, n, npw, false, kSrcPlain, ctx->tp_hpsi_b, st);
+    CK(tc_gemm(ctx->tp_psi_a, ctx->tp_hpsi_b, n, n, npw, kTcOutPartial, ctx->d_T1, n, ctx->d_tc_part,
+               ctx->d_tc_err, st));
+    symmetrize(ctx->d_T1, ctx->d_H, n, st);
+    CK(tc_gemm(ctx->tp_psi_a, ctx->tp_psi_b, n, n, npw, kTcOutPartial, ctx->d_T1, n, ctx->d_tc_part,
+               ctx->d_tc_err, st));
+    symmetrize(ctx->d_T1, ctx->d_S, n, st);
+    cholesky(ctx->d_S, n, ctx->d_flags + 0, st);
+    tri_inv(ctx->d_S, ctx->d_T1, n, st);
+    small_gemm(0, 0, ctx->d_T1, ctx->d_H, ctx->d_T2, n, st);
+    small_gemm(0, 1, ctx->d_T2, ctx->d_T1, ctx->d_H, n, st);
+    symmetrize(ctx->d_H, ctx->d_T2, n, st);
+    CK(jacobi(ctx->d_T2, ctx->d_V, n, ctx->jac_max_sweeps, 1e-26, ctx->d_jac, ctx->d_flags + 2, st));
+    sort_eig(ctx->d_T2, ctx->d_V, n, ctx->d_eig, ctx->d_H, st);
+    small_gemm(1, 0, ctx->d_T1, ctx->d_H, ctx->d_T2, n, st);  // Vf = Li^H U
+    // psi_new[i][g] = sum_j Vf[j][i] psi[j][g]  (tcgen05, FP64 output)
+    tc_pack<double2>(ctx->d_T2, n, n, n, true, kSrcConjT, ctx->tp_small_a, st);
+    tc_pack<float2>(psi, npw, npw, n, false, kSrcT, ctx->tp_psiT_b, st);
+    CK(tc_gemm(ctx->tp_small_a, ctx->tp_psiT_b, n, npw, n, kTcOutComplexF64, ctx->d_psi, npw, nullptr,
+               ctx->d_tc_err, st));
+    CK(cudaGetLastError());
+    return CHFSI_OK;
+}
+
+chfsi_status filter_any(chfsi_ctx* ctx, int ndeg, const double* eig_dev, int n_eig) {
+    if (ctx->mixed_active) return filter_dev32(ctx, ndeg, eig_dev, n_eig);
+    ctx->d_psi32 = nullptr;
+    return filter_dev(ctx, ndeg, eig_dev, n_eig);
+}
+
+chfsi_status rr_any(chfsi_ctx* ctx) {
+    if (ctx->mixed_active && ctx->d_psi32) {
+        chfsi_status s = rr_dev32(ctx);
+        ctx->d_psi32 = nullptr;
+        return s;
+    }
+    return rr_dev(ctx);
+}
+
 // Read back eigenvalues, flags, bounds and norms; translate device flags into
 // the reference's error variants.
 chfsi_status finish_diag(chfsi_ctx* ctx, double* eig_out, bool have_rr) {
@@ -359,7 +637,11 @@ chfsi_status finish_diag(chfsi_ctx* ctx, double* eig_out, bool have_rr) {
     CK(cudaMemcpyAsync(h + n + 6, ctx->d_flags, sizeof(int) * 4, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaMemcpyAsync(h + n + 8, ctx->d_nsq, sizeof(double) * (ctx->last_ndeg + 1),
                        cudaMemcpyDeviceToHost, ctx->st));
+    int tc_err = 0;
+    if (ctx->d_tc_err)
+        CK(cudaMemcpyAsync(&tc_err, ctx->d_tc_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
+    if (tc_err) return ctx->fail(CHFSI_ERR_CUDA, "tensor-core GEMM pipeline wait timed out");
     std::memcpy(ctx->h_coef, h + n, sizeof(double) * 6);
     int flags[4];
     std::memcpy(flags, h + n + 6, sizeof(flags));
@@ -517,6 +799,11 @@ void free_all(chfsi_ctx* ctx) {
                     ctx->d_hist_ptrs, ctx->d_dots};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    void* mp[] = {ctx->d_psi32a, ctx->d_psi32b, ctx->d_hpsi32, ctx->d_nl32, ctx->d_work32,
+                  ctx->d_planes, ctx->d_tc_part, ctx->d_tc_err, ctx->d_qmat, ctx->d_sinvT,
+                  ctx->d_cq, ctx->d_sx};
+    for (void* p : mp)
+        if (p) cudaFree(p);
     if (ctx->h_pin) cudaFreeHost(ctx->h_pin);
     if (ctx->st) cudaStreamDestroy(ctx->st);
 }
@@ -560,11 +847,12 @@ chfsi_status chfsi_create(const chfsi_dims* dims, const chfsi_config* cfg, chfsi
     if (!ctx) return CHFSI_ERR_OUT_OF_MEMORY;
     ctx->dims = *dims;
     if (cfg) ctx->cfg = *cfg; else chfsi_default_config(&ctx->cfg);
-    if (ctx->cfg.precision != CHFSI_PREC_FP64) {
+    if (ctx->cfg.precision != CHFSI_PREC_FP64 && ctx->cfg.precision != CHFSI_PREC_MIXED) {
         delete ctx;
-        g_last_error = "mixed precision is not available in this build";
-        return CHFSI_ERR_NOT_IMPLEMENTED;
+        g_last_error = "unknown precision mode";
+        return CHFSI_ERR_BAD_INPUT;
     }
+    ctx->mixed = ctx->mixed_active = ctx->cfg.precision == CHFSI_PREC_MIXED;
     ctx->device = ctx->cfg.device;
     chfsi_status s = CHFSI_OK;
     auto bail = [&](chfsi_status e) { free_all(ctx); delete ctx; return e; };
@@ -637,7 +925,8 @@ chfsi_status chfsi_set_basis(chfsi_ctx* ctx, const int32_t* miller, const double
         if (c != last) {
             col_start.push_back(i);
             const int px = ctx->dr[0][ix[g]], py = ctx->dr[1][iy[g]];
-            col_pos.push_back(py * (nx | 1) + px);
+            // plane rows and elements are XOR-swizzled in shared memory
+            col_pos.push_back(swz(py, ny) * (nx | 1) + swz(px, nx));
             xused[px] = 1;
             last = c;
         } else if (i > 0 && miller[3 * g + 2] == miller[3 * perm[i - 1] + 2]) {
@@ -650,7 +939,7 @@ chfsi_status chfsi_set_basis(chfsi_ctx* ctx, const int32_t* miller, const double
     const int ncol = (int)col_start.size();
     col_start.push_back(n);
     for (int x = 0; x < nx; ++x)
-        if (xused[x]) xact.push_back(x);
+        if (xused[x]) xact.push_back(swz(x, nx));
     double kmax = 0.0;
     for (int g = 0; g < n; ++g) kmax = std::max(kmax, kinetic[g]);
     // kinetic bound of the reference: 1/2 Gmax^2 (chebyshev.rs:232)
@@ -682,6 +971,10 @@ chfsi_status chfsi_set_basis(chfsi_ctx* ctx, const int32_t* miller, const double
         return ctx->fail(CHFSI_ERR_BAD_INPUT, "xy plane does not fit in shared memory");
     if ((size_t)nx * ny > kDensityPlanePoints)
         return ctx->fail(CHFSI_ERR_BAD_INPUT, "xy plane too large for the density kernel");
+    if (ctx->mixed) {
+        chfsi_status s = alloc_mixed(ctx, ncol);
+        if (s) return s;
+    }
     ctx->basis_set = true;
     return CHFSI_OK;
 }
@@ -727,6 +1020,77 @@ chfsi_status chfsi_set_projectors(chfsi_ctx* ctx, const chfsi_c128* beta,
         CK(cudaGetLastError());
     }
     ctx->proj_set = true;
+    ctx->beta_planes_ready = false;
+    return pack_beta_planes(ctx);
+}
+
+chfsi_status chfsi_set_qmat(chfsi_ctx* ctx, const chfsi_c128* qmat) {
+    if (!ctx || !qmat || !ctx->proj_set || ctx->np == 0) return CHFSI_ERR_BAD_INPUT;
+    if (ctx->mixed) return ctx->fail(CHFSI_ERR_NOT_IMPLEMENTED, "ultrasoft overlap runs in FP64 only");
+    cudaSetDevice(ctx->device);
+    const int np = ctx->np, ni = ctx->nions;
+    std::vector<int> poff(ni + 1), doff(ni);
+    CK(cudaMemcpy(poff.data(), ctx->d_poff, sizeof(int) * (ni + 1), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(doff.data(), ctx->d_doff, sizeof(int) * ni, cudaMemcpyDeviceToHost));
+    size_t dt = 0;
+    for (int i = 0; i < ni; ++i) dt += (size_t)(poff[i + 1] - poff[i]) * (poff[i + 1] - poff[i]);
+    if (!ctx->d_qmat) CK(dalloc(&ctx->d_qmat, dt));
+    CK(cudaMemcpy(ctx->d_qmat, qmat, dt * sizeof(double2), cudaMemcpyHostToDevice));
+    // B = beta^H beta on the device
+    double2 *part = nullptr, *dB = nullptr;
+    CK(cudaMalloc((void**)&part, splitk_partial_elems(np, np, ctx->n_pw) * sizeof(double2)));
+    CK(cudaMalloc((void**)&dB, (size_t)np * np * sizeof(double2)));
+    gemm_cn(ctx->d_beta, ctx->n_pw, ctx->d_beta, ctx->n_pw, np, np, ctx->n_pw, part, dB, ctx->st);
+    std::vector<std::complex<double>> B((size_t)np * np), Q((size_t)np * np, 0.0);
+    cudaError_t e = cudaMemcpyAsync(B.data(), dB, B.size() * sizeof(double2), cudaMemcpyDeviceToHost, ctx->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->st);
+    cudaFree(part);
+    cudaFree(dB);
+    CK(e);
+    const std::complex<double>* qh = reinterpret_cast<const std::complex<double>*>(qmat);
+    for (int i = 0; i < ni; ++i) {
+        const int p0 = poff[i], ne = poff[i + 1] - p0;
+        for (int a = 0; a < ne; ++a)
+            for (int b = 0; b < ne; ++b) Q[(size_t)(p0 + a) * np + p0 + b] = qh[doff[i] + a * ne + b];
+    }
+    // s_min = 1 - max row sum |q B|; A = 1 + B q; M = q A^-1
+    double rs = 0.0;
+    std::vector<std::complex<double>> A((size_t)np * np, 0.0);
+    for (int i = 0; i < np; ++i) {
+        double r = 0.0;
+        for (int j = 0; j < np; ++j) {
+            std::complex<double> qb = 0.0, bq = 0.0;
+            const int ion_i = std::upper_bound(poff.begin(), poff.end(), i) - poff.begin() - 1;
+            const int ion_j = std::upper_bound(poff.begin(), poff.end(), j) - poff.begin() - 1;
+            for (int k = poff[ion_i]; k < poff[ion_i + 1]; ++k) qb += Q[(size_t)i * np + k] * B[(size_t)k * np + j];
+            for (int k = poff[ion_j]; k < poff[ion_j + 1]; ++k) bq += B[(size_t)i * np + k] * Q[(size_t)k * np + j];
+            r += std::abs(qb);
+            A[(size_t)i * np + j] = bq + (i == j ? 1.0 : 0.0);
+        }
+        rs = std::max(rs, r);
+    }
+    ctx->s_min = std::max(0.1, 1.0 - rs);
+    if (!invert_complex(A, np)) return ctx->fail(CHFSI_ERR_NUMERIC, "1 + B q is singular");
+    std::vector<std::complex<double>> MT((size_t)np * np, 0.0);
+    for (int i = 0; i < np; ++i) {
+        const int ion_i = std::upper_bound(poff.begin(), poff.end(), i) - poff.begin() - 1;
+        for (int j = 0; j < np; ++j) {
+            std::complex<double> m = 0.0;
+            for (int k = poff[ion_i]; k < poff[ion_i + 1]; ++k) m += Q[(size_t)i * np + k] * A[(size_t)k * np + j];
+            MT[(size_t)j * np + i] = m;
+        }
+    }
+    if (!ctx->d_sinvT) CK(dalloc(&ctx->d_sinvT, (size_t)np * np));
+    if (!ctx->d_cq) CK(dalloc(&ctx->d_cq, (size_t)np * ctx->nb));
+    if (!ctx->d_sx) CK(dalloc(&ctx->d_sx, (size_t)ctx->nb * ctx->n_pw));
+    CK(cudaMemcpy(ctx->d_sinvT, MT.data(), MT.size() * sizeof(double2), cudaMemcpyHostToDevice));
+    ctx->uspp = true;
+    return CHFSI_OK;
+}
+
+chfsi_status chfsi_get_s_min(chfsi_ctx* ctx, double* out) {
+    if (!ctx || !out) return CHFSI_ERR_BAD_INPUT;
+    *out = ctx->s_min;
     return CHFSI_OK;
 }
 
@@ -840,7 +1204,7 @@ chfsi_status chfsi_chebyshev_filter(chfsi_ctx* ctx, int ndeg, const double* eig_
     const double* ed = nullptr;
     s = upload_eig(ctx, eig_prev, n_eig, &ed);
     if (s) return s;
-    s = filter_dev(ctx, ndeg, ed, ed ? n_eig : 0);
+    s = filter_any(ctx, ndeg, ed, ed ? n_eig : 0);
     if (s) return s;
     return finish_diag(ctx, nullptr, false);
 }
@@ -848,7 +1212,7 @@ chfsi_status chfsi_chebyshev_filter(chfsi_ctx* ctx, int ndeg, const double* eig_
 chfsi_status chfsi_rayleigh_ritz(chfsi_ctx* ctx, double* eig_out) {
     chfsi_status s = ready(ctx);
     if (s) return s;
-    s = rr_dev(ctx);
+    s = rr_any(ctx);
     if (s) return s;
     return finish_diag(ctx, eig_out, true);
 }
@@ -861,9 +1225,9 @@ chfsi_status chfsi_diagonalize(chfsi_ctx* ctx, int ndeg, const double* eig_prev,
     const double* ed = nullptr;
     s = upload_eig(ctx, eig_prev, n_eig, &ed);
     if (s) return s;
-    s = filter_dev(ctx, ndeg, ed, ed ? n_eig : 0);
+    s = filter_any(ctx, ndeg, ed, ed ? n_eig : 0);
     if (s) return s;
-    s = rr_dev(ctx);
+    s = rr_any(ctx);
     if (s) return s;
     return finish_diag(ctx, eig_out, true);
 }
@@ -1144,8 +1508,8 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
         // diagonalize (scf.rs:169)
         const int passes = it == 1 ? std::max(1, p->first_passes) : 1;
         for (int q = 0; q < passes; ++q) {
-            s = filter_dev(ctx, p->ndeg, have_eig ? ctx->d_eig : nullptr, have_eig ? ctx->nb : 0);
-            if (!s) s = rr_dev(ctx);
+            s = filter_any(ctx, p->ndeg, have_eig ? ctx->d_eig : nullptr, have_eig ? ctx->nb : 0);
+            if (!s) s = rr_any(ctx);
             if (!s) s = finish_diag(ctx, eig.data(), true);
             if (s) break;
             have_eig = true;
@@ -1177,12 +1541,17 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
         r->e_band = eband; r->e_hartree = acc[0]; r->e_xc = acc[1]; r->e_dc = acc[2];
         r->e_total = etot;
         r->n_iter = it;
-        // check (scf.rs:328): |dE| per atom below tolerance
-        if (it > 1 && std::fabs(etot - e_prev) / ctx->n_atoms < p->tol_per_atom) {
+        // check (scf.rs:328): |dE| per atom below tolerance; a mixed-precision
+        // run only converges on FP64 iterations (the final filter passes are FP64)
+        const double de = it > 1 ? std::fabs(etot - e_prev) / ctx->n_atoms : 1e300;
+        if (ctx->mixed_active) ++r->n_iter_mixed;
+        if (de < p->tol_per_atom && !ctx->mixed_active) {
             status = CHFSI_OK;
             e_prev = etot;
             break;
         }
+        if (ctx->mixed_active && (de < p->fp64_switch_per_atom || de < p->tol_per_atom))
+            ctx->mixed_active = false;
         e_prev = etot;
         // mix (mixing.rs:24): Pulay over (rho_in, rho_out - rho_in)
         if (ps.m == p->max_hist) {
@@ -1224,6 +1593,7 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
         std::swap(ctx->d_rho_in, ctx->d_rho_next);
         CK(cudaGetLastError());
     }
+    ctx->mixed_active = ctx->mixed;
     cudaEventRecord(t1, st);
     cudaEventSynchronize(t1);
     float ms = 0.f;
@@ -1295,8 +1665,8 @@ extern "C" chfsi_status chfsi_zgemm_cn_bf16x3(const chfsi_c128* a_dev, int lda,
     }
     int* err = (int*)(buf + 3 * (na + nbe) * 2);
     float* part = (float*)(buf + 3 * (na + nbe) * 2 + 256);
-    tc_pack<double2>(reinterpret_cast<const double2*>(a_dev), lda, m, k, true, false, pa, st);
-    tc_pack<double2>(reinterpret_cast<const double2*>(b_dev), ldb, n, k, false, false, pb, st);
+    tc_pack<double2>(reinterpret_cast<const double2*>(a_dev), lda, m, k, true, kSrcPlain, pa, st);
+    tc_pack<double2>(reinterpret_cast<const double2*>(b_dev), ldb, n, k, false, kSrcPlain, pb, st);
     e = tc_gemm(pa, pb, m, n, k, kTcOutPartial, c_dev, n, part, err, st);
     int herr = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st);

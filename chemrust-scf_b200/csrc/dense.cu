@@ -261,6 +261,150 @@ k_jacobi(double2* A, double2* V, int n, int max_sweeps, double tol2, double* scr
     if (gtid == 0) *sweeps_out = sweep;
 }
 
+// Circle-method pairing of step s over m = n + (n & 1) indices: pair i of
+// step s is (min(a, b), max(a, b)).
+__device__ __forceinline__ void jac_pair(int m, int s, int i, int& p, int& q) {
+    const int a = i == 0 ? 0 : 1 + ((i - 1 + s) % (m - 1));
+    const int b = 1 + ((m - 2 - i + s) % (m - 1));
+    p = min(a, b);
+    q = max(a, b);
+}
+// Pair index and partner of column k at step s.
+__device__ __forceinline__ void jac_partner(int m, int s, int k, int& pi, int& partner) {
+    const int j = k == 0 ? 0 : ((k - 1 - s) % (m - 1) + (m - 1)) % (m - 1) + 1;
+    const int jj = m - 1 - j;
+    pi = min(j, jj);
+    partner = jj == 0 ? 0 : 1 + ((jj - 1 + s) % (m - 1));
+}
+
+// Parallel cyclic Jacobi with one grid barrier per rotation step.
+//   phase 1 (step s): each warp takes its pairs (p, q), computes the rotation
+//     from A, writes rows p, q of X = G^H A and the rotation parameters
+//     (double-buffered by step parity)
+//   grid barrier
+//   phase 2 (step s): each warp builds the rows it owns at step s + 1 as
+//     A[r] = X[r] G, mixing the columns of every pair of step s, and updates
+//     its share of V rows the same way (through a shared-memory row buffer)
+// Rows read in phase 1 of step s + 1 were written by the same warp in phase 2
+// of step s, so no second barrier is needed.  All accesses are row-wise.
+__global__ void __launch_bounds__(256)
+k_jacobi2(double2* A, double2* V, double2* X, int n, int max_sweeps, double tol2, double* scratch,
+          double* rot, int* sweeps_out) {
+    cg::grid_group grid = cg::this_grid();
+    extern __shared__ double2 rowbuf_all[];  // 8 warps x n
+    __shared__ double red[32];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    double2* rowbuf = rowbuf_all + (size_t)wib * n;
+    const size_t nn = (size_t)n * n;
+    const size_t gtid = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    const size_t gstride = (size_t)gridDim.x * blockDim.x;
+    for (size_t t = gtid; t < nn; t += gstride)
+        V[t] = make_double2((t / n) == (t % n) ? 1.0 : 0.0, 0.0);
+    double tot = 0.0;
+    for (size_t t = gtid; t < nn; t += gstride) tot += A[t].x * A[t].x + A[t].y * A[t].y;
+    tot = block_sum(tot, red);
+    if (threadIdx.x == 0) atomicAdd(&scratch[0], tot);
+    grid.sync();
+    const double total = scratch[0];
+    const int m = n + (n & 1);
+    const int npairs = m / 2;
+    const int nsteps = m - 1;
+    int sweep = 0;
+    bool converged = false;
+    for (; sweep < max_sweeps && !converged; ++sweep) {
+        for (int s = 0; s < nsteps; ++s) {
+            double* rs = rot + 4 * (size_t)npairs * (s & 1);
+            // ---- phase 1
+            for (int pi = gw; pi < npairs; pi += nwarps) {
+                int p, q;
+                jac_pair(m, s, pi, p, q);
+                double c = 1.0, sn = 0.0, phr = 1.0, phi = 0.0;
+                if (q < n) {
+                    const double2 apq = A[(size_t)p * n + q];
+                    const double app = A[(size_t)p * n + p].x, aqq = A[(size_t)q * n + q].x;
+                    const double bm = hypot(apq.x, apq.y);
+                    if (bm > 1e-300 && bm > 1e-18 * sqrt(fabs(app * aqq))) {
+                        phr = apq.x / bm;
+                        phi = apq.y / bm;
+                        const double tau = (aqq - app) / (2.0 * bm);
+                        const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+                        c = 1.0 / sqrt(1.0 + t * t);
+                        sn = t * c;
+                    }
+                    for (int k = lane; k < n; k += 32) {
+                        const double2 apk = A[(size_t)p * n + k], aqk = A[(size_t)q * n + k];
+                        const double2 pa = make_double2(phr * aqk.x - phi * aqk.y, phr * aqk.y + phi * aqk.x);
+                        X[(size_t)p * n + k] = make_double2(c * apk.x - sn * pa.x, c * apk.y - sn * pa.y);
+                        X[(size_t)q * n + k] = make_double2(sn * apk.x + c * pa.x, sn * apk.y + c * pa.y);
+                    }
+                } else if (p < n) {
+                    for (int k = lane; k < n; k += 32) X[(size_t)p * n + k] = A[(size_t)p * n + k];
+                }
+                if (lane == 0) {
+                    rs[4 * pi + 0] = c; rs[4 * pi + 1] = sn; rs[4 * pi + 2] = phr; rs[4 * pi + 3] = phi;
+                }
+            }
+            grid.sync();
+            // ---- phase 2: rows owned at the next step, A[r] = X[r] G(s)
+            const int s2 = (s + 1) % nsteps;
+            auto mix = [&](const double2* src, int k) -> double2 {
+                int pi, partner;
+                jac_partner(m, s, k, pi, partner);
+                const double2 xk = src[k];
+                if (partner >= n) return xk;
+                const double c = rs[4 * pi + 0], sn = rs[4 * pi + 1];
+                const double phr = rs[4 * pi + 2], phi = rs[4 * pi + 3];
+                const double2 xp = src[partner];
+                if (k < partner) {  // k is p: X_rp c + X_rq (-s conj(ph))
+                    const double2 qc = make_double2(phr * xp.x + phi * xp.y, phr * xp.y - phi * xp.x);
+                    return make_double2(c * xk.x - sn * qc.x, c * xk.y - sn * qc.y);
+                }
+                // k is q: X_rp s + X_rq c conj(ph)
+                const double2 qc = make_double2(phr * xk.x + phi * xk.y, phr * xk.y - phi * xk.x);
+                return make_double2(sn * xp.x + c * qc.x, sn * xp.y + c * qc.y);
+            };
+            for (int pi = gw; pi < npairs; pi += nwarps) {
+                int p, q;
+                jac_pair(m, s2, pi, p, q);
+                for (int h = 0; h < 2; ++h) {
+                    const int r = h == 0 ? p : q;
+                    if (r >= n) continue;
+                    const double2* xr = X + (size_t)r * n;
+                    for (int k = lane; k < n; k += 32) A[(size_t)r * n + k] = mix(xr, k);
+                }
+            }
+            for (int r = gw; r < n; r += nwarps) {
+                double2* vr = V + (size_t)r * n;
+                for (int k = lane; k < n; k += 32) rowbuf[k] = mix(vr, k);
+                __syncwarp();
+                for (int k = lane; k < n; k += 32) vr[k] = rowbuf[k];
+                __syncwarp();
+            }
+            __syncwarp();
+        }
+        // off-diagonal norm of the rows this warp owns at step 0
+        double off = 0.0;
+        for (int pi = gw; pi < npairs; pi += nwarps) {
+            int p, q;
+            jac_pair(m, 0, pi, p, q);
+            for (int h = 0; h < 2; ++h) {
+                const int r = h == 0 ? p : q;
+                if (r >= n) continue;
+                for (int k = lane; k < n; k += 32)
+                    if (k != r) off += A[(size_t)r * n + k].x * A[(size_t)r * n + k].x +
+                                       A[(size_t)r * n + k].y * A[(size_t)r * n + k].y;
+            }
+        }
+        off = block_sum(off, red);
+        if (threadIdx.x == 0) atomicAdd(&scratch[1 + sweep], off);
+        grid.sync();
+        converged = scratch[1 + sweep] <= tol2 * total;
+    }
+    if (gtid == 0) *sweeps_out = converged ? sweep : max_sweeps;
+}
+
 // Sort eigenvalues ascending (stable by index) and permute eigenvector columns.
 __global__ void __launch_bounds__(1024)
 k_sort_eig(const double2* __restrict__ A, const double2* __restrict__ V, int n,
@@ -346,7 +490,7 @@ __device__ double tridiag_max(const double* d, const double* e, int k) {
 // range bound); the Lanczos bound is lambda_max(T_k) + |f_k| (Zhou 2010).
 __global__ void k_bounds(double kin_max, const double* __restrict__ minmax,
                          const double* __restrict__ eig, int n_eig, const double* lanczos, int k,
-                         double* coef) {
+                         double lm_scale, double* coef) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     double lm;
     if (lanczos) {
@@ -356,6 +500,7 @@ __global__ void k_bounds(double kin_max, const double* __restrict__ minmax,
     } else {
         lm = kin_max + (minmax[1] - minmax[0]);
     }
+    lm *= lm_scale;  // generalised problem: lambda_max(H) / lambda_min(S)
     double cut;
     if (!eig || n_eig == 0) cut = lm / 3.0;
     else {
@@ -502,25 +647,31 @@ void small_gemm(int opa, int opb, const double2* A, const double2* B, double2* C
     else k_small_gemm<1, 1><<<grid, 256, 0, st>>>(A, B, C, n);
 }
 size_t jacobi_scratch_doubles(int n, int max_sweeps) {
-    return 1 + (size_t)max_sweeps + 4 * (size_t)((n + 1) / 2 + 1);
+    // sweep norms, double-buffered rotations, X (n x n complex)
+    return 1 + (size_t)max_sweeps + 8 * (size_t)((n + 1) / 2 + 1) + 2 * (size_t)n * n + 2;
 }
 cudaError_t jacobi(double2* A, double2* V, int n, int max_sweeps, double tol2, double* scratch,
                    int* sweeps_out, cudaStream_t st) {
     count_launch();
     cudaMemsetAsync(scratch, 0, sizeof(double) * (1 + max_sweeps), st);
-    double* rot = scratch + 1 + max_sweeps;
     const int npairs = (n + 1) / 2;
+    double* rot = scratch + 1 + max_sweeps;
+    double2* X = (double2*)(rot + 8 * (size_t)(npairs + 1));
+    if (((uintptr_t)X) & 15) X = (double2*)(((uintptr_t)X + 15) & ~(uintptr_t)15);
     const int warps_per_block = 8;
     int blocks = (npairs + warps_per_block - 1) / warps_per_block;
+    const size_t smem = (size_t)warps_per_block * n * sizeof(double2);
+    if (smem > 48 * 1024)
+        cudaFuncSetAttribute(k_jacobi2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_jacobi, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_jacobi2, 256, smem);
     if (per_sm < 1) per_sm = 1;
     if (blocks > sms * per_sm) blocks = sms * per_sm;
     if (blocks < 1) blocks = 1;
-    void* args[] = {&A, &V, &n, &max_sweeps, &tol2, &scratch, &rot, &sweeps_out};
-    return cudaLaunchCooperativeKernel((const void*)k_jacobi, dim3(blocks), dim3(256), args, 0, st);
+    void* args[] = {&A, &V, &X, &n, &max_sweeps, &tol2, &scratch, &rot, &sweeps_out};
+    return cudaLaunchCooperativeKernel((const void*)k_jacobi2, dim3(blocks), dim3(256), args, smem, st);
 }
 void sort_eig(const double2* A, const double2* V, int n, double* w, double2* U, cudaStream_t st) {
     count_launch();
@@ -535,9 +686,9 @@ void sumsq(const double2* x, size_t n, double* acc, cudaStream_t st) {
     k_sumsq<<<grid_for(n), 256, 0, st>>>(x, n, acc);
 }
 void bounds(double kin_max, const double* minmax_dev, const double* eig_dev, int n_eig,
-            const double* lanczos, int k, double* coef, cudaStream_t st) {
+            const double* lanczos, int k, double lm_scale, double* coef, cudaStream_t st) {
     count_launch();
-    k_bounds<<<1, 32, 0, st>>>(kin_max, minmax_dev, eig_dev, n_eig, lanczos, k, coef);
+    k_bounds<<<1, 32, 0, st>>>(kin_max, minmax_dev, eig_dev, n_eig, lanczos, k, lm_scale, coef);
 }
 void norm_guard(const double* nsq, int ndeg, int* status, cudaStream_t st) {
     count_launch();

@@ -20,7 +20,7 @@ void sort_eig(const double2* A, const double2* V, int n, double* w, double2* U, 
 void minmax(const double* v, size_t n, double* out, cudaStream_t st);
 void sumsq(const double2* x, size_t n, double* acc, cudaStream_t st);
 void bounds(double kin_max, const double* minmax_dev, const double* eig_dev, int n_eig,
-            const double* lanczos, int k, double* coef, cudaStream_t st);
+            const double* lanczos, int k, double lm_scale, double* coef, cudaStream_t st);
 void norm_guard(const double* nsq, int ndeg, int* status, cudaStream_t st);
 void scale_by_rsqrt(double2* v, size_t n, const double* nsq, cudaStream_t st);
 void lanczos_a(double2* f, const double2* v, const double2* v0, const double* beta_sq, size_t n,

@@ -26,7 +26,57 @@ struct AxisPlan {
     int n;
     int nst;
     int r[kMaxStages];  // radices in DIF order
+    int tpl;            // threads per line: max over stages of n / r (<= 32)
 };
+
+// Shared-memory position of element i of a line of length n: the low three
+// bits are XORed with the next three inside every full block of 8 elements,
+// so the power-of-two strides of the FFT stages spread over all banks.
+__host__ __device__ __forceinline__ int swz(int i, int n) {
+    return i < (n & ~7) ? (i ^ ((i >> 3) & 7)) : i;
+}
+
+// cos / sin of 2 pi e / n evaluated at compile time (Taylor series on the
+// octant-reduced angle; |error| < 1e-18): inner twiddles of composite radices.
+__host__ __device__ constexpr double taylor_cos(double x) {
+    double t = 1.0, s = 1.0;
+    for (int k = 1; k <= 12; ++k) {
+        t *= -x * x / ((2 * k - 1) * (2 * k));
+        s += t;
+    }
+    return s;
+}
+__host__ __device__ constexpr double taylor_sin(double x) {
+    double t = x, s = x;
+    for (int k = 1; k <= 12; ++k) {
+        t *= -x * x / ((2 * k) * (2 * k + 1));
+        s += t;
+    }
+    return s;
+}
+// cos(2 pi e / n) via exact reduction of e/n to the first octant
+__host__ __device__ constexpr double tw_cos(int n, int e) {
+    e = ((e % n) + n) % n;
+    // angle = 2 pi e / n = (pi/4) * (8 e / n); octant o, remainder in [0, 1)
+    const int num = 8 * e;
+    const int o = num / n;
+    const double f = (double)(num - o * n) / (double)n;  // in [0, 1)
+    const double q = 0.78539816339744830962;             // pi / 4
+    switch (o) {
+    case 0: return taylor_cos(f * q);
+    case 1: return taylor_sin((1.0 - f) * q);
+    case 2: return -taylor_sin(f * q);
+    case 3: return -taylor_cos((1.0 - f) * q);
+    case 4: return -taylor_cos(f * q);
+    case 5: return -taylor_sin((1.0 - f) * q);
+    case 6: return taylor_sin(f * q);
+    default: return taylor_cos((1.0 - f) * q);
+    }
+}
+__host__ __device__ constexpr double tw_sin(int n, int e) {
+    // sin(t) = cos(t - pi/2) = cos(2 pi (4 e - n) / (4 n))
+    return tw_cos(4 * n, 4 * e - n);
+}
 
 // r-point DFT in registers, exponent sign SIGN (+1 or -1).
 template <typename C> __device__ __forceinline__ void dft2(C* x) {
@@ -98,12 +148,62 @@ template <int SIGN, typename C> __device__ __forceinline__ void dft8(C* x) {
     }
 }
 
+template <int R, int SIGN, typename C> __device__ __forceinline__ void dft_r(C* x);
+
+// Compile-time table of exp(i 2 pi e / N), e < N.
+template <int N> struct TwTable {
+    double c[N], s[N];
+    __host__ __device__ constexpr TwTable() : c(), s() {
+        for (int e = 0; e < N; ++e) {
+            c[e] = tw_cos(N, e);
+            s[e] = tw_sin(N, e);
+        }
+    }
+};
+
+// DFT of size R1 R2 from R2 DFTs of size R1, inner twiddles, R1 DFTs of size
+// R2: input index j = R2 j1 + j2, output index k = k1 + R1 k2 (natural order).
+template <int R1, int R2, int SIGN, typename C> __device__ __forceinline__ void dft_comp(C* x) {
+    using R = typename RealOf<C>::type;
+    constexpr int N = R1 * R2;
+    constexpr TwTable<N> tab{};
+    C y[N];
+#pragma unroll
+    for (int j2 = 0; j2 < R2; ++j2) {
+        C t[R1];
+#pragma unroll
+        for (int j1 = 0; j1 < R1; ++j1) t[j1] = x[R2 * j1 + j2];
+        dft_r<R1, SIGN>(t);
+#pragma unroll
+        for (int k1 = 0; k1 < R1; ++k1) {
+            const int e = j2 * k1;
+            if (e == 0) { y[j2 * R1 + k1] = t[k1]; continue; }
+            const R c = (R)tab.c[e % N], sn = (R)(SIGN * tab.s[e % N]);
+            y[j2 * R1 + k1] = mk(t[k1].x * c - t[k1].y * sn, t[k1].x * sn + t[k1].y * c);
+        }
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) {
+        C t[R2];
+#pragma unroll
+        for (int j2 = 0; j2 < R2; ++j2) t[j2] = y[j2 * R1 + k1];
+        dft_r<R2, SIGN>(t);
+#pragma unroll
+        for (int k2 = 0; k2 < R2; ++k2) x[k1 + R1 * k2] = t[k2];
+    }
+}
+
 template <int R, int SIGN, typename C> __device__ __forceinline__ void dft_r(C* x) {
     if constexpr (R == 2) dft2(x);
     else if constexpr (R == 3) dft3<SIGN>(x);
     else if constexpr (R == 4) dft4<SIGN>(x);
     else if constexpr (R == 5) dft5<SIGN>(x);
     else if constexpr (R == 8) dft8<SIGN>(x);
+    else if constexpr (R == 6) dft_comp<2, 3, SIGN>(x);
+    else if constexpr (R == 9) dft_comp<3, 3, SIGN>(x);
+    else if constexpr (R == 10) dft_comp<2, 5, SIGN>(x);
+    else if constexpr (R == 12) dft_comp<4, 3, SIGN>(x);
+    else if constexpr (R == 15) dft_comp<3, 5, SIGN>(x);
 }
 
 // One DIF (FWD=true, sign -1) or DIT (FWD=false, sign +1) stage of radix R
@@ -120,11 +220,11 @@ __device__ __forceinline__ void fft_stage(C* s, int nlines, LineBase lb, int es,
         const int v = u - l * nb;
         const int blk = v / S;
         const int n1 = v - blk * S;
-        C* p = s + lb(l) + (blk * B + n1) * es;
-        const int se = S * es;
+        C* line = s + lb(l);
+        const int e0 = blk * B + n1;
         C x[R];
 #pragma unroll
-        for (int j = 0; j < R; ++j) x[j] = p[j * se];
+        for (int j = 0; j < R; ++j) x[j] = line[swz(e0 + j * S, n) * es];
         const int e = step * n1;
         if (FWD) {
             dft_r<R, -1>(x);
@@ -136,7 +236,7 @@ __device__ __forceinline__ void fft_stage(C* s, int nlines, LineBase lb, int es,
             dft_r<R, 1>(x);
         }
 #pragma unroll
-        for (int m = 0; m < R; ++m) p[m * se] = x[m];
+        for (int m = 0; m < R; ++m) line[swz(e0 + m * S, n) * es] = x[m];
     }
 }
 
@@ -148,7 +248,12 @@ __device__ __forceinline__ void fft_dispatch(int r, C* s, int nlines, LineBase l
     case 3: fft_stage<3, FWD>(s, nlines, lb, es, n, B, tw); break;
     case 4: fft_stage<4, FWD>(s, nlines, lb, es, n, B, tw); break;
     case 5: fft_stage<5, FWD>(s, nlines, lb, es, n, B, tw); break;
+    case 6: fft_stage<6, FWD>(s, nlines, lb, es, n, B, tw); break;
     case 8: fft_stage<8, FWD>(s, nlines, lb, es, n, B, tw); break;
+    case 9: fft_stage<9, FWD>(s, nlines, lb, es, n, B, tw); break;
+    case 10: fft_stage<10, FWD>(s, nlines, lb, es, n, B, tw); break;
+    case 12: fft_stage<12, FWD>(s, nlines, lb, es, n, B, tw); break;
+    case 15: fft_stage<15, FWD>(s, nlines, lb, es, n, B, tw); break;
     default: break;
     }
 }
@@ -178,9 +283,120 @@ __device__ __forceinline__ void fft_inverse(C* s, int nlines, LineBase lb, int e
     }
 }
 
+// One butterfly (index v of the stage) of a DIF or DIT stage on one line.
+template <int R, bool FWD, typename C>
+__device__ __forceinline__ void butterfly(C* line, int v, int es, int n, int B, const C* tw) {
+    const int S = B / R;
+    const int blk = v / S;
+    const int n1 = v - blk * S;
+    const int e0 = blk * B + n1;
+    C x[R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) x[j] = line[swz(e0 + j * S, n) * es];
+    const int e = (n / B) * n1;
+    if (FWD) {
+        dft_r<R, -1>(x);
+#pragma unroll
+        for (int m = 1; m < R; ++m) x[m] = cmulc(tw[e * m], x[m]);
+    } else {
+#pragma unroll
+        for (int m = 1; m < R; ++m) x[m] = cmul(tw[e * m], x[m]);
+        dft_r<R, 1>(x);
+    }
+#pragma unroll
+    for (int m = 0; m < R; ++m) line[swz(e0 + m * S, n) * es] = x[m];
+}
+
+template <bool FWD, typename C>
+__device__ __forceinline__ void butterfly_dispatch(int r, C* line, int v, int es, int n, int B,
+                                                   const C* tw) {
+    switch (r) {
+    case 2: butterfly<2, FWD>(line, v, es, n, B, tw); break;
+    case 3: butterfly<3, FWD>(line, v, es, n, B, tw); break;
+    case 4: butterfly<4, FWD>(line, v, es, n, B, tw); break;
+    case 5: butterfly<5, FWD>(line, v, es, n, B, tw); break;
+    case 6: butterfly<6, FWD>(line, v, es, n, B, tw); break;
+    case 8: butterfly<8, FWD>(line, v, es, n, B, tw); break;
+    case 9: butterfly<9, FWD>(line, v, es, n, B, tw); break;
+    case 10: butterfly<10, FWD>(line, v, es, n, B, tw); break;
+    case 12: butterfly<12, FWD>(line, v, es, n, B, tw); break;
+    case 15: butterfly<15, FWD>(line, v, es, n, B, tw); break;
+    default: break;
+    }
+}
+
+// Transform of one line by a group of P.tpl lanes of one warp (lane index i
+// within the group); stages are separated by __syncwarp only.  Every lane of
+// the warp must call this the same number of times (act = false: idle).
+template <bool FWD, typename C>
+__device__ __forceinline__ void line_fft_group(C* line, bool act, int i, int es, const AxisPlan& P,
+                                               const C* tw) {
+    if (FWD) {
+        int B = P.n;
+        for (int t = 0; t < P.nst; ++t) {
+            const int r = P.r[t];
+            if (act && i < P.n / r) butterfly_dispatch<true>(r, line, i, es, P.n, B, tw);
+            __syncwarp();
+            B /= r;
+        }
+    } else {
+        int S = 1;
+        for (int t = P.nst - 1; t >= 0; --t) {
+            const int r = P.r[t];
+            const int B = S * r;
+            if (act && i < P.n / r) butterfly_dispatch<false>(r, line, i, es, P.n, B, tw);
+            __syncwarp();
+            S = B;
+        }
+    }
+}
+
+// Lane groups of a CTA: groups of P.tpl lanes inside each warp.
+struct LaneGroups {
+    int g;        // group index within the warp
+    int i;        // lane index within the group
+    int per_warp; // groups per warp
+    int total;    // groups in the CTA
+    int id;       // CTA-wide group id (valid when in_group)
+    bool in_group;
+    __device__ __forceinline__ explicit LaneGroups(int tpl) {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        per_warp = 32 / tpl;
+        g = lane / tpl;
+        i = lane - g * tpl;
+        in_group = g < per_warp;
+        total = (blockDim.x >> 5) * per_warp;
+        id = warp * per_warp + g;
+    }
+};
+
+// Transform nlines lines with lane groups; ends with __syncthreads.
+template <bool FWD, typename C, class LineBase>
+__device__ __forceinline__ void fft_lines_grouped(C* s, int nlines, LineBase lb, int es,
+                                                  const AxisPlan& P, const C* tw) {
+    if (P.tpl > 32) {  // a line needs more than one warp: CTA-wide stages
+        if (FWD) fft_forward(s, nlines, lb, es, P, tw);
+        else fft_inverse(s, nlines, lb, es, P, tw);
+        return;
+    }
+    const LaneGroups lg(P.tpl);
+    const int rounds = (nlines + lg.total - 1) / lg.total;
+    for (int rd = 0; rd < rounds; ++rd) {
+        const int l = rd * lg.total + lg.id;
+        const bool act = lg.in_group && l < nlines;
+        line_fft_group<FWD>(act ? s + lb(l) : s, act, lg.i, es, P, tw);
+    }
+    __syncthreads();
+}
+
 struct LinesStrided {
     int ls;
     __device__ __forceinline__ int operator()(int l) const { return l * ls; }
+};
+// line l starts at row swz(l) of a plane whose rows are swizzled too
+struct LinesStridedSwz {
+    int ls, n;
+    __device__ __forceinline__ int operator()(int l) const { return swz(l, n) * ls; }
 };
 struct LinesListed {
     const int* list;

@@ -282,27 +282,29 @@ __device__ __forceinline__ void split3(float v, __nv_bfloat16& h1, __nv_bfloat16
     h3 = __float2bfloat16_rn(r2);
 }
 
-template <typename CIn, bool DOUBLED, bool CONJ_T>
+// SRC: 0 element (r, k) = x[r][k]; 1 = conj(x[k][r]); 2 = x[k][r]
+template <typename CIn, bool DOUBLED, int SRC>
 __global__ void k_pack3(const CIn* __restrict__ x, long long ldx, int rows, int K, int kp,
                         __nv_bfloat16* __restrict__ p0, __nv_bfloat16* __restrict__ p1,
                         __nv_bfloat16* __restrict__ p2) {
     // DOUBLED: output rows 2r, 2r+1 per input row (conj-first operand)
-    // CONJ_T:  input element (r, k) is read as conj(x[k][r]) (transposed source)
     const long long kc = kp / 2;  // complex columns incl. padding
     const long long tot = (long long)rows * kc;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
          t += (long long)gridDim.x * blockDim.x) {
-        const int r = (int)(t / kc), k = (int)(t % kc);
+        int r, k;
+        if (SRC == 0) { r = (int)(t / kc); k = (int)(t % kc); }
+        else { k = (int)(t / rows); r = (int)(t % rows); }  // coalesced reads of x[k][*]
         float re = 0.f, im = 0.f;
         if (k < K) {
-            if (CONJ_T) {
-                const CIn v = x[(long long)k * ldx + r];
-                re = (float)v.x;
-                im = -(float)v.y;
-            } else {
+            if (SRC == 0) {
                 const CIn v = x[(long long)r * ldx + k];
                 re = (float)v.x;
                 im = (float)v.y;
+            } else {
+                const CIn v = x[(long long)k * ldx + r];
+                re = (float)v.x;
+                im = SRC == 1 ? -(float)v.y : (float)v.y;
             }
         }
         __nv_bfloat16 a1, a2, a3, b1, b2, b3;
@@ -311,11 +313,10 @@ __global__ void k_pack3(const CIn* __restrict__ x, long long ldx, int rows, int 
         if (DOUBLED) {
             const long long o0 = (2LL * r) * kp + 2 * k, o1 = (2LL * r + 1) * kp + 2 * k;
             p0[o0] = a1; p0[o0 + 1] = b1; p1[o0] = a2; p1[o0 + 1] = b2; p2[o0] = a3; p2[o0 + 1] = b3;
-            const __nv_bfloat16 z = __float2bfloat16_rn(0.f);
             // (-im, re)
-            p0[o1] = __hsub(z, b1); p0[o1 + 1] = a1;
-            p1[o1] = __hsub(z, b2); p1[o1 + 1] = a2;
-            p2[o1] = __hsub(z, b3); p2[o1 + 1] = a3;
+            p0[o1] = __hneg(b1); p0[o1 + 1] = a1;
+            p1[o1] = __hneg(b2); p1[o1 + 1] = a2;
+            p2[o1] = __hneg(b3); p2[o1 + 1] = a3;
         } else {
             const long long o = (long long)r * kp + 2 * k;
             p0[o] = a1; p0[o + 1] = b1; p1[o] = a2; p1[o + 1] = b2; p2[o] = a3; p2[o + 1] = b3;
@@ -398,7 +399,7 @@ size_t tc_partial_floats(int M, int N, int K) {
 }
 
 template <typename CIn>
-void tc_pack(const CIn* x, long long ldx, int rows, int K, bool doubled, bool conj_transposed,
+void tc_pack(const CIn* x, long long ldx, int rows, int K, bool doubled, int src,
              TcPlanes& planes, cudaStream_t st) {
     count_launch();
     const int kp = tc_kpad(K);
@@ -407,13 +408,17 @@ void tc_pack(const CIn* x, long long ldx, int rows, int K, bool doubled, bool co
     __nv_bfloat16* p2 = (__nv_bfloat16*)planes.p[2];
     const long long tot = (long long)rows * (kp / 2);
     const int g = grid_for(tot);
+#define CHFSI_PACK(D, S) k_pack3<CIn, D, S><<<g, 256, 0, st>>>(x, ldx, rows, K, kp, p0, p1, p2)
     if (doubled) {
-        if (conj_transposed) k_pack3<CIn, true, true><<<g, 256, 0, st>>>(x, ldx, rows, K, kp, p0, p1, p2);
-        else k_pack3<CIn, true, false><<<g, 256, 0, st>>>(x, ldx, rows, K, kp, p0, p1, p2);
+        if (src == kSrcConjT) CHFSI_PACK(true, 1);
+        else if (src == kSrcT) CHFSI_PACK(true, 2);
+        else CHFSI_PACK(true, 0);
     } else {
-        if (conj_transposed) k_pack3<CIn, false, true><<<g, 256, 0, st>>>(x, ldx, rows, K, kp, p0, p1, p2);
-        else k_pack3<CIn, false, false><<<g, 256, 0, st>>>(x, ldx, rows, K, kp, p0, p1, p2);
+        if (src == kSrcConjT) CHFSI_PACK(false, 1);
+        else if (src == kSrcT) CHFSI_PACK(false, 2);
+        else CHFSI_PACK(false, 0);
     }
+#undef CHFSI_PACK
     planes.rows = doubled ? 2 * rows : rows;
     planes.kp = kp;
 }
@@ -465,7 +470,7 @@ cudaError_t tc_gemm(const TcPlanes& a, const TcPlanes& b, int M, int N, int K, i
     return cudaGetLastError();
 }
 
-template void tc_pack<double2>(const double2*, long long, int, int, bool, bool, TcPlanes&, cudaStream_t);
-template void tc_pack<float2>(const float2*, long long, int, int, bool, bool, TcPlanes&, cudaStream_t);
+template void tc_pack<double2>(const double2*, long long, int, int, bool, int, TcPlanes&, cudaStream_t);
+template void tc_pack<float2>(const float2*, long long, int, int, bool, int, TcPlanes&, cudaStream_t);
 
 }  // namespace chfsi

@@ -23,11 +23,12 @@ int tc_rows_alloc(int rows, bool a_operand, int n_for_b);
 // scratch floats for kTcOutPartial of an M x N x K complex product
 size_t tc_partial_floats(int M, int N, int K);
 
+// Source element (r, k) of a packed operand: x[r][k], conj(x[k][r]) or x[k][r].
+enum { kSrcPlain = 0, kSrcConjT = 1, kSrcT = 2 };
 // Split rows of a complex matrix into bf16 planes.  doubled: conj-first
-// operand layout (2 rows per complex row); conj_transposed: element (r, k)
-// is conj(x[k][r]).
+// operand layout (2 rows per complex row).
 template <typename CIn>
-void tc_pack(const CIn* x, long long ldx, int rows, int K, bool doubled, bool conj_transposed,
+void tc_pack(const CIn* x, long long ldx, int rows, int K, bool doubled, int src,
              TcPlanes& planes, cudaStream_t st);
 
 // C[m][n] = sum_k conj(A[m][k]) B[n][k]; a: doubled planes (2M rows),

@@ -73,13 +73,13 @@ k_zsticks_inverse(const C* __restrict__ psi, int ldp, C* __restrict__ work, HGeo
     const int g0 = g.col_start[c0], g1 = g.col_start[c1];
     const C* pb = psi + (size_t)b * ldp;
     for (int q = g0 + threadIdx.x; q < g1; q += blockDim.x)
-        lines[(g.pw_col[q] - c0) * g.lsz + g.pw_zpos[q]] = pb[q];
+        lines[(g.pw_col[q] - c0) * g.lsz + swz(g.pw_zpos[q], g.nz)] = pb[q];
     __syncthreads();
-    fft_inverse(lines, nl, LinesStrided{g.lsz}, 1, g.az, tw);
+    fft_lines_grouped<false>(lines, nl, LinesStrided{g.lsz}, 1, g.az, tw);
     C* wb = work + (size_t)b * g.nz * g.ncol;
     for (int u = threadIdx.x; u < g.nz * kColsPerBlock; u += blockDim.x) {
         const int z = u / kColsPerBlock, cl = u - z * kColsPerBlock;
-        if (cl < nl) wb[(size_t)z * g.ncol + c0 + cl] = lines[cl * g.lsz + z];
+        if (cl < nl) wb[(size_t)z * g.ncol + c0 + cl] = lines[cl * g.lsz + swz(z, g.nz)];
     }
 }
 
@@ -101,18 +101,31 @@ k_planes_vloc(C* __restrict__ work, const double* __restrict__ veff, HGeom g) {
     C* wp = work + ((size_t)b * g.nz + z) * g.ncol;
     for (int c = threadIdx.x; c < g.ncol; c += blockDim.x) plane[g.col_pos[c]] = wp[c];
     __syncthreads();
-    fft_inverse(plane, g.nxact, LinesListed{xl}, g.lsx, g.ay, twy);
-    fft_inverse(plane, g.ny, LinesStrided{g.lsx}, 1, g.ax, twx);
+    fft_lines_grouped<false>(plane, g.nxact, LinesListed{xl}, g.lsx, g.ay, twy);
+    // x rows: inverse, x V(r), forward, all inside one lane group per row
     const double* vz = veff + (size_t)z * g.nx * g.ny;
     using R = typename RealOf<C>::type;
-    for (int i = threadIdx.x; i < g.nx * g.ny; i += blockDim.x) {
-        const int y = i / g.nx, x = i - y * g.nx;
-        C& v = plane[y * g.lsx + x];
-        v = cscale(v, (R)vz[i]);
+    {
+        const LaneGroups lg(g.ax.tpl);
+        const int rounds = (g.ny + lg.total - 1) / lg.total;
+        for (int rd = 0; rd < rounds; ++rd) {
+            const int y = rd * lg.total + lg.id;
+            const bool act = lg.in_group && y < g.ny;
+            C* row = plane + (act ? swz(y, g.ny) * g.lsx : 0);
+            line_fft_group<false>(row, act, lg.i, 1, g.ax, twx);
+            if (act) {
+                const double* vr = vz + (size_t)y * g.nx;
+                for (int x = lg.i; x < g.nx; x += g.ax.tpl) {
+                    C& e = row[swz(x, g.nx)];
+                    e = cscale(e, (R)vr[x]);
+                }
+            }
+            __syncwarp();
+            line_fft_group<true>(row, act, lg.i, 1, g.ax, twx);
+        }
     }
     __syncthreads();
-    fft_forward(plane, g.ny, LinesStrided{g.lsx}, 1, g.ax, twx);
-    fft_forward(plane, g.nxact, LinesListed{xl}, g.lsx, g.ay, twy);
+    fft_lines_grouped<true>(plane, g.nxact, LinesListed{xl}, g.lsx, g.ay, twy);
     for (int c = threadIdx.x; c < g.ncol; c += blockDim.x) wp[c] = plane[g.col_pos[c]];
 }
 
@@ -134,10 +147,10 @@ k_zsticks_forward(const C* __restrict__ work, const C* __restrict__ psi, int ldp
     const C* wb = work + (size_t)b * g.nz * g.ncol;
     for (int u = threadIdx.x; u < g.nz * kColsPerBlock; u += blockDim.x) {
         const int z = u / kColsPerBlock, cl = u - z * kColsPerBlock;
-        lines[cl * g.lsz + z] = cl < nl ? wb[(size_t)z * g.ncol + c0 + cl] : czero<C>();
+        lines[cl * g.lsz + swz(z, g.nz)] = cl < nl ? wb[(size_t)z * g.ncol + c0 + cl] : czero<C>();
     }
     __syncthreads();
-    fft_forward(lines, nl, LinesStrided{g.lsz}, 1, g.az, tw);
+    fft_lines_grouped<true>(lines, nl, LinesStrided{g.lsz}, 1, g.az, tw);
     const int g0 = g.col_start[c0], g1 = g.col_start[c1];
     const C* pb = psi + (size_t)b * ldp;
     C* ob = out + (size_t)b * ldo;
@@ -150,7 +163,7 @@ k_zsticks_forward(const C* __restrict__ work, const C* __restrict__ psi, int ldp
     const R inv_n = (R)e.inv_n;
     double nacc = 0.0;
     for (int q = g0 + threadIdx.x; q < g1; q += blockDim.x) {
-        const C v = lines[(g.pw_col[q] - c0) * g.lsz + g.pw_zpos[q]];
+        const C v = lines[(g.pw_col[q] - c0) * g.lsz + swz(g.pw_zpos[q], g.nz)];
         const C p = pb[q];
         const R k = (R)e.kin[q];
         C h = mk(p.x * k, p.y * k);
@@ -203,14 +216,14 @@ k_planes_density(const C* __restrict__ work, const double* __restrict__ occ, int
         const C* wp = work + ((size_t)b * g.nz + z) * g.ncol;
         for (int c = threadIdx.x; c < g.ncol; c += blockDim.x) plane[g.col_pos[c]] = wp[c];
         __syncthreads();
-        fft_inverse(plane, g.nxact, LinesListed{xl}, g.lsx, g.ay, twy);
-        fft_inverse(plane, g.ny, LinesStrided{g.lsx}, 1, g.ax, twx);
+        fft_lines_grouped<false>(plane, g.nxact, LinesListed{xl}, g.lsx, g.ay, twy);
+        fft_lines_grouped<false>(plane, g.ny, LinesStridedSwz{g.lsx, g.ny}, 1, g.ax, twx);
 #pragma unroll
         for (int k = 0; k < MAXPT; ++k) {
             const int i = threadIdx.x + k * blockDim.x;
             if (i < npl) {
                 const int y = i / g.nx, x = i - y * g.nx;
-                const C v = plane[y * g.lsx + x];
+                const C v = plane[swz(y, g.ny) * g.lsx + swz(x, g.nx)];
                 acc[k] += f * ((double)v.x * v.x + (double)v.y * v.y);
             }
         }
@@ -257,16 +270,16 @@ k_axis_fft(C* data, int nx, int ny, int nz, int axis, AxisPlan P, int lb) {
         int l, j;
         if (axis == 0) { l = u / n; j = u - l * n; }
         else { j = u / lb; l = u - j * lb; }
-        lines[l * ls + j] = l < nl ? data[base + l * lstride + j * estride] : czero<C>();
+        lines[l * ls + swz(j, n)] = l < nl ? data[base + l * lstride + j * estride] : czero<C>();
     }
     __syncthreads();
-    if (FWD) fft_forward(lines, nl, LinesStrided{ls}, 1, P, tw);
-    else fft_inverse(lines, nl, LinesStrided{ls}, 1, P, tw);
+    if (FWD) fft_lines_grouped<true>(lines, nl, LinesStrided{ls}, 1, P, tw);
+    else fft_lines_grouped<false>(lines, nl, LinesStrided{ls}, 1, P, tw);
     for (int u = threadIdx.x; u < lb * n; u += blockDim.x) {
         int l, j;
         if (axis == 0) { l = u / n; j = u - l * n; }
         else { j = u / lb; l = u - j * lb; }
-        if (l < nl) data[base + l * lstride + j * estride] = lines[l * ls + j];
+        if (l < nl) data[base + l * lstride + j * estride] = lines[l * ls + swz(j, n)];
     }
 }
 

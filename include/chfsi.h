@@ -181,6 +181,13 @@ chfsi_status chfsi_set_basis(chfsi_ctx* ctx, const int32_t* miller, const double
                              double gmax);
 chfsi_status chfsi_set_projectors(chfsi_ctx* ctx, const chfsi_c128* beta,
                                   const int32_t* proj_offsets, const chfsi_c128* dmat);
+/* Ultrasoft overlap S = 1 + sum_I beta q_I beta^H (per-ion q blocks, layout of
+ * dmat): the filter then runs on S^-1 H (Woodbury inverse) and Rayleigh-Ritz
+ * solves H x = e S x with S_sub = psi^H S psi.  FP64 contexts only.  The GPU
+ * ChFSI of the reference ignores S (it has no generalised path). */
+chfsi_status chfsi_set_qmat(chfsi_ctx* ctx, const chfsi_c128* qmat);
+/* Lower bound of the spectrum of S used to scale the filter's upper bound. */
+chfsi_status chfsi_get_s_min(chfsi_ctx* ctx, double* out);
 chfsi_status chfsi_set_veff(chfsi_ctx* ctx, const double* veff);
 chfsi_status chfsi_set_psi(chfsi_ctx* ctx, const chfsi_c128* psi);
 chfsi_status chfsi_get_psi(chfsi_ctx* ctx, chfsi_c128* psi);
@@ -262,11 +269,15 @@ typedef struct chfsi_scf_params {
     int    max_hist;      /* Pulay history length, 1..8 (1 = linear mixing)     */
     int    first_passes;  /* filter + Rayleigh-Ritz passes in the first step    */
     double kT;            /* Fermi-Dirac smearing (Ha); <= 0: fixed aufbau occupations */
+    double fp64_switch_per_atom; /* mixed precision: switch the filter to FP64 once
+                                    |dE|/atom < this (convergence is only declared on
+                                    FP64 steps)                                        */
 } chfsi_scf_params;
 
 typedef struct chfsi_scf_result {
     int     status;       /* CHFSI_OK (converged), CHFSI_NOT_CONVERGED or error */
     int     n_iter;
+    int     n_iter_mixed; /* iterations whose filter ran in mixed precision       */
     double  e_total;      /* free energy: sum f eps - int (V_H+V_xc)[in] rho_out
                              + E_H + E_xc + E_ion-ion - kT S                    */
     double  e_band, e_hartree, e_xc, e_dc, e_entropy, mu;

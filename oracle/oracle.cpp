@@ -330,6 +330,11 @@ struct OracleCtx {
     std::vector<double> bounds;   // lambda_max, cut, c, e
     std::vector<double> norms;    // |psi_k| per degree
     int bound_mode = 0, lanczos_steps = 10;
+    // ultrasoft overlap S = 1 + beta q beta^H (per-ion q blocks, same layout as D)
+    bool uspp = false;
+    std::vector<cplx> qmat;
+    std::vector<cplx> sinv_m;  // M = q (1 + B q)^-1, B = beta^H beta: S^-1 = 1 - beta M beta^H
+    double s_min = 1.0;        // lower bound of the spectrum of S
     // density / mixing state
     std::vector<double> rho_in, rho_out;
     std::vector<std::vector<double>> hist_rho, hist_res;
@@ -338,6 +343,109 @@ struct OracleCtx {
 };
 
 namespace {
+
+// out += beta Blk beta^H x for per-ion blocks Blk (D or q), nb vectors.
+void add_beta_blocks(const OracleCtx& c, const std::vector<cplx>& blocks, const cplx* x, cplx* out,
+                     int nb) {
+    if (c.n_proj == 0) return;
+    std::vector<cplx> cp((size_t)c.n_proj * nb), cd((size_t)c.n_proj * nb);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int p = 0; p < c.n_proj; ++p)
+        for (int b = 0; b < nb; ++b) {
+            const cplx* bp = &c.beta[(size_t)p * c.n_pw];
+            const cplx* ps = x + (size_t)b * c.n_pw;
+            cplx s = 0.0;
+            for (int g = 0; g < c.n_pw; ++g) s += std::conj(bp[g]) * ps[g];
+            cp[(size_t)p * nb + b] = s;
+        }
+    for (int ion = 0; ion < c.n_ions; ++ion) {
+        int p0 = c.poff[ion], ne = c.poff[ion + 1] - p0;
+        const cplx* D = &blocks[c.dmat_off[ion]];
+        for (int i = 0; i < ne; ++i)
+            for (int b = 0; b < nb; ++b) {
+                cplx s = 0.0;
+                for (int j = 0; j < ne; ++j) s += D[i * ne + j] * cp[(size_t)(p0 + j) * nb + b];
+                cd[(size_t)(p0 + i) * nb + b] = s;
+            }
+    }
+#pragma omp parallel for schedule(static)
+    for (int b = 0; b < nb; ++b) {
+        cplx* h = out + (size_t)b * c.n_pw;
+        for (int g = 0; g < c.n_pw; ++g) {
+            cplx s = 0.0;
+            for (int p = 0; p < c.n_proj; ++p) s += c.beta[(size_t)p * c.n_pw + g] * cd[(size_t)p * nb + b];
+            h[g] += s;
+        }
+    }
+}
+
+// y = S x = x + beta q beta^H x
+void apply_s(const OracleCtx& c, const cplx* x, cplx* y, int nb) {
+    std::memcpy(y, x, sizeof(cplx) * (size_t)nb * c.n_pw);
+    if (c.uspp) add_beta_blocks(c, c.qmat, x, y, nb);
+}
+
+// y = S^-1 x = x - beta M beta^H x  (Woodbury with M = q (1 + B q)^-1)
+void apply_sinv(const OracleCtx& c, const cplx* x, cplx* y, int nb) {
+    std::memcpy(y, x, sizeof(cplx) * (size_t)nb * c.n_pw);
+    if (!c.uspp || c.n_proj == 0) return;
+    const int np = c.n_proj;
+    std::vector<cplx> cp((size_t)np * nb), cm((size_t)np * nb, 0.0);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int p = 0; p < np; ++p)
+        for (int b = 0; b < nb; ++b) {
+            const cplx* bp = &c.beta[(size_t)p * c.n_pw];
+            const cplx* ps = x + (size_t)b * c.n_pw;
+            cplx s = 0.0;
+            for (int g = 0; g < c.n_pw; ++g) s += std::conj(bp[g]) * ps[g];
+            cp[(size_t)p * nb + b] = s;
+        }
+    for (int p = 0; p < np; ++p)
+        for (int q = 0; q < np; ++q) {
+            const cplx m = c.sinv_m[(size_t)p * np + q];
+            if (m == 0.0) continue;
+            for (int b = 0; b < nb; ++b) cm[(size_t)p * nb + b] += m * cp[(size_t)q * nb + b];
+        }
+#pragma omp parallel for schedule(static)
+    for (int b = 0; b < nb; ++b) {
+        cplx* h = y + (size_t)b * c.n_pw;
+        for (int g = 0; g < c.n_pw; ++g) {
+            cplx s = 0.0;
+            for (int p = 0; p < np; ++p) s += c.beta[(size_t)p * c.n_pw + g] * cm[(size_t)p * nb + b];
+            h[g] -= s;
+        }
+    }
+}
+
+// Inverse of a dense complex matrix by Gauss-Jordan with partial pivoting.
+bool invert(std::vector<cplx>& a, int n) {
+    std::vector<cplx> inv((size_t)n * n, 0.0);
+    for (int i = 0; i < n; ++i) inv[(size_t)i * n + i] = 1.0;
+    for (int col = 0; col < n; ++col) {
+        int piv = col;
+        for (int r = col + 1; r < n; ++r)
+            if (std::abs(a[(size_t)r * n + col]) > std::abs(a[(size_t)piv * n + col])) piv = r;
+        if (std::abs(a[(size_t)piv * n + col]) == 0.0) return false;
+        if (piv != col)
+            for (int k = 0; k < n; ++k) {
+                std::swap(a[(size_t)col * n + k], a[(size_t)piv * n + k]);
+                std::swap(inv[(size_t)col * n + k], inv[(size_t)piv * n + k]);
+            }
+        const cplx d = a[(size_t)col * n + col];
+        for (int k = 0; k < n; ++k) { a[(size_t)col * n + k] /= d; inv[(size_t)col * n + k] /= d; }
+        for (int r = 0; r < n; ++r) {
+            if (r == col) continue;
+            const cplx f = a[(size_t)r * n + col];
+            if (f == 0.0) continue;
+            for (int k = 0; k < n; ++k) {
+                a[(size_t)r * n + k] -= f * a[(size_t)col * n + k];
+                inv[(size_t)r * n + k] -= f * inv[(size_t)col * n + k];
+            }
+        }
+    }
+    a.swap(inv);
+    return true;
+}
 
 // H|psi> = T psi + (1/N^3) FFT[-1]( V .* FFT[+1](scatter psi) ) + beta D beta^H psi
 // Order of operations follows apply_v_loc_hamiltonian (chebyshev.rs:279-365):
@@ -363,36 +471,7 @@ void apply_h(const OracleCtx& c, const cplx* psi, cplx* hpsi, int nb) {
             for (int g = 0; g < c.n_pw; ++g) h[g] += grid[c.fft_idx[g]] * inv_n;
         }
     }
-    if (c.n_proj == 0) return;
-    std::vector<cplx> cp((size_t)c.n_proj * nb), cd((size_t)c.n_proj * nb);
-#pragma omp parallel for collapse(2) schedule(static)
-    for (int p = 0; p < c.n_proj; ++p)
-        for (int b = 0; b < nb; ++b) {
-            const cplx* bp = &c.beta[(size_t)p * c.n_pw];
-            const cplx* ps = psi + (size_t)b * c.n_pw;
-            cplx s = 0.0;
-            for (int g = 0; g < c.n_pw; ++g) s += std::conj(bp[g]) * ps[g];
-            cp[(size_t)p * nb + b] = s;
-        }
-    for (int ion = 0; ion < c.n_ions; ++ion) {
-        int p0 = c.poff[ion], ne = c.poff[ion + 1] - p0;
-        const cplx* D = &c.dmat[c.dmat_off[ion]];
-        for (int i = 0; i < ne; ++i)
-            for (int b = 0; b < nb; ++b) {
-                cplx s = 0.0;
-                for (int j = 0; j < ne; ++j) s += D[i * ne + j] * cp[(size_t)(p0 + j) * nb + b];
-                cd[(size_t)(p0 + i) * nb + b] = s;
-            }
-    }
-#pragma omp parallel for schedule(static)
-    for (int b = 0; b < nb; ++b) {
-        cplx* h = hpsi + (size_t)b * c.n_pw;
-        for (int g = 0; g < c.n_pw; ++g) {
-            cplx s = 0.0;
-            for (int p = 0; p < c.n_proj; ++p) s += c.beta[(size_t)p * c.n_pw + g] * cd[(size_t)p * nb + b];
-            h[g] += s;
-        }
-    }
+    add_beta_blocks(c, c.dmat, psi, hpsi, nb);
 }
 
 double frob_norm(const std::vector<cplx>& x) {
@@ -556,6 +635,69 @@ void oracle_set_num_threads(int n) {
 }
 
 void oracle_set_veff(OracleCtx* c, const double* v) { c->veff.assign(v, v + c->ng()); }
+
+// Ultrasoft overlap: per-ion q blocks (layout of D).  Builds the Woodbury
+// factor M = q (1 + B q)^-1 with B = beta^H beta and the lower bound
+// s_min = 1 - max_i sum_j |(q B)_ij| of the spectrum of S.  Returns 0 or -6.
+int oracle_set_qmat(OracleCtx* c, const double* qmat) {
+    const int np = c->n_proj;
+    c->qmat.assign(c->dmat.size(), 0.0);
+    if (np == 0) return -6;
+    std::memcpy(c->qmat.data(), qmat, sizeof(cplx) * c->qmat.size());
+    std::vector<cplx> Q((size_t)np * np, 0.0), B((size_t)np * np), QB((size_t)np * np, 0.0);
+    for (int ion = 0; ion < c->n_ions; ++ion) {
+        const int p0 = c->poff[ion], ne = c->poff[ion + 1] - p0;
+        for (int i = 0; i < ne; ++i)
+            for (int j = 0; j < ne; ++j) Q[(size_t)(p0 + i) * np + p0 + j] = c->qmat[c->dmat_off[ion] + i * ne + j];
+    }
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int p = 0; p < np; ++p)
+        for (int q = 0; q < np; ++q) {
+            cplx s = 0.0;
+            for (int g = 0; g < c->n_pw; ++g) s += std::conj(c->beta[(size_t)p * c->n_pw + g]) * c->beta[(size_t)q * c->n_pw + g];
+            B[(size_t)p * np + q] = s;
+        }
+    for (int i = 0; i < np; ++i)
+        for (int k = 0; k < np; ++k) {
+            const cplx qik = Q[(size_t)i * np + k];
+            if (qik == 0.0) continue;
+            for (int j = 0; j < np; ++j) QB[(size_t)i * np + j] += qik * B[(size_t)k * np + j];
+        }
+    double rs = 0.0;
+    for (int i = 0; i < np; ++i) {
+        double r = 0.0;
+        for (int j = 0; j < np; ++j) r += std::abs(QB[(size_t)i * np + j]);
+        rs = std::max(rs, r);
+    }
+    c->s_min = std::max(0.1, 1.0 - rs);
+    // (1 + B q)^-1
+    std::vector<cplx> A((size_t)np * np, 0.0);
+    for (int i = 0; i < np; ++i)
+        for (int k = 0; k < np; ++k) {
+            const cplx bik = B[(size_t)i * np + k];
+            if (bik == 0.0) continue;
+            for (int j = 0; j < np; ++j) A[(size_t)i * np + j] += bik * Q[(size_t)k * np + j];
+        }
+    for (int i = 0; i < np; ++i) A[(size_t)i * np + i] += 1.0;
+    if (!invert(A, np)) return -6;
+    c->sinv_m.assign((size_t)np * np, 0.0);
+    for (int i = 0; i < np; ++i)
+        for (int k = 0; k < np; ++k) {
+            const cplx qik = Q[(size_t)i * np + k];
+            if (qik == 0.0) continue;
+            for (int j = 0; j < np; ++j) c->sinv_m[(size_t)i * np + j] += qik * A[(size_t)k * np + j];
+        }
+    c->uspp = true;
+    return 0;
+}
+
+void oracle_apply_s(OracleCtx* c, const double* x, double* y, int nb) {
+    apply_s(*c, reinterpret_cast<const cplx*>(x), reinterpret_cast<cplx*>(y), nb);
+}
+void oracle_apply_sinv(OracleCtx* c, const double* x, double* y, int nb) {
+    apply_sinv(*c, reinterpret_cast<const cplx*>(x), reinterpret_cast<cplx*>(y), nb);
+}
+double oracle_s_min(OracleCtx* c) { return c->s_min; }
 void oracle_get_veff(OracleCtx* c, double* v) { std::memcpy(v, c->veff.data(), sizeof(double) * c->ng()); }
 void oracle_get_vloc_r(OracleCtx* c, double* v) { std::memcpy(v, c->vloc_r.data(), sizeof(double) * c->ng()); }
 void oracle_set_psi(OracleCtx* c, const double* p) { std::memcpy(c->psi.data(), p, sizeof(cplx) * c->psi.size()); }
@@ -587,6 +729,8 @@ void oracle_spectral_bounds(OracleCtx* c, const double* eig, int n_eig, double* 
     double lm;
     if (c->bound_mode == 1) lm = lanczos_upper(*c, c->lanczos_steps);
     else lm = 0.5 * c->gmax * c->gmax + (maxv - minv);
+    // generalised problem: the spectrum of S^-1 H lies below lambda_max(H) / lambda_min(S)
+    if (c->uspp) lm /= c->s_min;
     double cut;
     if (!eig || n_eig == 0) cut = lm / 3.0;
     else {
@@ -613,14 +757,20 @@ int oracle_chebyshev_filter(OracleCtx* c, int ndeg, const double* eig, int n_eig
     c->norms.push_back(frob_norm(a));
     if (fail_k) *fail_k = 0;
     int status = 0;
+    std::vector<cplx> hs(c->uspp ? n : 0);
+    auto op = [&](const cplx* x, cplx* y) {  // y = H x, or S^-1 H x for the generalised problem
+        if (!c->uspp) { apply_h(*c, x, y, c->n_bands); return; }
+        apply_h(*c, x, hs.data(), c->n_bands);
+        apply_sinv(*c, hs.data(), y, c->n_bands);
+    };
     if (ndeg >= 1) {
-        apply_h(*c, a.data(), h.data(), c->n_bands);
+        op(a.data(), h.data());
 #pragma omp parallel for
         for (size_t i = 0; i < n; ++i) bb[i] = h[i] * inv_e + ncoe * a[i];
         c->norms.push_back(frob_norm(bb));
     }
     for (int k = 2; k <= ndeg; ++k) {
-        apply_h(*c, bb.data(), h.data(), c->n_bands);
+        op(bb.data(), h.data());
 #pragma omp parallel for
         for (size_t i = 0; i < n; ++i) {
             cplx s = h[i] * inv_e + ncoe * bb[i];
@@ -650,11 +800,13 @@ int oracle_chebyshev_filter(OracleCtx* c, int ndeg, const double* eig, int n_eig
 int oracle_rayleigh_ritz(OracleCtx* c, double* eig_out, int* info) {
     const int nb = c->n_bands, np = c->n_pw;
     std::vector<cplx> H((size_t)nb * nb), S((size_t)nb * nb);
+    std::vector<cplx> spsi(c->psi.size());
+    apply_s(*c, c->psi.data(), spsi.data(), nb);  // S_sub = psi^H S psi (generalised RR)
 #pragma omp parallel for schedule(dynamic, 1)
     for (int i = 0; i < nb; ++i)
         for (int j = i; j < nb; ++j) {
             const cplx* pi = &c->psi[(size_t)i * np];
-            const cplx* pj = &c->psi[(size_t)j * np];
+            const cplx* pj = &spsi[(size_t)j * np];
             const cplx* hj = &c->hpsi[(size_t)j * np];
             cplx sh = 0.0, ss = 0.0;
             for (int g = 0; g < np; ++g) {

@@ -55,6 +55,10 @@ def lib():
         "oracle_scf_run": ([vp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int,
                             C.c_double, dp, ip, dp, dp], C.c_int),
         "oracle_fermi": ([dp, C.c_int, C.c_double, C.c_double, dp], C.c_double),
+        "oracle_set_qmat": ([vp, vp], C.c_int),
+        "oracle_apply_s": ([vp, vp, vp, C.c_int], None),
+        "oracle_apply_sinv": ([vp, vp, vp, C.c_int], None),
+        "oracle_s_min": ([vp], C.c_double),
     }
     for name, (args, res) in protos.items():
         f = getattr(L, name)
@@ -163,6 +167,28 @@ class Oracle:
         p = np.zeros((self.n_bands, self.n_pw), dtype=np.complex128)
         lib().oracle_get_hpsi(self.h, _p(p))
         return p
+
+    def set_qmat(self, qmat):
+        """Ultrasoft overlap S = 1 + beta q beta^H (per-ion q blocks)."""
+        self._q = np.ascontiguousarray(qmat, dtype=np.complex128)
+        st = lib().oracle_set_qmat(self.h, _p(self._q))
+        if st != 0:
+            raise RuntimeError("oracle_set_qmat failed")
+
+    def apply_s(self, x):
+        x = np.ascontiguousarray(x, dtype=np.complex128)
+        y = np.zeros_like(x)
+        lib().oracle_apply_s(self.h, _p(x), _p(y), x.shape[0])
+        return y
+
+    def apply_sinv(self, x):
+        x = np.ascontiguousarray(x, dtype=np.complex128)
+        y = np.zeros_like(x)
+        lib().oracle_apply_sinv(self.h, _p(x), _p(y), x.shape[0])
+        return y
+
+    def s_min(self):
+        return lib().oracle_s_min(self.h)
 
     def set_bound_mode(self, mode, k=10):
         lib().oracle_set_bound_mode(self.h, mode, k)

@@ -1,0 +1,63 @@
+"""Mixed-precision ChFSI (FP32 filter; projector, overlap, subspace and
+rotation GEMMs on tcgen05 in BF16 3-way split with FP32 accumulation; FP64
+Cholesky and eigensolve) against the FP64 oracle.  Errors are reported per
+result; the SCF test holds the north-star bar: converged energy and occupied
+eigenvalues within 1e-6 Ha of the FP64 run."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module")
+def sys0(chfsi):
+    return chfsi.SyntheticSystem(config_index=0)
+
+
+@pytest.fixture(scope="module")
+def sys1s(chfsi):
+    return chfsi.SyntheticSystem(config_index=1, n_bands=132)
+
+
+@pytest.mark.parametrize("which,ndeg,passes", [("sys0", 12, 3), ("sys1s", 16, 2)])
+def test_mixed_diagonalize_close_to_fp64(chfsi, oracle, which, ndeg, passes, request):
+    s = request.getfixturevalue(which)
+    ctx = chfsi.Context(s, precision=chfsi.PREC_MIXED)
+    o = oracle.Oracle.from_system(s)
+    v = o.vloc_r()
+    ctx.set_veff(v)
+    o.set_veff(v)
+    wg = wc = None
+    for _ in range(passes):
+        wg = ctx.diagonalize(ndeg, wg)
+        wc = o.diagonalize(ndeg, wc)
+    err = np.abs(wg - wc).max()
+    print("mixed vs FP64 eigenvalue error after %d passes: %.3e Ha" % (passes, err))
+    assert err < 1e-4
+
+
+def test_mixed_apply_matches_fp64_filter_norms(chfsi, oracle, sys1s):
+    """One mixed filter: the per-degree |psi_k| follow the FP64 recurrence."""
+    ctx = chfsi.Context(sys1s, precision=chfsi.PREC_MIXED)
+    o = oracle.Oracle.from_system(sys1s)
+    v = o.vloc_r()
+    ctx.set_veff(v)
+    o.set_veff(v)
+    ctx.chebyshev_filter(8)
+    o.chebyshev_filter(8)
+    np.testing.assert_allclose(ctx.filter_norms(8), o.norms(), rtol=1e-4)
+
+
+def test_mixed_scf_matches_fp64(chfsi, sys0):
+    rf = chfsi.Context(sys0).run_scf(12, max_iter=40, kT=0.01)
+    rm = chfsi.Context(sys0, precision=chfsi.PREC_MIXED).run_scf(12, max_iter=40, kT=0.01,
+                                                                 fp64_switch_per_atom=1e-4)
+    assert rf["converged"] and rm["converged"]
+    assert rm["n_iter_mixed"] >= 1
+    de = abs(rm["e_total"] - rf["e_total"]) / sys0.n_atoms
+    docc = np.abs(rm["eigenvalues"][:16] - rf["eigenvalues"][:16]).max()
+    print("mixed SCF: %d iterations (%d mixed), dE/atom %.2e Ha, occupied eigenvalues %.2e Ha"
+          % (rm["n_iter"], rm["n_iter_mixed"], de, docc))
+    assert de < 1e-6
+    assert docc < 1e-6

@@ -212,3 +212,54 @@ def test_cfg0_golden_regression(chfsi, oracle, cfg0):
     w = o.diagonalize(12)
     np.testing.assert_allclose(w, g["eig_iter1"], atol=1e-10)
     np.testing.assert_allclose(o.bounds(), g["bounds_iter1"], rtol=1e-13)
+
+
+def uspp_small(chfsi):
+    # ultrasoft physics of the 216-atom configuration on one conventional cell
+    return chfsi.SyntheticSystem(config_index=2, n_rep=1, ecut=4.0, ngrid=[0, 0, 0], n_bands=20)
+
+
+def dense_s(s):
+    beta = s.beta()
+    off = s.proj_offsets()
+    qm = s.qmat()
+    Q = np.zeros((s.n_proj, s.n_proj), complex)
+    pos = 0
+    for i in range(len(off) - 1):
+        ne = off[i + 1] - off[i]
+        Q[off[i]:off[i + 1], off[i]:off[i + 1]] = qm[pos:pos + ne * ne].reshape(ne, ne)
+        pos += ne * ne
+    return np.eye(s.n_pw) + beta.T @ Q @ beta.conj()
+
+
+def test_uspp_overlap_and_woodbury_inverse(chfsi, oracle):
+    s = uspp_small(chfsi)
+    o = oracle.Oracle.from_system(s)
+    o.set_qmat(s.qmat())
+    x = s.psi0()[:4]
+    Sd = dense_s(s)
+    np.testing.assert_allclose(o.apply_s(x), (Sd @ x.T).T, atol=1e-12)
+    np.testing.assert_allclose(o.apply_sinv(o.apply_s(x)), x, atol=1e-11)
+    ev = np.linalg.eigvalsh(0.5 * (Sd + Sd.conj().T))
+    assert ev.min() > 0 and o.s_min() <= ev.min() + 1e-12
+
+
+def test_uspp_generalised_ritz_values(chfsi, oracle):
+    """Filtered subspace iteration on S^-1 H converges to the lowest
+    generalised eigenvalues of (H, S) (the H psi = e S psi problem)."""
+    scipy_linalg = pytest.importorskip("scipy.linalg")
+    s = uspp_small(chfsi)
+    o = oracle.Oracle.from_system(s)
+    o.set_qmat(s.qmat())
+    v = o.vloc_r()
+    o.set_veff(v)
+    w = o.diagonalize(10)
+    for _ in range(30):
+        w = o.diagonalize(10, w)
+    Hd = numpy_apply_h(s, o, np.eye(s.n_pw, dtype=complex), v).T
+    Sd = dense_s(s)
+    ev = scipy_linalg.eigh(0.5 * (Hd + Hd.conj().T), 0.5 * (Sd + Sd.conj().T), eigvals_only=True)
+    np.testing.assert_allclose(w[:16], ev[:16], atol=1e-8)
+    # the rotated bands are S-orthonormal
+    psi = o.get_psi()
+    np.testing.assert_allclose(psi.conj() @ o.apply_s(psi).T, np.eye(s.n_bands), atol=1e-10)
