@@ -180,6 +180,18 @@ template <typename T> cudaError_t dalloc(T** p, size_t n) {
     return cudaMalloc((void**)p, n * sizeof(T));
 }
 
+// The context stream is non-blocking, so a legacy-stream cudaMemcpy or
+// cudaMemset is not ordered with its kernels (a pageable host-to-device
+// cudaMemcpy may even return before its DMA lands).  Every set-up copy and
+// fill therefore goes through the context stream; copies wait for it so
+// that pageable host buffers can be released or read right after.
+cudaError_t copy_sync(void* dst, const void* src, size_t bytes, cudaMemcpyKind kind,
+                      cudaStream_t st) {
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, kind, st);
+    if (e != cudaSuccess) return e;
+    return cudaStreamSynchronize(st);
+}
+
 }  // namespace
 
 void set_last_error(const char* msg) { g_last_error = msg; }
@@ -215,6 +227,8 @@ struct chfsi_ctx {
     int* d_col_start = nullptr; int* d_col_pos = nullptr; int* d_pw_col = nullptr;
     int* d_pw_zpos = nullptr; int* d_xact = nullptr; int* d_idr[3] = {nullptr, nullptr, nullptr};
     int* d_perm = nullptr; bool perm_identity = true;
+    double2* d_twd = nullptr;  // twiddle tables x | y | z, FP64
+    float2* d_twf = nullptr;   // same, FP32
     double* d_kin = nullptr;
     // potentials
     double* d_veff = nullptr; double* d_vloc = nullptr; double* d_minmax = nullptr;
@@ -483,7 +497,7 @@ chfsi_status alloc_mixed(chfsi_ctx* ctx, int ncol) {
     size_t total = 0;
     for (auto& s : specs) total += 3 * (size_t)s.rows_alloc * s.kp;
     CK(cudaMalloc(&ctx->d_planes, total * 2));
-    CK(cudaMemset(ctx->d_planes, 0, total * 2));
+    CK(cudaMemsetAsync(ctx->d_planes, 0, total * 2, ctx->st));
     char* p = (char*)ctx->d_planes;
     for (auto& s : specs) {
         for (int i = 0; i < 3; ++i) {
@@ -497,7 +511,7 @@ chfsi_status alloc_mixed(chfsi_ctx* ctx, int ncol) {
     if (np > 0) pf = std::max(pf, tc_partial_floats(np, nb, npw));
     CK(dalloc(&ctx->d_tc_part, pf));
     CK(dalloc(&ctx->d_tc_err, 4));
-    CK(cudaMemset(ctx->d_tc_err, 0, 4 * sizeof(int)));
+    CK(cudaMemsetAsync(ctx->d_tc_err, 0, 4 * sizeof(int), ctx->st));
     return CHFSI_OK;
 }
 
@@ -738,7 +752,7 @@ chfsi_status alloc_all(chfsi_ctx* ctx) {
     CK(dalloc(&ctx->d_eig, ctx->nb)); CK(dalloc(&ctx->d_eig_prev, ctx->nb));
     CK(dalloc(&ctx->d_jac, jacobi_scratch_doubles(ctx->nb, ctx->jac_max_sweeps)));
     CK(dalloc(&ctx->d_flags, 8));
-    CK(cudaMemset(ctx->d_flags, 0, 8 * sizeof(int)));
+    CK(cudaMemsetAsync(ctx->d_flags, 0, 8 * sizeof(int), ctx->st));
     CK(dalloc(&ctx->d_coef, 8));
     CK(dalloc(&ctx->d_nsq, ctx->max_deg + 2));
     CK(dalloc(&ctx->d_lz_v, ctx->n_pw)); CK(dalloc(&ctx->d_lz_v0, ctx->n_pw));
@@ -775,14 +789,14 @@ chfsi_status alloc_all(chfsi_ctx* ctx) {
             double im = (double)(next() >> 11) * (1.0 / 9007199254740992.0) - 0.5;
             v[g] = make_double2(re, im);
         }
-        CK(cudaMemcpy(ctx->d_lz_start, v.data(), v.size() * sizeof(double2), cudaMemcpyHostToDevice));
+        CK(copy_sync(ctx->d_lz_start, v.data(), v.size() * sizeof(double2), cudaMemcpyHostToDevice, ctx->st));
     }
     std::vector<double*> hp(2 * kPulayMax);
     for (int i = 0; i < 2 * kPulayMax; ++i) hp[i] = ctx->d_hist + (size_t)i * ctx->ng;
-    CK(cudaMemcpy(ctx->d_hist_ptrs, hp.data(), hp.size() * sizeof(double*), cudaMemcpyHostToDevice));
+    CK(copy_sync(ctx->d_hist_ptrs, hp.data(), hp.size() * sizeof(double*), cudaMemcpyHostToDevice, ctx->st));
     ctx->occ.assign(ctx->nb, 0.0);
-    CK(cudaMemset(ctx->d_occ, 0, sizeof(double) * ctx->nb));
-    CK(cudaMemset(ctx->d_vloc, 0, sizeof(double) * ctx->ng));
+    CK(cudaMemsetAsync(ctx->d_occ, 0, sizeof(double) * ctx->nb, ctx->st));
+    CK(cudaMemsetAsync(ctx->d_vloc, 0, sizeof(double) * ctx->ng, ctx->st));
     return CHFSI_OK;
 }
 
@@ -799,7 +813,7 @@ void free_all(chfsi_ctx* ctx) {
                     ctx->d_hist_ptrs, ctx->d_dots};
     for (void* p : ptrs)
         if (p) cudaFree(p);
-    void* mp[] = {ctx->d_psi32a, ctx->d_psi32b, ctx->d_hpsi32, ctx->d_nl32, ctx->d_work32,
+    void* mp[] = {ctx->d_twd, ctx->d_twf, ctx->d_psi32a, ctx->d_psi32b, ctx->d_hpsi32, ctx->d_nl32, ctx->d_work32,
                   ctx->d_planes, ctx->d_tc_part, ctx->d_tc_err, ctx->d_qmat, ctx->d_sinvT,
                   ctx->d_cq, ctx->d_sx};
     for (void* p : mp)
@@ -876,7 +890,9 @@ chfsi_status chfsi_create(const chfsi_dims* dims, const chfsi_config* cfg, chfsi
         std::vector<int> inv(p.size());
         for (size_t k = 0; k < p.size(); ++k) inv[p[k]] = (int)k;
         if (cudaMalloc((void**)&ctx->d_idr[d], inv.size() * sizeof(int)) != cudaSuccess) return bail(CHFSI_ERR_OUT_OF_MEMORY);
-        cudaMemcpy(ctx->d_idr[d], inv.data(), inv.size() * sizeof(int), cudaMemcpyHostToDevice);
+        if (copy_sync(ctx->d_idr[d], inv.data(), inv.size() * sizeof(int), cudaMemcpyHostToDevice,
+                      ctx->st) != cudaSuccess)
+            return bail(CHFSI_ERR_CUDA);
     }
     *out = ctx;
     return CHFSI_OK;
@@ -954,14 +970,32 @@ chfsi_status chfsi_set_basis(chfsi_ctx* ctx, const int32_t* miller, const double
     CK(dalloc(&ctx->d_col_pos, ncol));
     CK(dalloc(&ctx->d_xact, xact.size()));
     CK(dalloc(&ctx->d_work, (size_t)ctx->nb * nz * ncol));
-    CK(cudaMemcpy(ctx->d_col_start, col_start.data(), sizeof(int) * (ncol + 1), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(ctx->d_col_pos, col_pos.data(), sizeof(int) * ncol, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(ctx->d_xact, xact.data(), sizeof(int) * xact.size(), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(ctx->d_pw_col, pw_col.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(ctx->d_pw_zpos, pw_zpos.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(ctx->d_kin, kin.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(ctx->d_perm, perm.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    CK(copy_sync(ctx->d_col_start, col_start.data(), sizeof(int) * (ncol + 1), cudaMemcpyHostToDevice, ctx->st));
+    CK(copy_sync(ctx->d_col_pos, col_pos.data(), sizeof(int) * ncol, cudaMemcpyHostToDevice, ctx->st));
+    CK(copy_sync(ctx->d_xact, xact.data(), sizeof(int) * xact.size(), cudaMemcpyHostToDevice, ctx->st));
+    CK(copy_sync(ctx->d_pw_col, pw_col.data(), sizeof(int) * n, cudaMemcpyHostToDevice, ctx->st));
+    CK(copy_sync(ctx->d_pw_zpos, pw_zpos.data(), sizeof(int) * n, cudaMemcpyHostToDevice, ctx->st));
+    CK(copy_sync(ctx->d_kin, kin.data(), sizeof(double) * n, cudaMemcpyHostToDevice, ctx->st));
+    CK(copy_sync(ctx->d_perm, perm.data(), sizeof(int) * n, cudaMemcpyHostToDevice, ctx->st));
+    // twiddle tables exp(+2 pi i j / n) of the three axes (cos/sin in FP64)
+    if (!ctx->d_twd) {
+        std::vector<double2> twd(nx + ny + nz);
+        std::vector<float2> twf(nx + ny + nz);
+        int o = 0;
+        for (int m : {nx, ny, nz})
+            for (int j = 0; j < m; ++j, ++o) {
+                const double a = 2.0 * 3.14159265358979323846 * (double)j / (double)m;
+                twd[o] = make_double2(std::cos(a), std::sin(a));
+                twf[o] = make_float2((float)twd[o].x, (float)twd[o].y);
+            }
+        CK(dalloc(&ctx->d_twd, twd.size()));
+        CK(dalloc(&ctx->d_twf, twf.size()));
+        CK(copy_sync(ctx->d_twd, twd.data(), twd.size() * sizeof(double2), cudaMemcpyHostToDevice, ctx->st));
+        CK(copy_sync(ctx->d_twf, twf.data(), twf.size() * sizeof(float2), cudaMemcpyHostToDevice, ctx->st));
+    }
     HGeom& g = ctx->geo;
+    g.twd_x = ctx->d_twd; g.twd_y = ctx->d_twd + nx; g.twd_z = ctx->d_twd + nx + ny;
+    g.twf_x = ctx->d_twf; g.twf_y = ctx->d_twf + nx; g.twf_z = ctx->d_twf + nx + ny;
     g.nx = nx; g.ny = ny; g.nz = nz; g.n_pw = n; g.ncol = ncol;
     g.lsz = nz | 1; g.lsx = nx | 1; g.nxact = (int)xact.size();
     g.col_start = ctx->d_col_start; g.col_pos = ctx->d_col_pos; g.pw_col = ctx->d_pw_col;
@@ -1000,18 +1034,22 @@ chfsi_status chfsi_set_projectors(chfsi_ctx* ctx, const chfsi_c128* beta,
     if (ctx->d_dmat) cudaFree(ctx->d_dmat);
     ctx->d_dmat = nullptr;
     CK(dalloc(&ctx->d_dmat, dt));
-    CK(cudaMemcpy(ctx->d_dmat, dmat, dt * sizeof(double2), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(ctx->d_proj_ion, pion.data(), sizeof(int) * ctx->np, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(ctx->d_poff, proj_offsets, sizeof(int) * (ni + 1), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(ctx->d_doff, doff.data(), sizeof(int) * ni, cudaMemcpyHostToDevice));
+    CK(copy_sync(ctx->d_dmat, dmat, dt * sizeof(double2), cudaMemcpyHostToDevice, ctx->st));
+    CK(copy_sync(ctx->d_proj_ion, pion.data(), sizeof(int) * ctx->np, cudaMemcpyHostToDevice, ctx->st));
+    CK(copy_sync(ctx->d_poff, proj_offsets, sizeof(int) * (ni + 1), cudaMemcpyHostToDevice, ctx->st));
+    CK(copy_sync(ctx->d_doff, doff.data(), sizeof(int) * ni, cudaMemcpyHostToDevice, ctx->st));
     const size_t nbeta = (size_t)ctx->np * ctx->n_pw;
     if (ctx->perm_identity) {
-        CK(cudaMemcpy(ctx->d_beta, beta, nbeta * sizeof(double2), cudaMemcpyHostToDevice));
+        CK(copy_sync(ctx->d_beta, beta, nbeta * sizeof(double2), cudaMemcpyHostToDevice, ctx->st));
     } else {
         // stage in the hpsi buffer when it is large enough, else in a temporary
         double2* stage = nullptr;
         CK(cudaMalloc((void**)&stage, nbeta * sizeof(double2)));
-        cudaMemcpy(stage, beta, nbeta * sizeof(double2), cudaMemcpyHostToDevice);
+        if (cudaError_t e = copy_sync(stage, beta, nbeta * sizeof(double2), cudaMemcpyHostToDevice,
+                                      ctx->st)) {
+            cudaFree(stage);
+            return cuda_fail(e, "copy_sync(stage)", __FILE__, __LINE__);
+        }
         count_launch();
         k_gather_rows<<<grid_for(nbeta), 256, 0, ctx->st>>>(stage, ctx->n_pw, ctx->d_perm,
                                                            ctx->d_beta, ctx->n_pw, ctx->np);
@@ -1030,12 +1068,12 @@ chfsi_status chfsi_set_qmat(chfsi_ctx* ctx, const chfsi_c128* qmat) {
     cudaSetDevice(ctx->device);
     const int np = ctx->np, ni = ctx->nions;
     std::vector<int> poff(ni + 1), doff(ni);
-    CK(cudaMemcpy(poff.data(), ctx->d_poff, sizeof(int) * (ni + 1), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(doff.data(), ctx->d_doff, sizeof(int) * ni, cudaMemcpyDeviceToHost));
+    CK(copy_sync(poff.data(), ctx->d_poff, sizeof(int) * (ni + 1), cudaMemcpyDeviceToHost, ctx->st));
+    CK(copy_sync(doff.data(), ctx->d_doff, sizeof(int) * ni, cudaMemcpyDeviceToHost, ctx->st));
     size_t dt = 0;
     for (int i = 0; i < ni; ++i) dt += (size_t)(poff[i + 1] - poff[i]) * (poff[i + 1] - poff[i]);
     if (!ctx->d_qmat) CK(dalloc(&ctx->d_qmat, dt));
-    CK(cudaMemcpy(ctx->d_qmat, qmat, dt * sizeof(double2), cudaMemcpyHostToDevice));
+    CK(copy_sync(ctx->d_qmat, qmat, dt * sizeof(double2), cudaMemcpyHostToDevice, ctx->st));
     // B = beta^H beta on the device
     double2 *part = nullptr, *dB = nullptr;
     CK(cudaMalloc((void**)&part, splitk_partial_elems(np, np, ctx->n_pw) * sizeof(double2)));
@@ -1083,7 +1121,7 @@ chfsi_status chfsi_set_qmat(chfsi_ctx* ctx, const chfsi_c128* qmat) {
     if (!ctx->d_sinvT) CK(dalloc(&ctx->d_sinvT, (size_t)np * np));
     if (!ctx->d_cq) CK(dalloc(&ctx->d_cq, (size_t)np * ctx->nb));
     if (!ctx->d_sx) CK(dalloc(&ctx->d_sx, (size_t)ctx->nb * ctx->n_pw));
-    CK(cudaMemcpy(ctx->d_sinvT, MT.data(), MT.size() * sizeof(double2), cudaMemcpyHostToDevice));
+    CK(copy_sync(ctx->d_sinvT, MT.data(), MT.size() * sizeof(double2), cudaMemcpyHostToDevice, ctx->st));
     ctx->uspp = true;
     return CHFSI_OK;
 }
@@ -1269,7 +1307,9 @@ chfsi_status chfsi_create_from_system(const chfsi_system* sys, const chfsi_confi
     if ((st = chfsi_set_cell(ctx, lat, s.e_ewald, s.n_atoms))) return bail(st);
     // a usable V_eff before the first SCF step: V_loc alone
     std::vector<double> v(ctx->ng);
-    cudaMemcpy(v.data(), ctx->d_vloc, sizeof(double) * ctx->ng, cudaMemcpyDeviceToHost);
+    if (cudaError_t e = copy_sync(v.data(), ctx->d_vloc, sizeof(double) * ctx->ng,
+                                  cudaMemcpyDeviceToHost, ctx->st))
+        return bail(cuda_fail(e, "copy_sync(vloc)", __FILE__, __LINE__));
     if ((st = chfsi_set_veff(ctx, v.data()))) return bail(st);
     *out = ctx;
     return CHFSI_OK;
@@ -1282,7 +1322,7 @@ chfsi_status chfsi_set_occupations(chfsi_ctx* ctx, const double* occ) {
     ctx->occ.assign(occ, occ + ctx->nb);
     ctx->n_elec = 0.0;
     for (double f : ctx->occ) ctx->n_elec += f;
-    CK(cudaMemcpy(ctx->d_occ, occ, sizeof(double) * ctx->nb, cudaMemcpyHostToDevice));
+    CK(copy_sync(ctx->d_occ, occ, sizeof(double) * ctx->nb, cudaMemcpyHostToDevice, ctx->st));
     return CHFSI_OK;
 }
 
@@ -1323,7 +1363,7 @@ chfsi_status chfsi_set_vloc_g(chfsi_ctx* ctx, const chfsi_c128* vloc_g) {
                                   (size_t)ctx->nx * (ctx->dr[1][iy] + (size_t)ctx->ny * ctx->dr[2][iz]);
                 h[to] = src[from];
             }
-    CK(cudaMemcpy(ctx->d_cgrid, h.data(), sizeof(double2) * ctx->ng, cudaMemcpyHostToDevice));
+    CK(copy_sync(ctx->d_cgrid, h.data(), sizeof(double2) * ctx->ng, cudaMemcpyHostToDevice, ctx->st));
     grid_fft3(ctx, ctx->d_cgrid, false);
     launch_take_real(ctx->d_cgrid, ctx->d_vloc, ctx->ng, ctx->st);
     CK(cudaStreamSynchronize(ctx->st));
@@ -1335,7 +1375,7 @@ chfsi_status chfsi_set_vloc_g(chfsi_ctx* ctx, const chfsi_c128* vloc_g) {
 chfsi_status chfsi_get_vloc(chfsi_ctx* ctx, double* out) {
     if (!ctx || !out) return CHFSI_ERR_BAD_INPUT;
     cudaSetDevice(ctx->device);
-    CK(cudaMemcpy(out, ctx->d_vloc, sizeof(double) * ctx->ng, cudaMemcpyDeviceToHost));
+    CK(copy_sync(out, ctx->d_vloc, sizeof(double) * ctx->ng, cudaMemcpyDeviceToHost, ctx->st));
     return CHFSI_OK;
 }
 
@@ -1343,7 +1383,7 @@ chfsi_status chfsi_get_veff(chfsi_ctx* ctx, double* out) {
     if (!ctx || !out) return CHFSI_ERR_BAD_INPUT;
     cudaSetDevice(ctx->device);
     CK(cudaStreamSynchronize(ctx->st));
-    CK(cudaMemcpy(out, ctx->d_veff, sizeof(double) * ctx->ng, cudaMemcpyDeviceToHost));
+    CK(copy_sync(out, ctx->d_veff, sizeof(double) * ctx->ng, cudaMemcpyDeviceToHost, ctx->st));
     return CHFSI_OK;
 }
 
@@ -1610,7 +1650,7 @@ extern "C" chfsi_status chfsi_get_density(chfsi_ctx* ctx, double* rho) {
     if (!ctx || !rho) return CHFSI_ERR_BAD_INPUT;
     cudaSetDevice(ctx->device);
     CK(cudaStreamSynchronize(ctx->st));
-    CK(cudaMemcpy(rho, ctx->d_rho_out, sizeof(double) * ctx->ng, cudaMemcpyDeviceToHost));
+    CK(copy_sync(rho, ctx->d_rho_out, sizeof(double) * ctx->ng, cudaMemcpyDeviceToHost, ctx->st));
     return CHFSI_OK;
 }
 

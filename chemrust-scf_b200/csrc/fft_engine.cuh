@@ -403,6 +403,14 @@ struct LinesListed {
     __device__ __forceinline__ int operator()(int l) const { return list[l]; }
 };
 
+// Copy a precomputed twiddle table (global memory, L2-resident) into smem.
+__device__ __forceinline__ void copy_twiddles(double2* tw, const double2* twd, const float2*, int n) {
+    for (int j = threadIdx.x; j < n; j += blockDim.x) tw[j] = twd[j];
+}
+__device__ __forceinline__ void copy_twiddles(float2* tw, const double2*, const float2* twf, int n) {
+    for (int j = threadIdx.x; j < n; j += blockDim.x) tw[j] = twf[j];
+}
+
 // tw[j] = exp(+2 pi i j / n), computed in FP64 then rounded to C.
 template <typename C> __device__ __forceinline__ void load_twiddles(C* tw, int n) {
     for (int j = threadIdx.x; j < n; j += blockDim.x) {

@@ -35,7 +35,7 @@ __device__ __forceinline__ void cfma(double2& acc, double2 a, double2 b) {
     acc.y = fma(a.y, b.x, acc.y);
 }
 
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 2)
 k_gemm_cn_splitk(const double2* __restrict__ A, int lda, const double2* __restrict__ B, int ldb,
                  int M, int N, int K, int kchunk, double2* __restrict__ part) {
     __shared__ double2 As[BK][BM + 1];
@@ -49,26 +49,30 @@ k_gemm_cn_splitk(const double2* __restrict__ A, int lda, const double2* __restri
     for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc[i][j] = make_double2(0.0, 0.0);
-    // loader mapping: row r = t / 4, k offset (t % 4) * 4
+    // loader mapping: row r = t / 4, k offset (t % 4) * 4; the next tile is
+    // fetched into registers while the current one is consumed from smem
     const int lr = threadIdx.x >> 2, lk = (threadIdx.x & 3) * 4;
+    const int am = m0 + lr, bn_ = n0 + lr;
+    const double2* ap = A + (size_t)am * lda;
+    const double2* bp = B + (size_t)bn_ * ldb;
+    double2 ra[4], rb[4];
+    auto fetch = [&](int k0) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int k = k0 + lk + i;
+            ra[i] = (am < M && k < ke) ? ap[k] : make_double2(0.0, 0.0);
+            rb[i] = (bn_ < N && k < ke) ? bp[k] : make_double2(0.0, 0.0);
+        }
+    };
+    if (kb < ke) fetch(kb);
     for (int k0 = kb; k0 < ke; k0 += BK) {
-        {
-            const int m = m0 + lr;
-            const double2* ap = A + (size_t)m * lda + k0 + lk;
 #pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                const int k = k0 + lk + i;
-                As[lk + i][lr] = (m < M && k < ke) ? ap[i] : make_double2(0.0, 0.0);
-            }
-            const int n = n0 + lr;
-            const double2* bp = B + (size_t)n * ldb + k0 + lk;
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                const int k = k0 + lk + i;
-                Bs[lk + i][lr] = (n < N && k < ke) ? bp[i] : make_double2(0.0, 0.0);
-            }
+        for (int i = 0; i < 4; ++i) {
+            As[lk + i][lr] = ra[i];
+            Bs[lk + i][lr] = rb[i];
         }
         __syncthreads();
+        if (k0 + BK < ke) fetch(k0 + BK);
 #pragma unroll
         for (int k = 0; k < BK; ++k) {
             double2 a[4], b[4];
@@ -110,7 +114,7 @@ __global__ void k_reduce_partials(const double2* __restrict__ part, int splits, 
     }
 }
 
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 2)
 k_gemm_tn(const double2* __restrict__ W, int ldw, const double2* __restrict__ X, int ldx,
           double2* O, int ldo, int M, int N, int K, double alpha, double beta) {
     __shared__ double2 Ws[BK][BM];
@@ -124,16 +128,25 @@ k_gemm_tn(const double2* __restrict__ W, int ldw, const double2* __restrict__ X,
         for (int j = 0; j < 4; ++j) acc[i][j] = make_double2(0.0, 0.0);
     // loader: 16 x 64 tile, thread t loads row k = t / 16, cols (t % 16) * 4 .. +3
     const int lk = threadIdx.x >> 4, lc = (threadIdx.x & 15) * 4;
-    for (int k0 = 0; k0 < K; k0 += BK) {
+    double2 rw[4], rx[4];
+    auto fetch = [&](int k0) {
         const int k = k0 + lk;
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            const int m = m0 + lc + i;
-            Ws[lk][lc + i] = (k < K && m < M) ? W[(size_t)k * ldw + m] : make_double2(0.0, 0.0);
-            const int n = n0 + lc + i;
-            Xs[lk][lc + i] = (k < K && n < N) ? X[(size_t)k * ldx + n] : make_double2(0.0, 0.0);
+            const int m = m0 + lc + i, n = n0 + lc + i;
+            rw[i] = (k < K && m < M) ? W[(size_t)k * ldw + m] : make_double2(0.0, 0.0);
+            rx[i] = (k < K && n < N) ? X[(size_t)k * ldx + n] : make_double2(0.0, 0.0);
+        }
+    };
+    fetch(0);
+    for (int k0 = 0; k0 < K; k0 += BK) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            Ws[lk][lc + i] = rw[i];
+            Xs[lk][lc + i] = rx[i];
         }
         __syncthreads();
+        if (k0 + BK < K) fetch(k0 + BK);
 #pragma unroll
         for (int kk = 0; kk < BK; ++kk) {
             double2 a[4], b[4];

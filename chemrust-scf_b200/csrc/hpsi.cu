@@ -67,7 +67,7 @@ k_zsticks_inverse(const C* __restrict__ psi, int ldp, C* __restrict__ work, HGeo
     const int c0 = blockIdx.x * kColsPerBlock;
     const int c1 = min(c0 + kColsPerBlock, g.ncol);
     const int nl = c1 - c0;
-    load_twiddles(tw, g.nz);
+    copy_twiddles(tw, g.twd_z, g.twf_z, g.nz);
     for (int i = threadIdx.x; i < kColsPerBlock * g.lsz; i += blockDim.x) lines[i] = czero<C>();
     __syncthreads();
     const int g0 = g.col_start[c0], g1 = g.col_start[c1];
@@ -93,8 +93,8 @@ k_planes_vloc(C* __restrict__ work, const double* __restrict__ veff, HGeom g) {
     C* plane = reinterpret_cast<C*>(smem_raw + align16<C>(g.nx) + align16<C>(g.ny));
     int* xl = reinterpret_cast<int*>(plane + (size_t)g.ny * g.lsx);
     const int z = blockIdx.x, b = blockIdx.y;
-    load_twiddles(twx, g.nx);
-    load_twiddles(twy, g.ny);
+    copy_twiddles(twx, g.twd_x, g.twf_x, g.nx);
+    copy_twiddles(twy, g.twd_y, g.twf_y, g.ny);
     for (int i = threadIdx.x; i < g.nxact; i += blockDim.x) xl[i] = g.xact[i];
     for (int i = threadIdx.x; i < g.ny * g.lsx; i += blockDim.x) plane[i] = czero<C>();
     __syncthreads();
@@ -143,7 +143,7 @@ k_zsticks_forward(const C* __restrict__ work, const C* __restrict__ psi, int ldp
     const int c0 = blockIdx.x * kColsPerBlock;
     const int c1 = min(c0 + kColsPerBlock, g.ncol);
     const int nl = c1 - c0;
-    load_twiddles(tw, g.nz);
+    copy_twiddles(tw, g.twd_z, g.twf_z, g.nz);
     const C* wb = work + (size_t)b * g.nz * g.ncol;
     for (int u = threadIdx.x; u < g.nz * kColsPerBlock; u += blockDim.x) {
         const int z = u / kColsPerBlock, cl = u - z * kColsPerBlock;
@@ -201,8 +201,8 @@ k_planes_density(const C* __restrict__ work, const double* __restrict__ occ, int
     int* xl = reinterpret_cast<int*>(plane + (size_t)g.ny * g.lsx);
     const int z = blockIdx.x;
     const int b0 = blockIdx.y * bpg, b1 = min(b0 + bpg, nb);
-    load_twiddles(twx, g.nx);
-    load_twiddles(twy, g.ny);
+    copy_twiddles(twx, g.twd_x, g.twf_x, g.nx);
+    copy_twiddles(twy, g.twd_y, g.twf_y, g.ny);
     for (int i = threadIdx.x; i < g.nxact; i += blockDim.x) xl[i] = g.xact[i];
     double acc[MAXPT];
 #pragma unroll

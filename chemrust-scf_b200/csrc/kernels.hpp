@@ -22,6 +22,9 @@ struct HGeom {
     const int* pw_zpos;    // n_pw: digit-reversed z position
     const int* xact;       // nxact: digit-reversed x positions
     AxisPlan ax, ay, az;
+    // twiddle tables exp(+2 pi i j / n) per axis, precomputed once per context
+    const double2* twd_x; const double2* twd_y; const double2* twd_z;
+    const float2* twf_x; const float2* twf_y; const float2* twf_z;
 };
 
 // Pass-3 epilogue: what to do with (H psi)_g once it is assembled.

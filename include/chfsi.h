@@ -34,6 +34,9 @@
  * Ownership: a context owns all of its device memory and one CUDA stream.
  * Calls on one context are not re-entrant.  Host arrays passed in are copied;
  * device pointers passed to chfsi_apply_h stay owned by the caller.
+ * The context stream is created non-blocking: work on a device pointer is
+ * ordered after earlier work on that stream (chfsi_get_stream) only, so a
+ * caller that fills the buffer on another stream synchronises first.
  * Errors are returned as chfsi_status (mirror of the crate's Error enum,
  * src/types.rs:226-248); chfsi_last_error() gives the message.
  */

@@ -570,7 +570,245 @@ double fermi_occupations(const double* e, int n, double n_elec, double kT, doubl
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// Band-by-band preconditioned CG refinement (src/eigensolver/band_cg.rs:157-437)
+// with the closed-form 2x2 line search (line_search.rs:57-212), residual /
+// S-orthogonalisation helpers (cg_helpers.rs:49-216) and the TPA + ultrasoft
+// Woodbury preconditioner (uspp_preconditioner.rs:56-300).
+// ---------------------------------------------------------------------------
+struct LineSearch { double step, eig, norm; int status; };
+
+LineSearch line_search_2d(double a, double hpsi_dir, double c, double d) {
+    const double b = -2.0 * hpsi_dir;
+    double step = 0.0, eig = a;
+    int status = 0;
+    if (std::fabs(d) > 2.2250738585072014e-308) {
+        const double ad = a * d, bd = b * d;
+        if (std::fabs(bd) < 1e-30) return {0.0, a, 1.0, -2};
+        const double tmp = ad * ad - 2.0 * ad * c + c * c + b * bd;
+        if (tmp < 0.0) return {0.0, a, 1.0, -1};
+        const double det = std::sqrt(tmp);
+        const double r1 = (-ad + c + det) / bd, r2 = (-ad + c - det) / bd;
+        auto e_at = [&](double r, bool& ok) {
+            const double den = 1.0 + d * r * r;
+            ok = den > 0.0;
+            return ok ? (a + b * r + c * r * r) / den : 0.0;
+        };
+        bool ok1, ok2;
+        const double e1 = e_at(r1, ok1), e2 = e_at(r2, ok2);
+        double rr, ee;
+        if (ok1 && ok2) { if (e1 < e2) { rr = r1; ee = e1; } else { rr = r2; ee = e2; } }
+        else if (ok1 && e1 < a) { rr = r1; ee = e1; }
+        else if (ok2 && e2 < a) { rr = r2; ee = e2; }
+        else return {0.0, a, 1.0, -1};
+        step = -rr;
+        eig = ee;
+    } else {
+        if (c > 0.0) {
+            step = -b / (2.0 * c);
+            eig = (a + b * step + c * step * step) / (1.0 + d * step * step);
+        } else {
+            return {0.0, a, 1.0, -1};
+        }
+    }
+    if (step > 15.0) {
+        step = 15.0;
+        eig = (a + b * step + c * step * step) / (1.0 + d * step * step);
+        status = 1;
+    } else if (step < 0.0) {
+        status = -1;
+    }
+    const double t = 1.0 + d * step * step;
+    if (t > 0.0) return {step, eig, std::sqrt(t), status};
+    return {step, eig, 0.0, 2};
+}
+
+// TPA diagonal 1 / (1 + 16 x^4 / (27 + 18 x + 12 x^2 + 8 x^3)), x = E_k / <E_k>
+void tpa_diag(const double* kin, int n, double* out) {
+    double s = 0.0;
+    for (int g = 0; g < n; ++g) s += kin[g];
+    const double mean = n > 0 ? s / n : 0.0;
+    const double inv = mean > 0.0 ? 1.0 / mean : 1.0;
+    for (int g = 0; g < n; ++g) {
+        const double x = kin[g] * inv;
+        const double den = 27.0 + x * (18.0 + x * (12.0 + 8.0 * x));
+        out[g] = 1.0 / (1.0 + 16.0 * x * x * x * x / den);
+    }
+}
+
 extern "C" {
+
+}  // extern "C"
+
+namespace {
+
+cplx dotc(const cplx* a, const cplx* b, int n) {
+    cplx s = 0.0;
+    for (int i = 0; i < n; ++i) s += std::conj(a[i]) * b[i];
+    return s;
+}
+
+// Preconditioner P^-1 r = T r + T beta R beta^H T r with R = (-q^-1 - beta^H T beta)^-1
+// (uspp_preconditioner.rs:80-131, 180-300); without q it is the TPA diagonal.
+struct Precond {
+    std::vector<double> t;
+    std::vector<cplx> r;  // n_proj x n_proj, empty: TPA only
+};
+
+Precond build_precond(const OracleCtx& c) {
+    Precond P;
+    P.t.resize(c.n_pw);
+    tpa_diag(c.kin.data(), c.n_pw, P.t.data());
+    if (!c.uspp || c.n_proj == 0) return P;
+    const int np = c.n_proj;
+    std::vector<cplx> Q((size_t)np * np, 0.0), Cm((size_t)np * np);
+    for (int ion = 0; ion < c.n_ions; ++ion) {
+        const int p0 = c.poff[ion], ne = c.poff[ion + 1] - p0;
+        for (int i = 0; i < ne; ++i)
+            for (int j = 0; j < ne; ++j) Q[(size_t)(p0 + i) * np + p0 + j] = c.qmat[c.dmat_off[ion] + i * ne + j];
+    }
+    if (!invert(Q, np)) return P;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int p = 0; p < np; ++p)
+        for (int q = 0; q < np; ++q) {
+            cplx s = 0.0;
+            for (int g = 0; g < c.n_pw; ++g)
+                s += std::conj(c.beta[(size_t)p * c.n_pw + g]) * P.t[g] * c.beta[(size_t)q * c.n_pw + g];
+            Cm[(size_t)p * np + q] = s;
+        }
+    std::vector<cplx> M((size_t)np * np);
+    for (size_t i = 0; i < M.size(); ++i) M[i] = -Q[i] - Cm[i];
+    if (!invert(M, np)) return P;
+    P.r = M;
+    return P;
+}
+
+void apply_precond(const OracleCtx& c, const Precond& P, const cplx* r, cplx* out) {
+    const int n = c.n_pw;
+    std::vector<cplx> tr(n);
+    for (int g = 0; g < n; ++g) tr[g] = r[g] * P.t[g];
+    if (P.r.empty()) { std::copy(tr.begin(), tr.end(), out); return; }
+    const int np = c.n_proj;
+    std::vector<cplx> w(np), wr(np, 0.0);
+    for (int p = 0; p < np; ++p) w[p] = dotc(&c.beta[(size_t)p * n], tr.data(), n);
+    for (int i = 0; i < np; ++i)
+        for (int j = 0; j < np; ++j) wr[i] += P.r[(size_t)i * np + j] * w[j];
+    for (int g = 0; g < n; ++g) {
+        cplx s = 0.0;
+        for (int p = 0; p < np; ++p) s += c.beta[(size_t)p * n + g] * wr[p];
+        out[g] = tr[g] + s * P.t[g];
+    }
+}
+
+struct CgOut { double eig; int steps; bool converged; double rnorm; };
+
+// band_cg_minimize (band_cg.rs:157-437) for one band; psi is replaced by the
+// S-normalised refined band.  lower: (psi_j, S psi_j) of the refined lower bands.
+CgOut band_cg_one(const OracleCtx& c, const Precond& P, std::vector<cplx>& psi,
+                  const std::vector<std::pair<std::vector<cplx>, std::vector<cplx>>>& lower,
+                  int max_steps, double tol) {
+    const int n = c.n_pw;
+    std::vector<cplx> hpsi(n), spsi(n);
+    auto apply_hs = [&](const std::vector<cplx>& x, std::vector<cplx>& hx, std::vector<cplx>& sx) {
+        apply_h(c, x.data(), hx.data(), 1);
+        apply_s(c, x.data(), sx.data(), 1);
+    };
+    apply_hs(psi, hpsi, spsi);
+    const double s0 = dotc(psi.data(), spsi.data(), n).real();
+    const double inv0 = 1.0 / std::sqrt(s0);
+    for (int g = 0; g < n; ++g) { psi[g] *= inv0; hpsi[g] *= inv0; spsi[g] *= inv0; }
+    double eig = dotc(psi.data(), hpsi.data(), n).real();
+    auto residual = [&](std::vector<cplx>& r) {
+        const double he = dotc(psi.data(), hpsi.data(), n).real();
+        const double se = dotc(psi.data(), spsi.data(), n).real();
+        const double e = he / se;
+        for (int g = 0; g < n; ++g) r[g] = hpsi[g] - e * spsi[g];
+    };
+    auto norm = [&](const std::vector<cplx>& v) {
+        double s = 0.0;
+        for (auto& x : v) s += std::norm(x);
+        return std::sqrt(s);
+    };
+    std::vector<cplx> r(n), g(n), sg(n), d(n), d_old, hd(n), sd(n);
+    residual(r);
+    double beta_old = 0.0;
+    for (int step = 1; step <= max_steps; ++step) {
+        apply_precond(c, P, r.data(), g.data());
+        if (norm(g) < 2.220446049250313e-16 * 1000.0) return {eig, step - 1, true, norm(r)};
+        const double prev = eig;
+        apply_s(c, g.data(), sg.data(), 1);
+        // S-orthogonalise g against the refined lower bands, then S-normalise
+        for (auto& lb : lower) {
+            const cplx ov = dotc(lb.first.data(), sg.data(), n);
+            for (int i = 0; i < n; ++i) { g[i] -= ov * lb.first[i]; sg[i] -= ov * lb.second[i]; }
+        }
+        const double gn = std::sqrt(std::max(dotc(g.data(), sg.data(), n).real(), 1e-300));
+        for (int i = 0; i < n; ++i) { g[i] /= gn; sg[i] /= gn; }
+        if (step <= 2) {
+            d = g;
+            beta_old = dotc(g.data(), r.data(), n).real();
+        } else {
+            const double beta = dotc(g.data(), r.data(), n).real();
+            const double gamma = std::fabs(beta_old) > 1e-300 ? beta / beta_old : 0.0;
+            for (int i = 0; i < n; ++i) d[i] = gamma * d_old[i] - g[i];
+            beta_old = beta;
+        }
+        apply_hs(d, hd, sd);
+        const cplx ov = dotc(psi.data(), sd.data(), n);
+        if (std::abs(ov) > 1e-30)
+            for (int i = 0; i < n; ++i) { d[i] -= ov * psi[i]; hd[i] -= ov * hpsi[i]; sd[i] -= ov * spsi[i]; }
+        d_old = d;
+        const double rn = norm(r);
+        if (rn < tol * 0.01 && rn < 1e-12 * std::max(std::fabs(eig), 1.0)) return {eig, step - 1, true, rn};
+        const LineSearch ls = line_search_2d(eig, dotc(hpsi.data(), d.data(), n).real(),
+                                             dotc(hd.data(), d.data(), n).real(),
+                                             dotc(sd.data(), d.data(), n).real());
+        const double inv = ls.norm > 0.0 ? 1.0 / ls.norm : 1.0;
+        for (int i = 0; i < n; ++i) {
+            psi[i] = (psi[i] + ls.step * d[i]) * inv;
+            hpsi[i] = (hpsi[i] + ls.step * hd[i]) * inv;
+            spsi[i] = (spsi[i] + ls.step * sd[i]) * inv;
+        }
+        const double e_new = dotc(psi.data(), hpsi.data(), n).real();
+        residual(r);
+        if (std::fabs(e_new - prev) < tol) return {e_new, step, true, norm(r)};
+        eig = e_new;
+    }
+    return {eig, max_steps, false, norm(r)};
+}
+
+}  // namespace
+
+extern "C" {
+
+// Refine every band in turn with band_cg_minimize against the already
+// refined lower bands (the gate tests' driver, tests/phase0_gate2_convergence.rs:387-418).
+// eig_out[b], steps_out[b] per band; returns the number of converged bands.
+int oracle_band_cg(OracleCtx* c, int max_steps, double tol, double* eig_out, int* steps_out) {
+    const Precond P = build_precond(*c);
+    const int n = c->n_pw;
+    std::vector<std::pair<std::vector<cplx>, std::vector<cplx>>> lower;
+    int nconv = 0;
+    for (int b = 0; b < c->n_bands; ++b) {
+        std::vector<cplx> psi(c->psi.begin() + (size_t)b * n, c->psi.begin() + (size_t)(b + 1) * n);
+        const CgOut o = band_cg_one(*c, P, psi, lower, max_steps, tol);
+        std::copy(psi.begin(), psi.end(), c->psi.begin() + (size_t)b * n);
+        std::vector<cplx> sp(n);
+        apply_s(*c, psi.data(), sp.data(), 1);
+        lower.emplace_back(psi, sp);
+        if (eig_out) eig_out[b] = o.eig;
+        if (steps_out) steps_out[b] = o.steps;
+        nconv += o.converged;
+    }
+    return nconv;
+}
+
+void oracle_line_search(double a, double hpsi_dir, double c, double d, double* out4) {
+    const LineSearch r = line_search_2d(a, hpsi_dir, c, d);
+    out4[0] = r.step; out4[1] = r.eig; out4[2] = r.norm; out4[3] = r.status;
+}
+
+void oracle_tpa_diag(const double* kin, int n, double* out) { tpa_diag(kin, n, out); }
 
 double oracle_fermi(const double* e, int n, double n_elec, double kT, double* f) {
     return fermi_occupations(e, n, n_elec, kT, f);

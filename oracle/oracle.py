@@ -56,6 +56,9 @@ def lib():
                             C.c_double, dp, ip, dp, dp], C.c_int),
         "oracle_fermi": ([dp, C.c_int, C.c_double, C.c_double, dp], C.c_double),
         "oracle_set_qmat": ([vp, vp], C.c_int),
+        "oracle_line_search": ([C.c_double, C.c_double, C.c_double, C.c_double, dp], None),
+        "oracle_tpa_diag": ([dp, C.c_int, dp], None),
+        "oracle_band_cg": ([vp, C.c_int, C.c_double, dp, ip], C.c_int),
         "oracle_apply_s": ([vp, vp, vp, C.c_int], None),
         "oracle_apply_sinv": ([vp, vp, vp, C.c_int], None),
         "oracle_s_min": ([vp], C.c_double),
@@ -86,6 +89,20 @@ def fermi(eig, n_elec, kT):
     f = np.zeros_like(e)
     ts = lib().oracle_fermi(_p(e, C.c_double), len(e), n_elec, kT, _p(f, C.c_double))
     return f, ts
+
+
+def line_search(a, hpsi_dir, hdir_dir, sdir_dir):
+    """Closed-form 2x2 Rayleigh-quotient line search -> (step, eigenvalue, norm, status)."""
+    out = np.zeros(4)
+    lib().oracle_line_search(a, hpsi_dir, hdir_dir, sdir_dir, _p(out, C.c_double))
+    return out[0], out[1], out[2], int(out[3])
+
+
+def tpa_diag(kin):
+    k = np.ascontiguousarray(kin, dtype=np.float64)
+    out = np.zeros_like(k)
+    lib().oracle_tpa_diag(_p(k, C.c_double), len(k), _p(out, C.c_double))
+    return out
 
 
 def hegv(h, s):
@@ -189,6 +206,14 @@ class Oracle:
 
     def s_min(self):
         return lib().oracle_s_min(self.h)
+
+    def band_cg(self, max_steps, tol):
+        """Sequential band-by-band preconditioned CG refinement of the current psi."""
+        e = np.zeros(self.n_bands)
+        steps = np.zeros(self.n_bands, dtype=np.int32)
+        nconv = lib().oracle_band_cg(self.h, max_steps, tol, _p(e, C.c_double),
+                                     steps.ctypes.data_as(C.POINTER(C.c_int)))
+        return e, steps, nconv
 
     def set_bound_mode(self, mode, k=10):
         lib().oracle_set_bound_mode(self.h, mode, k)

@@ -18,6 +18,10 @@ cell (seed 0): eigenvalues after one and after three ChFSI iterations on
 V_eff = V_loc (degree 12, reference spectral bounds), and the first three SCF
 energies (Fermi-Dirac kT = 0.01 Ha, Pulay alpha 0.3 / history 6).
 
+  * src/eigensolver/line_search.rs:217-394  closed-form line search: parabola
+    (1, 1, 3, 0) -> step 1/3, E 2/3; rational (0, -0.5, 1, 1) -> step sqrt2 - 1;
+    clamp (0, -5, 0.01, 0.001) -> 15 (status 1); no minimum (0, 0, -0.1, 0) -> status -1
+
 Run from the repository root:  python tests/golden/make_golden.py
 """
 import json
@@ -56,6 +60,18 @@ def known_answers():
                       "expected": [[[1, 1], [2, 2]], [[3, -3], [4, -4]]], "tol": 1e-10},
         "lcg_seed42": {"source": "src/eigensolver/subspace_diag.rs:434-447",
                        "first8": lcg_sequence(42, 8)},
+        "line_search_parabola": {"source": "src/eigensolver/line_search.rs:219-234",
+                                 "args": [1.0, 1.0, 3.0, 0.0], "step": 1.0 / 3.0,
+                                 "eigenvalue": 2.0 / 3.0, "norm": 1.0, "status": 0, "tol": 1e-12},
+        "line_search_rational": {"source": "src/eigensolver/line_search.rs:250-280",
+                                 "args": [0.0, -0.5, 1.0, 1.0], "step": 2.0 ** 0.5 - 1.0,
+                                 "eigenvalue": ((1 - 2 ** 0.5) + (1 - 2 ** 0.5) ** 2) / (1 + (1 - 2 ** 0.5) ** 2),
+                                 "tol": 1e-12},
+        "line_search_clamp": {"source": "src/eigensolver/line_search.rs:318-333",
+                              "args": [0.0, -5.0, 0.01, 0.001], "step": 15.0, "status": 1,
+                              "tol": 1e-12},
+        "line_search_no_minimum": {"source": "src/eigensolver/line_search.rs:335-345",
+                                   "args": [0.0, 0.0, -0.1, 0.0], "step": 0.0, "status": -1},
     }
 
 
@@ -80,8 +96,9 @@ def cfg0_oracle():
 def main():
     with open(os.path.join(HERE, "reference_known_answers.json"), "w") as f:
         json.dump(known_answers(), f, indent=1)
-    with open(os.path.join(HERE, "cfg0_oracle.json"), "w") as f:
-        json.dump(cfg0_oracle(), f, indent=1)
+    if "--known-answers-only" not in sys.argv:
+        with open(os.path.join(HERE, "cfg0_oracle.json"), "w") as f:
+            json.dump(cfg0_oracle(), f, indent=1)
 
 
 if __name__ == "__main__":

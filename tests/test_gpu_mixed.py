@@ -61,3 +61,17 @@ def test_mixed_scf_matches_fp64(chfsi, sys0):
           % (rm["n_iter"], rm["n_iter_mixed"], de, docc))
     assert de < 1e-6
     assert docc < 1e-6
+
+
+def test_scf_does_not_depend_on_earlier_contexts(chfsi, oracle, sys0):
+    """Set-up copies are ordered on the context stream: an SCF run gives the
+    oracle's energies whatever contexts were created and freed before it."""
+    ref = oracle.Oracle.from_system(sys0).run_scf(12, max_iter=3, kT=0.01)["energies"]
+    a = chfsi.Context(sys0)
+    a.run_scf(12, max_iter=1, kT=0.01)
+    b = chfsi.Context(sys0, precision=chfsi.PREC_MIXED)
+    b.run_scf(12, max_iter=1, kT=0.01, fp64_switch_per_atom=0.0)
+    c = chfsi.Context(sys0)  # created while a and b still hold their memory
+    del a, b
+    e = c.run_scf(12, max_iter=3, kT=0.01)["energies"]
+    np.testing.assert_allclose(e, ref, rtol=0, atol=1e-8)

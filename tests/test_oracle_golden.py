@@ -263,3 +263,59 @@ def test_uspp_generalised_ritz_values(chfsi, oracle):
     # the rotated bands are S-orthonormal
     psi = o.get_psi()
     np.testing.assert_allclose(psi.conj() @ o.apply_s(psi).T, np.eye(s.n_bands), atol=1e-10)
+
+
+@pytest.mark.parametrize("case", ["line_search_parabola", "line_search_rational", "line_search_clamp",
+                                  "line_search_no_minimum"])
+def test_line_search_known_answers(oracle, case):
+    # line_search.rs:217-394
+    c = ka()[case]
+    step, eig, norm, status = oracle.line_search(*c["args"])
+    assert abs(step - c["step"]) < c.get("tol", 1e-12)
+    if "eigenvalue" in c:
+        assert abs(eig - c["eigenvalue"]) < c["tol"]
+    if "status" in c:
+        assert status == c["status"]
+    if "norm" in c:
+        assert abs(norm - c["norm"]) < 1e-12
+
+
+@pytest.mark.parametrize("args", [(-0.4, -0.15, 1.2, 0.8), (-0.38, -0.2, 1.5, 0.7)])
+def test_line_search_energy_decreases(oracle, args):
+    # line_search.rs energy_decrease / energy_monotonicity
+    step, eig, norm, status = oracle.line_search(*args)
+    assert eig <= args[0] + 1e-14 and norm > 0 and step > 0 and status in (0, -1)
+
+
+def test_tpa_diag_properties(oracle):
+    # uspp_preconditioner.rs: T(0) = 1, monotone decreasing, floor > 0
+    k = np.linspace(0.0, 40.0, 200)
+    t = oracle.tpa_diag(k)
+    assert abs(t[0] - 1.0) < 1e-15 and np.all(np.diff(t) <= 0) and t[-1] > 0
+
+
+def test_band_cg_refines_towards_eigenpairs(chfsi, oracle):
+    """band_cg.rs semantics: after a coarse filter, a few CG steps per band lower
+    the band energies towards the exact generalised eigenvalues and keep the
+    refined bands S-orthonormal (cg_helpers.rs S-orthogonalisation)."""
+    scipy_linalg = pytest.importorskip("scipy.linalg")
+    s = uspp_small(chfsi)
+    o = oracle.Oracle.from_system(s)
+    o.set_qmat(s.qmat())
+    v = o.vloc_r()
+    o.set_veff(v)
+    w = o.diagonalize(8)
+    w = o.diagonalize(8, w)
+    e, steps, nconv = o.band_cg(6, 1e-10)
+    Hd = numpy_apply_h(s, o, np.eye(s.n_pw, dtype=complex), v).T
+    Sd = dense_s(s)
+    ev = scipy_linalg.eigh(0.5 * (Hd + Hd.conj().T), 0.5 * (Sd + Sd.conj().T), eigvals_only=True)
+    # Ky Fan: the band energies of an S-orthonormal set sum to at least the sum
+    # of the lowest exact eigenvalues; CG lowers that sum from the Ritz values
+    k = 12
+    assert e[:k].sum() >= ev[:k].sum() - 1e-10
+    assert e[:k].sum() <= w[:k].sum() + 1e-10
+    assert np.all(steps >= 1)
+    # each refined band is S-normalised (cg_helpers.rs s_normalize)
+    psi = o.get_psi()
+    np.testing.assert_allclose(np.einsum("bg,bg->b", psi.conj(), o.apply_s(psi)).real, 1.0, atol=1e-10)
