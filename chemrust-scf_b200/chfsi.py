@@ -28,6 +28,8 @@ OK, NOT_CONVERGED, NOT_IMPLEMENTED, CHEB_DIVERGED, RR_FAILED, CUDA_ERROR, BAD_IN
     NO_DEVICE, OUT_OF_MEMORY, NUMERIC = 0, -1, -2, -3, -4, -5, -6, -7, -8, -9
 PREC_FP64, PREC_MIXED = 0, 1
 BOUND_HEURISTIC, BOUND_LANCZOS = 0, 1
+MIXER_PULAY, MIXER_LEARNED, MIXER_LEARNED_PULAY = 0, 1, 2
+MIXER_FEATURES, MIXER_OUTPUTS, MIXER_TARGETS, MIXER_SHELLS = 512, 128, 320, 64
 
 
 class ChfsiError(RuntimeError):
@@ -106,7 +108,8 @@ class Config(C.Structure):
 class ScfParams(C.Structure):
     _fields_ = [("ndeg", C.c_int), ("max_iter", C.c_int), ("tol_per_atom", C.c_double),
                 ("alpha", C.c_double), ("max_hist", C.c_int), ("first_passes", C.c_int),
-                ("kT", C.c_double), ("fp64_switch_per_atom", C.c_double)]
+                ("kT", C.c_double), ("fp64_switch_per_atom", C.c_double),
+                ("mixer", C.c_int), ("reserved", C.c_int), ("trace", C.POINTER(C.c_double))]
 
 
 class ScfResult(C.Structure):
@@ -115,7 +118,9 @@ class ScfResult(C.Structure):
                 ("e_band", C.c_double), ("e_hartree", C.c_double), ("e_xc", C.c_double),
                 ("e_dc", C.c_double), ("e_entropy", C.c_double), ("mu", C.c_double),
                 ("seconds", C.c_double),
-                ("energies", C.POINTER(C.c_double)), ("eigenvalues", C.POINTER(C.c_double))]
+                ("energies", C.POINTER(C.c_double)), ("eigenvalues", C.POINTER(C.c_double)),
+                ("n_iter_learned", C.c_int), ("fell_back", C.c_int),
+                ("residuals", C.POINTER(C.c_double))]
 
 
 _lib = None
@@ -130,6 +135,7 @@ def lib():
         raise ImportError("libchfsi_b200.so is missing: run chemrust-scf_b200/build.py")
     L = C.CDLL(LIB_PATH)
     vp, i32p, dp = C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_double)
+    fp = C.POINTER(C.c_float)
     sig = {
         "chfsi_synth_defaults": [C.c_int, C.POINTER(SynthParams)],
         "chfsi_system_generate": [C.POINTER(SynthParams), C.POINTER(vp)],
@@ -175,6 +181,14 @@ def lib():
         "chfsi_build_veff": [vp, dp, dp],
         "chfsi_get_density": [vp, dp],
         "chfsi_scf_run": [vp, C.POINTER(ScfParams), C.POINTER(ScfResult)],
+        "chfsi_mixer_create": [C.c_int, C.c_uint64, C.POINTER(vp)],
+        "chfsi_mixer_get_params": [vp, fp],
+        "chfsi_mixer_set_params": [vp, fp],
+        "chfsi_mixer_forward": [vp, fp, C.c_int, fp],
+        "chfsi_mixer_gradient": [vp, fp, fp, C.c_int, fp, fp],
+        "chfsi_mixer_train": [vp, fp, fp, C.c_int, C.c_int, C.c_int, C.c_float, C.c_uint64, fp],
+        "chfsi_set_mixer": [vp, vp],
+        "chfsi_mixer_samples": [vp, dp, dp, C.c_int, dp, fp, fp],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -184,12 +198,72 @@ def lib():
     L.chfsi_system_destroy.restype = None
     L.chfsi_destroy.argtypes = [vp]
     L.chfsi_destroy.restype = None
+    L.chfsi_mixer_destroy.argtypes = [vp]
+    L.chfsi_mixer_destroy.restype = None
+    L.chfsi_mixer_num_params.argtypes = []
+    L.chfsi_mixer_num_params.restype = C.c_size_t
     L.chfsi_launch_count.argtypes = []
     L.chfsi_launch_count.restype = C.c_longlong
     L.chfsi_last_error.argtypes = [vp]
     L.chfsi_last_error.restype = C.c_char_p
     _lib = L
     return L
+
+
+class Mixer:
+    """Learned density mixer: MLP 512 -> 256 -> 256 -> 128 (GELU), BF16 weights,
+    FP32 accumulation; forward, backward and Adam run as the library's kernels."""
+
+    def __init__(self, device=0, seed=0, params=None):
+        h = C.c_void_p()
+        _check(lib().chfsi_mixer_create(device, seed, C.byref(h)))
+        self.handle = h
+        self.num_params = int(lib().chfsi_mixer_num_params())
+        if params is not None:
+            self.set_params(params)
+
+    def close(self):
+        if getattr(self, "handle", None) and _lib is not None:
+            _lib.chfsi_mixer_destroy(self.handle)
+            self.handle = None
+
+    __del__ = close
+
+    def get_params(self):
+        w = np.zeros(self.num_params, dtype=np.float32)
+        _check(lib().chfsi_mixer_get_params(self.handle, _ptr(w, C.c_float)))
+        return w
+
+    def set_params(self, w):
+        w = np.ascontiguousarray(w, dtype=np.float32).ravel()
+        if w.size != self.num_params:
+            raise ValueError("expected %d parameters" % self.num_params)
+        _check(lib().chfsi_mixer_set_params(self.handle, _ptr(w, C.c_float)))
+
+    def forward(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, MIXER_FEATURES)
+        y = np.zeros((x.shape[0], MIXER_OUTPUTS), dtype=np.float32)
+        _check(lib().chfsi_mixer_forward(self.handle, _ptr(x, C.c_float), x.shape[0],
+                                         _ptr(y, C.c_float)))
+        return y
+
+    def gradient(self, x, t):
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, MIXER_FEATURES)
+        t = np.ascontiguousarray(t, dtype=np.float32).reshape(-1, MIXER_TARGETS)
+        g = np.zeros(self.num_params, dtype=np.float32)
+        loss = C.c_float()
+        _check(lib().chfsi_mixer_gradient(self.handle, _ptr(x, C.c_float), _ptr(t, C.c_float),
+                                          x.shape[0], _ptr(g, C.c_float), C.byref(loss)))
+        return g, loss.value
+
+    def train(self, x, t, epochs=50, batch=256, lr=1e-3, seed=0):
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, MIXER_FEATURES)
+        t = np.ascontiguousarray(t, dtype=np.float32).reshape(-1, MIXER_TARGETS)
+        losses = np.zeros(epochs, dtype=np.float32)
+        _check(lib().chfsi_mixer_train(self.handle, _ptr(x, C.c_float), _ptr(t, C.c_float),
+                                       x.shape[0], epochs, batch, lr, seed,
+                                       _ptr(losses, C.c_float)))
+        return losses
 
 
 def zgemm_cn(a_dev, lda, b_dev, ldb, m, n, k, c_dev, stream=0):
@@ -478,19 +552,53 @@ class Context:
         return r
 
     def run_scf(self, ndeg, tol_per_atom=1e-6, max_iter=30, alpha=0.3, max_hist=6,
-                first_passes=4, kT=0.01, fp64_switch_per_atom=1e-4, raise_not_converged=False):
+                first_passes=4, kT=0.01, fp64_switch_per_atom=1e-4, raise_not_converged=False,
+                mixer=MIXER_PULAY, trace=False):
+        """Full SCF; mixer is MIXER_PULAY or, after set_mixer(), MIXER_LEARNED /
+        MIXER_LEARNED_PULAY.  trace=True also returns rho_in and rho_out of every
+        iteration (n_iter x N^3 each) as 'trace_in' / 'trace_out'."""
         p = ScfParams(ndeg, max_iter, tol_per_atom, alpha, max_hist, first_passes, kT,
-                      fp64_switch_per_atom)
+                      fp64_switch_per_atom, mixer, 0, None)
+        tr = None
+        if trace:
+            tr = np.zeros((max_iter, 2, self.ng))
+            p.trace = _ptr(tr, C.c_double)
         energies = np.zeros(max_iter)
+        residuals = np.zeros(max_iter)
         eigs = np.zeros(self.n_bands)
         r = ScfResult()
         r.energies = _ptr(energies, C.c_double)
         r.eigenvalues = _ptr(eigs, C.c_double)
+        r.residuals = _ptr(residuals, C.c_double)
         st = lib().chfsi_scf_run(self.handle, C.byref(p), C.byref(r))
         if st not in (OK, NOT_CONVERGED) or (st == NOT_CONVERGED and raise_not_converged):
             _check(st, self.handle)
-        return {"converged": st == OK, "n_iter": r.n_iter, "n_iter_mixed": r.n_iter_mixed,
-                "e_total": r.e_total,
-                "e_band": r.e_band, "e_hartree": r.e_hartree, "e_xc": r.e_xc, "e_dc": r.e_dc,
-                "e_entropy": r.e_entropy, "mu": r.mu,
-                "seconds": r.seconds, "energies": energies[:r.n_iter].copy(), "eigenvalues": eigs}
+        out = {"converged": st == OK, "n_iter": r.n_iter, "n_iter_mixed": r.n_iter_mixed,
+               "e_total": r.e_total,
+               "e_band": r.e_band, "e_hartree": r.e_hartree, "e_xc": r.e_xc, "e_dc": r.e_dc,
+               "e_entropy": r.e_entropy, "mu": r.mu,
+               "seconds": r.seconds, "energies": energies[:r.n_iter].copy(), "eigenvalues": eigs,
+               "residuals": residuals[:r.n_iter].copy(), "n_iter_learned": r.n_iter_learned,
+               "fell_back": bool(r.fell_back)}
+        if trace:
+            out["trace_in"] = tr[:r.n_iter, 0].copy()
+            out["trace_out"] = tr[:r.n_iter, 1].copy()
+        return out
+
+    # --- learned density mixer ------------------------------------------------
+    def set_mixer(self, mixer):
+        self._mixer = mixer  # keep the handle alive while attached
+        self._c(lib().chfsi_set_mixer(self.handle, mixer.handle if mixer is not None else None))
+
+    def mixer_samples(self, rho_in, rho_out, rho_star):
+        """Features (T x 512) and targets (T x 320) of one trajectory on this grid."""
+        a = np.ascontiguousarray(rho_in, dtype=np.float64).reshape(-1, self.ng)
+        b = np.ascontiguousarray(rho_out, dtype=np.float64).reshape(-1, self.ng)
+        st = np.ascontiguousarray(rho_star, dtype=np.float64).ravel()
+        T = a.shape[0]
+        x = np.zeros((T, MIXER_FEATURES), dtype=np.float32)
+        t = np.zeros((T, MIXER_TARGETS), dtype=np.float32)
+        self._c(lib().chfsi_mixer_samples(self.handle, _ptr(a, C.c_double), _ptr(b, C.c_double), T,
+                                          _ptr(st, C.c_double), _ptr(x, C.c_float),
+                                          _ptr(t, C.c_float)))
+        return x, t

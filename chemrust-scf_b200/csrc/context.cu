@@ -18,6 +18,7 @@
 #include "fft_plan.hpp"
 #include "kernels.hpp"
 #include "launch_count.hpp"
+#include "mixer.hpp"
 #include "system.hpp"
 
 #include <algorithm>
@@ -277,6 +278,13 @@ struct chfsi_ctx {
     TcPlanes tp_beta_a, tp_betaT_b, tp_psi_b, tp_psi_a, tp_hpsi_b, tp_small_a, tp_psiT_b;
     float* d_tc_part = nullptr; int* d_tc_err = nullptr;
     bool beta_planes_ready = false;
+    // learned density mixer (G-space residual history on the density grid)
+    chfsi_mixer* mixer = nullptr;
+    unsigned char* d_shell = nullptr;  // |G| shell per grid point (digit-reversed layout)
+    double2* d_mix_c = nullptr;        // 7 complex grids: R_0..R_3 ring, D, E, work
+    double* d_mix_r = nullptr;         // 4 real grids: prev rho_in, rho*, two uploads
+    double* d_mix_acc = nullptr;       // kMixShells x kShellAcc
+    float* d_mix_x = nullptr;          // features, targets, outputs
     // pinned host scratch
     double* h_pin = nullptr; size_t h_pin_n = 0;
 
@@ -725,6 +733,53 @@ chfsi_status density_dev(chfsi_ctx* ctx, double* rho) {
     return CHFSI_OK;
 }
 
+// ---------------------------------------------------------------- learned mixer
+chfsi_status alloc_mix(chfsi_ctx* ctx) {
+    if (ctx->d_mix_c) return CHFSI_OK;
+    const size_t ng = ctx->ng;
+    CK(dalloc(&ctx->d_shell, ng));
+    CK(dalloc(&ctx->d_mix_c, 7 * ng));
+    CK(dalloc(&ctx->d_mix_r, 4 * ng));
+    CK(dalloc(&ctx->d_mix_acc, (size_t)kMixShells * kShellAcc));
+    CK(dalloc(&ctx->d_mix_x, (size_t)kMixIn + kMixShells * kMixTargets + kMixOut));
+    launch_shell_index(grid_recip(ctx), ctx->d_shell, ctx->st);
+    CK(cudaGetLastError());
+    return CHFSI_OK;
+}
+
+// Residual history R_0 (newest) .. R_3 in G space: complex grids 0..3 of d_mix_c.
+struct MixRing {
+    int n = 0, head = -1;
+    double2* slot(const chfsi_ctx* ctx, int age) const {
+        return ctx->d_mix_c + (size_t)((head - age + 4) % 4) * ctx->ng;
+    }
+};
+double2* mix_grid(const chfsi_ctx* ctx, int k) { return ctx->d_mix_c + (size_t)k * ctx->ng; }
+double* mix_real(const chfsi_ctx* ctx, int k) { return ctx->d_mix_r + (size_t)k * ctx->ng; }
+constexpr int kGridD = 4, kGridE = 5, kGridW = 6;  // complex grid slots
+float* mix_y(const chfsi_ctx* ctx) { return ctx->d_mix_x + kMixIn + kMixShells * kMixTargets; }
+
+// FFT(out - in) becomes the newest residual.
+void ring_push(chfsi_ctx* ctx, MixRing& r, const double* out, const double* in) {
+    r.head = (r.head + 1) % 4;
+    r.n = std::min(r.n + 1, 4);
+    double2* dst = r.slot(ctx, 0);
+    launch_diff_complex(out, in, dst, ctx->ng, ctx->st);
+    grid_fft3(ctx, dst, true);
+}
+
+// Shell features of the ring (and targets when E != nullptr) into d_mix_x.
+chfsi_status mix_features(chfsi_ctx* ctx, const MixRing& r, const double2* D, const double2* E) {
+    CK(cudaMemsetAsync(ctx->d_mix_acc, 0, sizeof(double) * kMixShells * kShellAcc, ctx->st));
+    const double2* R[4] = {nullptr, nullptr, nullptr, nullptr};
+    for (int a = 0; a < r.n; ++a) R[a] = r.slot(ctx, a);
+    launch_shell_acc(R[0], R[1], R[2], R[3], D, E, ctx->d_shell, ctx->ng, ctx->d_mix_acc, ctx->st);
+    launch_shell_features(ctx->d_mix_acc, ctx->d_mix_x, E ? ctx->d_mix_x + kMixIn : nullptr,
+                          ctx->st);
+    CK(cudaGetLastError());
+    return CHFSI_OK;
+}
+
 chfsi_status alloc_all(chfsi_ctx* ctx) {
     const size_t nbpw = (size_t)ctx->nb * ctx->n_pw;
     CK(dalloc(&ctx->d_kin, ctx->n_pw));
@@ -815,7 +870,8 @@ void free_all(chfsi_ctx* ctx) {
         if (p) cudaFree(p);
     void* mp[] = {ctx->d_twd, ctx->d_twf, ctx->d_psi32a, ctx->d_psi32b, ctx->d_hpsi32, ctx->d_nl32, ctx->d_work32,
                   ctx->d_planes, ctx->d_tc_part, ctx->d_tc_err, ctx->d_qmat, ctx->d_sinvT,
-                  ctx->d_cq, ctx->d_sx};
+                  ctx->d_cq, ctx->d_sx, ctx->d_shell, ctx->d_mix_c, ctx->d_mix_r,
+                  ctx->d_mix_acc, ctx->d_mix_x};
     for (void* p : mp)
         if (p) cudaFree(p);
     if (ctx->h_pin) cudaFreeHost(ctx->h_pin);
@@ -1516,11 +1572,20 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
     if (p->max_hist < 1 || p->max_hist > kPulayMax || p->max_iter < 1 || p->ndeg < 0)
         return CHFSI_ERR_BAD_INPUT;
     cudaSetDevice(ctx->device);
+    const bool learned = p->mixer == CHFSI_MIXER_LEARNED || p->mixer == CHFSI_MIXER_LEARNED_PULAY;
+    if (p->mixer < CHFSI_MIXER_PULAY || p->mixer > CHFSI_MIXER_LEARNED_PULAY)
+        return ctx->fail(CHFSI_ERR_BAD_INPUT, "unknown mixer");
+    if (learned && !ctx->mixer)
+        return ctx->fail(CHFSI_ERR_BAD_INPUT, "learned mixer requested but none set (chfsi_set_mixer)");
+    if (learned && ctx->mixer->mlp.device != ctx->device)
+        return ctx->fail(CHFSI_ERR_BAD_INPUT, "mixer lives on another device");
     double* r_energies = r->energies;
     double* r_eigs = r->eigenvalues;
+    double* r_res = r->residuals;
     std::memset(r, 0, sizeof(*r));
     r->energies = r_energies;
     r->eigenvalues = r_eigs;
+    r->residuals = r_res;
     const size_t ng = ctx->ng;
     const double dv = ctx->omega / (double)ng;
     cudaStream_t st = ctx->st;
@@ -1530,6 +1595,11 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
     PulayState ps;
     chfsi_status s = ensure_pinned(ctx, (size_t)ctx->nb + 64 + ctx->max_deg);
     if (s) return s;
+    if (learned && (s = alloc_mix(ctx))) return s;
+    MixRing ring;
+    bool have_prev = false, fell_back = false;
+    int rises = 0;
+    double r_prev = -1.0;
     std::vector<double> eig(ctx->nb);
     bool have_eig = false;
     double e_prev = 0.0;
@@ -1581,6 +1651,12 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
         r->e_band = eband; r->e_hartree = acc[0]; r->e_xc = acc[1]; r->e_dc = acc[2];
         r->e_total = etot;
         r->n_iter = it;
+        if (p->trace) {
+            double* tr = p->trace + (size_t)2 * (it - 1) * ng;
+            CK(cudaMemcpyAsync(tr, ctx->d_rho_in, sizeof(double) * ng, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(tr + ng, ctx->d_rho_out, sizeof(double) * ng, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+        }
         // check (scf.rs:328): |dE| per atom below tolerance; a mixed-precision
         // run only converges on FP64 iterations (the final filter passes are FP64)
         const double de = it > 1 ? std::fabs(etot - e_prev) / ctx->n_atoms : 1e300;
@@ -1628,12 +1704,62 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
             for (int j = 0; j < ps.m; ++j) c[j] = 0.0;
             c[ps.m - 1] = 1.0;
         }
-        pulay_combine(ctx->d_hist_ptrs + kPulayMax, ctx->d_hist_ptrs, ps.m, c, p->alpha, ng,
-                      ctx->d_rho_next, st);
+        // residual norm |rho_out - rho_in|_2 and the fallback rule of the
+        // learned mixers: two rises in a row hand the run to Pulay
+        const double rnorm = std::sqrt(std::max(0.0, dd[nw]) * dv);
+        if (r->residuals) r->residuals[it - 1] = rnorm;
+        if (learned && !fell_back) {
+            rises = (r_prev >= 0.0 && rnorm > r_prev) ? rises + 1 : 0;
+            if (rises >= 2) fell_back = true;
+        }
+        r_prev = rnorm;
+        if (learned) ring_push(ctx, ring, ctx->d_rho_out, ctx->d_rho_in);
+        if (!learned || fell_back) {
+            pulay_combine(ctx->d_hist_ptrs + kPulayMax, ctx->d_hist_ptrs, ps.m, c, p->alpha, ng,
+                          ctx->d_rho_next, st);
+        } else {
+            double2* Dg = nullptr;
+            if (have_prev) {
+                Dg = mix_grid(ctx, kGridD);
+                launch_diff_complex(ctx->d_rho_in, mix_real(ctx, 0), Dg, ng, st);
+                grid_fft3(ctx, Dg, true);
+            }
+            if ((s = mix_features(ctx, ring, Dg, nullptr))) { status = s; break; }
+            mlp_forward(ctx->mixer->mlp, ctx->d_mix_x, 1, mix_y(ctx), st);
+            double2* W = mix_grid(ctx, kGridW);
+            if (p->mixer == CHFSI_MIXER_LEARNED) {
+                // rho_in + a_s R_0 + b_s D per shell
+                launch_diff_complex(ctx->d_rho_in, nullptr, W, ng, st);
+                grid_fft3(ctx, W, true);
+                launch_shell_update(W, ring.slot(ctx, 0), Dg, mix_y(ctx), ctx->d_shell, ng, st);
+            } else {
+                // Pulay extrapolation with a_s in place of alpha:
+                // sum c_j rho_j + a_s (sum c_j R_j)
+                double* rbar = mix_real(ctx, 2);
+                pulay_combine(ctx->d_hist_ptrs + kPulayMax, ctx->d_hist_ptrs, ps.m, c, 0.0, ng,
+                              ctx->d_rho_next, st);
+                pulay_combine(ctx->d_hist_ptrs, ctx->d_hist_ptrs, ps.m, c, 0.0, ng, rbar, st);
+                double2* Rg = mix_grid(ctx, kGridE);
+                launch_diff_complex(ctx->d_rho_next, nullptr, W, ng, st);
+                grid_fft3(ctx, W, true);
+                launch_diff_complex(rbar, nullptr, Rg, ng, st);
+                grid_fft3(ctx, Rg, true);
+                launch_shell_update(W, Rg, nullptr, mix_y(ctx), ctx->d_shell, ng, st);
+            }
+            grid_fft3(ctx, W, false);
+            launch_take_real_scaled(W, ctx->d_rho_next, ng, 1.0 / (double)ng, st);
+            ++r->n_iter_learned;
+        }
+        if (learned) {
+            CK(cudaMemcpyAsync(mix_real(ctx, 0), ctx->d_rho_in, sizeof(double) * ng,
+                               cudaMemcpyDeviceToDevice, st));
+            have_prev = true;
+        }
         std::swap(ctx->d_rho_in, ctx->d_rho_next);
         CK(cudaGetLastError());
     }
     ctx->mixed_active = ctx->mixed;
+    r->fell_back = fell_back ? 1 : 0;
     cudaEventRecord(t1, st);
     cudaEventSynchronize(t1);
     float ms = 0.f;
@@ -1651,6 +1777,58 @@ extern "C" chfsi_status chfsi_get_density(chfsi_ctx* ctx, double* rho) {
     cudaSetDevice(ctx->device);
     CK(cudaStreamSynchronize(ctx->st));
     CK(copy_sync(rho, ctx->d_rho_out, sizeof(double) * ctx->ng, cudaMemcpyDeviceToHost, ctx->st));
+    return CHFSI_OK;
+}
+
+extern "C" chfsi_status chfsi_set_mixer(chfsi_ctx* ctx, chfsi_mixer* m) {
+    if (!ctx) return CHFSI_ERR_BAD_INPUT;
+    if (m && m->mlp.device != ctx->device)
+        return ctx->fail(CHFSI_ERR_BAD_INPUT, "mixer lives on another device");
+    ctx->mixer = m;
+    return CHFSI_OK;
+}
+
+// Features and least-squares targets of one recorded SCF trajectory, with
+// the same shell reductions the SCF loop uses for inference.
+extern "C" chfsi_status chfsi_mixer_samples(chfsi_ctx* ctx, const double* rho_in,
+                                            const double* rho_out, int n_iter,
+                                            const double* rho_star, float* x, float* t) {
+    if (!ctx || !rho_in || !rho_out || !rho_star || !x || !t || n_iter <= 0)
+        return CHFSI_ERR_BAD_INPUT;
+    if (!ctx->basis_set || ctx->omega <= 0.0)
+        return ctx->fail(CHFSI_ERR_BAD_INPUT, "context not fully initialised");
+    cudaSetDevice(ctx->device);
+    chfsi_status s = alloc_mix(ctx);
+    if (s) return s;
+    const size_t ng = ctx->ng;
+    cudaStream_t st = ctx->st;
+    double* prev = mix_real(ctx, 0);
+    double* star = mix_real(ctx, 1);
+    double* a = mix_real(ctx, 2);
+    double* b = mix_real(ctx, 3);
+    CK(cudaMemcpyAsync(star, rho_star, sizeof(double) * ng, cudaMemcpyHostToDevice, st));
+    MixRing ring;
+    for (int it = 0; it < n_iter; ++it) {
+        CK(cudaMemcpyAsync(a, rho_in + (size_t)it * ng, sizeof(double) * ng, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(b, rho_out + (size_t)it * ng, sizeof(double) * ng, cudaMemcpyHostToDevice, st));
+        ring_push(ctx, ring, b, a);
+        double2* Dg = nullptr;
+        if (it > 0) {
+            Dg = mix_grid(ctx, kGridD);
+            launch_diff_complex(a, prev, Dg, ng, st);
+            grid_fft3(ctx, Dg, true);
+        }
+        double2* Eg = mix_grid(ctx, kGridE);
+        launch_diff_complex(star, a, Eg, ng, st);
+        grid_fft3(ctx, Eg, true);
+        if ((s = mix_features(ctx, ring, Dg, Eg))) return s;
+        CK(cudaMemcpyAsync(x + (size_t)it * kMixIn, ctx->d_mix_x, sizeof(float) * kMixIn,
+                           cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(t + (size_t)it * kMixShells * kMixTargets, ctx->d_mix_x + kMixIn,
+                           sizeof(float) * kMixShells * kMixTargets, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(prev, a, sizeof(double) * ng, cudaMemcpyDeviceToDevice, st));
+    }
+    CK(cudaStreamSynchronize(st));
     return CHFSI_OK;
 }
 

@@ -405,6 +405,152 @@ k_jacobi2(double2* A, double2* V, double2* X, int n, int max_sweeps, double tol2
     if (gtid == 0) *sweeps_out = converged ? sweep : max_sweeps;
 }
 
+// Same rotation sequence as k_jacobi2 with the working rows kept on chip.
+// Warp w owns pair w at every step: the two A rows of that pair live in its
+// shared memory (phase 2 of step s builds exactly the rows the warp rotates
+// in phase 1 of step s + 1), and V rows 2w, 2w + 1 stay in shared memory for
+// the whole solve (V <- V G only mixes columns).  Per step the only global
+// traffic is the X rows of each pair and the rotation parameters: phase 1
+// writes them, one grid barrier, phase 2 reads them back.  Requires every
+// pair to have a resident warp (the host checks co-residency).
+__global__ void __launch_bounds__(256)
+k_jacobi3(double2* __restrict__ A, double2* __restrict__ V, double2* __restrict__ X, int n,
+          int max_sweeps, double tol2, double* scratch, double* rot, int* sweeps_out) {
+    cg::grid_group grid = cg::this_grid();
+    extern __shared__ double2 jsm[];
+    __shared__ double red[32];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    const int gw = blockIdx.x * wpb + wib;
+    const int m = n + (n & 1), npairs = m / 2, nsteps = m - 1;
+    double* rs_s = reinterpret_cast<double*>(jsm);  // 4 * npairs doubles
+    double2* wbase = jsm + 2 * (size_t)npairs + (size_t)wib * 6 * n;
+    double2* sA = wbase;          // rows p, q of this warp's pair
+    double2* sV = wbase + 2 * n;  // V rows 2w, 2w + 1 (ping-pong with sT)
+    double2* sT = wbase + 4 * n;  // staging for X rows / next V rows
+    const bool active = gw < npairs;
+    const int r0 = 2 * gw, r1 = 2 * gw + 1;
+    const size_t nn = (size_t)n * n;
+    const size_t gtid = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    const size_t gstride = (size_t)gridDim.x * blockDim.x;
+    double tot = 0.0;
+    for (size_t t = gtid; t < nn; t += gstride) tot += A[t].x * A[t].x + A[t].y * A[t].y;
+    tot = block_sum(tot, red);
+    if (threadIdx.x == 0) atomicAdd(&scratch[0], tot);
+    int p = 0, q = 0;
+    if (active) {
+        jac_pair(m, 0, gw, p, q);
+        for (int k = lane; k < n; k += 32) {
+            sA[k] = A[(size_t)p * n + k];
+            sA[n + k] = q < n ? A[(size_t)q * n + k] : make_double2(0.0, 0.0);
+            sV[k] = make_double2(k == r0 ? 1.0 : 0.0, 0.0);
+            sV[n + k] = make_double2(k == r1 ? 1.0 : 0.0, 0.0);
+        }
+    }
+    grid.sync();
+    const double total = scratch[0];
+    int sweep = 0;
+    bool converged = false;
+    for (; sweep < max_sweeps && !converged; ++sweep) {
+        for (int s = 0; s < nsteps; ++s) {
+            double* rs = rot + 4 * (size_t)npairs * (s & 1);
+            // ---- phase 1: rotation of this warp's pair from its rows on chip
+            if (active) {
+                jac_pair(m, s, gw, p, q);
+                double c = 1.0, sn = 0.0, phr = 1.0, phi = 0.0;
+                if (q < n) {
+                    const double2 apq = sA[q];
+                    const double app = sA[p].x, aqq = sA[n + q].x;
+                    const double bm = hypot(apq.x, apq.y);
+                    if (bm > 1e-300 && bm > 1e-18 * sqrt(fabs(app * aqq))) {
+                        phr = apq.x / bm;
+                        phi = apq.y / bm;
+                        const double tau = (aqq - app) / (2.0 * bm);
+                        const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+                        c = 1.0 / sqrt(1.0 + t * t);
+                        sn = t * c;
+                    }
+                    for (int k = lane; k < n; k += 32) {
+                        const double2 apk = sA[k], aqk = sA[n + k];
+                        const double2 pa = make_double2(phr * aqk.x - phi * aqk.y, phr * aqk.y + phi * aqk.x);
+                        X[(size_t)p * n + k] = make_double2(c * apk.x - sn * pa.x, c * apk.y - sn * pa.y);
+                        X[(size_t)q * n + k] = make_double2(sn * apk.x + c * pa.x, sn * apk.y + c * pa.y);
+                    }
+                } else {
+                    for (int k = lane; k < n; k += 32) X[(size_t)p * n + k] = sA[k];
+                }
+                if (lane == 0) {
+                    rs[4 * gw + 0] = c; rs[4 * gw + 1] = sn; rs[4 * gw + 2] = phr; rs[4 * gw + 3] = phi;
+                }
+            }
+            grid.sync();
+            // ---- phase 2: rows of the next pair, A[r] = X[r] G(s); V <- V G(s)
+            const int s2 = (s + 1) % nsteps;
+            int p2 = 0, q2 = 0;
+            if (active) {
+                jac_pair(m, s2, gw, p2, q2);
+                for (int k = lane; k < n; k += 32) {
+                    sT[k] = X[(size_t)p2 * n + k];
+                    if (q2 < n) sT[n + k] = X[(size_t)q2 * n + k];
+                }
+            }
+            for (int i = threadIdx.x; i < 4 * npairs; i += blockDim.x) rs_s[i] = rs[i];
+            __syncthreads();
+            if (active) {
+                auto mix = [&](const double2* src, int k) -> double2 {
+                    int pi, partner;
+                    jac_partner(m, s, k, pi, partner);
+                    const double2 xk = src[k];
+                    if (partner >= n) return xk;
+                    const double c = rs_s[4 * pi + 0], sn = rs_s[4 * pi + 1];
+                    const double phr = rs_s[4 * pi + 2], phi = rs_s[4 * pi + 3];
+                    const double2 xp = src[partner];
+                    if (k < partner) {
+                        const double2 qc = make_double2(phr * xp.x + phi * xp.y, phr * xp.y - phi * xp.x);
+                        return make_double2(c * xk.x - sn * qc.x, c * xk.y - sn * qc.y);
+                    }
+                    const double2 qc = make_double2(phr * xk.x + phi * xk.y, phr * xk.y - phi * xk.x);
+                    return make_double2(sn * xp.x + c * qc.x, sn * xp.y + c * qc.y);
+                };
+                __syncwarp();
+                for (int k = lane; k < n; k += 32) {
+                    sA[k] = mix(sT, k);
+                    if (q2 < n) sA[n + k] = mix(sT + n, k);
+                }
+                __syncwarp();
+                for (int k = lane; k < n; k += 32) {
+                    if (r0 < n) sT[k] = mix(sV, k);
+                    if (r1 < n) sT[n + k] = mix(sV + n, k);
+                }
+                __syncwarp();
+                double2* t = sV; sV = sT; sT = t;
+            }
+        }
+        // off-diagonal norm of this warp's rows (the pair of step 0)
+        double off = 0.0;
+        if (active) {
+            jac_pair(m, 0, gw, p, q);
+            for (int k = lane; k < n; k += 32) {
+                if (k != p) off += sA[k].x * sA[k].x + sA[k].y * sA[k].y;
+                if (q < n && k != q) off += sA[n + k].x * sA[n + k].x + sA[n + k].y * sA[n + k].y;
+            }
+        }
+        off = block_sum(off, red);
+        if (threadIdx.x == 0) atomicAdd(&scratch[1 + sweep], off);
+        grid.sync();
+        converged = scratch[1 + sweep] <= tol2 * total;
+    }
+    if (active) {
+        jac_pair(m, 0, gw, p, q);
+        for (int k = lane; k < n; k += 32) {
+            A[(size_t)p * n + k] = sA[k];
+            if (q < n) A[(size_t)q * n + k] = sA[n + k];
+            if (r0 < n) V[(size_t)r0 * n + k] = sV[k];
+            if (r1 < n) V[(size_t)r1 * n + k] = sV[n + k];
+        }
+    }
+    if (gtid == 0) *sweeps_out = converged ? sweep : max_sweeps;
+}
+
 // Sort eigenvalues ascending (stable by index) and permute eigenvector columns.
 __global__ void __launch_bounds__(1024)
 k_sort_eig(const double2* __restrict__ A, const double2* __restrict__ V, int n,
@@ -658,14 +804,28 @@ cudaError_t jacobi(double2* A, double2* V, int n, int max_sweeps, double tol2, d
     double* rot = scratch + 1 + max_sweeps;
     double2* X = (double2*)(rot + 8 * (size_t)(npairs + 1));
     if (((uintptr_t)X) & 15) X = (double2*)(((uintptr_t)X + 15) & ~(uintptr_t)15);
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    // on-chip variant: one warp per pair, all warps co-resident
+    for (int wpb = 8; wpb >= 1; wpb >>= 1) {
+        const size_t smem3 = (size_t)npairs * 4 * sizeof(double) + (size_t)wpb * 6 * n * sizeof(double2);
+        if (smem3 > 200 * 1024) continue;
+        cudaFuncSetAttribute(k_jacobi3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem3);
+        int per_sm3 = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm3, k_jacobi3, 32 * wpb, smem3);
+        const int blocks3 = (npairs + wpb - 1) / wpb;
+        if (per_sm3 < 1 || blocks3 > sms * per_sm3) continue;
+        void* args3[] = {&A, &V, &X, &n, &max_sweeps, &tol2, &scratch, &rot, &sweeps_out};
+        return cudaLaunchCooperativeKernel((const void*)k_jacobi3, dim3(blocks3), dim3(32 * wpb),
+                                           args3, smem3, st);
+    }
     const int warps_per_block = 8;
     int blocks = (npairs + warps_per_block - 1) / warps_per_block;
     const size_t smem = (size_t)warps_per_block * n * sizeof(double2);
     if (smem > 48 * 1024)
         cudaFuncSetAttribute(k_jacobi2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_jacobi2, 256, smem);
     if (per_sm < 1) per_sm = 1;
     if (blocks > sms * per_sm) blocks = sms * per_sm;

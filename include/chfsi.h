@@ -76,8 +76,6 @@ enum {
     CHFSI_BOUND_HEURISTIC = 0, /* chebyshev.rs:225-254: 1/2 Gmax^2 + (maxV - minV) */
     CHFSI_BOUND_LANCZOS   = 1  /* k-step Lanczos: lambda_max(T_k) + |f_k| (Zhou 2010) */
 };
-/* Density mixer. */
-enum { CHFSI_MIX_PULAY = 0, CHFSI_MIX_LINEAR = 1 };
 
 /* ------------------------------------------------------------------------ */
 /* Synthetic systems (the seeded inputs of the benchmark configurations).   */
@@ -275,7 +273,23 @@ typedef struct chfsi_scf_params {
     double fp64_switch_per_atom; /* mixed precision: switch the filter to FP64 once
                                     |dE|/atom < this (convergence is only declared on
                                     FP64 steps)                                        */
+    int    mixer;         /* CHFSI_MIXER_PULAY / _LEARNED / _LEARNED_PULAY            */
+    int    reserved;
+    double* trace;        /* optional host buffer of 2 * max_iter * N^3 doubles: rho_in
+                             and rho_out of every iteration (training trajectories)   */
 } chfsi_scf_params;
+
+/* Density mixers of chfsi_scf_run.  PULAY: Pulay/DIIS over (rho_in,
+ * rho_out - rho_in) with scalar alpha (mixing.rs:24 as planned in the crate).
+ * LEARNED: rho_next(G) = rho_in(G) + a_s R(G) + b_s (rho_in - rho_in_prev)(G)
+ * with (a_s, b_s) per |G| shell from the MLP of chfsi_set_mixer.
+ * LEARNED_PULAY: Pulay extrapolation with the MLP's a_s as per-shell
+ * preconditioner in place of alpha.  Both learned modes fall back to plain
+ * Pulay for the rest of the run once the residual norm rises two steps in a
+ * row (the Pulay history is kept up to date throughout). */
+#define CHFSI_MIXER_PULAY 0
+#define CHFSI_MIXER_LEARNED 1
+#define CHFSI_MIXER_LEARNED_PULAY 2
 
 typedef struct chfsi_scf_result {
     int     status;       /* CHFSI_OK (converged), CHFSI_NOT_CONVERGED or error */
@@ -287,12 +301,53 @@ typedef struct chfsi_scf_result {
     double  seconds;      /* device time of the whole loop                      */
     double* energies;     /* caller array of max_iter entries, or NULL          */
     double* eigenvalues;  /* caller array of n_bands entries, or NULL           */
+    int     n_iter_learned; /* iterations mixed by the learned mixer            */
+    int     fell_back;    /* 1 if a learned run fell back to Pulay              */
+    double* residuals;    /* caller array of max_iter entries (|rho_out - rho_in|_2
+                             on the grid), or NULL                              */
 } chfsi_scf_result;
 
 /* Full SCF from a uniform density: build_v_eff -> diagonalize -> density ->
  * energy -> check -> Pulay mix (run_scf, src/scf.rs:358-376).  Returns
  * CHFSI_OK when converged, CHFSI_NOT_CONVERGED after max_iter. */
 chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p, chfsi_scf_result* r);
+
+/* ---- learned density mixer (no counterpart in the reference crate) ------
+ * MLP 512 -> 256 -> 256 -> 128 with GELU, BF16 weights and FP32 accumulation.
+ * Input: the last 4 density residuals R_0..R_3 binned into 64 |G| shells:
+ * per shell (|R_0|^2, Re<R_0, D>) and, for t = 1..3, (Re<R_0, R_t>, |R_t|^2),
+ * each over the total |R_0|^2 (x 64) and compressed by sign(x) log(1 + |x|);
+ * D = rho_in - rho_in_prev.  Output: per shell (a_s, b_s).
+ * Training targets per shell (a*, b*, M00, M01, M11): the least-squares
+ * (a, b) of rho* - rho_in ~ a R_0 + b D and its normal matrix M over
+ * |rho* - rho_in|^2; the loss sum_s (y_s - y*_s)^T M_s (y_s - y*_s) is the
+ * relative density error left after the update. */
+#define CHFSI_MIXER_SHELLS 64
+#define CHFSI_MIXER_FEATURES 512
+#define CHFSI_MIXER_OUTPUTS 128
+#define CHFSI_MIXER_TARGETS 320   /* 64 shells x 5 */
+typedef struct chfsi_mixer chfsi_mixer;
+chfsi_status chfsi_mixer_create(int device, uint64_t seed, chfsi_mixer** out);
+void         chfsi_mixer_destroy(chfsi_mixer* m);
+size_t       chfsi_mixer_num_params(void);
+/* fp32 master parameters: W1 (256x512), b1, W2 (256x256), b2, W3 (128x256), b3 */
+chfsi_status chfsi_mixer_get_params(chfsi_mixer* m, float* out);
+chfsi_status chfsi_mixer_set_params(chfsi_mixer* m, const float* in);
+/* host x (batch x 512) -> host y (batch x 128) */
+chfsi_status chfsi_mixer_forward(chfsi_mixer* m, const float* x, int batch, float* y);
+/* loss and gradient (num_params floats) of one batch; host arrays */
+chfsi_status chfsi_mixer_gradient(chfsi_mixer* m, const float* x, const float* t, int batch,
+                                  float* grad, float* loss);
+/* Adam (lr, beta 0.9/0.999) over n samples resident on the device, shuffled
+ * minibatches from seed; loss_per_epoch (epochs floats) may be NULL. */
+chfsi_status chfsi_mixer_train(chfsi_mixer* m, const float* x, const float* t, int n, int epochs,
+                               int batch, float lr, uint64_t seed, float* loss_per_epoch);
+/* use m in chfsi_scf_run when params.mixer is LEARNED or LEARNED_PULAY (NULL to detach) */
+chfsi_status chfsi_set_mixer(chfsi_ctx* ctx, chfsi_mixer* m);
+/* features (n_iter x 512) and targets (n_iter x 320) of one SCF trajectory on
+ * this context's grid: rho_in / rho_out are n_iter x N^3, rho_star N^3 */
+chfsi_status chfsi_mixer_samples(chfsi_ctx* ctx, const double* rho_in, const double* rho_out,
+                                 int n_iter, const double* rho_star, float* x, float* t);
 
 #ifdef __cplusplus
 }

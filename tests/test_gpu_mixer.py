@@ -1,0 +1,119 @@
+"""Learned density mixer on the GPU against the CPU oracle
+(oracle/mixer_oracle.py): forward pass and gradients of the MLP (BF16
+weights, FP32 accumulation), shell features and least-squares targets of a
+recorded SCF trajectory, on-device training, and SCF runs driven by the
+learned mixer with Pulay as fallback."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+sys.path.insert(0, os.path.join(os.path.dirname(__file__), "..", "oracle"))
+import mixer_oracle as mo  # noqa: E402
+
+
+@pytest.fixture(scope="module")
+def sys0(chfsi):
+    return chfsi.SyntheticSystem(config_index=0)
+
+
+@pytest.fixture(scope="module")
+def traj(chfsi, sys0):
+    ctx = chfsi.Context(sys0)
+    r = ctx.run_scf(12, tol_per_atom=1e-9, max_iter=40, kT=0.01, trace=True)
+    assert r["converged"]
+    return ctx, r
+
+
+def _batch(seed, B):
+    rng = np.random.default_rng(seed)
+    x = rng.standard_normal((B, mo.N_IN)).astype(np.float32)
+    t = rng.standard_normal((B, mo.SHELLS, mo.N_T)).astype(np.float32)
+    t[:, :, 2] = np.abs(t[:, :, 2]) / mo.SHELLS
+    t[:, :, 4] = np.abs(t[:, :, 4]) / mo.SHELLS
+    t[:, :, 3] = 0.1 * np.minimum(t[:, :, 2], t[:, :, 4]) * np.sign(t[:, :, 3])
+    return x, t.reshape(B, -1)
+
+
+def test_forward_matches_oracle(chfsi):
+    m = chfsi.Mixer(seed=5)
+    rng = np.random.default_rng(0)
+    p = (rng.standard_normal(m.num_params) * 0.05).astype(np.float32)
+    m.set_params(p)
+    np.testing.assert_array_equal(m.get_params(), p)
+    x, _ = _batch(1, 37)
+    y = m.forward(x)
+    yr, _ = mo.forward(p, x)
+    err = np.abs(y - yr).max() / np.abs(yr).max()
+    print("forward max rel error %.2e" % err)
+    assert err < 1e-4
+
+
+def test_gradient_matches_oracle(chfsi):
+    m = chfsi.Mixer(seed=6)
+    x, t = _batch(2, 64)
+    p = m.get_params()
+    g, loss = m.gradient(x, t)
+    lr, gr = mo.loss_grad(p, x, t)
+    rel = np.linalg.norm(g - gr) / np.linalg.norm(gr)
+    print("loss %.6e vs %.6e, gradient rel error %.2e" % (loss, lr, rel))
+    assert abs(loss - lr) <= 1e-4 * abs(lr)
+    assert rel < 1e-3
+    for lo, hi in [(mo.OFF_W1, mo.OFF_B1), (mo.OFF_W2, mo.OFF_B2), (mo.OFF_W3, mo.OFF_B3),
+                   (mo.OFF_B3, mo.N_PARAMS)]:
+        assert np.linalg.norm(g[lo:hi] - gr[lo:hi]) <= 2e-3 * np.linalg.norm(gr[lo:hi]) + 1e-12
+
+
+def test_samples_match_oracle(chfsi, sys0, traj):
+    ctx, r = traj
+    rin, rout = r["trace_in"], r["trace_out"]
+    star = rout[-1]
+    x, t = ctx.mixer_samples(rin, rout, star)
+    recip = 2 * np.pi * np.linalg.inv(sys0.lattice).T
+    xr, tr = mo.trajectory_samples(rin, rout, star, sys0.ngrid, recip)
+    assert np.isfinite(x).all() and np.isfinite(t).all()
+    np.testing.assert_allclose(x, xr, atol=2e-4, rtol=1e-4)
+    tr3 = tr.reshape(len(rin), mo.SHELLS, mo.N_T)
+    t3 = t.reshape(len(rin), mo.SHELLS, mo.N_T)
+    # normal matrices: absolute (they are fractions of |E|^2)
+    np.testing.assert_allclose(t3[..., 2:], tr3[..., 2:], atol=1e-6, rtol=1e-4)
+    # optimal coefficients where the shell carries weight
+    w = tr3[..., 2] > 1e-6
+    np.testing.assert_allclose(t3[..., 0][w], tr3[..., 0][w], atol=1e-3, rtol=1e-3)
+
+
+def test_training_reduces_loss(chfsi, traj):
+    ctx, r = traj
+    x, t = ctx.mixer_samples(r["trace_in"], r["trace_out"], r["trace_out"][-1])
+    m = chfsi.Mixer(seed=7)
+    _, l0 = m.gradient(x, t)
+    losses = m.train(x, t, epochs=60, batch=8, lr=1e-3, seed=1)
+    _, l1 = m.gradient(x, t)
+    print("training loss %.4f -> %.4f (epochs: %s)" % (l0, l1, losses[[0, -1]]))
+    assert np.isfinite(losses).all()
+    assert l1 < 0.5 * l0
+
+
+@pytest.mark.parametrize("mode", ["learned", "learned_pulay"])
+def test_scf_with_untrained_mixer_reaches_pulay_energy(chfsi, sys0, mode):
+    """An untrained network mixes like linear alpha = 0.3 (its output bias);
+    the run must still end at the Pulay fixed point, falling back to Pulay if
+    its residual rises twice."""
+    ref = chfsi.Context(sys0).run_scf(12, max_iter=60, kT=0.01)
+    ctx = chfsi.Context(sys0)
+    m = chfsi.Mixer(seed=3)
+    ctx.set_mixer(m)
+    mixer = chfsi.MIXER_LEARNED if mode == "learned" else chfsi.MIXER_LEARNED_PULAY
+    r = ctx.run_scf(12, max_iter=60, kT=0.01, mixer=mixer)
+    print("%s: %d iterations (%d learned, fell back: %s) vs Pulay %d"
+          % (mode, r["n_iter"], r["n_iter_learned"], r["fell_back"], ref["n_iter"]))
+    assert r["converged"] and r["n_iter_learned"] >= 1
+    assert abs(r["e_total"] - ref["e_total"]) / sys0.n_atoms < 2e-6
+
+
+def test_learned_mode_requires_a_mixer(chfsi, sys0):
+    ctx = chfsi.Context(sys0)
+    with pytest.raises(chfsi.ChfsiError):
+        ctx.run_scf(12, max_iter=3, mixer=chfsi.MIXER_LEARNED)
