@@ -32,6 +32,10 @@ NDEG = 16
 CONFIG_INDEX = 1
 METRIC = "H|psi> band-applies/s (ChFSI iteration: degree-16 Chebyshev filter + Rayleigh-Ritz)"
 UNIT = "band-applies/s"
+# DRAM bytes (read + write) per band of one local H|psi> launch (the three
+# FFT-pass kernels, 160 bands: 1,147,462,656 bytes), from the ncu capture
+# summarised in profiles/local_hpsi_cfg1_traffic.md
+TRAFFIC_PER_BAND = 1147462656 / 160
 
 
 def peaks():
@@ -170,14 +174,23 @@ def run_ours(args):
     e1.synchronize()
     t_loc = e0.elapsed_time(e1) / reps * 1e-3
     ncol, nz = s.info.n_columns, s.ngrid[2]
-    bytes_per_band = 16 * (4 * ncol * nz + 4 * s.n_pw)  # sticks x4, psi x2, kin-scaled psi, out
+    n3 = s.ngrid[0] * s.ngrid[1] * s.ngrid[2]
+    # algorithmic bytes of one band-apply of local H|psi> for the fused 3-pass
+    # FFT: grid written, read+written, read (4 N^3) plus psi_k, psi_{k-1} in
+    # and psi_{k+1} out (3 n_pw), complex128
+    bytes_per_band = 16 * (4 * n3 + 3 * s.n_pw)
     algo_bytes = bytes_per_band * nb
+    # what this pruned design itself moves: only the (x, y) columns that hold
+    # plane waves are stored between the passes
+    pruned_bytes = 16 * (4 * ncol * nz + 4 * s.n_pw) * nb
     pk = peaks()
     achieved = algo_bytes / t_loc / 1e9
     roofline = {"kernel": "local H|psi> (z-sticks inverse, xy-planes x V, z-sticks forward)",
                 "bound": "hbm", "achieved": round(achieved, 1), "peak": pk["hbm_gbs"],
                 "unit": "GB/s", "frac": round(achieved / pk["hbm_gbs"], 4),
-                "traffic": None, "algorithmic_bytes_per_launch": algo_bytes,
+                "traffic": TRAFFIC_PER_BAND * nb if TRAFFIC_PER_BAND else None,
+                "algorithmic_bytes_per_launch": algo_bytes,
+                "pruned_design_bytes_per_launch": pruned_bytes,
                 "launch_ms": round(t_loc * 1e3, 4),
                 "peak_source": "measured" if not pk.get("fallback") else "fallback"}
 

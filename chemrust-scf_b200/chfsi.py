@@ -84,7 +84,7 @@ class SynthParams(C.Structure):
                 ("n_shell", C.c_int), ("rc_proj", C.c_double * 4), ("lmax", C.c_int),
                 ("d_min", C.c_double), ("d_max", C.c_double), ("uspp", C.c_int),
                 ("q_width", C.c_double), ("q_amp", C.c_double), ("kpt", C.c_double * 3),
-                ("seed", C.c_uint64)]
+                ("seed", C.c_uint64), ("ngrid_density", C.c_int * 3)]
 
 
 class SystemInfo(C.Structure):
@@ -92,7 +92,8 @@ class SystemInfo(C.Structure):
                 ("n_occ", C.c_int), ("n_atoms", C.c_int), ("n_proj", C.c_int),
                 ("n_ions_with_proj", C.c_int), ("n_columns", C.c_int), ("omega", C.c_double),
                 ("n_elec", C.c_double), ("gmax", C.c_double), ("e_ewald", C.c_double),
-                ("lattice", C.c_double * 9)]
+                ("lattice", C.c_double * 9), ("ngrid_density", C.c_int * 3),
+                ("q_width", C.c_double), ("uspp", C.c_int)]
 
 
 class Dims(C.Structure):
@@ -189,6 +190,9 @@ def lib():
         "chfsi_mixer_train": [vp, fp, fp, C.c_int, C.c_int, C.c_int, C.c_float, C.c_uint64, fp],
         "chfsi_set_mixer": [vp, vp],
         "chfsi_mixer_samples": [vp, dp, dp, C.c_int, dp, fp, fp],
+        "chfsi_set_density_grid": [vp, C.POINTER(C.c_int)],
+        "chfsi_get_density_grid": [vp, C.POINTER(C.c_int)],
+        "chfsi_set_augmentation": [vp, dp, C.c_double],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -316,7 +320,7 @@ class SyntheticSystem:
             _check(L.chfsi_synth_defaults(0 if config_index is None else config_index,
                                           C.byref(params)))
         for k, v in overrides.items():
-            if k in ("ngrid", "rc_proj", "kpt"):
+            if k in ("ngrid", "rc_proj", "kpt", "ngrid_density"):
                 arr = getattr(params, k)
                 for i, x in enumerate(v):
                     arr[i] = x
@@ -334,6 +338,9 @@ class SyntheticSystem:
         self.n_atoms, self.n_proj, self.n_ions = info.n_atoms, info.n_proj, info.n_ions_with_proj
         self.omega, self.n_elec, self.gmax, self.e_ewald = info.omega, info.n_elec, info.gmax, info.e_ewald
         self.lattice = np.array(info.lattice[:]).reshape(3, 3)
+        self.ngrid_density = tuple(info.ngrid_density)
+        self.ng_density = int(np.prod(self.ngrid_density))
+        self.uspp, self.q_width = bool(info.uspp), info.q_width
 
     def __del__(self):
         if getattr(self, "handle", None) and _lib is not None:
@@ -412,6 +419,22 @@ class Context:
             self.ngrid, self.n_pw, self.n_bands = tuple(dims["ngrid"]), d.n_pw, d.n_bands
         self.handle = h
         self.ng = int(np.prod(self.ngrid))
+        self._refresh_density_grid()
+
+    def _refresh_density_grid(self):
+        n3 = (C.c_int * 3)()
+        _check(lib().chfsi_get_density_grid(self.handle, n3))
+        self.ngrid_density = tuple(n3)
+        self.ng_density = int(np.prod(self.ngrid_density))
+
+    def set_density_grid(self, ngrid):
+        n3 = (C.c_int * 3)(*ngrid)
+        self._c(lib().chfsi_set_density_grid(self.handle, n3))
+        self._refresh_density_grid()
+
+    def set_augmentation(self, positions, width):
+        p = np.ascontiguousarray(positions, dtype=np.float64).ravel()
+        self._c(lib().chfsi_set_augmentation(self.handle, _ptr(p, C.c_double), width))
 
     def close(self):
         if getattr(self, "handle", None) and _lib is not None:
@@ -471,7 +494,8 @@ class Context:
         self._c(lib().chfsi_set_occupations(self.handle, _ptr(o, C.c_double)))
 
     def get_vloc(self):
-        v = np.zeros(self.ng)
+        """V_loc on the density grid."""
+        v = np.zeros(self.ng_density)
         self._c(lib().chfsi_get_vloc(self.handle, _ptr(v, C.c_double)))
         return v
 
@@ -536,7 +560,8 @@ class Context:
 
     # --- SCF ---------------------------------------------------------------
     def construct_density(self):
-        r = np.zeros(self.ng)
+        """rho on the density grid (with augmentation when set)."""
+        r = np.zeros(self.ng_density)
         self._c(lib().chfsi_construct_density(self.handle, _ptr(r, C.c_double)))
         return r
 
@@ -547,7 +572,7 @@ class Context:
         return e2
 
     def get_density(self):
-        r = np.zeros(self.ng)
+        r = np.zeros(self.ng_density)
         self._c(lib().chfsi_get_density(self.handle, _ptr(r, C.c_double)))
         return r
 
@@ -561,7 +586,7 @@ class Context:
                       fp64_switch_per_atom, mixer, 0, None)
         tr = None
         if trace:
-            tr = np.zeros((max_iter, 2, self.ng))
+            tr = np.zeros((max_iter, 2, self.ng_density))
             p.trace = _ptr(tr, C.c_double)
         energies = np.zeros(max_iter)
         residuals = np.zeros(max_iter)
@@ -592,8 +617,8 @@ class Context:
 
     def mixer_samples(self, rho_in, rho_out, rho_star):
         """Features (T x 512) and targets (T x 320) of one trajectory on this grid."""
-        a = np.ascontiguousarray(rho_in, dtype=np.float64).reshape(-1, self.ng)
-        b = np.ascontiguousarray(rho_out, dtype=np.float64).reshape(-1, self.ng)
+        a = np.ascontiguousarray(rho_in, dtype=np.float64).reshape(-1, self.ng_density)
+        b = np.ascontiguousarray(rho_out, dtype=np.float64).reshape(-1, self.ng_density)
         st = np.ascontiguousarray(rho_star, dtype=np.float64).ravel()
         T = a.shape[0]
         x = np.zeros((T, MIXER_FEATURES), dtype=np.float32)

@@ -122,26 +122,30 @@ __global__ void k_conj(const double2* __restrict__ a, double2* __restrict__ b, s
 
 // Chebyshev step of the generalised problem: y = S^-1 H x = hx - corr, then
 // the recurrence epilogue of the local pass (first degree / later degrees).
+// C = double2 (FP64 filter) or float2 (FP32 filter; norms still summed in FP64).
+template <typename C>
 __global__ void __launch_bounds__(256)
-k_cheb_combine(const double2* __restrict__ hx, const double2* __restrict__ corr,
-               const double2* __restrict__ x, double2* out, size_t n, const double* coef, int mode,
-               double* norm_acc) {
+k_cheb_combine(const C* __restrict__ hx, const C* __restrict__ corr, const C* __restrict__ x,
+               C* out, size_t n, const double* coef, int mode, double* norm_acc) {
+    using R = decltype(C{}.x);
     __shared__ double red[8];
-    const double ie = coef[4], nc = coef[5];
+    const R ie = (R)coef[4], nc = (R)coef[5];
     double acc = 0.0;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
          i += (size_t)gridDim.x * blockDim.x) {
-        const double2 h = make_double2(hx[i].x - corr[i].x, hx[i].y - corr[i].y);
-        const double2 p = x[i];
-        const double2 s = make_double2(h.x * ie + nc * p.x, h.y * ie + nc * p.y);
-        double2 o;
-        if (mode == 1) o = s;
+        const R hr = hx[i].x - corr[i].x, hi = hx[i].y - corr[i].y;
+        const C p = x[i];
+        const R sr = hr * ie + nc * p.x, si = hi * ie + nc * p.y;
+        R orr, oi;
+        if (mode == 1) { orr = sr; oi = si; }
         else {
-            const double2 prev = out[i];
-            o = make_double2(2.0 * s.x - prev.x, 2.0 * s.y - prev.y);
+            const C prev = out[i];
+            orr = (R)2 * sr - prev.x;
+            oi = (R)2 * si - prev.y;
         }
-        out[i] = o;
-        acc += o.x * o.x + o.y * o.y;
+        out[i].x = orr;
+        out[i].y = oi;
+        acc += (double)orr * orr + (double)oi * oi;
     }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
@@ -278,6 +282,26 @@ struct chfsi_ctx {
     TcPlanes tp_beta_a, tp_betaT_b, tp_psi_b, tp_psi_a, tp_hpsi_b, tp_small_a, tp_psiT_b;
     float* d_tc_part = nullptr; int* d_tc_err = nullptr;
     bool beta_planes_ready = false;
+    // density grid: density, potentials, mixing and augmentation live here.
+    // It is the wavefunction grid unless chfsi_set_density_grid chose a
+    // finer one; then the smooth density is interpolated up by zero padding
+    // in G and V_eff comes back by truncation.
+    int fnx = 0, fny = 0, fnz = 0; size_t fng = 0;
+    AxisPlan fax{}, fay{}, faz{};
+    std::vector<int> fdr[3];
+    int* d_fidr[3] = {nullptr, nullptr, nullptr};
+    bool fine = false;
+    int* d_gmap_w = nullptr; int* d_gmap_f = nullptr; int n_gmap = 0;  // shared G vectors
+    double* d_veff_d = nullptr;   // V_eff on the density grid
+    double* d_rho_w = nullptr;    // smooth density on the wavefunction grid
+    double2* d_wgrid = nullptr;   // wavefunction-grid complex scratch
+    // ultrasoft augmentation Q_ij(r) = q_ij g(|r - R_I|)
+    bool aug = false; double aug_width = 0.0;
+    std::vector<double> ion_pos;  // ions with projectors, x 3 (bohr)
+    double2* d_phase = nullptr;   // per ion e^{-i 2 pi f_d h}: [ion][fnx | fny | fnz]
+    double2* d_dmat0 = nullptr;   // unscreened D
+    double* d_cion = nullptr;     // per ion sum_n f_n C^H q C
+    double* d_vion = nullptr;     // per ion int V_eff g(r - R_I)
     // learned density mixer (G-space residual history on the density grid)
     chfsi_mixer* mixer = nullptr;
     unsigned char* d_shell = nullptr;  // |G| shell per grid point (digit-reversed layout)
@@ -364,7 +388,7 @@ chfsi_status apply_op_dev(chfsi_ctx* ctx, const double2* x, double2* out, int nb
             0.0, st);
     const size_t n = (size_t)nb * ctx->n_pw;
     count_launch();
-    k_cheb_combine<<<grid_for(n), 256, 0, st>>>(ctx->d_hpsi, ctx->d_sx, x, out, n, ctx->d_coef,
+    k_cheb_combine<double2><<<grid_for(n), 256, 0, st>>>(ctx->d_hpsi, ctx->d_sx, x, out, n, ctx->d_coef,
                                                  mode == kEpiChebFirst ? 1 : 2, norm_acc);
     CK(cudaGetLastError());
     return CHFSI_OK;
@@ -563,6 +587,31 @@ chfsi_status apply_h_dev32(chfsi_ctx* ctx, const float2* psi, float2* out, int n
     return CHFSI_OK;
 }
 
+// S^-1 H x for the FP32 filter of the generalised problem: H x (FP32 local
+// pass), C = beta^H Hx (tcgen05), M C (FP64), beta (M C) (tcgen05, FP32
+// out), then the recurrence epilogue in k_cheb_combine<float2>.
+chfsi_status apply_op_dev32(chfsi_ctx* ctx, const float2* x, float2* out, int nb, int mode,
+                            double* norm_acc) {
+    if (!ctx->uspp || mode == kEpiApply) return apply_h_dev32(ctx, x, out, nb, mode, norm_acc);
+    chfsi_status s = apply_h_dev32(ctx, x, ctx->d_hpsi32, nb, kEpiApply, nullptr);
+    if (s) return s;
+    cudaStream_t st = ctx->st;
+    tc_pack<float2>(ctx->d_hpsi32, ctx->n_pw, nb, ctx->n_pw, false, kSrcPlain, ctx->tp_psi_b, st);
+    CK(tc_gemm(ctx->tp_beta_a, ctx->tp_psi_b, ctx->np, nb, ctx->n_pw, kTcOutPartial, ctx->d_cp, nb,
+               ctx->d_tc_part, ctx->d_tc_err, st));
+    gemm_tn(ctx->d_sinvT, ctx->np, ctx->d_cp, nb, ctx->d_cq, nb, ctx->np, nb, ctx->np, 1.0, 0.0, st);
+    tc_pack<double2>(ctx->d_cq, nb, nb, ctx->np, true, kSrcConjT, ctx->tp_small_a, st);
+    CK(tc_gemm(ctx->tp_small_a, ctx->tp_betaT_b, nb, ctx->n_pw, ctx->np, kTcOutComplexF32,
+               ctx->d_nl32, ctx->n_pw, nullptr, ctx->d_tc_err, st));
+    const size_t n = (size_t)nb * ctx->n_pw;
+    count_launch();
+    k_cheb_combine<float2><<<grid_for(n), 256, 0, st>>>(ctx->d_hpsi32, ctx->d_nl32, x, out, n,
+                                                         ctx->d_coef, mode == kEpiChebFirst ? 1 : 2,
+                                                         norm_acc);
+    CK(cudaGetLastError());
+    return CHFSI_OK;
+}
+
 chfsi_status filter_dev32(chfsi_ctx* ctx, int ndeg, const double* eig_dev, int n_eig) {
     if (ndeg < 0 || ndeg > ctx->max_deg) return ctx->fail(CHFSI_ERR_BAD_INPUT, "ndeg out of range");
     if (ctx->np > 0 && !ctx->beta_planes_ready) {
@@ -581,11 +630,11 @@ chfsi_status filter_dev32(chfsi_ctx* ctx, int ndeg, const double* eig_dev, int n
     float2* A = ctx->d_psi32a;
     float2* B = ctx->d_psi32b;
     if (ndeg >= 1) {
-        s = apply_h_dev32(ctx, A, B, ctx->nb, kEpiChebFirst, ctx->d_nsq + 1);
+        s = apply_op_dev32(ctx, A, B, ctx->nb, kEpiChebFirst, ctx->d_nsq + 1);
         if (s) return s;
     }
     for (int k = 2; k <= ndeg; ++k) {
-        s = apply_h_dev32(ctx, B, A, ctx->nb, kEpiCheb, ctx->d_nsq + k);
+        s = apply_op_dev32(ctx, B, A, ctx->nb, kEpiCheb, ctx->d_nsq + k);
         if (s) return s;
         std::swap(A, B);
     }
@@ -614,6 +663,17 @@ chfsi_status rr_dev32(chfsi_ctx* ctx) {
     symmetrize(ctx->d_T1, ctx->d_H, n, st);
     CK(tc_gemm(ctx->tp_psi_a, ctx->tp_psi_b, n, n, npw, kTcOutPartial, ctx->d_T1, n, ctx->d_tc_part,
                ctx->d_tc_err, st));
+    if (ctx->uspp) {
+        // S_sub += C^H q C, C = beta^H psi (tcgen05, FP64 out); the rest in FP64
+        CK(tc_gemm(ctx->tp_beta_a, ctx->tp_psi_b, ctx->np, n, npw, kTcOutPartial, ctx->d_cp, n,
+                   ctx->d_tc_part, ctx->d_tc_err, st));
+        count_launch();
+        k_apply_dmat<<<grid_for((size_t)ctx->np * n), 256, 0, st>>>(
+            ctx->d_cp, ctx->d_cd, ctx->np, n, ctx->d_proj_ion, ctx->d_poff, ctx->d_doff, ctx->d_qmat);
+        count_launch();
+        k_conj<<<grid_for((size_t)ctx->np * n), 256, 0, st>>>(ctx->d_cp, ctx->d_cq, (size_t)ctx->np * n);
+        gemm_tn(ctx->d_cq, n, ctx->d_cd, n, ctx->d_T1, n, n, n, ctx->np, 1.0, 1.0, st);
+    }
     symmetrize(ctx->d_T1, ctx->d_S, n, st);
     cholesky(ctx->d_S, n, ctx->d_flags + 0, st);
     tri_inv(ctx->d_S, ctx->d_T1, n, st);
@@ -693,7 +753,15 @@ chfsi_status finish_diag(chfsi_ctx* ctx, double* eig_out, bool have_rr) {
 }
 
 // ---------------------------------------------------------------- potentials
+// 3D FFT on the density grid (unnormalised; digit-reversed G layout)
 void grid_fft3(chfsi_ctx* ctx, double2* g, bool forward) {
+    launch_axis_fft<double2>(g, ctx->fnx, ctx->fny, ctx->fnz, 0, forward, ctx->fax, ctx->st);
+    launch_axis_fft<double2>(g, ctx->fnx, ctx->fny, ctx->fnz, 1, forward, ctx->fay, ctx->st);
+    launch_axis_fft<double2>(g, ctx->fnx, ctx->fny, ctx->fnz, 2, forward, ctx->faz, ctx->st);
+}
+
+// 3D FFT on the wavefunction grid
+void wave_fft3(chfsi_ctx* ctx, double2* g, bool forward) {
     launch_axis_fft<double2>(g, ctx->nx, ctx->ny, ctx->nz, 0, forward, ctx->ax, ctx->st);
     launch_axis_fft<double2>(g, ctx->nx, ctx->ny, ctx->nz, 1, forward, ctx->ay, ctx->st);
     launch_axis_fft<double2>(g, ctx->nx, ctx->ny, ctx->nz, 2, forward, ctx->az, ctx->st);
@@ -701,47 +769,185 @@ void grid_fft3(chfsi_ctx* ctx, double2* g, bool forward) {
 
 GridRecip grid_recip(chfsi_ctx* ctx) {
     GridRecip gr{};
-    gr.nx = ctx->nx; gr.ny = ctx->ny; gr.nz = ctx->nz;
-    gr.idr_x = ctx->d_idr[0]; gr.idr_y = ctx->d_idr[1]; gr.idr_z = ctx->d_idr[2];
+    gr.nx = ctx->fnx; gr.ny = ctx->fny; gr.nz = ctx->fnz;
+    gr.idr_x = ctx->d_fidr[0]; gr.idr_y = ctx->d_fidr[1]; gr.idr_z = ctx->d_fidr[2];
     std::memcpy(gr.b, ctx->recip, sizeof(gr.b));
     return gr;
 }
 
-// veff = vloc + V_H[rho] + V_xc[rho]; acc[0] += E_H[rho], acc[1] += E_xc[rho]
-chfsi_status build_veff_dev(chfsi_ctx* ctx, const double* rho, double* acc) {
-    launch_real_to_complex(rho, ctx->d_cgrid, ctx->ng, ctx->st);
+// V_eff of the density grid -> the wavefunction grid (G truncation) + min/max
+void project_veff(chfsi_ctx* ctx) {
+    cudaStream_t st = ctx->st;
+    if (!ctx->fine) {
+        cudaMemcpyAsync(ctx->d_veff, ctx->d_veff_d, sizeof(double) * ctx->ng,
+                        cudaMemcpyDeviceToDevice, st);
+    } else {
+        launch_real_to_complex(ctx->d_veff_d, ctx->d_cgrid, ctx->fng, st);
+        grid_fft3(ctx, ctx->d_cgrid, true);
+        cudaMemsetAsync(ctx->d_wgrid, 0, sizeof(double2) * ctx->ng, st);
+        launch_scatter_g(ctx->d_cgrid, ctx->d_gmap_f, ctx->d_gmap_w, ctx->n_gmap,
+                         1.0 / (double)ctx->fng, ctx->d_wgrid, st);
+        wave_fft3(ctx, ctx->d_wgrid, false);
+        launch_take_real(ctx->d_wgrid, ctx->d_veff, ctx->ng, st);
+    }
+    minmax(ctx->d_veff, ctx->ng, ctx->d_minmax, st);
+}
+
+// Screened D = D0 + q v_I from the density-grid V_eff (ultrasoft only).
+chfsi_status screen_dmat(chfsi_ctx* ctx) {
+    if (!ctx->aug) return CHFSI_OK;
+    cudaStream_t st = ctx->st;
+    launch_real_to_complex(ctx->d_veff_d, ctx->d_cgrid, ctx->fng, st);
     grid_fft3(ctx, ctx->d_cgrid, true);
-    launch_hartree_gspace(ctx->d_cgrid, grid_recip(ctx), ctx->omega, acc + 0, ctx->st);
-    grid_fft3(ctx, ctx->d_cgrid, false);
-    launch_assemble_veff(ctx->d_vloc, ctx->d_cgrid, rho, ctx->d_veff, ctx->ng,
-                         ctx->omega / (double)ctx->ng, acc + 1, ctx->st);
-    minmax(ctx->d_veff, ctx->ng, ctx->d_minmax, ctx->st);
+    CK(cudaMemsetAsync(ctx->d_vion, 0, sizeof(double) * ctx->nions, st));
+    launch_ion_potential(ctx->d_cgrid, grid_recip(ctx), ctx->d_phase, ctx->nions, ctx->aug_width,
+                         1.0 / (double)ctx->fng, ctx->d_vion, st);
+    launch_screen_d(ctx->d_dmat0, ctx->d_qmat, ctx->d_vion, ctx->d_poff, ctx->d_doff, ctx->nions,
+                    ctx->d_dmat, st);
     CK(cudaGetLastError());
     return CHFSI_OK;
 }
 
+// veff = vloc + V_H[rho] + V_xc[rho]; acc[0] += E_H[rho], acc[1] += E_xc[rho]
+chfsi_status build_veff_dev(chfsi_ctx* ctx, const double* rho, double* acc) {
+    const size_t ng = ctx->fng;
+    launch_real_to_complex(rho, ctx->d_cgrid, ng, ctx->st);
+    grid_fft3(ctx, ctx->d_cgrid, true);
+    launch_hartree_gspace(ctx->d_cgrid, grid_recip(ctx), ctx->omega, acc + 0, ctx->st);
+    grid_fft3(ctx, ctx->d_cgrid, false);
+    launch_assemble_veff(ctx->d_vloc, ctx->d_cgrid, rho, ctx->d_veff_d, ng,
+                         ctx->omega / (double)ng, acc + 1, ctx->st);
+    project_veff(ctx);
+    CK(cudaGetLastError());
+    return CHFSI_OK;
+}
+
+// rho (density grid) = sum_n f_n |psi_n|^2 (+ augmentation)
 chfsi_status density_dev(chfsi_ctx* ctx, double* rho) {
     int nocc = 0;
     for (int b = 0; b < ctx->nb; ++b)
         if (ctx->occ[b] != 0.0) nocc = b + 1;
-    CK(cudaMemsetAsync(rho, 0, sizeof(double) * ctx->ng, ctx->st));
-    if (nocc == 0) return CHFSI_OK;
-    launch_zsticks_inverse<double2>(ctx->d_psi, ctx->n_pw, ctx->d_work, nocc, ctx->geo, ctx->st);
-    launch_planes_density<double2>(ctx->d_work, ctx->d_occ, nocc, 1.0 / ctx->omega, rho, ctx->geo,
-                                   ctx->st);
+    cudaStream_t st = ctx->st;
+    const bool direct = !ctx->fine && !ctx->aug;
+    double* rw = direct ? rho : ctx->d_rho_w;
+    CK(cudaMemsetAsync(rw, 0, sizeof(double) * ctx->ng, st));
+    if (nocc > 0) {
+        launch_zsticks_inverse<double2>(ctx->d_psi, ctx->n_pw, ctx->d_work, nocc, ctx->geo, st);
+        launch_planes_density<double2>(ctx->d_work, ctx->d_occ, nocc, 1.0 / ctx->omega, rw,
+                                       ctx->geo, st);
+    }
+    if (direct) {
+        CK(cudaGetLastError());
+        return CHFSI_OK;
+    }
+    // Fourier coefficients of the smooth part on the density grid
+    launch_real_to_complex(rw, ctx->d_wgrid, ctx->ng, st);
+    wave_fft3(ctx, ctx->d_wgrid, true);
+    if (ctx->fine) {
+        CK(cudaMemsetAsync(ctx->d_cgrid, 0, sizeof(double2) * ctx->fng, st));
+        launch_scatter_g(ctx->d_wgrid, ctx->d_gmap_w, ctx->d_gmap_f, ctx->n_gmap,
+                         1.0 / (double)ctx->ng, ctx->d_cgrid, st);
+    } else {
+        launch_scale_copy(ctx->d_wgrid, 1.0 / (double)ctx->ng, ctx->d_cgrid, ctx->ng, st);
+    }
+    if (ctx->aug && nocc > 0) {
+        // c_I = sum_n f_n C_n^H q C_n with C = beta^H psi
+        gemm_cn(ctx->d_beta, ctx->n_pw, ctx->d_psi, ctx->n_pw, ctx->np, ctx->nb, ctx->n_pw,
+                ctx->d_part, ctx->d_cp, st);
+        count_launch();
+        k_apply_dmat<<<grid_for((size_t)ctx->np * ctx->nb), 256, 0, st>>>(
+            ctx->d_cp, ctx->d_cd, ctx->np, ctx->nb, ctx->d_proj_ion, ctx->d_poff, ctx->d_doff,
+            ctx->d_qmat);
+        CK(cudaMemsetAsync(ctx->d_cion, 0, sizeof(double) * ctx->nions, st));
+        launch_aug_coeffs(ctx->d_cp, ctx->d_cd, ctx->d_occ, ctx->nb, ctx->d_proj_ion, ctx->np,
+                          ctx->d_cion, st);
+        launch_aug_add(ctx->d_cgrid, grid_recip(ctx), ctx->d_phase, ctx->d_cion, ctx->nions,
+                       ctx->aug_width, 1.0 / ctx->omega, st);
+    }
+    grid_fft3(ctx, ctx->d_cgrid, false);
+    launch_take_real(ctx->d_cgrid, rho, ctx->fng, st);
     CK(cudaGetLastError());
+    return CHFSI_OK;
+}
+
+// (Re)allocate every density-grid buffer for the current fnx, fny, fnz.
+chfsi_status alloc_density(chfsi_ctx* ctx) {
+    void* old[] = {ctx->d_veff_d, ctx->d_vloc, ctx->d_rho_in, ctx->d_rho_out, ctx->d_rho_next,
+                   ctx->d_cgrid, ctx->d_hist, ctx->d_shell, ctx->d_mix_c, ctx->d_mix_r,
+                   ctx->d_fidr[0], ctx->d_fidr[1], ctx->d_fidr[2], ctx->d_phase};
+    for (void* p : old)
+        if (p) cudaFree(p);
+    ctx->d_veff_d = ctx->d_vloc = ctx->d_rho_in = ctx->d_rho_out = ctx->d_rho_next = nullptr;
+    ctx->d_cgrid = ctx->d_mix_c = nullptr;
+    ctx->d_hist = ctx->d_mix_r = nullptr;
+    ctx->d_shell = nullptr;
+    ctx->d_phase = nullptr;
+    for (int d = 0; d < 3; ++d) ctx->d_fidr[d] = nullptr;
+    const size_t ng = ctx->fng;
+    CK(dalloc(&ctx->d_veff_d, ng));
+    CK(dalloc(&ctx->d_vloc, ng));
+    CK(dalloc(&ctx->d_rho_in, ng)); CK(dalloc(&ctx->d_rho_out, ng));
+    CK(dalloc(&ctx->d_rho_next, ng));
+    CK(dalloc(&ctx->d_cgrid, ng));
+    CK(dalloc(&ctx->d_hist, 2 * (size_t)kPulayMax * ng));
+    std::vector<double*> hp(2 * kPulayMax);
+    for (int i = 0; i < 2 * kPulayMax; ++i) hp[i] = ctx->d_hist + (size_t)i * ng;
+    CK(copy_sync(ctx->d_hist_ptrs, hp.data(), hp.size() * sizeof(double*), cudaMemcpyHostToDevice,
+                 ctx->st));
+    CK(cudaMemsetAsync(ctx->d_vloc, 0, sizeof(double) * ng, ctx->st));
+    const int n3[3] = {ctx->fnx, ctx->fny, ctx->fnz};
+    for (int d = 0; d < 3; ++d) {
+        const std::vector<int>& p = ctx->fdr[d];
+        std::vector<int> inv(p.size());
+        for (size_t k = 0; k < p.size(); ++k) inv[p[k]] = (int)k;
+        CK(dalloc(&ctx->d_fidr[d], (size_t)n3[d]));
+        CK(copy_sync(ctx->d_fidr[d], inv.data(), inv.size() * sizeof(int), cudaMemcpyHostToDevice,
+                     ctx->st));
+    }
+    ctx->have_vloc = false;
+    return CHFSI_OK;
+}
+
+// Per-ion axis phase tables e^{-i 2 pi f_d h} on the density grid.
+chfsi_status upload_phases(chfsi_ctx* ctx) {
+    if (!ctx->aug) return CHFSI_OK;
+    double inv[9];
+    {
+        // fractional coordinates f = R . b / 2 pi (rows of recip are b_i)
+        for (int i = 0; i < 9; ++i) inv[i] = ctx->recip[i] / (2.0 * 3.14159265358979323846);
+    }
+    const int n3[3] = {ctx->fnx, ctx->fny, ctx->fnz};
+    const int stride = n3[0] + n3[1] + n3[2];
+    std::vector<double2> ph((size_t)ctx->nions * stride);
+    for (int I = 0; I < ctx->nions; ++I) {
+        const double* R = &ctx->ion_pos[3 * I];
+        int off = 0;
+        for (int d = 0; d < 3; ++d) {
+            const double f = R[0] * inv[3 * d] + R[1] * inv[3 * d + 1] + R[2] * inv[3 * d + 2];
+            for (int h = 0; h < n3[d]; ++h) {
+                const int hs = h >= (n3[d] + 1) / 2 ? h - n3[d] : h;
+                const double a = -2.0 * 3.14159265358979323846 * f * hs;
+                ph[(size_t)I * stride + off + h] = make_double2(std::cos(a), std::sin(a));
+            }
+            off += n3[d];
+        }
+    }
+    if (ctx->d_phase) cudaFree(ctx->d_phase);
+    ctx->d_phase = nullptr;
+    CK(dalloc(&ctx->d_phase, ph.size()));
+    CK(copy_sync(ctx->d_phase, ph.data(), ph.size() * sizeof(double2), cudaMemcpyHostToDevice, ctx->st));
     return CHFSI_OK;
 }
 
 // ---------------------------------------------------------------- learned mixer
 chfsi_status alloc_mix(chfsi_ctx* ctx) {
     if (ctx->d_mix_c) return CHFSI_OK;
-    const size_t ng = ctx->ng;
+    const size_t ng = ctx->fng;
     CK(dalloc(&ctx->d_shell, ng));
     CK(dalloc(&ctx->d_mix_c, 7 * ng));
     CK(dalloc(&ctx->d_mix_r, 4 * ng));
-    CK(dalloc(&ctx->d_mix_acc, (size_t)kMixShells * kShellAcc));
-    CK(dalloc(&ctx->d_mix_x, (size_t)kMixIn + kMixShells * kMixTargets + kMixOut));
+    if (!ctx->d_mix_acc) CK(dalloc(&ctx->d_mix_acc, (size_t)kMixShells * kShellAcc));
+    if (!ctx->d_mix_x) CK(dalloc(&ctx->d_mix_x, (size_t)kMixIn + kMixShells * kMixTargets + kMixOut));
     launch_shell_index(grid_recip(ctx), ctx->d_shell, ctx->st);
     CK(cudaGetLastError());
     return CHFSI_OK;
@@ -751,11 +957,11 @@ chfsi_status alloc_mix(chfsi_ctx* ctx) {
 struct MixRing {
     int n = 0, head = -1;
     double2* slot(const chfsi_ctx* ctx, int age) const {
-        return ctx->d_mix_c + (size_t)((head - age + 4) % 4) * ctx->ng;
+        return ctx->d_mix_c + (size_t)((head - age + 4) % 4) * ctx->fng;
     }
 };
-double2* mix_grid(const chfsi_ctx* ctx, int k) { return ctx->d_mix_c + (size_t)k * ctx->ng; }
-double* mix_real(const chfsi_ctx* ctx, int k) { return ctx->d_mix_r + (size_t)k * ctx->ng; }
+double2* mix_grid(const chfsi_ctx* ctx, int k) { return ctx->d_mix_c + (size_t)k * ctx->fng; }
+double* mix_real(const chfsi_ctx* ctx, int k) { return ctx->d_mix_r + (size_t)k * ctx->fng; }
 constexpr int kGridD = 4, kGridE = 5, kGridW = 6;  // complex grid slots
 float* mix_y(const chfsi_ctx* ctx) { return ctx->d_mix_x + kMixIn + kMixShells * kMixTargets; }
 
@@ -764,7 +970,7 @@ void ring_push(chfsi_ctx* ctx, MixRing& r, const double* out, const double* in) 
     r.head = (r.head + 1) % 4;
     r.n = std::min(r.n + 1, 4);
     double2* dst = r.slot(ctx, 0);
-    launch_diff_complex(out, in, dst, ctx->ng, ctx->st);
+    launch_diff_complex(out, in, dst, ctx->fng, ctx->st);
     grid_fft3(ctx, dst, true);
 }
 
@@ -773,7 +979,7 @@ chfsi_status mix_features(chfsi_ctx* ctx, const MixRing& r, const double2* D, co
     CK(cudaMemsetAsync(ctx->d_mix_acc, 0, sizeof(double) * kMixShells * kShellAcc, ctx->st));
     const double2* R[4] = {nullptr, nullptr, nullptr, nullptr};
     for (int a = 0; a < r.n; ++a) R[a] = r.slot(ctx, a);
-    launch_shell_acc(R[0], R[1], R[2], R[3], D, E, ctx->d_shell, ctx->ng, ctx->d_mix_acc, ctx->st);
+    launch_shell_acc(R[0], R[1], R[2], R[3], D, E, ctx->d_shell, ctx->fng, ctx->d_mix_acc, ctx->st);
     launch_shell_features(ctx->d_mix_acc, ctx->d_mix_x, E ? ctx->d_mix_x + kMixIn : nullptr,
                           ctx->st);
     CK(cudaGetLastError());
@@ -787,7 +993,8 @@ chfsi_status alloc_all(chfsi_ctx* ctx) {
     CK(dalloc(&ctx->d_pw_col, ctx->n_pw));
     CK(dalloc(&ctx->d_pw_zpos, ctx->n_pw));
     CK(dalloc(&ctx->d_veff, ctx->ng));
-    CK(dalloc(&ctx->d_vloc, ctx->ng));
+    CK(dalloc(&ctx->d_rho_w, ctx->ng));
+    CK(dalloc(&ctx->d_wgrid, ctx->ng));
     CK(dalloc(&ctx->d_minmax, 2));
     CK(dalloc(&ctx->d_psi, nbpw));
     CK(dalloc(&ctx->d_psi2, nbpw));
@@ -814,11 +1021,7 @@ chfsi_status alloc_all(chfsi_ctx* ctx) {
     CK(dalloc(&ctx->d_lz_f, ctx->n_pw)); CK(dalloc(&ctx->d_lz_start, ctx->n_pw));
     CK(dalloc(&ctx->d_lz, 2 * 64));
     CK(dalloc(&ctx->d_occ, ctx->nb));
-    CK(dalloc(&ctx->d_rho_in, ctx->ng)); CK(dalloc(&ctx->d_rho_out, ctx->ng));
-    CK(dalloc(&ctx->d_rho_next, ctx->ng));
-    CK(dalloc(&ctx->d_cgrid, ctx->ng));
     CK(dalloc(&ctx->d_acc, 8));
-    CK(dalloc(&ctx->d_hist, 2 * (size_t)kPulayMax * ctx->ng));
     CK(dalloc(&ctx->d_hist_ptrs, 2 * kPulayMax));
     CK(dalloc(&ctx->d_dots, kPulayMax));
     // split-K partials: max over the GEMMs that use them
@@ -846,13 +1049,9 @@ chfsi_status alloc_all(chfsi_ctx* ctx) {
         }
         CK(copy_sync(ctx->d_lz_start, v.data(), v.size() * sizeof(double2), cudaMemcpyHostToDevice, ctx->st));
     }
-    std::vector<double*> hp(2 * kPulayMax);
-    for (int i = 0; i < 2 * kPulayMax; ++i) hp[i] = ctx->d_hist + (size_t)i * ctx->ng;
-    CK(copy_sync(ctx->d_hist_ptrs, hp.data(), hp.size() * sizeof(double*), cudaMemcpyHostToDevice, ctx->st));
     ctx->occ.assign(ctx->nb, 0.0);
     CK(cudaMemsetAsync(ctx->d_occ, 0, sizeof(double) * ctx->nb, ctx->st));
-    CK(cudaMemsetAsync(ctx->d_vloc, 0, sizeof(double) * ctx->ng, ctx->st));
-    return CHFSI_OK;
+    return alloc_density(ctx);
 }
 
 void free_all(chfsi_ctx* ctx) {
@@ -871,7 +1070,9 @@ void free_all(chfsi_ctx* ctx) {
     void* mp[] = {ctx->d_twd, ctx->d_twf, ctx->d_psi32a, ctx->d_psi32b, ctx->d_hpsi32, ctx->d_nl32, ctx->d_work32,
                   ctx->d_planes, ctx->d_tc_part, ctx->d_tc_err, ctx->d_qmat, ctx->d_sinvT,
                   ctx->d_cq, ctx->d_sx, ctx->d_shell, ctx->d_mix_c, ctx->d_mix_r,
-                  ctx->d_mix_acc, ctx->d_mix_x};
+                  ctx->d_mix_acc, ctx->d_mix_x, ctx->d_fidr[0], ctx->d_fidr[1], ctx->d_fidr[2],
+                  ctx->d_gmap_w, ctx->d_gmap_f, ctx->d_veff_d, ctx->d_rho_w, ctx->d_wgrid,
+                  ctx->d_phase, ctx->d_dmat0, ctx->d_cion, ctx->d_vion};
     for (void* p : mp)
         if (p) cudaFree(p);
     if (ctx->h_pin) cudaFreeHost(ctx->h_pin);
@@ -938,6 +1139,9 @@ chfsi_status chfsi_create(const chfsi_dims* dims, const chfsi_config* cfg, chfsi
     digit_reversal(ctx->ax, ctx->dr[0]);
     digit_reversal(ctx->ay, ctx->dr[1]);
     digit_reversal(ctx->az, ctx->dr[2]);
+    ctx->fnx = ctx->nx; ctx->fny = ctx->ny; ctx->fnz = ctx->nz; ctx->fng = ctx->ng;
+    ctx->fax = ctx->ax; ctx->fay = ctx->ay; ctx->faz = ctx->az;
+    for (int d = 0; d < 3; ++d) ctx->fdr[d] = ctx->dr[d];
     s = alloc_all(ctx);
     if (s) return bail(s);
     // inverse digit reversal tables (position -> frequency) for the potential kernels
@@ -1088,9 +1292,13 @@ chfsi_status chfsi_set_projectors(chfsi_ctx* ctx, const chfsi_c128* beta,
         dt += (size_t)ne * ne;
     }
     if (ctx->d_dmat) cudaFree(ctx->d_dmat);
-    ctx->d_dmat = nullptr;
+    if (ctx->d_dmat0) cudaFree(ctx->d_dmat0);
+    ctx->d_dmat = ctx->d_dmat0 = nullptr;
     CK(dalloc(&ctx->d_dmat, dt));
+    CK(dalloc(&ctx->d_dmat0, dt));
     CK(copy_sync(ctx->d_dmat, dmat, dt * sizeof(double2), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->d_dmat0, ctx->d_dmat, dt * sizeof(double2), cudaMemcpyDeviceToDevice,
+                       ctx->st));
     CK(copy_sync(ctx->d_proj_ion, pion.data(), sizeof(int) * ctx->np, cudaMemcpyHostToDevice, ctx->st));
     CK(copy_sync(ctx->d_poff, proj_offsets, sizeof(int) * (ni + 1), cudaMemcpyHostToDevice, ctx->st));
     CK(copy_sync(ctx->d_doff, doff.data(), sizeof(int) * ni, cudaMemcpyHostToDevice, ctx->st));
@@ -1120,7 +1328,6 @@ chfsi_status chfsi_set_projectors(chfsi_ctx* ctx, const chfsi_c128* beta,
 
 chfsi_status chfsi_set_qmat(chfsi_ctx* ctx, const chfsi_c128* qmat) {
     if (!ctx || !qmat || !ctx->proj_set || ctx->np == 0) return CHFSI_ERR_BAD_INPUT;
-    if (ctx->mixed) return ctx->fail(CHFSI_ERR_NOT_IMPLEMENTED, "ultrasoft overlap runs in FP64 only");
     cudaSetDevice(ctx->device);
     const int np = ctx->np, ni = ctx->nions;
     std::vector<int> poff(ni + 1), doff(ni);
@@ -1357,16 +1564,26 @@ chfsi_status chfsi_create_from_system(const chfsi_system* sys, const chfsi_confi
         return bail(st);
     if ((st = chfsi_set_psi(ctx, reinterpret_cast<const chfsi_c128*>(s.psi0.data())))) return bail(st);
     if ((st = chfsi_set_occupations(ctx, s.occ.data()))) return bail(st);
-    if ((st = chfsi_set_vloc_g(ctx, reinterpret_cast<const chfsi_c128*>(s.vloc_g.data())))) return bail(st);
     double lat[9];
     std::memcpy(lat, s.lattice, sizeof(lat));
     if ((st = chfsi_set_cell(ctx, lat, s.e_ewald, s.n_atoms))) return bail(st);
+    if (s.ngrid_density[0] != s.ngrid[0] || s.ngrid_density[1] != s.ngrid[1] ||
+        s.ngrid_density[2] != s.ngrid[2])
+        if ((st = chfsi_set_density_grid(ctx, s.ngrid_density))) return bail(st);
+    if ((st = chfsi_set_vloc_g(ctx, reinterpret_cast<const chfsi_c128*>(s.vloc_g.data())))) return bail(st);
+    if (s.uspp && s.n_proj > 0) {
+        if ((st = chfsi_set_qmat(ctx, reinterpret_cast<const chfsi_c128*>(s.qmat.data()))))
+            return bail(st);
+        if ((st = chfsi_set_augmentation(ctx, s.pos.data(), s.q_width))) return bail(st);
+    }
     // a usable V_eff before the first SCF step: V_loc alone
-    std::vector<double> v(ctx->ng);
-    if (cudaError_t e = copy_sync(v.data(), ctx->d_vloc, sizeof(double) * ctx->ng,
-                                  cudaMemcpyDeviceToHost, ctx->st))
-        return bail(cuda_fail(e, "copy_sync(vloc)", __FILE__, __LINE__));
-    if ((st = chfsi_set_veff(ctx, v.data()))) return bail(st);
+    if (cudaError_t e = cudaMemcpyAsync(ctx->d_veff_d, ctx->d_vloc, sizeof(double) * ctx->fng,
+                                        cudaMemcpyDeviceToDevice, ctx->st))
+        return bail(cuda_fail(e, "cudaMemcpyAsync(vloc)", __FILE__, __LINE__));
+    project_veff(ctx);
+    if (cudaError_t e = cudaStreamSynchronize(ctx->st))
+        return bail(cuda_fail(e, "project_veff", __FILE__, __LINE__));
+    ctx->veff_set = true;
     *out = ctx;
     return CHFSI_OK;
 }
@@ -1408,20 +1625,37 @@ chfsi_status chfsi_set_cell(chfsi_ctx* ctx, const double* lattice, double e_ewal
 chfsi_status chfsi_set_vloc_g(chfsi_ctx* ctx, const chfsi_c128* vloc_g) {
     if (!ctx || !vloc_g) return CHFSI_ERR_BAD_INPUT;
     cudaSetDevice(ctx->device);
-    // natural G order -> digit-reversed layout, then inverse transform
-    std::vector<double2> h(ctx->ng);
+    // natural G order of the wavefunction grid -> digit-reversed layout of
+    // the density grid (zero where the density grid has G the wavefunction
+    // grid lacks, and at the wavefunction grid's Nyquist planes when the
+    // grids differ), then inverse transform
+    std::vector<double2> h(ctx->fng, make_double2(0.0, 0.0));
     const double2* src = reinterpret_cast<const double2*>(vloc_g);
-    for (int iz = 0; iz < ctx->nz; ++iz)
-        for (int iy = 0; iy < ctx->ny; ++iy)
+    const int n[3] = {ctx->nx, ctx->ny, ctx->nz};
+    const int f[3] = {ctx->fnx, ctx->fny, ctx->fnz};
+    auto fpos = [&](int d, int i) -> int {
+        if (!ctx->fine) return ctx->fdr[d][i];
+        const int hs = i >= (n[d] + 1) / 2 ? i - n[d] : i;
+        if ((n[d] % 2 == 0) && i == n[d] / 2) return -1;
+        return ctx->fdr[d][(hs + f[d]) % f[d]];
+    };
+    for (int iz = 0; iz < ctx->nz; ++iz) {
+        const int pz = fpos(2, iz);
+        if (pz < 0) continue;
+        for (int iy = 0; iy < ctx->ny; ++iy) {
+            const int py = fpos(1, iy);
+            if (py < 0) continue;
             for (int ix = 0; ix < ctx->nx; ++ix) {
+                const int px = fpos(0, ix);
+                if (px < 0) continue;
                 const size_t from = ix + (size_t)ctx->nx * (iy + (size_t)ctx->ny * iz);
-                const size_t to = ctx->dr[0][ix] +
-                                  (size_t)ctx->nx * (ctx->dr[1][iy] + (size_t)ctx->ny * ctx->dr[2][iz]);
-                h[to] = src[from];
+                h[px + (size_t)ctx->fnx * (py + (size_t)ctx->fny * pz)] = src[from];
             }
-    CK(copy_sync(ctx->d_cgrid, h.data(), sizeof(double2) * ctx->ng, cudaMemcpyHostToDevice, ctx->st));
+        }
+    }
+    CK(copy_sync(ctx->d_cgrid, h.data(), sizeof(double2) * ctx->fng, cudaMemcpyHostToDevice, ctx->st));
     grid_fft3(ctx, ctx->d_cgrid, false);
-    launch_take_real(ctx->d_cgrid, ctx->d_vloc, ctx->ng, ctx->st);
+    launch_take_real(ctx->d_cgrid, ctx->d_vloc, ctx->fng, ctx->st);
     CK(cudaStreamSynchronize(ctx->st));
     CK(cudaGetLastError());
     ctx->have_vloc = true;
@@ -1431,7 +1665,7 @@ chfsi_status chfsi_set_vloc_g(chfsi_ctx* ctx, const chfsi_c128* vloc_g) {
 chfsi_status chfsi_get_vloc(chfsi_ctx* ctx, double* out) {
     if (!ctx || !out) return CHFSI_ERR_BAD_INPUT;
     cudaSetDevice(ctx->device);
-    CK(copy_sync(out, ctx->d_vloc, sizeof(double) * ctx->ng, cudaMemcpyDeviceToHost, ctx->st));
+    CK(copy_sync(out, ctx->d_vloc, sizeof(double) * ctx->fng, cudaMemcpyDeviceToHost, ctx->st));
     return CHFSI_OK;
 }
 
@@ -1450,7 +1684,7 @@ chfsi_status chfsi_construct_density(chfsi_ctx* ctx, double* rho_out) {
     chfsi_status s = density_dev(ctx, ctx->d_rho_out);
     if (s) return s;
     if (rho_out) {
-        CK(cudaMemcpyAsync(rho_out, ctx->d_rho_out, sizeof(double) * ctx->ng, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaMemcpyAsync(rho_out, ctx->d_rho_out, sizeof(double) * ctx->fng, cudaMemcpyDeviceToHost, ctx->st));
     }
     CK(cudaStreamSynchronize(ctx->st));
     return CHFSI_OK;
@@ -1460,7 +1694,7 @@ chfsi_status chfsi_build_veff(chfsi_ctx* ctx, const double* rho, double* e2) {
     if (!ctx || !rho) return CHFSI_ERR_BAD_INPUT;
     if (!ctx->have_vloc || ctx->omega <= 0.0) return ctx->fail(CHFSI_ERR_BAD_INPUT, "V_loc / cell not set");
     cudaSetDevice(ctx->device);
-    CK(cudaMemcpyAsync(ctx->d_rho_in, rho, sizeof(double) * ctx->ng, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->d_rho_in, rho, sizeof(double) * ctx->fng, cudaMemcpyHostToDevice, ctx->st));
     CK(cudaMemsetAsync(ctx->d_acc, 0, sizeof(double) * 8, ctx->st));
     chfsi_status s = build_veff_dev(ctx, ctx->d_rho_in, ctx->d_acc);
     if (s) return s;
@@ -1586,7 +1820,7 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
     r->energies = r_energies;
     r->eigenvalues = r_eigs;
     r->residuals = r_res;
-    const size_t ng = ctx->ng;
+    const size_t ng = ctx->fng;  // density grid
     const double dv = ctx->omega / (double)ng;
     cudaStream_t st = ctx->st;
     const double n_elec = ctx->n_elec;
@@ -1613,6 +1847,7 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
         // build_v_eff (scf.rs:157)
         CK(cudaMemsetAsync(ctx->d_acc, 0, sizeof(double) * 8, st));
         s = build_veff_dev(ctx, ctx->d_rho_in, ctx->d_acc);
+        if (!s) s = screen_dmat(ctx);
         if (s) { status = s; break; }
         ctx->veff_set = true;
         // diagonalize (scf.rs:169)
@@ -1636,7 +1871,7 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
         launch_real_to_complex(ctx->d_rho_out, ctx->d_cgrid, ng, st);
         grid_fft3(ctx, ctx->d_cgrid, true);
         launch_hartree_gspace(ctx->d_cgrid, grid_recip(ctx), ctx->omega, ctx->d_acc + 0, st);
-        launch_energy_terms(ctx->d_rho_out, ctx->d_veff, ctx->d_vloc, ng, dv, ctx->d_acc + 1,
+        launch_energy_terms(ctx->d_rho_out, ctx->d_veff_d, ctx->d_vloc, ng, dv, ctx->d_acc + 1,
                             ctx->d_acc + 2, st);
         CK(cudaGetLastError());
         double acc[3];
@@ -1776,8 +2011,89 @@ extern "C" chfsi_status chfsi_get_density(chfsi_ctx* ctx, double* rho) {
     if (!ctx || !rho) return CHFSI_ERR_BAD_INPUT;
     cudaSetDevice(ctx->device);
     CK(cudaStreamSynchronize(ctx->st));
-    CK(copy_sync(rho, ctx->d_rho_out, sizeof(double) * ctx->ng, cudaMemcpyDeviceToHost, ctx->st));
+    CK(copy_sync(rho, ctx->d_rho_out, sizeof(double) * ctx->fng, cudaMemcpyDeviceToHost, ctx->st));
     return CHFSI_OK;
+}
+
+// Density (augmentation) grid: must be set before V_loc, the cell's
+// augmentation and any density work; it may not be coarser than the
+// wavefunction grid.
+extern "C" chfsi_status chfsi_set_density_grid(chfsi_ctx* ctx, const int* ngrid) {
+    if (!ctx || !ngrid) return CHFSI_ERR_BAD_INPUT;
+    const int n[3] = {ctx->nx, ctx->ny, ctx->nz};
+    for (int d = 0; d < 3; ++d)
+        if (ngrid[d] < n[d]) return ctx->fail(CHFSI_ERR_BAD_INPUT, "density grid coarser than the wavefunction grid");
+    cudaSetDevice(ctx->device);
+    AxisPlan pl[3];
+    for (int d = 0; d < 3; ++d)
+        if (!plan_axis(ngrid[d], pl[d]))
+            return ctx->fail(CHFSI_ERR_BAD_INPUT, "density grid dimensions must be 2,3,5-smooth");
+    CK(cudaStreamSynchronize(ctx->st));
+    ctx->fnx = ngrid[0]; ctx->fny = ngrid[1]; ctx->fnz = ngrid[2];
+    ctx->fng = (size_t)ngrid[0] * ngrid[1] * ngrid[2];
+    ctx->fax = pl[0]; ctx->fay = pl[1]; ctx->faz = pl[2];
+    digit_reversal(ctx->fax, ctx->fdr[0]);
+    digit_reversal(ctx->fay, ctx->fdr[1]);
+    digit_reversal(ctx->faz, ctx->fdr[2]);
+    ctx->fine = ngrid[0] != n[0] || ngrid[1] != n[1] || ngrid[2] != n[2];
+    chfsi_status s = alloc_density(ctx);
+    if (s) return s;
+    // G vectors the two grids share: every wavefunction-grid frequency except
+    // the Nyquist planes of even axes
+    if (ctx->d_gmap_w) cudaFree(ctx->d_gmap_w);
+    if (ctx->d_gmap_f) cudaFree(ctx->d_gmap_f);
+    ctx->d_gmap_w = ctx->d_gmap_f = nullptr;
+    ctx->n_gmap = 0;
+    if (ctx->fine) {
+        std::vector<int> wp, fp;
+        const int f[3] = {ctx->fnx, ctx->fny, ctx->fnz};
+        auto sgn = [&](int d, int i) { return i >= (n[d] + 1) / 2 ? i - n[d] : i; };
+        auto nyq = [&](int d, int i) { return n[d] % 2 == 0 && i == n[d] / 2; };
+        for (int iz = 0; iz < n[2]; ++iz) {
+            if (nyq(2, iz)) continue;
+            for (int iy = 0; iy < n[1]; ++iy) {
+                if (nyq(1, iy)) continue;
+                for (int ix = 0; ix < n[0]; ++ix) {
+                    if (nyq(0, ix)) continue;
+                    const int w = ctx->dr[0][ix] + n[0] * (ctx->dr[1][iy] + n[1] * ctx->dr[2][iz]);
+                    const int fx = ctx->fdr[0][(sgn(0, ix) + f[0]) % f[0]];
+                    const int fy = ctx->fdr[1][(sgn(1, iy) + f[1]) % f[1]];
+                    const int fz = ctx->fdr[2][(sgn(2, iz) + f[2]) % f[2]];
+                    wp.push_back(w);
+                    fp.push_back(fx + f[0] * (fy + f[1] * fz));
+                }
+            }
+        }
+        ctx->n_gmap = (int)wp.size();
+        CK(dalloc(&ctx->d_gmap_w, wp.size()));
+        CK(dalloc(&ctx->d_gmap_f, fp.size()));
+        CK(copy_sync(ctx->d_gmap_w, wp.data(), wp.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+        CK(copy_sync(ctx->d_gmap_f, fp.data(), fp.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+    }
+    return upload_phases(ctx);
+}
+
+extern "C" chfsi_status chfsi_get_density_grid(chfsi_ctx* ctx, int* ngrid) {
+    if (!ctx || !ngrid) return CHFSI_ERR_BAD_INPUT;
+    ngrid[0] = ctx->fnx; ngrid[1] = ctx->fny; ngrid[2] = ctx->fnz;
+    return CHFSI_OK;
+}
+
+// Ultrasoft augmentation charges Q_ij(r) = q_ij g(|r - R_I|) (unit Gaussian
+// of the given width) for the ions that carry projectors; needs the cell,
+// the projectors and q (chfsi_set_qmat).
+extern "C" chfsi_status chfsi_set_augmentation(chfsi_ctx* ctx, const double* positions,
+                                               double width) {
+    if (!ctx || !positions || !(width > 0.0)) return CHFSI_ERR_BAD_INPUT;
+    if (!ctx->uspp || !ctx->proj_set || ctx->omega <= 0.0)
+        return ctx->fail(CHFSI_ERR_BAD_INPUT, "augmentation needs the cell, projectors and q");
+    cudaSetDevice(ctx->device);
+    ctx->ion_pos.assign(positions, positions + 3 * (size_t)ctx->nions);
+    ctx->aug_width = width;
+    ctx->aug = true;
+    if (!ctx->d_cion) CK(dalloc(&ctx->d_cion, (size_t)ctx->nions));
+    if (!ctx->d_vion) CK(dalloc(&ctx->d_vion, (size_t)ctx->nions));
+    return upload_phases(ctx);
 }
 
 extern "C" chfsi_status chfsi_set_mixer(chfsi_ctx* ctx, chfsi_mixer* m) {
@@ -1800,7 +2116,7 @@ extern "C" chfsi_status chfsi_mixer_samples(chfsi_ctx* ctx, const double* rho_in
     cudaSetDevice(ctx->device);
     chfsi_status s = alloc_mix(ctx);
     if (s) return s;
-    const size_t ng = ctx->ng;
+    const size_t ng = ctx->fng;
     cudaStream_t st = ctx->st;
     double* prev = mix_real(ctx, 0);
     double* star = mix_real(ctx, 1);

@@ -84,8 +84,16 @@ k_zsticks_inverse(const C* __restrict__ psi, int ldp, C* __restrict__ work, HGeo
 }
 
 // ---------------------------------------------------------------- pass 2
+// 256 threads with 2 (FP64) or 3 (FP32) resident blocks per SM: the
+// global-memory phases of one plane overlap the FFT stages of another.
 template <typename C>
-__global__ void __launch_bounds__(512)
+struct PlanesCfg {
+    static constexpr int threads = 256;
+    static constexpr int min_blocks = sizeof(C) == 16 ? 2 : 3;
+};
+
+template <typename C>
+__global__ void __launch_bounds__(PlanesCfg<C>::threads, PlanesCfg<C>::min_blocks)
 k_planes_vloc(C* __restrict__ work, const double* __restrict__ veff, HGeom g) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* twx = reinterpret_cast<C*>(smem_raw);
@@ -420,7 +428,7 @@ void launch_planes_vloc(C* work, const double* veff, int nb, const HGeom& g, cud
     dim3 grid(g.nz, nb);
     size_t sm = planes_smem_bytes(g, sizeof(C));
     allow_smem(k_planes_vloc<C>, sm);
-    k_planes_vloc<C><<<grid, 512, sm, st>>>(work, veff, g);
+    k_planes_vloc<C><<<grid, PlanesCfg<C>::threads, sm, st>>>(work, veff, g);
 }
 
 template <typename C>

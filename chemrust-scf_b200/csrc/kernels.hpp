@@ -85,4 +85,23 @@ void launch_energy_terms(const double* rho_out, const double* veff, const double
                          double dv, double* exc_acc, double* dc_acc, cudaStream_t st);
 void launch_take_real(const double2* c, double* r, size_t n, cudaStream_t st);
 
+// ---- density grid and ultrasoft augmentation (aug.cu)
+// dst[dst_pos[i]] = scale * src[src_pos[i]]: G vectors shared by two grids
+void launch_scatter_g(const double2* src, const int* src_pos, const int* dst_pos, int n,
+                      double scale, double2* dst, cudaStream_t st);
+void launch_scale_copy(const double2* src, double scale, double2* dst, size_t n, cudaStream_t st);
+// F(G) += scale exp(-G^2 w^2 / 4) sum_I c_I e^{-i G.R_I}; ph: per ion the
+// axis phase tables e^{-i 2 pi f_d h}, [ion][nx | ny | nz] (frequency order)
+void launch_aug_add(double2* F, const GridRecip& gr, const double2* ph, const double* c, int nions,
+                    double width, double scale, cudaStream_t st);
+// v_I += scale Re sum_G V(G) exp(-G^2 w^2 / 4) e^{+i G.R_I}  (v zeroed by caller)
+void launch_ion_potential(const double2* V, const GridRecip& gr, const double2* ph, int nions,
+                          double width, double scale, double* v, cudaStream_t st);
+// c_I += f_n Re(conj(C_in) (qC)_in)  (C, qC: n_proj x nb; c zeroed by caller)
+void launch_aug_coeffs(const double2* C, const double2* qC, const double* occ, int nb,
+                       const int* proj_ion, int np, double* c, cudaStream_t st);
+// D_I = D0_I + v_I q_I per ion block
+void launch_screen_d(const double2* D0, const double2* q, const double* v, const int* poff,
+                     const int* doff, int nions, double2* D, cudaStream_t st);
+
 }  // namespace chfsi

@@ -193,7 +193,12 @@ chfsi_status generate_system(const chfsi_synth_params& p, System& s) {
         int n = p.ngrid[d] > 0 ? p.ngrid[d] : next_smooth235(4 * mabs[d] + 1);
         if (n < 2 * mabs[d] + 1) return CHFSI_ERR_BAD_INPUT;
         s.ngrid[d] = n;
+        const int nd = p.ngrid_density[d] > 0 ? p.ngrid_density[d] : n;
+        if (nd < n) return CHFSI_ERR_BAD_INPUT;
+        s.ngrid_density[d] = nd;
     }
+    s.uspp = p.uspp;
+    s.q_width = p.q_width;
     const int nx = s.ngrid[0], ny = s.ngrid[1], nz = s.ngrid[2];
     // Sort by column (iy, ix) wrapped, then l ascending: every (x,y) column
     // owns one contiguous run of plane waves.
@@ -395,6 +400,7 @@ chfsi_status chfsi_synth_defaults(int cfg, chfsi_synth_params* p) {
         p->n_shell = 2; p->rc_proj[0] = 1.0; p->rc_proj[1] = 1.4; p->lmax = 1;
         p->d_min = 0.5; p->d_max = 2.0;
         p->uspp = 1; p->q_width = 0.8; p->q_amp = 0.1;
+        p->ngrid_density[0] = p->ngrid_density[1] = p->ngrid_density[2] = 144;
         break;
     default: return CHFSI_ERR_BAD_INPUT;
     }
@@ -423,6 +429,9 @@ chfsi_status chfsi_system_get_info(const chfsi_system* s, chfsi_system_info* o) 
     if (!s || !o) return CHFSI_ERR_BAD_INPUT;
     std::memset(o, 0, sizeof(*o));
     for (int d = 0; d < 3; ++d) o->ngrid[d] = s->ngrid[d];
+    for (int d = 0; d < 3; ++d) o->ngrid_density[d] = s->ngrid_density[d];
+    o->q_width = s->q_width;
+    o->uspp = s->uspp;
     o->n_pw = s->n_pw;
     o->n_bands = s->n_bands;
     o->n_occ = s->n_occ;

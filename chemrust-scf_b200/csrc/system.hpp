@@ -13,6 +13,9 @@ struct System {
     chfsi_synth_params params{};
     double a = 0.0, omega = 0.0, lattice[9] = {};
     int ngrid[3] = {0, 0, 0};
+    int ngrid_density[3] = {0, 0, 0};
+    double q_width = 0.0;
+    int uspp = 0;
     int n_atoms = 0, n_occ = 0, n_bands = 0, n_pw = 0, n_columns = 0;
     int n_proj = 0, n_ions_proj = 0;
     double n_elec = 0.0, gmax = 0.0, e_ewald = 0.0;

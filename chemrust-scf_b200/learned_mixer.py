@@ -8,7 +8,7 @@ into (features, targets) with the library's shell reductions, trains the
 network with the library's own forward/backward/Adam kernels, and compares
 SCF iteration counts and wall time against Pulay.
 
-    python chemrust-scf_b200/learned_mixer.py train --cells 300 --out mixer.npz
+    python chemrust-scf_b200/learned_mixer.py train --cells 300 --dagger-cells 150 --out mixer.npz
     python chemrust-scf_b200/learned_mixer.py evaluate --weights mixer.npz --cells 8
 
 The reference crate has no mixer implementation (src/mixing.rs:24 is a
@@ -30,8 +30,9 @@ import chfsi  # noqa: E402
 WEIGHTS = os.path.join(HERE, "mixer_weights.npz")
 
 # (lattice: 0 diamond, 1 simple cubic, 2 bcc; n_rep; atoms per conventional
-# cell): 8, 16, 27 and 64 atoms
-CELL_KINDS = [(0, 1, 8), (2, 2, 2), (1, 3, 1), (0, 2, 8)]
+# cell): 8, 16, 27 and 64 atoms for training; 216 atoms (the size of the
+# 216-atom diamond supercell) for evaluation only
+CELL_KINDS = [(0, 1, 8), (2, 2, 2), (1, 3, 1), (0, 2, 8), (0, 3, 8)]
 VOLUME_PER_ATOM = 10.26 ** 3 / 8.0  # the 8-atom diamond cell's density
 
 
@@ -73,6 +74,21 @@ def trajectories(seed, ndeg=12, max_iter=60, tol=1e-8):
     return s, ctx, [(a, b, star) for a, b in out]
 
 
+def on_policy_samples(mixer, seed, ndeg=12, max_iter=60, tol=1e-8):
+    """Samples from the network's own trajectories (learned-preconditioned
+    Pulay and pure learned mixing), so that training sees the states the
+    network itself produces."""
+    s = chfsi.SyntheticSystem(cell_params(seed))
+    out = []
+    for mode in (chfsi.MIXER_LEARNED_PULAY, chfsi.MIXER_LEARNED):
+        ctx = chfsi.Context(s)
+        ctx.set_mixer(mixer)
+        r = ctx.run_scf(ndeg, tol_per_atom=tol, max_iter=max_iter, kT=0.01, mixer=mode, trace=True)
+        if r["converged"]:
+            out.append(ctx.mixer_samples(r["trace_in"], r["trace_out"], r["trace_out"][-1]))
+    return out
+
+
 def dataset(seeds, log=print):
     X, T = [], []
     t0 = time.time()
@@ -97,18 +113,43 @@ def load(path=WEIGHTS, device=0):
     return chfsi.Mixer(device=device, params=z["params"])
 
 
-def train(n_cells=300, epochs=150, batch=256, lr=1e-3, seed=0, out=WEIGHTS, log=print):
+def train(n_cells=300, epochs=150, batch=256, lr=1e-3, seed=0, out=WEIGHTS, dagger_cells=0,
+          log=print):
+    """Off-policy data (Pulay and linear-mixing trajectories), Adam at lr then
+    lr/10; optionally one on-policy round on dagger_cells further cells."""
     seeds = list(range(10_000 + seed, 10_000 + seed + n_cells))
     log("generating trajectories on %d cells" % n_cells)
+    t0 = time.time()
     X, T = dataset(seeds, log)
+    gen_s = time.time() - t0
     log("%d samples; training" % len(X))
     m = chfsi.Mixer(seed=seed)
     t0 = time.time()
-    losses = m.train(X, T, epochs=epochs, batch=batch, lr=lr, seed=seed)
-    log("loss %.4f -> %.4f in %.1f s" % (losses[0], losses[-1], time.time() - t0))
+    l1 = m.train(X, T, epochs=epochs, batch=batch, lr=lr, seed=seed)
+    l2 = m.train(X, T, epochs=max(1, epochs // 2), batch=batch, lr=lr * 0.1, seed=seed + 1)
+    train_s = time.time() - t0
+    log("loss %.4f -> %.4f -> %.4f in %.1f s" % (l1[0], l1[-1], l2[-1], train_s))
     meta = {"cells": n_cells, "samples": int(len(X)), "epochs": epochs, "batch": batch, "lr": lr,
-            "loss_first": float(losses[0]), "loss_last": float(losses[-1]),
-            "train_seconds": time.time() - t0}
+            "loss_first": float(l1[0]), "loss_last": float(l2[-1]),
+            "generate_seconds": gen_s, "train_seconds": train_s}
+    if dagger_cells:
+        t0 = time.time()
+        Xd, Td = [], []
+        for sd in range(50_000 + seed, 50_000 + seed + dagger_cells):
+            for x, t in on_policy_samples(m, sd):
+                Xd.append(x)
+                Td.append(t)
+        X = np.concatenate([X] + Xd)
+        T = np.concatenate([T] + Td)
+        gen2 = time.time() - t0
+        t0 = time.time()
+        l3 = m.train(X, T, epochs=max(1, epochs // 2), batch=batch, lr=lr * 0.3, seed=seed + 2)
+        l4 = m.train(X, T, epochs=max(1, epochs // 2), batch=batch, lr=lr * 0.03, seed=seed + 3)
+        log("on-policy round: %d cells, %d samples in all; loss %.4f -> %.4f" %
+            (dagger_cells, len(X), l3[0], l4[-1]))
+        meta.update({"on_policy_cells": dagger_cells, "samples_total": int(len(X)),
+                     "loss_last": float(l4[-1]), "generate_seconds_on_policy": gen2,
+                     "train_seconds_on_policy": time.time() - t0})
     save(m, out, meta)
     return m, meta
 
@@ -143,17 +184,20 @@ def main():
     a.add_argument("--lr", type=float, default=1e-3)
     a.add_argument("--seed", type=int, default=0)
     a.add_argument("--out", default=WEIGHTS)
+    a.add_argument("--dagger-cells", type=int, default=0)
     b = sub.add_parser("evaluate")
     b.add_argument("--weights", default=WEIGHTS)
     b.add_argument("--cells", type=int, default=8)
     b.add_argument("--first-seed", type=int, default=90_000)
     b.add_argument("--out", default=None)
+    b.add_argument("--kinds", default="0,1,2,3", help="cell kinds (4 = 216 atoms)")
     args = ap.parse_args()
     if args.cmd == "train":
-        train(args.cells, args.epochs, args.batch, args.lr, args.seed, args.out)
+        train(args.cells, args.epochs, args.batch, args.lr, args.seed, args.out, args.dagger_cells)
     else:
         m = load(args.weights)
-        rows = evaluate(m, list(range(args.first_seed, args.first_seed + args.cells)))
+        kinds = tuple(int(k) for k in args.kinds.split(","))
+        rows = evaluate(m, list(range(args.first_seed, args.first_seed + args.cells)), kinds=kinds)
         summary = {}
         for k in ("pulay", "learned", "learned_pulay"):
             it = [r[k]["iterations"] for r in rows]

@@ -103,6 +103,7 @@ typedef struct chfsi_synth_params {
     double   q_amp;          /* A_ij ~ U[-q_amp, q_amp]                           */
     double   kpt[3];         /* k in reduced (fractional) coordinates             */
     uint64_t seed;
+    int      ngrid_density[3]; /* density/augmentation grid; 0 = the FFT grid     */
 } chfsi_synth_params;
 
 typedef struct chfsi_system chfsi_system;
@@ -121,6 +122,9 @@ typedef struct chfsi_system_info {
     double gmax;            /* max |G+k| over the plane-wave sphere             */
     double e_ewald;         /* ion-ion energy of point charges (Ha)             */
     double lattice[9];      /* rows a1, a2, a3 (bohr)                           */
+    int    ngrid_density[3];
+    double q_width;         /* Gaussian width of Q_ij(r) when ultrasoft (bohr)  */
+    int    uspp;
 } chfsi_system_info;
 
 chfsi_status chfsi_synth_defaults(int config_index, chfsi_synth_params* out);
@@ -187,6 +191,19 @@ chfsi_status chfsi_set_projectors(chfsi_ctx* ctx, const chfsi_c128* beta,
  * solves H x = e S x with S_sub = psi^H S psi.  FP64 contexts only.  The GPU
  * ChFSI of the reference ignores S (it has no generalised path). */
 chfsi_status chfsi_set_qmat(chfsi_ctx* ctx, const chfsi_c128* qmat);
+/* Density (augmentation) grid, at least as fine as the FFT grid of the
+ * wavefunctions; call before chfsi_set_vloc_g.  Density, V_eff, mixing and
+ * energies then live on it: the smooth density is interpolated up by zero
+ * padding in G and V_eff is brought down by truncation
+ * (downsample_array_to_wave_grid, src/scf.rs:413-454). */
+chfsi_status chfsi_set_density_grid(chfsi_ctx* ctx, const int* ngrid);
+chfsi_status chfsi_get_density_grid(chfsi_ctx* ctx, int* ngrid);
+/* Ultrasoft augmentation: Q_ij(r) = q_ij g(|r - R_I|), g a unit Gaussian of
+ * the given width (bohr), for the ions with projectors (positions n_ions x 3,
+ * bohr, the order of chfsi_set_projectors).  chfsi_construct_density then
+ * adds sum_ij rho_ij Q_ij and chfsi_scf_run screens D = D0 + int V_eff Q
+ * every iteration.  Needs the cell, the projectors and chfsi_set_qmat. */
+chfsi_status chfsi_set_augmentation(chfsi_ctx* ctx, const double* positions, double width);
 /* Lower bound of the spectrum of S used to scale the filter's upper bound. */
 chfsi_status chfsi_get_s_min(chfsi_ctx* ctx, double* out);
 chfsi_status chfsi_set_veff(chfsi_ctx* ctx, const double* veff);

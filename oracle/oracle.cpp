@@ -737,7 +737,13 @@ CgOut band_cg_one(const OracleCtx& c, const Precond& P, std::vector<cplx>& psi,
         if (norm(g) < 2.220446049250313e-16 * 1000.0) return {eig, step - 1, true, norm(r)};
         const double prev = eig;
         apply_s(c, g.data(), sg.data(), 1);
-        // S-orthogonalise g against the refined lower bands, then S-normalise
+        // S-orthogonalise g against the refined lower bands (modified
+        // Gram-Schmidt, s_orthogonalize_against, cg_helpers.rs:161-216), then
+        // S-normalise.  The reference keeps only Re<psi_j|S|g>
+        // (cg_helpers.rs:189), which is the whole overlap for the real-valued
+        // Gamma-point bands it targets; with general complex bands that drops
+        // Im<psi_j|S|g> and lets the refined bands collapse onto lower ones,
+        // so the full complex overlap is removed here.
         for (auto& lb : lower) {
             const cplx ov = dotc(lb.first.data(), sg.data(), n);
             for (int i = 0; i < n; ++i) { g[i] -= ov * lb.first[i]; sg[i] -= ov * lb.second[i]; }
@@ -873,6 +879,12 @@ void oracle_set_num_threads(int n) {
 }
 
 void oracle_set_veff(OracleCtx* c, const double* v) { c->veff.assign(v, v + c->ng()); }
+// screened D (same block layout as at creation) and occupations, for SCF
+// loops driven from Python (ultrasoft augmentation)
+void oracle_set_dmat(OracleCtx* c, const double* dmat) {
+    std::memcpy(c->dmat.data(), dmat, sizeof(cplx) * c->dmat.size());
+}
+void oracle_set_occ(OracleCtx* c, const double* occ) { c->occ.assign(occ, occ + c->n_bands); }
 
 // Ultrasoft overlap: per-ion q blocks (layout of D).  Builds the Woodbury
 // factor M = q (1 + B q)^-1 with B = beta^H beta and the lower bound

@@ -33,6 +33,8 @@ def lib():
         "oracle_num_threads": ([], C.c_int),
         "oracle_set_num_threads": ([C.c_int], None),
         "oracle_set_veff": ([vp, dp], None),
+        "oracle_set_dmat": ([vp, vp], None),
+        "oracle_set_occ": ([vp, dp], None),
         "oracle_get_veff": ([vp, dp], None),
         "oracle_get_vloc_r": ([vp, dp], None),
         "oracle_set_psi": ([vp, vp], None),
@@ -264,6 +266,14 @@ class Oracle:
         r = np.zeros(self.ng)
         lib().oracle_density(self.h, _p(r, C.c_double))
         return r
+
+    def set_dmat(self, dmat):
+        d = np.ascontiguousarray(dmat, dtype=np.complex128)
+        lib().oracle_set_dmat(self.h, _p(d))
+
+    def set_occ(self, occ):
+        o = np.ascontiguousarray(occ, dtype=np.float64)
+        lib().oracle_set_occ(self.h, _p(o, C.c_double))
 
     def build_veff(self, rho):
         r = np.ascontiguousarray(rho, dtype=np.float64).ravel()

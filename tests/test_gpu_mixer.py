@@ -117,3 +117,27 @@ def test_learned_mode_requires_a_mixer(chfsi, sys0):
     ctx = chfsi.Context(sys0)
     with pytest.raises(chfsi.ChfsiError):
         ctx.run_scf(12, max_iter=3, mixer=chfsi.MIXER_LEARNED)
+
+
+def test_trained_mixer_beats_pulay_on_held_out_cells(chfsi):
+    """A/B test: the committed trained network, used as the per-shell
+    preconditioner inside Pulay, against plain Pulay (alpha 0.3, history 6)
+    on the ten held-out random cells 90000-90009 (training uses seeds from
+    10000).  Both must reach the same energy; the learned runs must need
+    fewer iterations in total."""
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "..", "chemrust-scf_b200"))
+    import learned_mixer as lm
+    m = lm.load()
+    rows = lm.evaluate(m, list(range(90000, 90010)), log=lambda *_: None)
+    it_p = sum(r["pulay"]["iterations"] for r in rows)
+    it_l = sum(r["learned_pulay"]["iterations"] for r in rows)
+    t_p = sum(r["pulay"]["seconds"] for r in rows)
+    t_l = sum(r["learned_pulay"]["seconds"] for r in rows)
+    print("held-out cells: Pulay %d iterations %.3f s, learned-preconditioned Pulay %d "
+          "iterations %.3f s" % (it_p, t_p, it_l, t_l))
+    for r in rows:
+        assert r["pulay"]["converged"] and r["learned_pulay"]["converged"]
+        # both stop at |dE| < 1e-6 Ha/atom between iterations, which bounds the
+        # distance to the common fixed point only loosely for slow runs
+        assert abs(r["pulay"]["e_total"] - r["learned_pulay"]["e_total"]) / r["atoms"] < 5e-5
+    assert it_l < it_p
