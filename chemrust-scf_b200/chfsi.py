@@ -110,7 +110,7 @@ class ScfParams(C.Structure):
     _fields_ = [("ndeg", C.c_int), ("max_iter", C.c_int), ("tol_per_atom", C.c_double),
                 ("alpha", C.c_double), ("max_hist", C.c_int), ("first_passes", C.c_int),
                 ("kT", C.c_double), ("fp64_switch_per_atom", C.c_double),
-                ("mixer", C.c_int), ("reserved", C.c_int), ("trace", C.POINTER(C.c_double))]
+                ("mixer", C.c_int), ("cg_steps", C.c_int), ("trace", C.POINTER(C.c_double))]
 
 
 class ScfResult(C.Structure):
@@ -121,7 +121,7 @@ class ScfResult(C.Structure):
                 ("seconds", C.c_double),
                 ("energies", C.POINTER(C.c_double)), ("eigenvalues", C.POINTER(C.c_double)),
                 ("n_iter_learned", C.c_int), ("fell_back", C.c_int),
-                ("residuals", C.POINTER(C.c_double))]
+                ("residuals", C.POINTER(C.c_double)), ("n_fp64_retries", C.c_int)]
 
 
 _lib = None
@@ -193,6 +193,13 @@ def lib():
         "chfsi_set_density_grid": [vp, C.POINTER(C.c_int)],
         "chfsi_get_density_grid": [vp, C.POINTER(C.c_int)],
         "chfsi_set_augmentation": [vp, dp, C.c_double],
+        "chfsi_band_cg": [vp, C.c_int, C.c_double, dp, i32p, i32p],
+        "chfsi_batch_create": [C.POINTER(vp), C.c_int, C.POINTER(vp)],
+        "chfsi_batch_capture": [vp, C.c_int],
+        "chfsi_batch_run": [vp, dp, i32p],
+        "chfsi_batch_graph_nodes": [vp, C.POINTER(C.c_size_t)],
+        "chfsi_autotune": [vp, C.POINTER(C.c_int), fp],
+        "chfsi_set_launch_config": [vp, C.c_int],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -202,6 +209,8 @@ def lib():
     L.chfsi_system_destroy.restype = None
     L.chfsi_destroy.argtypes = [vp]
     L.chfsi_destroy.restype = None
+    L.chfsi_batch_destroy.argtypes = [vp]
+    L.chfsi_batch_destroy.restype = None
     L.chfsi_mixer_destroy.argtypes = [vp]
     L.chfsi_mixer_destroy.restype = None
     L.chfsi_mixer_num_params.argtypes = []
@@ -212,6 +221,41 @@ def lib():
     L.chfsi_last_error.restype = C.c_char_p
     _lib = L
     return L
+
+
+class Batch:
+    """Mixed-precision diagonalisation passes of many contexts replayed as one
+    CUDA graph (members on their own streams)."""
+
+    def __init__(self, contexts):
+        self.contexts = list(contexts)
+        arr = (C.c_void_p * len(self.contexts))(*[c.handle.value for c in self.contexts])
+        h = C.c_void_p()
+        _check(lib().chfsi_batch_create(arr, len(self.contexts), C.byref(h)))
+        self.handle = h
+        self.n_bands = [c.n_bands for c in self.contexts]
+
+    def close(self):
+        if getattr(self, "handle", None) and _lib is not None:
+            _lib.chfsi_batch_destroy(self.handle)
+            self.handle = None
+
+    __del__ = close
+
+    def capture(self, ndeg):
+        _check(lib().chfsi_batch_capture(self.handle, ndeg))
+        n = C.c_size_t()
+        _check(lib().chfsi_batch_graph_nodes(self.handle, C.byref(n)))
+        return n.value
+
+    def run(self):
+        """Replay; returns the list of per-member eigenvalue arrays."""
+        e = np.zeros(sum(self.n_bands))
+        st = np.zeros(len(self.contexts), dtype=np.int32)
+        code = lib().chfsi_batch_run(self.handle, _ptr(e, C.c_double), _ptr(st, C.c_int32))
+        if code != OK:
+            _check(code)
+        return np.split(e, np.cumsum(self.n_bands)[:-1])
 
 
 class Mixer:
@@ -578,12 +622,12 @@ class Context:
 
     def run_scf(self, ndeg, tol_per_atom=1e-6, max_iter=30, alpha=0.3, max_hist=6,
                 first_passes=4, kT=0.01, fp64_switch_per_atom=1e-4, raise_not_converged=False,
-                mixer=MIXER_PULAY, trace=False):
+                mixer=MIXER_PULAY, trace=False, cg_steps=0):
         """Full SCF; mixer is MIXER_PULAY or, after set_mixer(), MIXER_LEARNED /
         MIXER_LEARNED_PULAY.  trace=True also returns rho_in and rho_out of every
         iteration (n_iter x N^3 each) as 'trace_in' / 'trace_out'."""
         p = ScfParams(ndeg, max_iter, tol_per_atom, alpha, max_hist, first_passes, kT,
-                      fp64_switch_per_atom, mixer, 0, None)
+                      fp64_switch_per_atom, mixer, cg_steps, None)
         tr = None
         if trace:
             tr = np.zeros((max_iter, 2, self.ng_density))
@@ -604,11 +648,30 @@ class Context:
                "e_entropy": r.e_entropy, "mu": r.mu,
                "seconds": r.seconds, "energies": energies[:r.n_iter].copy(), "eigenvalues": eigs,
                "residuals": residuals[:r.n_iter].copy(), "n_iter_learned": r.n_iter_learned,
-               "fell_back": bool(r.fell_back)}
+               "fell_back": bool(r.fell_back), "n_fp64_retries": r.n_fp64_retries}
         if trace:
             out["trace_in"] = tr[:r.n_iter, 0].copy()
             out["trace_out"] = tr[:r.n_iter, 1].copy()
         return out
+
+    def autotune(self):
+        """Time the local H|psi> launch configurations; returns (choice, 9 timings)."""
+        ch = C.c_int()
+        t = np.zeros(9, dtype=np.float32)
+        self._c(lib().chfsi_autotune(self.handle, C.byref(ch), _ptr(t, C.c_float)))
+        return ch.value, t
+
+    def set_launch_config(self, choice):
+        self._c(lib().chfsi_set_launch_config(self.handle, choice))
+
+    def band_cg(self, max_steps, tol=1e-10):
+        """Band-by-band CG refinement; returns (band energies, steps, n_converged)."""
+        e = np.zeros(self.n_bands)
+        st = np.zeros(self.n_bands, dtype=np.int32)
+        nc = C.c_int32()
+        self._c(lib().chfsi_band_cg(self.handle, max_steps, tol, _ptr(e, C.c_double),
+                                    _ptr(st, C.c_int32), C.byref(nc)))
+        return e, st, nc.value
 
     # --- learned density mixer ------------------------------------------------
     def set_mixer(self, mixer):

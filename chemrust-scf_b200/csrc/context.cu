@@ -97,6 +97,32 @@ __global__ void k_f32_to_f64(const float2* __restrict__ a, double2* __restrict__
          i += (size_t)gridDim.x * blockDim.x)
         b[i] = make_double2((double)a[i].x, (double)a[i].y);
 }
+// Scale band b of x and y (FP32, band-major, n per band) by 1 / |x_b| (one
+// block per band; the norm is accumulated in FP64).
+__global__ void __launch_bounds__(256)
+k_normalize_bands32(float2* __restrict__ x, float2* __restrict__ y, int n) {
+    __shared__ double red[8];
+    __shared__ float inv;
+    float2* xb = x + (size_t)blockIdx.x * n;
+    float2* yb = y + (size_t)blockIdx.x * n;
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s += (double)xb[i].x * xb[i].x + (double)xb[i].y * xb[i].y;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+        inv = t > 0.0 ? (float)(1.0 / sqrt(t)) : 1.f;
+    }
+    __syncthreads();
+    const float f = inv;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        xb[i].x *= f; xb[i].y *= f;
+        yb[i].x *= f; yb[i].y *= f;
+    }
+}
+
 __global__ void __launch_bounds__(256) k_sumsq32(const float2* __restrict__ x, size_t n, double* acc) {
     __shared__ double red[8];
     double s = 0.0;
@@ -155,6 +181,102 @@ k_cheb_combine(const C* __restrict__ hx, const C* __restrict__ corr, const C* __
         double t = 0.0;
         for (int w = 0; w < 8; ++w) t += red[w];
         atomicAdd(norm_acc, t);
+    }
+}
+
+// ---- band-CG vector kernels
+__global__ void k_tpa(const double* __restrict__ kin, double inv_mean, double* __restrict__ t,
+                      size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const double x = kin[i] * inv_mean;
+        const double den = 27.0 + x * (18.0 + x * (12.0 + 8.0 * x));
+        t[i] = 1.0 / (1.0 + 16.0 * x * x * x * x / den);
+    }
+}
+
+// out = diag(t) (x + u), u optional
+__global__ void k_diag_apply(const double* __restrict__ t, const double2* __restrict__ x,
+                             const double2* __restrict__ u, double2* __restrict__ out, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        double2 v = x[i];
+        if (u) { v.x += u[i].x; v.y += u[i].y; }
+        out[i] = make_double2(t[i] * v.x, t[i] * v.y);
+    }
+}
+
+// y = a y + b x (complex a, b)
+__global__ void k_lincomb(double2* __restrict__ y, double2 a, const double2* __restrict__ x,
+                          double2 b, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const double2 yv = y[i];
+        double2 r = make_double2(a.x * yv.x - a.y * yv.y, a.x * yv.y + a.y * yv.x);
+        if (x) {
+            const double2 xv = x[i];
+            r.x += b.x * xv.x - b.y * xv.y;
+            r.y += b.x * xv.y + b.y * xv.x;
+        }
+        y[i] = r;
+    }
+}
+
+// Modified Gram-Schmidt overlaps from the classical ones: ov_j = v_j -
+// sum_{i<j} G[j][i] ov_i with G[j][i] = <psi_j|S psi_i> (one warp, j in order).
+__global__ void k_mgs_overlaps(const double2* __restrict__ v, const double2* __restrict__ G, int ld,
+                               int k, double2* __restrict__ ov) {
+    const int lane = threadIdx.x;
+    for (int j = 0; j < k; ++j) {
+        double sr = 0.0, si = 0.0;
+        const double2* g = G + (size_t)j * ld;
+        for (int i = lane; i < j; i += 32) {
+            const double2 a = g[i], b = ov[i];
+            sr += a.x * b.x - a.y * b.y;
+            si += a.x * b.y + a.y * b.x;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            sr += __shfl_xor_sync(0xffffffffu, sr, o);
+            si += __shfl_xor_sync(0xffffffffu, si, o);
+        }
+        if (lane == 0) ov[j] = make_double2(v[j].x - sr, v[j].y - si);
+        __syncwarp();
+    }
+}
+
+struct DotSet {
+    const double2* a[6];
+    const double2* b[6];
+};
+// out[2i], out[2i + 1] += Re, Im <a_i | b_i>
+__global__ void __launch_bounds__(256)
+k_multi_dot(DotSet ds, int k, size_t n, double* __restrict__ out) {
+    __shared__ double red[6][2][8];
+    double acc[6][2];
+    for (int j = 0; j < 6; ++j) acc[j][0] = acc[j][1] = 0.0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int j = 0; j < 6; ++j) {
+            if (j >= k) break;
+            const double2 x = ds.a[j][i], y = ds.b[j][i];
+            acc[j][0] += x.x * y.x + x.y * y.y;
+            acc[j][1] += x.x * y.y - x.y * y.x;
+        }
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int j = 0; j < k; ++j)
+        for (int c = 0; c < 2; ++c) {
+            double v = acc[j][c];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) red[j][c][w] = v;
+        }
+    __syncthreads();
+    if (threadIdx.x < 2 * k) {
+        const int j = threadIdx.x >> 1, c = threadIdx.x & 1;
+        double t = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t += red[j][c][q];
+        atomicAdd(out + threadIdx.x, t);
     }
 }
 
@@ -261,6 +383,18 @@ struct chfsi_ctx {
     double2* d_lz_start = nullptr; double* d_lz = nullptr;
     // density / SCF
     double* d_occ = nullptr; std::vector<double> occ;
+    std::vector<double> kin_host;  // 1/2 |G+k|^2 in the internal plane-wave order
+    // band-by-band CG refinement (band_cg.rs)
+    double* d_tpa = nullptr;       // TPA preconditioner diagonal
+    double2* d_cgR = nullptr;      // conj((-q^-1 - beta^H T beta)^-1), ultrasoft only
+    double2* d_cgv = nullptr;      // 10 work vectors of n_pw
+    double2* d_cgc = nullptr;      // 3 x n_proj projections
+    double2* d_cgov = nullptr;     // 2 x n_bands overlaps with the refined lower bands
+    double2* d_cgG = nullptr;      // <psi_j|S psi_i> of the refined bands, j > i (n_bands^2)
+    double2* d_cgpart = nullptr;   // split-K partials of the CG GEMVs
+    double* d_cgdot = nullptr;     // 16 dot-product accumulators
+    bool cg_ready = false;
+    double2* d_psi_save = nullptr; // start of a mixed-precision pass (FP64 retry)
     double* d_rho_in = nullptr; double* d_rho_out = nullptr; double* d_rho_next = nullptr;
     double2* d_cgrid = nullptr; double* d_acc = nullptr;
     double* d_hist = nullptr;  // 2 * kPulayMax * ng
@@ -282,6 +416,7 @@ struct chfsi_ctx {
     TcPlanes tp_beta_a, tp_betaT_b, tp_psi_b, tp_psi_a, tp_hpsi_b, tp_small_a, tp_psiT_b;
     float* d_tc_part = nullptr; int* d_tc_err = nullptr;
     bool beta_planes_ready = false;
+    bool last_pass_fp32 = false;  // the last filter ran in FP32
     // density grid: density, potentials, mixing and augmentation live here.
     // It is the wavefunction grid unless chfsi_set_density_grid chose a
     // finer one; then the smooth density is interpolated up by zero padding
@@ -654,6 +789,12 @@ chfsi_status filter_dev32(chfsi_ctx* ctx, int ndeg, const double* eig_dev, int n
 chfsi_status rr_dev32(chfsi_ctx* ctx) {
     const int n = ctx->nb, npw = ctx->n_pw;
     cudaStream_t st = ctx->st;
+    // unit-norm columns: the filter leaves band norms spread over orders of
+    // magnitude, and the FP32 / BF16x3 overlap of unscaled columns loses the
+    // weakly amplified top of the subspace; scaling changes neither the span
+    // nor the Ritz pairs
+    count_launch();
+    k_normalize_bands32<<<n, 256, 0, st>>>(ctx->d_psi32, ctx->d_hpsi32, npw);
     const float2* psi = ctx->d_psi32;
     tc_pack<float2>(psi, npw, n, npw, true, kSrcPlain, ctx->tp_psi_a, st);
     tc_pack<float2>(psi, npw, n, npw, false, kSrcPlain, ctx->tp_psi_b, st);
@@ -692,8 +833,13 @@ chfsi_status rr_dev32(chfsi_ctx* ctx) {
     return CHFSI_OK;
 }
 
+// A pass without previous eigenvalues (the random start) filters with the
+// cut at lambda_max / 3, where the deepest states grow by ~1e9 over degree
+// 16 relative to the cut: FP32 rounding of the weakly amplified top bands
+// would swamp them, so such passes always run in FP64.
 chfsi_status filter_any(chfsi_ctx* ctx, int ndeg, const double* eig_dev, int n_eig) {
-    if (ctx->mixed_active) return filter_dev32(ctx, ndeg, eig_dev, n_eig);
+    ctx->last_pass_fp32 = ctx->mixed_active && eig_dev != nullptr && n_eig > 0;
+    if (ctx->last_pass_fp32) return filter_dev32(ctx, ndeg, eig_dev, n_eig);
     ctx->d_psi32 = nullptr;
     return filter_dev(ctx, ndeg, eig_dev, n_eig);
 }
@@ -747,6 +893,12 @@ chfsi_status finish_diag(chfsi_ctx* ctx, double* eig_out, bool have_rr) {
         }
         for (int i = 0; i < n; ++i)
             if (!std::isfinite(h[i])) return ctx->fail(CHFSI_ERR_NUMERIC, "non-finite eigenvalue");
+        // after an FP32 filter, a top Ritz value well inside the damped
+        // interval [cut, lambda_max] means rounding swamped the top of the
+        // subspace (reported so that the pass can be redone in FP64)
+        if (ctx->last_pass_fp32 &&
+            h[n - 1] > ctx->h_coef[1] + 0.1 * (ctx->h_coef[0] - ctx->h_coef[1]))
+            return ctx->fail(CHFSI_ERR_RR_FAILED, "Rayleigh-Ritz failed: Ritz value inside the damped interval");
         if (eig_out) std::memcpy(eig_out, h, sizeof(double) * n);
     }
     return CHFSI_OK;
@@ -1072,11 +1224,326 @@ void free_all(chfsi_ctx* ctx) {
                   ctx->d_cq, ctx->d_sx, ctx->d_shell, ctx->d_mix_c, ctx->d_mix_r,
                   ctx->d_mix_acc, ctx->d_mix_x, ctx->d_fidr[0], ctx->d_fidr[1], ctx->d_fidr[2],
                   ctx->d_gmap_w, ctx->d_gmap_f, ctx->d_veff_d, ctx->d_rho_w, ctx->d_wgrid,
-                  ctx->d_phase, ctx->d_dmat0, ctx->d_cion, ctx->d_vion};
+                  ctx->d_phase, ctx->d_dmat0, ctx->d_cion, ctx->d_vion, ctx->d_tpa, ctx->d_cgR,
+                  ctx->d_cgv, ctx->d_cgc, ctx->d_cgov, ctx->d_cgpart, ctx->d_cgdot, ctx->d_cgG,
+                  ctx->d_psi_save};
     for (void* p : mp)
         if (p) cudaFree(p);
     if (ctx->h_pin) cudaFreeHost(ctx->h_pin);
     if (ctx->st) cudaStreamDestroy(ctx->st);
+}
+
+// ---------------------------------------------------------------- band-CG
+// Band-by-band preconditioned CG refinement after the filter
+// (band_cg_minimize, src/eigensolver/band_cg.rs:157-437): steepest descent
+// for two steps, then the modified Fletcher-Reeves direction
+// d = (Re<g|r> / Re<g_old|r_old>) d_old - g; the preconditioned gradient is
+// S-orthogonalised against the refined lower bands (cg_helpers.rs:161-216)
+// and S-normalised; the direction is S-orthogonalised against the band; the
+// step comes from the closed-form 2x2 line search (line_search.rs:57-212).
+// The preconditioner is the TPA diagonal plus, with q, the ultrasoft
+// Woodbury term (uspp_preconditioner.rs:80-131).  Vector work runs on the
+// device; the handful of scalars per step come back to the host.
+struct CgLineSearch { double step, eig, norm; int status; };
+
+// Closed-form minimum of E(t) = (a + b t + c t^2) / (1 + d t^2), b = -2 Re<H psi|d>,
+// with the step of the lower root clamped to 15 (line_search.rs:57-212).
+CgLineSearch cg_line_search(double a, double hpsi_dir, double c, double d) {
+    const double b = -2.0 * hpsi_dir;
+    CgLineSearch out{0.0, a, 1.0, 0};
+    double t = 0.0, e = a;
+    if (std::fabs(d) > 2.2250738585072014e-308) {
+        const double ad = a * d, bd = b * d;
+        if (std::fabs(bd) < 1e-30) return {0.0, a, 1.0, -2};
+        const double disc = ad * ad - 2.0 * ad * c + c * c + b * bd;
+        if (disc < 0.0) return {0.0, a, 1.0, -1};
+        const double sq = std::sqrt(disc);
+        const double roots[2] = {(-ad + c + sq) / bd, (-ad + c - sq) / bd};
+        double ev[2];
+        bool ok[2];
+        for (int i = 0; i < 2; ++i) {
+            const double den = 1.0 + d * roots[i] * roots[i];
+            ok[i] = den > 0.0;
+            ev[i] = ok[i] ? (a + b * roots[i] + c * roots[i] * roots[i]) / den : 0.0;
+        }
+        int pick = -1;
+        if (ok[0] && ok[1]) pick = ev[0] < ev[1] ? 0 : 1;
+        else if (ok[0] && ev[0] < a) pick = 0;
+        else if (ok[1] && ev[1] < a) pick = 1;
+        if (pick < 0) return {0.0, a, 1.0, -1};
+        t = -roots[pick];
+        e = ev[pick];
+    } else {
+        if (!(c > 0.0)) return {0.0, a, 1.0, -1};
+        t = -b / (2.0 * c);
+        e = (a + b * t + c * t * t) / (1.0 + d * t * t);
+    }
+    if (t > 15.0) {
+        t = 15.0;
+        e = (a + b * t + c * t * t) / (1.0 + d * t * t);
+        out.status = 1;
+    } else if (t < 0.0) {
+        out.status = -1;
+    }
+    const double nn = 1.0 + d * t * t;
+    out.step = t;
+    out.eig = e;
+    out.norm = nn > 0.0 ? std::sqrt(nn) : 0.0;
+    if (!(nn > 0.0)) out.status = 2;
+    return out;
+}
+
+struct Cg {
+    chfsi_ctx* ctx;
+    size_t n;
+    double2 *hpsi, *spsi, *r, *g, *sg, *d, *dold, *hd, *sd, *tmp;
+    std::vector<std::complex<double>> dots(std::initializer_list<std::pair<const double2*, const double2*>> l) {
+        DotSet ds{};
+        int k = 0;
+        for (auto& pr : l) { ds.a[k] = pr.first; ds.b[k] = pr.second; ++k; }
+        cudaMemsetAsync(ctx->d_cgdot, 0, sizeof(double) * 2 * k, ctx->st);
+        count_launch();
+        k_multi_dot<<<grid_for(n), 256, 0, ctx->st>>>(ds, k, n, ctx->d_cgdot);
+        double h[12];
+        cudaMemcpyAsync(h, ctx->d_cgdot, sizeof(double) * 2 * k, cudaMemcpyDeviceToHost, ctx->st);
+        cudaStreamSynchronize(ctx->st);
+        std::vector<std::complex<double>> out(k);
+        for (int j = 0; j < k; ++j) out[j] = {h[2 * j], h[2 * j + 1]};
+        return out;
+    }
+    void lin(double2* y, std::complex<double> a, const double2* x, std::complex<double> b) {
+        count_launch();
+        k_lincomb<<<grid_for(n), 256, 0, ctx->st>>>(y, make_double2(a.real(), a.imag()), x,
+                                                    make_double2(b.real(), b.imag()), n);
+    }
+    void copy(double2* dst, const double2* src) {
+        cudaMemcpyAsync(dst, src, n * sizeof(double2), cudaMemcpyDeviceToDevice, ctx->st);
+    }
+    // S x = x + beta q beta^H x
+    void apply_s(const double2* x, double2* sx) {
+        copy(sx, x);
+        if (!ctx->uspp) return;
+        const int np = ctx->np;
+        gemm_cn(ctx->d_beta, (int)n, x, (int)n, np, 1, (int)n, ctx->d_cgpart, ctx->d_cgc, ctx->st);
+        count_launch();
+        k_apply_dmat<<<grid_for((size_t)np), 256, 0, ctx->st>>>(ctx->d_cgc, ctx->d_cgc + np, np, 1,
+                                                               ctx->d_proj_ion, ctx->d_poff,
+                                                               ctx->d_doff, ctx->d_qmat);
+        gemm_tn(ctx->d_cgc + np, 1, ctx->d_beta, (int)n, sx, (int)n, 1, (int)n, np, 1.0, 1.0, ctx->st);
+    }
+    chfsi_status apply_hs(const double2* x, double2* hx, double2* sx) {
+        chfsi_status st = apply_h_dev(ctx, x, hx, 1, kEpiApply, nullptr);
+        if (st) return st;
+        apply_s(x, sx);
+        return CHFSI_OK;
+    }
+    // out = T r + T beta R beta^H T r
+    void precond(const double2* rr, double2* out) {
+        count_launch();
+        k_diag_apply<<<grid_for(n), 256, 0, ctx->st>>>(ctx->d_tpa, rr, nullptr, out, n);
+        if (!ctx->d_cgR) return;
+        const int np = ctx->np;
+        gemm_cn(ctx->d_beta, (int)n, out, (int)n, np, 1, (int)n, ctx->d_cgpart, ctx->d_cgc, ctx->st);
+        gemm_cn(ctx->d_cgR, np, ctx->d_cgc, np, np, 1, np, ctx->d_cgpart, ctx->d_cgc + np, ctx->st);
+        gemm_tn(ctx->d_cgc + np, 1, ctx->d_beta, (int)n, tmp, (int)n, 1, (int)n, np, 1.0, 0.0, ctx->st);
+        count_launch();
+        k_diag_apply<<<grid_for(n), 256, 0, ctx->st>>>(ctx->d_tpa, rr, tmp, out, n);
+    }
+};
+
+chfsi_status cg_prepare(chfsi_ctx* ctx) {
+    if (ctx->cg_ready) return CHFSI_OK;
+    const size_t n = ctx->n_pw;
+    const int np = ctx->np, nb = ctx->nb;
+    if (!ctx->d_tpa) CK(dalloc(&ctx->d_tpa, n));
+    if (!ctx->d_cgv) CK(dalloc(&ctx->d_cgv, 10 * n));
+    if (!ctx->d_cgc) CK(dalloc(&ctx->d_cgc, (size_t)3 * std::max(np, 1)));
+    if (!ctx->d_cgov) CK(dalloc(&ctx->d_cgov, 2 * (size_t)nb));
+    if (!ctx->d_cgG) CK(dalloc(&ctx->d_cgG, (size_t)nb * nb));
+    if (!ctx->d_cgdot) CK(dalloc(&ctx->d_cgdot, 16));
+    size_t pe = 0;
+    for (int k = 1; k <= nb; ++k)
+        pe = std::max({pe, splitk_partial_elems(k, 1, (int)n), splitk_partial_elems(1, k, (int)n)});
+    if (np > 0) {
+        pe = std::max(pe, splitk_partial_elems(np, 1, (int)n));
+        pe = std::max(pe, splitk_partial_elems(np, 1, np));
+    }
+    if (!ctx->d_cgpart) CK(dalloc(&ctx->d_cgpart, pe));
+    double sum = 0.0;
+    for (double k : ctx->kin_host) sum += k;
+    const double mean = n ? sum / (double)n : 0.0;
+    count_launch();
+    k_tpa<<<grid_for(n), 256, 0, ctx->st>>>(ctx->d_kin, mean > 0.0 ? 1.0 / mean : 1.0, ctx->d_tpa, n);
+    if (ctx->uspp && np > 0) {
+        // R = (-q^-1 - beta^H T beta)^-1 on the host (once per context)
+        double2 *bt = nullptr, *part = nullptr, *cm = nullptr;
+        CK(cudaMalloc((void**)&bt, (size_t)np * n * sizeof(double2)));
+        cudaError_t e = cudaMalloc((void**)&part, splitk_partial_elems(np, np, (int)n) * sizeof(double2));
+        if (e == cudaSuccess) e = cudaMalloc((void**)&cm, (size_t)np * np * sizeof(double2));
+        if (e != cudaSuccess) {
+            cudaFree(bt); cudaFree(part); cudaFree(cm);
+            CK(e);
+        }
+        for (int p = 0; p < np; ++p) {
+            count_launch();
+            k_diag_apply<<<grid_for(n), 256, 0, ctx->st>>>(ctx->d_tpa, ctx->d_beta + (size_t)p * n,
+                                                           nullptr, bt + (size_t)p * n, n);
+        }
+        gemm_cn(ctx->d_beta, (int)n, bt, (int)n, np, np, (int)n, part, cm, ctx->st);
+        std::vector<std::complex<double>> C((size_t)np * np), Q((size_t)np * np, 0.0);
+        std::vector<double2> qh;
+        std::vector<int> poff(ctx->nions + 1), doff(ctx->nions);
+        e = cudaMemcpyAsync(C.data(), cm, C.size() * sizeof(double2), cudaMemcpyDeviceToHost, ctx->st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(poff.data(), ctx->d_poff, poff.size() * sizeof(int), cudaMemcpyDeviceToHost, ctx->st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(doff.data(), ctx->d_doff, doff.size() * sizeof(int), cudaMemcpyDeviceToHost, ctx->st);
+        size_t dt = 0;
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->st);
+        cudaFree(bt); cudaFree(part); cudaFree(cm);
+        CK(e);
+        for (int i = 0; i < ctx->nions; ++i) dt += (size_t)(poff[i + 1] - poff[i]) * (poff[i + 1] - poff[i]);
+        qh.resize(dt);
+        CK(copy_sync(qh.data(), ctx->d_qmat, dt * sizeof(double2), cudaMemcpyDeviceToHost, ctx->st));
+        for (int i = 0; i < ctx->nions; ++i) {
+            const int p0 = poff[i], ne = poff[i + 1] - p0;
+            for (int a = 0; a < ne; ++a)
+                for (int b = 0; b < ne; ++b) {
+                    const double2 q = qh[doff[i] + a * ne + b];
+                    Q[(size_t)(p0 + a) * np + p0 + b] = {q.x, q.y};
+                }
+        }
+        if (!invert_complex(Q, np)) return ctx->fail(CHFSI_ERR_NUMERIC, "q is singular");
+        for (size_t i = 0; i < Q.size(); ++i) Q[i] = -Q[i] - C[i];
+        if (!invert_complex(Q, np)) return ctx->fail(CHFSI_ERR_NUMERIC, "preconditioner matrix is singular");
+        // gemm_cn conjugates its first operand: store conj(R)
+        std::vector<double2> rc(Q.size());
+        for (size_t i = 0; i < Q.size(); ++i) rc[i] = make_double2(Q[i].real(), -Q[i].imag());
+        if (!ctx->d_cgR) CK(dalloc(&ctx->d_cgR, (size_t)np * np));
+        CK(copy_sync(ctx->d_cgR, rc.data(), rc.size() * sizeof(double2), cudaMemcpyHostToDevice, ctx->st));
+    }
+    CK(cudaGetLastError());
+    ctx->cg_ready = true;
+    return CHFSI_OK;
+}
+
+// y -= sum_j w_j L_j for the first k rows L_j of a band-major block
+void gemm_tn_complex_axpy(chfsi_ctx* ctx, const double2* w, int k, const double2* L, double2* y) {
+    const int n = ctx->n_pw;
+    gemm_tn(w, 1, L, n, y, n, 1, n, k, -1.0, 1.0, ctx->st);
+}
+
+// Refine every band of d_psi in turn; d_sx holds S psi of the refined bands
+// (ultrasoft), eig[b] the band energy, steps[b] the steps taken.
+chfsi_status band_cg_dev(chfsi_ctx* ctx, int max_steps, double tol, double* eig, int* steps,
+                         int* n_conv) {
+    chfsi_status st = cg_prepare(ctx);
+    if (st) return st;
+    Cg c{};
+    c.ctx = ctx;
+    c.n = ctx->n_pw;
+    double2* V = ctx->d_cgv;
+    c.hpsi = V; c.spsi = V + c.n; c.r = V + 2 * c.n; c.g = V + 3 * c.n; c.sg = V + 4 * c.n;
+    c.d = V + 5 * c.n; c.dold = V + 6 * c.n; c.hd = V + 7 * c.n; c.sd = V + 8 * c.n;
+    c.tmp = V + 9 * c.n;
+    const size_t n = c.n;
+    const int nb = ctx->nb;
+    const double2* lower_s = ctx->uspp ? ctx->d_sx : ctx->d_psi;
+    int nconv = 0;
+    for (int b = 0; b < nb; ++b) {
+        double2* psi = ctx->d_psi + (size_t)b * n;
+        if ((st = c.apply_hs(psi, c.hpsi, c.spsi))) return st;
+        const double s0 = c.dots({{psi, c.spsi}})[0].real();
+        const double inv0 = 1.0 / std::sqrt(s0);
+        c.lin(psi, inv0, nullptr, 0.0);
+        c.lin(c.hpsi, inv0, nullptr, 0.0);
+        c.lin(c.spsi, inv0, nullptr, 0.0);
+        auto residual = [&](double& e_out) {
+            const auto dd = c.dots({{psi, c.hpsi}, {psi, c.spsi}});
+            const double he = dd[0].real(), se = dd[1].real();
+            e_out = he;
+            c.copy(c.r, c.hpsi);
+            c.lin(c.r, 1.0, c.spsi, -he / se);
+        };
+        double e = 0.0;
+        residual(e);
+        double beta_old = 0.0;
+        int taken = max_steps;
+        bool conv = false;
+        for (int step = 1; step <= max_steps; ++step) {
+            c.precond(c.r, c.g);
+            const double gn0 = std::sqrt(c.dots({{c.g, c.g}})[0].real());
+            if (gn0 < 2.220446049250313e-16 * 1000.0) { taken = step - 1; conv = true; break; }
+            const double prev = e;
+            c.apply_s(c.g, c.sg);
+            if (b > 0) {
+                // modified Gram-Schmidt against the refined lower bands
+                // (s_orthogonalize_against, cg_helpers.rs:161-216) in closed
+                // form: v = Psi^H S g, ov = (1 + L)^-1 v with L the strictly
+                // lower part of Psi^H S Psi, then g -= Psi ov, S g -= S Psi ov
+                gemm_cn(ctx->d_psi, (int)n, c.sg, (int)n, b, 1, (int)n, ctx->d_cgpart, ctx->d_cgov, ctx->st);
+                count_launch();
+                k_mgs_overlaps<<<1, 32, 0, ctx->st>>>(ctx->d_cgov, ctx->d_cgG, nb, b, ctx->d_cgov + nb);
+                gemm_tn_complex_axpy(ctx, ctx->d_cgov + nb, b, ctx->d_psi, c.g);
+                gemm_tn_complex_axpy(ctx, ctx->d_cgov + nb, b, lower_s, c.sg);
+            }
+            const auto gd = c.dots({{c.g, c.sg}, {c.g, c.r}});
+            const double gn = std::sqrt(std::max(gd[0].real(), 1e-300));
+            c.lin(c.g, 1.0 / gn, nullptr, 0.0);
+            c.lin(c.sg, 1.0 / gn, nullptr, 0.0);
+            const double beta = gd[1].real() / gn;
+            if (step <= 2) {
+                c.copy(c.d, c.g);
+                beta_old = beta;
+            } else {
+                const double gamma = std::fabs(beta_old) > 1e-300 ? beta / beta_old : 0.0;
+                c.copy(c.d, c.dold);
+                c.lin(c.d, gamma, c.g, -1.0);
+                beta_old = beta;
+            }
+            if ((st = c.apply_hs(c.d, c.hd, c.sd))) return st;
+            const auto od = c.dots({{psi, c.sd}, {c.r, c.r}});
+            const std::complex<double> ov = od[0];
+            if (std::abs(ov) > 1e-30) {
+                c.lin(c.d, 1.0, psi, -ov);
+                c.lin(c.hd, 1.0, c.hpsi, -ov);
+                c.lin(c.sd, 1.0, c.spsi, -ov);
+            }
+            c.copy(c.dold, c.d);
+            const double rn = std::sqrt(od[1].real());
+            if (rn < tol * 0.01 && rn < 1e-12 * std::max(std::fabs(e), 1.0)) {
+                taken = step - 1;
+                conv = true;
+                break;
+            }
+            const auto ld = c.dots({{c.hpsi, c.d}, {c.hd, c.d}, {c.sd, c.d}});
+            const CgLineSearch ls = cg_line_search(e, ld[0].real(), ld[1].real(), ld[2].real());
+            const double inv = ls.norm > 0.0 ? 1.0 / ls.norm : 1.0;
+            c.lin(psi, inv, c.d, ls.step * inv);
+            c.lin(c.hpsi, inv, c.hd, ls.step * inv);
+            c.lin(c.spsi, inv, c.sd, ls.step * inv);
+            double e_new = 0.0;
+            residual(e_new);
+            if (std::fabs(e_new - prev) < tol) {
+                e = e_new;
+                taken = step;
+                conv = true;
+                break;
+            }
+            e = e_new;
+        }
+        if (ctx->uspp) c.copy(ctx->d_sx + (size_t)b * n, c.spsi);
+        if (b > 0) {
+            // row b of the lower Gram matrix: G[b][i] = <psi_b|S psi_i>, i < b
+            gemm_cn(psi, (int)n, lower_s, (int)n, 1, b, (int)n, ctx->d_cgpart,
+                    ctx->d_cgG + (size_t)b * nb, ctx->st);
+        }
+        if (eig) eig[b] = e;
+        if (steps) steps[b] = taken;
+        nconv += conv;
+    }
+    CK(cudaStreamSynchronize(ctx->st));
+    CK(cudaGetLastError());
+    if (n_conv) *n_conv = nconv;
+    return CHFSI_OK;
 }
 
 }  // namespace
@@ -1269,6 +1736,8 @@ chfsi_status chfsi_set_basis(chfsi_ctx* ctx, const int32_t* miller, const double
         chfsi_status s = alloc_mixed(ctx, ncol);
         if (s) return s;
     }
+    ctx->kin_host = kin;
+    ctx->cg_ready = false;
     ctx->basis_set = true;
     return CHFSI_OK;
 }
@@ -1853,11 +2322,41 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
         // diagonalize (scf.rs:169)
         const int passes = it == 1 ? std::max(1, p->first_passes) : 1;
         for (int q = 0; q < passes; ++q) {
+            const bool mixed_pass = ctx->mixed_active;
+            const size_t npsi = (size_t)ctx->nb * ctx->n_pw;
+            if (mixed_pass) {
+                if (!ctx->d_psi_save) CK(dalloc(&ctx->d_psi_save, npsi));
+                CK(cudaMemcpyAsync(ctx->d_psi_save, ctx->d_psi, npsi * sizeof(double2),
+                                   cudaMemcpyDeviceToDevice, st));
+            }
             s = filter_any(ctx, p->ndeg, have_eig ? ctx->d_eig : nullptr, have_eig ? ctx->nb : 0);
             if (!s) s = rr_any(ctx);
             if (!s) s = finish_diag(ctx, eig.data(), true);
+            if (s && mixed_pass && (s == CHFSI_ERR_RR_FAILED || s == CHFSI_ERR_CHEB_DIVERGED)) {
+                // the FP32 filter lost the conditioning of the subspace (the
+                // overlap is no longer positive definite): redo this pass in FP64
+                CK(cudaMemcpyAsync(ctx->d_psi, ctx->d_psi_save, npsi * sizeof(double2),
+                                   cudaMemcpyDeviceToDevice, st));
+                ctx->mixed_active = false;
+                s = filter_any(ctx, p->ndeg, have_eig ? ctx->d_eig : nullptr, have_eig ? ctx->nb : 0);
+                if (!s) s = rr_any(ctx);
+                if (!s) s = finish_diag(ctx, eig.data(), true);
+                ctx->mixed_active = true;
+                ++r->n_fp64_retries;
+            }
             if (s) break;
             have_eig = true;
+        }
+        if (!s && p->cg_steps > 0) {
+            // a few band-CG steps per band after the filter; the band energies
+            // feed the occupations and the next filter's bounds
+            int nc = 0;
+            s = band_cg_dev(ctx, p->cg_steps, 1e-10, eig.data(), nullptr, &nc);
+            if (!s) {
+                CK(cudaMemcpyAsync(ctx->d_eig, eig.data(), sizeof(double) * ctx->nb,
+                                   cudaMemcpyHostToDevice, st));
+                CK(cudaStreamSynchronize(st));
+            }
         }
         if (s) { status = s; break; }
         // occupations from the new eigenvalues, then construct_density (scf.rs:275)
@@ -2094,6 +2593,203 @@ extern "C" chfsi_status chfsi_set_augmentation(chfsi_ctx* ctx, const double* pos
     if (!ctx->d_cion) CK(dalloc(&ctx->d_cion, (size_t)ctx->nions));
     if (!ctx->d_vion) CK(dalloc(&ctx->d_vion, (size_t)ctx->nions));
     return upload_phases(ctx);
+}
+
+// ---------------------------------------------------------------- batches
+// Many independent contexts (k-points of one cell, independent cells of
+// uneven size) advanced together: one diagonalisation pass of every member
+// (FP32 filter with bounds from the member's previous eigenvalues, FP64
+// Rayleigh-Ritz) is captured once into a CUDA graph, each member on its own
+// stream forked from and joined to the batch's origin stream, so a replay is
+// one graph launch with the members' kernels free to overlap on the SMs.
+struct chfsi_batch {
+    std::vector<chfsi_ctx*> members;
+    cudaStream_t origin = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<cudaEvent_t> events;
+    int ndeg = 0;
+    size_t nodes = 0;
+    std::string err;
+};
+
+extern "C" chfsi_status chfsi_batch_create(chfsi_ctx* const* ctxs, int n, chfsi_batch** out) {
+    if (!ctxs || n <= 0 || !out) return CHFSI_ERR_BAD_INPUT;
+    *out = nullptr;
+    const int dev = ctxs[0] ? ctxs[0]->device : 0;
+    for (int i = 0; i < n; ++i) {
+        chfsi_ctx* c = ctxs[i];
+        if (!c || c->device != dev) return CHFSI_ERR_BAD_INPUT;
+        if (!c->mixed) {
+            set_last_error("batched passes run the mixed-precision path (FP32 filter, FP64 Rayleigh-Ritz)");
+            return CHFSI_ERR_BAD_INPUT;
+        }
+    }
+    cudaSetDevice(dev);
+    chfsi_batch* b = new chfsi_batch();
+    b->members.assign(ctxs, ctxs + n);
+    if (cudaStreamCreateWithFlags(&b->origin, cudaStreamNonBlocking) != cudaSuccess) {
+        delete b;
+        return CHFSI_ERR_CUDA;
+    }
+    *out = b;
+    return CHFSI_OK;
+}
+
+extern "C" void chfsi_batch_destroy(chfsi_batch* b) {
+    if (!b) return;
+    if (b->origin) cudaStreamSynchronize(b->origin);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    for (cudaEvent_t e : b->events) cudaEventDestroy(e);
+    if (b->origin) cudaStreamDestroy(b->origin);
+    delete b;
+}
+
+// Capture one pass of every member.  Each member must have run one
+// uncaptured diagonalisation first (it sets up the projector planes and the
+// eigenvalues the captured filter takes its bounds from).
+extern "C" chfsi_status chfsi_batch_capture(chfsi_batch* b, int ndeg) {
+    if (!b || ndeg < 1) return CHFSI_ERR_BAD_INPUT;
+    for (chfsi_ctx* c : b->members) {
+        if (!c->veff_set || !c->psi_set || ndeg > c->max_deg) return CHFSI_ERR_BAD_INPUT;
+        if (!c->mixed_active || (c->np > 0 && !c->beta_planes_ready)) {
+            set_last_error("run one diagonalisation of every member before capturing");
+            return CHFSI_ERR_BAD_INPUT;
+        }
+        cudaStreamSynchronize(c->st);
+    }
+    cudaSetDevice(b->members[0]->device);
+    if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+    if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+    for (cudaEvent_t e : b->events) cudaEventDestroy(e);
+    b->events.assign(b->members.size() + 1, nullptr);
+    for (auto& e : b->events)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return CHFSI_ERR_CUDA;
+    cudaError_t e = cudaStreamBeginCapture(b->origin, cudaStreamCaptureModeRelaxed);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamBeginCapture", __FILE__, __LINE__);
+    cudaEventRecord(b->events[0], b->origin);
+    chfsi_status st = CHFSI_OK;
+    for (size_t i = 0; i < b->members.size() && !st; ++i) {
+        chfsi_ctx* c = b->members[i];
+        cudaStreamWaitEvent(c->st, b->events[0], 0);
+        st = filter_any(c, ndeg, c->d_eig, c->nb);
+        if (!st) st = rr_any(c);
+        cudaEventRecord(b->events[i + 1], c->st);
+        cudaStreamWaitEvent(b->origin, b->events[i + 1], 0);
+    }
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(b->origin, &g);
+    if (st) {
+        if (g) cudaGraphDestroy(g);
+        return st;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture", __FILE__, __LINE__);
+    b->graph = g;
+    e = cudaGraphInstantiate(&b->exec, g, 0);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate", __FILE__, __LINE__);
+    size_t nn = 0;
+    cudaGraphGetNodes(g, nullptr, &nn);
+    b->nodes = nn;
+    b->ndeg = ndeg;
+    return CHFSI_OK;
+}
+
+extern "C" chfsi_status chfsi_batch_graph_nodes(chfsi_batch* b, size_t* nodes) {
+    if (!b || !nodes) return CHFSI_ERR_BAD_INPUT;
+    *nodes = b->nodes;
+    return CHFSI_OK;
+}
+
+// Replay the captured pass; eig_out (optional) receives every member's
+// n_bands eigenvalues in member order, status_out (optional) each member's
+// status (filter divergence, failed Rayleigh-Ritz).
+extern "C" chfsi_status chfsi_batch_run(chfsi_batch* b, double* eig_out, int* status_out) {
+    if (!b || !b->exec) return CHFSI_ERR_BAD_INPUT;
+    cudaSetDevice(b->members[0]->device);
+    cudaError_t e = cudaGraphLaunch(b->exec, b->origin);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGraphLaunch", __FILE__, __LINE__);
+    e = cudaStreamSynchronize(b->origin);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize", __FILE__, __LINE__);
+    chfsi_status worst = CHFSI_OK;
+    size_t off = 0;
+    for (size_t i = 0; i < b->members.size(); ++i) {
+        chfsi_ctx* c = b->members[i];
+        c->last_ndeg = b->ndeg;
+        const chfsi_status s = finish_diag(c, eig_out ? eig_out + off : nullptr, true);
+        if (status_out) status_out[i] = s;
+        if (s && !worst) worst = s;
+        off += c->nb;
+    }
+    return worst;
+}
+
+// Launch configurations of the local H|psi> for this context's sizes: the
+// xy-plane kernel at 128, 256 or 512 threads per block and the z-stick
+// kernels at 16, 32 or 64 columns per block, each timed on the current psi
+// (all bands); the fastest is kept.  times_ms (optional, 9 entries) gets the
+// timing of every variant (planes variant * 3 + columns variant).
+extern "C" chfsi_status chfsi_autotune(chfsi_ctx* ctx, int* choice, float* times_ms) {
+    chfsi_status s = ready(ctx);
+    if (s) return s;
+    if (!ctx->psi_set) return ctx->fail(CHFSI_ERR_BAD_INPUT, "psi not set");
+    cudaSetDevice(ctx->device);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int np = ctx->np;
+    ctx->np = 0;  // the launch configurations only concern the local part
+    float best = 1e30f;
+    int best_i = 0;
+    for (int i = 0; i < 9 && !s; ++i) {
+        ctx->geo.tune_planes = i / 3;
+        ctx->geo.tune_cols = 16 << (i % 3);
+        for (int r = 0; r < 2 && !s; ++r) s = apply_h_dev(ctx, ctx->d_psi, ctx->d_hpsi, ctx->nb, kEpiApply, nullptr);
+        cudaEventRecord(e0, ctx->st);
+        for (int r = 0; r < 3 && !s; ++r) s = apply_h_dev(ctx, ctx->d_psi, ctx->d_hpsi, ctx->nb, kEpiApply, nullptr);
+        cudaEventRecord(e1, ctx->st);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        ms /= 3.f;
+        if (times_ms) times_ms[i] = ms;
+        if (ms < best) { best = ms; best_i = i; }
+    }
+    ctx->np = np;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ctx->geo.tune_planes = best_i / 3;
+    ctx->geo.tune_cols = 16 << (best_i % 3);
+    if (s) return s;
+    CK(cudaGetLastError());
+    if (choice) *choice = best_i;
+    return CHFSI_OK;
+}
+
+extern "C" chfsi_status chfsi_set_launch_config(chfsi_ctx* ctx, int choice) {
+    if (!ctx || choice < 0 || choice >= 9) return CHFSI_ERR_BAD_INPUT;
+    ctx->geo.tune_planes = choice / 3;
+    ctx->geo.tune_cols = 16 << (choice % 3);
+    return CHFSI_OK;
+}
+
+// Band-by-band CG refinement of the current wavefunctions (band_cg.rs).
+extern "C" chfsi_status chfsi_band_cg(chfsi_ctx* ctx, int max_steps, double tol, double* eig_out,
+                                      int* steps_out, int* n_converged) {
+    if (!ctx || max_steps < 0 || !(tol > 0.0)) return CHFSI_ERR_BAD_INPUT;
+    if (!ctx->basis_set || !ctx->psi_set || !ctx->veff_set)
+        return ctx->fail(CHFSI_ERR_BAD_INPUT, "context not ready");
+    if (ctx->np > 0 && !ctx->proj_set) return ctx->fail(CHFSI_ERR_BAD_INPUT, "projectors not set");
+    cudaSetDevice(ctx->device);
+    std::vector<double> e(ctx->nb);
+    std::vector<int> st(ctx->nb);
+    int nc = 0;
+    chfsi_status s = band_cg_dev(ctx, max_steps, tol, e.data(), st.data(), &nc);
+    if (s) return s;
+    if (eig_out) std::memcpy(eig_out, e.data(), sizeof(double) * ctx->nb);
+    if (steps_out) std::memcpy(steps_out, st.data(), sizeof(int) * ctx->nb);
+    if (n_converged) *n_converged = nc;
+    return CHFSI_OK;
 }
 
 extern "C" chfsi_status chfsi_set_mixer(chfsi_ctx* ctx, chfsi_mixer* m) {

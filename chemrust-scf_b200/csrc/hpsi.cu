@@ -57,7 +57,7 @@ template <typename C> __host__ __device__ __forceinline__ size_t align16(size_t 
 }
 
 // ---------------------------------------------------------------- pass 1
-template <typename C>
+template <typename C, int kColsPerBlock>
 __global__ void __launch_bounds__(256)
 k_zsticks_inverse(const C* __restrict__ psi, int ldp, C* __restrict__ work, HGeom g) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -86,14 +86,17 @@ k_zsticks_inverse(const C* __restrict__ psi, int ldp, C* __restrict__ work, HGeo
 // ---------------------------------------------------------------- pass 2
 // 256 threads with 2 (FP64) or 3 (FP32) resident blocks per SM: the
 // global-memory phases of one plane overlap the FFT stages of another.
-template <typename C>
+// Variant 0: 256 threads, 1: 128 threads, 2: 512 threads per block, with as
+// many resident blocks per SM as the registers of each precision allow.
+template <typename C, int V>
 struct PlanesCfg {
-    static constexpr int threads = 256;
-    static constexpr int min_blocks = sizeof(C) == 16 ? 2 : 3;
+    static constexpr int threads = V == 0 ? 256 : (V == 1 ? 128 : 512);
+    static constexpr int min_blocks =
+        V == 0 ? (sizeof(C) == 16 ? 2 : 3) : (V == 1 ? (sizeof(C) == 16 ? 4 : 6) : 1);
 };
 
-template <typename C>
-__global__ void __launch_bounds__(PlanesCfg<C>::threads, PlanesCfg<C>::min_blocks)
+template <typename C, int V>
+__global__ void __launch_bounds__(PlanesCfg<C, V>::threads, PlanesCfg<C, V>::min_blocks)
 k_planes_vloc(C* __restrict__ work, const double* __restrict__ veff, HGeom g) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* twx = reinterpret_cast<C*>(smem_raw);
@@ -138,7 +141,7 @@ k_planes_vloc(C* __restrict__ work, const double* __restrict__ veff, HGeom g) {
 }
 
 // ---------------------------------------------------------------- pass 3
-template <typename C, int MODE>
+template <typename C, int MODE, int kColsPerBlock>
 __global__ void __launch_bounds__(256)
 k_zsticks_forward(const C* __restrict__ work, const C* __restrict__ psi, int ldp, C* out, int ldo,
                   HGeom g, Epilogue e) {
@@ -406,14 +409,23 @@ int grid_for(size_t n, int threads) {
 }  // namespace
 
 // ------------------------------------------------------------------ launchers
+template <typename C, int COLS>
+void zsticks_inverse_cols(const C* psi, int ldp, C* work, int nb, const HGeom& g, cudaStream_t st) {
+    dim3 grid((g.ncol + COLS - 1) / COLS, nb);
+    size_t sm = align16<C>(g.nz) + (size_t)COLS * g.lsz * sizeof(C);
+    allow_smem(k_zsticks_inverse<C, COLS>, sm);
+    k_zsticks_inverse<C, COLS><<<grid, 256, sm, st>>>(psi, ldp, work, g);
+}
+
 template <typename C>
 void launch_zsticks_inverse(const C* psi, int ldp, C* work, int nb, const HGeom& g,
                             cudaStream_t st) {
     count_launch();
-    dim3 grid((g.ncol + kColsPerBlock - 1) / kColsPerBlock, nb);
-    size_t sm = align16<C>(g.nz) + (size_t)kColsPerBlock * g.lsz * sizeof(C);
-    allow_smem(k_zsticks_inverse<C>, sm);
-    k_zsticks_inverse<C><<<grid, 256, sm, st>>>(psi, ldp, work, g);
+    switch (g.tune_cols) {
+    case 16: zsticks_inverse_cols<C, 16>(psi, ldp, work, nb, g, st); break;
+    case 64: zsticks_inverse_cols<C, 64>(psi, ldp, work, nb, g, st); break;
+    default: zsticks_inverse_cols<C, 32>(psi, ldp, work, nb, g, st); break;
+    }
 }
 
 size_t planes_smem_bytes(const HGeom& g, size_t csize) {
@@ -422,28 +434,53 @@ size_t planes_smem_bytes(const HGeom& g, size_t csize) {
            (size_t)g.nxact * sizeof(int);
 }
 
+template <typename C, int V>
+void planes_vloc_variant(C* work, const double* veff, int nb, const HGeom& g, cudaStream_t st) {
+    dim3 grid(g.nz, nb);
+    size_t sm = planes_smem_bytes(g, sizeof(C));
+    allow_smem(k_planes_vloc<C, V>, sm);
+    k_planes_vloc<C, V><<<grid, PlanesCfg<C, V>::threads, sm, st>>>(work, veff, g);
+}
+
 template <typename C>
 void launch_planes_vloc(C* work, const double* veff, int nb, const HGeom& g, cudaStream_t st) {
     count_launch();
-    dim3 grid(g.nz, nb);
-    size_t sm = planes_smem_bytes(g, sizeof(C));
-    allow_smem(k_planes_vloc<C>, sm);
-    k_planes_vloc<C><<<grid, PlanesCfg<C>::threads, sm, st>>>(work, veff, g);
+    switch (g.tune_planes) {
+    case 1: planes_vloc_variant<C, 1>(work, veff, nb, g, st); break;
+    case 2: planes_vloc_variant<C, 2>(work, veff, nb, g, st); break;
+    default: planes_vloc_variant<C, 0>(work, veff, nb, g, st); break;
+    }
+}
+
+template <typename C, int COLS>
+void zsticks_forward_cols(const C* work, const C* psi, int ldp, C* out, int ldo, int nb,
+                          const HGeom& g, const Epilogue& e, cudaStream_t st) {
+    dim3 grid((g.ncol + COLS - 1) / COLS, nb);
+    size_t sm = align16<C>(g.nz) + (size_t)COLS * g.lsz * sizeof(C);
+    switch (e.mode) {
+    case kEpiApply:
+        allow_smem(k_zsticks_forward<C, kEpiApply, COLS>, sm);
+        k_zsticks_forward<C, kEpiApply, COLS><<<grid, 256, sm, st>>>(work, psi, ldp, out, ldo, g, e);
+        break;
+    case kEpiChebFirst:
+        allow_smem(k_zsticks_forward<C, kEpiChebFirst, COLS>, sm);
+        k_zsticks_forward<C, kEpiChebFirst, COLS><<<grid, 256, sm, st>>>(work, psi, ldp, out, ldo, g, e);
+        break;
+    default:
+        allow_smem(k_zsticks_forward<C, kEpiCheb, COLS>, sm);
+        k_zsticks_forward<C, kEpiCheb, COLS><<<grid, 256, sm, st>>>(work, psi, ldp, out, ldo, g, e);
+        break;
+    }
 }
 
 template <typename C>
 void launch_zsticks_forward(const C* work, const C* psi, int ldp, C* out, int ldo, int nb,
                             const HGeom& g, const Epilogue& e, cudaStream_t st) {
     count_launch();
-    dim3 grid((g.ncol + kColsPerBlock - 1) / kColsPerBlock, nb);
-    size_t sm = align16<C>(g.nz) + (size_t)kColsPerBlock * g.lsz * sizeof(C);
-    allow_smem(k_zsticks_forward<C, kEpiApply>, sm);
-    allow_smem(k_zsticks_forward<C, kEpiChebFirst>, sm);
-    allow_smem(k_zsticks_forward<C, kEpiCheb>, sm);
-    switch (e.mode) {
-    case kEpiApply: k_zsticks_forward<C, kEpiApply><<<grid, 256, sm, st>>>(work, psi, ldp, out, ldo, g, e); break;
-    case kEpiChebFirst: k_zsticks_forward<C, kEpiChebFirst><<<grid, 256, sm, st>>>(work, psi, ldp, out, ldo, g, e); break;
-    default: k_zsticks_forward<C, kEpiCheb><<<grid, 256, sm, st>>>(work, psi, ldp, out, ldo, g, e); break;
+    switch (g.tune_cols) {
+    case 16: zsticks_forward_cols<C, 16>(work, psi, ldp, out, ldo, nb, g, e, st); break;
+    case 64: zsticks_forward_cols<C, 64>(work, psi, ldp, out, ldo, nb, g, e, st); break;
+    default: zsticks_forward_cols<C, 32>(work, psi, ldp, out, ldo, nb, g, e, st); break;
     }
 }
 

@@ -25,6 +25,11 @@ struct HGeom {
     // twiddle tables exp(+2 pi i j / n) per axis, precomputed once per context
     const double2* twd_x; const double2* twd_y; const double2* twd_z;
     const float2* twf_x; const float2* twf_y; const float2* twf_z;
+    // launch configuration chosen by chfsi_autotune: xy-plane kernel
+    // 0 = 256 threads, 1 = 128 threads, 2 = 512 threads per block; z-stick
+    // kernels at tune_cols (16, 32, 64) columns per block
+    int tune_planes = 0;
+    int tune_cols = 32;
 };
 
 // Pass-3 epilogue: what to do with (H psi)_g once it is assembled.
@@ -39,7 +44,6 @@ struct Epilogue {
     double inv_n;          // 1 / N^3
 };
 
-constexpr int kColsPerBlock = 32;
 // density accumulation keeps 24 plane points per thread x 512 threads
 constexpr size_t kDensityPlanePoints = 24 * 512;
 

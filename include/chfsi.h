@@ -291,7 +291,7 @@ typedef struct chfsi_scf_params {
                                     |dE|/atom < this (convergence is only declared on
                                     FP64 steps)                                        */
     int    mixer;         /* CHFSI_MIXER_PULAY / _LEARNED / _LEARNED_PULAY            */
-    int    reserved;
+    int    cg_steps;      /* band-CG steps per band after each filter (0: none)      */
     double* trace;        /* optional host buffer of 2 * max_iter * N^3 doubles: rho_in
                              and rho_out of every iteration (training trajectories)   */
 } chfsi_scf_params;
@@ -322,12 +322,47 @@ typedef struct chfsi_scf_result {
     int     fell_back;    /* 1 if a learned run fell back to Pulay              */
     double* residuals;    /* caller array of max_iter entries (|rho_out - rho_in|_2
                              on the grid), or NULL                              */
+    int     n_fp64_retries; /* mixed-precision passes redone in FP64 after the FP32
+                               filter left a non-positive-definite overlap      */
 } chfsi_scf_result;
 
 /* Full SCF from a uniform density: build_v_eff -> diagonalize -> density ->
  * energy -> check -> Pulay mix (run_scf, src/scf.rs:358-376).  Returns
  * CHFSI_OK when converged, CHFSI_NOT_CONVERGED after max_iter. */
 chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p, chfsi_scf_result* r);
+
+/* Band-by-band preconditioned CG refinement of the current wavefunctions
+ * (band_cg_minimize, src/eigensolver/band_cg.rs:157-437): each band in turn,
+ * S-orthogonalised against the already refined lower bands, at most
+ * max_steps steps, stopping when its energy changes by less than tol (Ha).
+ * Preconditioner: TPA diagonal, plus the ultrasoft Woodbury term when q is
+ * set (uspp_preconditioner.rs).  eig_out / steps_out: n_bands entries or NULL. */
+chfsi_status chfsi_band_cg(chfsi_ctx* ctx, int max_steps, double tol, double* eig_out,
+                           int* steps_out, int* n_converged);
+
+/* ---- batches of independent systems (k-points, independent cells) -------
+ * One mixed-precision diagonalisation pass (FP32 filter with bounds from
+ * each member's previous eigenvalues, FP64 Rayleigh-Ritz) of every member is
+ * captured once into a CUDA graph, members on their own streams forked from
+ * and joined to one origin stream; chfsi_batch_run replays it as a single
+ * graph launch.  Members: contexts created with CHFSI_PREC_MIXED on one
+ * device, each having run one chfsi_diagonalize before capture.  The
+ * reference crate has no batched path (one context, one stream). */
+typedef struct chfsi_batch chfsi_batch;
+chfsi_status chfsi_batch_create(chfsi_ctx* const* ctxs, int n, chfsi_batch** out);
+void         chfsi_batch_destroy(chfsi_batch* b);
+chfsi_status chfsi_batch_capture(chfsi_batch* b, int ndeg);
+/* eig_out: every member's n_bands eigenvalues in member order (or NULL);
+ * status_out: per member status (or NULL); returns the first failure */
+chfsi_status chfsi_batch_run(chfsi_batch* b, double* eig_out, int* status_out);
+chfsi_status chfsi_batch_graph_nodes(chfsi_batch* b, size_t* nodes);
+/* Autotuner: times the local H|psi> of this context at 3 x 3 launch
+ * configurations (xy-plane kernel 256 / 128 / 512 threads per block; z-stick
+ * kernels 16 / 32 / 64 columns per block) on its current psi and keeps the
+ * fastest; choice = planes * 3 + columns, times_ms (9 floats) may be NULL.
+ * chfsi_set_launch_config applies a choice (e.g. one tuned per size class). */
+chfsi_status chfsi_autotune(chfsi_ctx* ctx, int* choice, float* times_ms);
+chfsi_status chfsi_set_launch_config(chfsi_ctx* ctx, int choice);
 
 /* ---- learned density mixer (no counterpart in the reference crate) ------
  * MLP 512 -> 256 -> 256 -> 128 with GELU, BF16 weights and FP32 accumulation.

@@ -43,3 +43,21 @@ def test_uspp_scf_converges_to_oracle(chfsi):
     assert r["converged"] and ref["converged"]
     assert abs(r["e_total"] - ref["energies"][-1]) / s.n_atoms < 1e-8
     np.testing.assert_allclose(r["eigenvalues"], ref["eigenvalues"], atol=1e-8)
+
+
+def test_mixed_precision_uspp_scf_matches_fp64(chfsi):
+    """FP32 filter of S^-1 H with tcgen05 projections, FP64 Rayleigh-Ritz with
+    the ultrasoft overlap, final FP64 passes: same converged energy and
+    occupied eigenvalues as the FP64 run."""
+    s = _system(chfsi, (32, 32, 32))
+    rf = chfsi.Context(s).run_scf(12, max_iter=40, kT=0.01)
+    rm = chfsi.Context(s, precision=chfsi.PREC_MIXED).run_scf(12, max_iter=40, kT=0.01,
+                                                              fp64_switch_per_atom=1e-4)
+    n_occ = int(round(s.n_elec / 2))
+    de = abs(rm["e_total"] - rf["e_total"]) / s.n_atoms
+    docc = np.abs(rm["eigenvalues"][:n_occ] - rf["eigenvalues"][:n_occ]).max()
+    print("mixed ultrasoft SCF: %d iterations (%d mixed) vs %d; dE/atom %.2e, occupied eig %.2e"
+          % (rm["n_iter"], rm["n_iter_mixed"], rf["n_iter"], de, docc))
+    assert rf["converged"] and rm["converged"] and rm["n_iter_mixed"] >= 1
+    assert de < 1e-6
+    assert docc < 1e-5
