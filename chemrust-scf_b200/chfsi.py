@@ -110,7 +110,8 @@ class ScfParams(C.Structure):
     _fields_ = [("ndeg", C.c_int), ("max_iter", C.c_int), ("tol_per_atom", C.c_double),
                 ("alpha", C.c_double), ("max_hist", C.c_int), ("first_passes", C.c_int),
                 ("kT", C.c_double), ("fp64_switch_per_atom", C.c_double),
-                ("mixer", C.c_int), ("cg_steps", C.c_int), ("trace", C.POINTER(C.c_double))]
+                ("mixer", C.c_int), ("cg_steps", C.c_int), ("trace", C.POINTER(C.c_double)),
+                ("verbose", C.c_int), ("reserved", C.c_int)]
 
 
 class ScfResult(C.Structure):
@@ -622,12 +623,12 @@ class Context:
 
     def run_scf(self, ndeg, tol_per_atom=1e-6, max_iter=30, alpha=0.3, max_hist=6,
                 first_passes=4, kT=0.01, fp64_switch_per_atom=1e-4, raise_not_converged=False,
-                mixer=MIXER_PULAY, trace=False, cg_steps=0):
+                mixer=MIXER_PULAY, trace=False, cg_steps=0, verbose=False):
         """Full SCF; mixer is MIXER_PULAY or, after set_mixer(), MIXER_LEARNED /
         MIXER_LEARNED_PULAY.  trace=True also returns rho_in and rho_out of every
         iteration (n_iter x N^3 each) as 'trace_in' / 'trace_out'."""
         p = ScfParams(ndeg, max_iter, tol_per_atom, alpha, max_hist, first_passes, kT,
-                      fp64_switch_per_atom, mixer, cg_steps, None)
+                      fp64_switch_per_atom, mixer, cg_steps, None, int(verbose), 0)
         tr = None
         if trace:
             tr = np.zeros((max_iter, 2, self.ng_density))

@@ -2325,8 +2325,11 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
             const bool mixed_pass = ctx->mixed_active;
             const size_t npsi = (size_t)ctx->nb * ctx->n_pw;
             if (mixed_pass) {
-                if (!ctx->d_psi_save) CK(dalloc(&ctx->d_psi_save, npsi));
+                // psi and the eigenvalues the bounds come from, for an FP64 retry
+                if (!ctx->d_psi_save) CK(dalloc(&ctx->d_psi_save, npsi + (ctx->nb + 1) / 2));
                 CK(cudaMemcpyAsync(ctx->d_psi_save, ctx->d_psi, npsi * sizeof(double2),
+                                   cudaMemcpyDeviceToDevice, st));
+                CK(cudaMemcpyAsync(ctx->d_psi_save + npsi, ctx->d_eig, ctx->nb * sizeof(double),
                                    cudaMemcpyDeviceToDevice, st));
             }
             s = filter_any(ctx, p->ndeg, have_eig ? ctx->d_eig : nullptr, have_eig ? ctx->nb : 0);
@@ -2335,7 +2338,17 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
             if (s && mixed_pass && (s == CHFSI_ERR_RR_FAILED || s == CHFSI_ERR_CHEB_DIVERGED)) {
                 // the FP32 filter lost the conditioning of the subspace (the
                 // overlap is no longer positive definite): redo this pass in FP64
+                // from the saved psi and eigenvalues (the failed pass's
+                // Rayleigh-Ritz has overwritten both)
+                if (p->verbose) {
+                    std::fprintf(stderr, "scf %3d pass %d fp32 failed: lm %.4f cut %.4f: %s; |psi_k|:", it,
+                                 q, ctx->h_coef[0], ctx->h_coef[1], g_last_error.c_str());
+                    for (double v : ctx->h_nsq) std::fprintf(stderr, " %.3e", std::sqrt(v));
+                    std::fprintf(stderr, "\n");
+                }
                 CK(cudaMemcpyAsync(ctx->d_psi, ctx->d_psi_save, npsi * sizeof(double2),
+                                   cudaMemcpyDeviceToDevice, st));
+                CK(cudaMemcpyAsync(ctx->d_eig, ctx->d_psi_save + npsi, ctx->nb * sizeof(double),
                                    cudaMemcpyDeviceToDevice, st));
                 ctx->mixed_active = false;
                 s = filter_any(ctx, p->ndeg, have_eig ? ctx->d_eig : nullptr, have_eig ? ctx->nb : 0);
@@ -2343,7 +2356,15 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
                 if (!s) s = finish_diag(ctx, eig.data(), true);
                 ctx->mixed_active = true;
                 ++r->n_fp64_retries;
+                if (p->verbose)
+                    std::fprintf(stderr, "scf %3d pass %d: mixed pass failed, redone in FP64 -> %d\n",
+                                 it, q, (int)s);
             }
+            if (p->verbose)
+                std::fprintf(stderr, "scf %3d pass %d %s status %d eig [%.5f, %.5f] lm %.4f cut %.4f %s\n",
+                             it, q, ctx->last_pass_fp32 ? "fp32" : "fp64", (int)s, eig[0],
+                             eig[ctx->nb - 1], ctx->h_coef[0], ctx->h_coef[1],
+                             s ? g_last_error.c_str() : "");
             if (s) break;
             have_eig = true;
         }
@@ -2385,6 +2406,15 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
         r->e_band = eband; r->e_hartree = acc[0]; r->e_xc = acc[1]; r->e_dc = acc[2];
         r->e_total = etot;
         r->n_iter = it;
+        if (p->verbose) {
+            std::fprintf(stderr,
+                         "scf %3d %s E %.10f dE/atom %.3e eig [%.5f, %.5f] bounds lm %.4f cut %.4f "
+                         "retries %d learned %d\n",
+                         it, ctx->mixed_active ? "mixed" : "fp64 ", etot,
+                         it > 1 ? std::fabs(etot - e_prev) / ctx->n_atoms : 0.0, eig[0],
+                         eig[ctx->nb - 1], ctx->h_coef[0], ctx->h_coef[1], r->n_fp64_retries,
+                         r->n_iter_learned);
+        }
         if (p->trace) {
             double* tr = p->trace + (size_t)2 * (it - 1) * ng;
             CK(cudaMemcpyAsync(tr, ctx->d_rho_in, sizeof(double) * ng, cudaMemcpyDeviceToHost, st));

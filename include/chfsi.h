@@ -294,6 +294,8 @@ typedef struct chfsi_scf_params {
     int    cg_steps;      /* band-CG steps per band after each filter (0: none)      */
     double* trace;        /* optional host buffer of 2 * max_iter * N^3 doubles: rho_in
                              and rho_out of every iteration (training trajectories)   */
+    int    verbose;       /* 1: one line per iteration on stderr                       */
+    int    reserved;
 } chfsi_scf_params;
 
 /* Density mixers of chfsi_scf_run.  PULAY: Pulay/DIIS over (rho_in,

@@ -49,7 +49,7 @@ def test_batched_graph_matches_sequential_passes(chfsi):
 
 def test_autotuner_keeps_results(chfsi):
     torch = pytest.importorskip("torch")
-    s = chfsi.SyntheticSystem(config_index=1, n_bands=64)
+    s = chfsi.SyntheticSystem(config_index=1, n_bands=132)
     ctx = chfsi.Context(s)
     x = torch.from_numpy(np.ascontiguousarray(s.psi0()[:64])).cuda()
     y0 = torch.empty_like(x)
