@@ -252,24 +252,36 @@ def run_ours(args):
                  "dtype": "f32 filter, bf16x3 tcgen05 GEMMs (fp32 accumulate), f64 eigensolve"}
         mctx.close()
         if not args.no_scf:
+            import learned_mixer
             res = {}
-            for name, prec in (("fp64", chfsi.PREC_FP64), ("mixed", chfsi.PREC_MIXED)):
+            arms = (("fp64", chfsi.PREC_FP64, chfsi.MIXER_PULAY),
+                    ("mixed", chfsi.PREC_MIXED, chfsi.MIXER_PULAY),
+                    ("mixed_learned", chfsi.PREC_MIXED, chfsi.MIXER_LEARNED_PULAY))
+            mixer_net = learned_mixer.load(device=local)
+            for name, prec, mode in arms:
                 sctx = chfsi.Context(s, device=local, precision=prec)
-                r = sctx.run_scf(NDEG, tol_per_atom=1e-6, max_iter=60, kT=0.01)
+                if mode != chfsi.MIXER_PULAY:
+                    sctx.set_mixer(mixer_net)
+                # FP64 only for the final confirming iterations of the mixed runs
+                r = sctx.run_scf(NDEG, tol_per_atom=1e-6, max_iter=60, kT=0.01, mixer=mode,
+                                 fp64_switch_per_atom=1e-6)
                 res[name] = r
                 sctx.close()
-            f, m = res["fp64"], res["mixed"]
-            mixed["time_to_scf"] = {
-                "criterion": "|dE| < 1e-6 Ha/atom (Fermi-Dirac kT = 0.01 Ha, Pulay 0.3/6)",
-                "fp64_s": round(f["seconds"], 4), "fp64_iterations": f["n_iter"],
-                "mixed_s": round(m["seconds"], 4), "mixed_iterations": m["n_iter"],
-                "mixed_iterations_in_mixed_precision": m["n_iter_mixed"],
-                "speedup": round(f["seconds"] / m["seconds"], 3) if m["seconds"] > 0 else None,
-                "converged": [bool(f["converged"]), bool(m["converged"])],
-                "energy_diff_per_atom_Ha": abs(f["e_total"] - m["e_total"]) / s.n_atoms,
-                "max_occupied_eigenvalue_diff_Ha":
-                    float(np.abs(f["eigenvalues"][:s.n_occ] - m["eigenvalues"][:s.n_occ]).max()),
-            }
+            f = res["fp64"]
+            tts = {"criterion": "|dE| < 1e-6 Ha/atom (Fermi-Dirac kT = 0.01 Ha, Pulay 0.3/6)",
+                   "fp64_s": round(f["seconds"], 4), "fp64_iterations": f["n_iter"]}
+            for name in ("mixed", "mixed_learned"):
+                m = res[name]
+                tts.update({
+                    name + "_s": round(m["seconds"], 4), name + "_iterations": m["n_iter"],
+                    name + "_iterations_in_mixed_precision": m["n_iter_mixed"],
+                    name + "_speedup": round(f["seconds"] / m["seconds"], 3) if m["seconds"] > 0 else None,
+                    name + "_energy_diff_per_atom_Ha": abs(f["e_total"] - m["e_total"]) / s.n_atoms,
+                    name + "_max_occupied_eigenvalue_diff_Ha":
+                        float(np.abs(f["eigenvalues"][:s.n_occ] - m["eigenvalues"][:s.n_occ]).max()),
+                })
+            tts["converged"] = [bool(res[k]["converged"]) for k in ("fp64", "mixed", "mixed_learned")]
+            mixed["time_to_scf"] = tts
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

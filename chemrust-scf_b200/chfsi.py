@@ -192,6 +192,7 @@ def lib():
         "chfsi_set_mixer": [vp, vp],
         "chfsi_mixer_samples": [vp, dp, dp, C.c_int, dp, fp, fp],
         "chfsi_set_density_grid": [vp, C.POINTER(C.c_int)],
+        "chfsi_get_rr_sweeps": [vp, C.POINTER(C.c_int)],
         "chfsi_get_density_grid": [vp, C.POINTER(C.c_int)],
         "chfsi_set_augmentation": [vp, dp, C.c_double],
         "chfsi_band_cg": [vp, C.c_int, C.c_double, dp, i32p, i32p],
@@ -471,6 +472,11 @@ class Context:
         _check(lib().chfsi_get_density_grid(self.handle, n3))
         self.ngrid_density = tuple(n3)
         self.ng_density = int(np.prod(self.ngrid_density))
+
+    def rr_sweeps(self):
+        v = C.c_int()
+        self._c(lib().chfsi_get_rr_sweeps(self.handle, C.byref(v)))
+        return v.value
 
     def set_density_grid(self, ngrid):
         n3 = (C.c_int * 3)(*ngrid)

@@ -417,6 +417,7 @@ struct chfsi_ctx {
     float* d_tc_part = nullptr; int* d_tc_err = nullptr;
     bool beta_planes_ready = false;
     bool last_pass_fp32 = false;  // the last filter ran in FP32
+    int last_sweeps = 0;          // Jacobi sweeps of the last Rayleigh-Ritz
     // density grid: density, potentials, mixing and augmentation live here.
     // It is the wavefunction grid unless chfsi_set_density_grid chose a
     // finer one; then the smooth density is interpolated up by zero padding
@@ -888,6 +889,7 @@ chfsi_status finish_diag(chfsi_ctx* ctx, double* eig_out, bool have_rr) {
             std::snprintf(buf, sizeof(buf), "Rayleigh-Ritz failed: info=%d (overlap not positive definite)", flags[0]);
             return ctx->fail(CHFSI_ERR_RR_FAILED, buf);
         }
+        ctx->last_sweeps = flags[2];
         if (flags[2] >= ctx->jac_max_sweeps) {
             return ctx->fail(CHFSI_ERR_RR_FAILED, "Rayleigh-Ritz failed: eigensolver did not converge");
         }
@@ -2600,6 +2602,13 @@ extern "C" chfsi_status chfsi_set_density_grid(chfsi_ctx* ctx, const int* ngrid)
         CK(copy_sync(ctx->d_gmap_f, fp.data(), fp.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
     }
     return upload_phases(ctx);
+}
+
+// Jacobi sweeps of the last Rayleigh-Ritz eigensolve (diagnostics).
+extern "C" chfsi_status chfsi_get_rr_sweeps(chfsi_ctx* ctx, int* sweeps) {
+    if (!ctx || !sweeps) return CHFSI_ERR_BAD_INPUT;
+    *sweeps = ctx->last_sweeps;
+    return CHFSI_OK;
 }
 
 extern "C" chfsi_status chfsi_get_density_grid(chfsi_ctx* ctx, int* ngrid) {

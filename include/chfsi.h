@@ -197,6 +197,8 @@ chfsi_status chfsi_set_qmat(chfsi_ctx* ctx, const chfsi_c128* qmat);
  * padding in G and V_eff is brought down by truncation
  * (downsample_array_to_wave_grid, src/scf.rs:413-454). */
 chfsi_status chfsi_set_density_grid(chfsi_ctx* ctx, const int* ngrid);
+/* Jacobi sweeps of the last Rayleigh-Ritz eigensolve (diagnostics). */
+chfsi_status chfsi_get_rr_sweeps(chfsi_ctx* ctx, int* sweeps);
 chfsi_status chfsi_get_density_grid(chfsi_ctx* ctx, int* ngrid);
 /* Ultrasoft augmentation: Q_ij(r) = q_ij g(|r - R_I|), g a unit Gaussian of
  * the given width (bohr), for the ions with projectors (positions n_ions x 3,
