@@ -17,6 +17,9 @@
 
 namespace cg = cooperative_groups;
 
+// V row entries one lane keeps in registers in k_jacobi_cluster (n <= 32 x this)
+constexpr int kJacClusterMaxPerLane = 8;
+
 namespace chfsi {
 
 namespace {
@@ -263,18 +266,23 @@ k_jacobi(double2* A, double2* V, int n, int max_sweeps, double tol2, double* scr
 
 // Circle-method pairing of step s over m = n + (n & 1) indices: pair i of
 // step s is (min(a, b), max(a, b)).
+// Every argument reduced below lies in (-(m - 1), 2 (m - 1)), so one
+// conditional add or subtract replaces the integer modulo.
+__device__ __forceinline__ int jac_wrap(int x, int M) { return x >= M ? x - M : (x < 0 ? x + M : x); }
 __device__ __forceinline__ void jac_pair(int m, int s, int i, int& p, int& q) {
-    const int a = i == 0 ? 0 : 1 + ((i - 1 + s) % (m - 1));
-    const int b = 1 + ((m - 2 - i + s) % (m - 1));
+    const int M = m - 1;
+    const int a = i == 0 ? 0 : 1 + jac_wrap(i - 1 + s, M);
+    const int b = 1 + jac_wrap(m - 2 - i + s, M);
     p = min(a, b);
     q = max(a, b);
 }
 // Pair index and partner of column k at step s.
 __device__ __forceinline__ void jac_partner(int m, int s, int k, int& pi, int& partner) {
-    const int j = k == 0 ? 0 : ((k - 1 - s) % (m - 1) + (m - 1)) % (m - 1) + 1;
+    const int M = m - 1;
+    const int j = k == 0 ? 0 : jac_wrap(k - 1 - s, M) + 1;
     const int jj = m - 1 - j;
     pi = min(j, jj);
-    partner = jj == 0 ? 0 : 1 + ((jj - 1 + s) % (m - 1));
+    partner = jj == 0 ? 0 : 1 + jac_wrap(jj - 1 + s, M);
 }
 
 // Parallel cyclic Jacobi with one grid barrier per rotation step.
@@ -551,6 +559,184 @@ k_jacobi3(double2* __restrict__ A, double2* __restrict__ V, double2* __restrict_
     if (gtid == 0) *sweeps_out = converged ? sweep : max_sweeps;
 }
 
+// The k_jacobi3 rotation sequence inside one thread-block cluster, for the
+// sizes whose rows fit the cluster's shared memory: the X rows of a pair go
+// straight into the shared memory of the warp that owns them at the next step
+// (distributed shared memory), the rotation parameters are broadcast to
+// every block of the cluster, and one cluster barrier per step replaces the
+// grid barrier and the global round trip.  Staging rows and parameters are
+// double-buffered by step parity, so a block that runs ahead into step s + 1
+// never overwrites what a slower block still reads in step s.
+// Shared layout (double2): params [2][2 * npairs] | per warp: A rows [2n],
+// V rows [2n], staging [2][2n].
+__global__ void __launch_bounds__(256)
+k_jacobi_cluster(double2* __restrict__ A, double2* __restrict__ V, int n, int max_sweeps,
+                 double tol2, double* scratch, int* sweeps_out) {
+    cg::cluster_group cluster = cg::this_cluster();
+    extern __shared__ double2 csm[];
+    __shared__ double red[32];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    const int crank = (int)cluster.block_rank();
+    const int gw = crank * wpb + wib;
+    const int m = n + (n & 1), npairs = m / 2, nsteps = m - 1;
+    double* prm = reinterpret_cast<double*>(csm);  // [2][4 * npairs]
+    double2* wbase = csm + 4 * (size_t)npairs + (size_t)wib * 8 * n;
+    double2* sA = wbase;
+    double2* sV = wbase + 2 * n;
+    double2* stg = wbase + 4 * n;  // [2][2n]
+    const bool active = gw < npairs;
+    const int r0 = 2 * gw, r1 = 2 * gw + 1;
+    // total |A|^2
+    double tot = 0.0;
+    const size_t nn = (size_t)n * n;
+    for (size_t t = crank * (size_t)blockDim.x + threadIdx.x; t < nn;
+         t += (size_t)cluster.num_blocks() * blockDim.x)
+        tot += A[t].x * A[t].x + A[t].y * A[t].y;
+    tot = block_sum(tot, red);
+    if (threadIdx.x == 0) atomicAdd(&scratch[0], tot);
+    int p = 0, q = 0;
+    if (active) {
+        jac_pair(m, 0, gw, p, q);
+        for (int k = lane; k < n; k += 32) {
+            sA[k] = A[(size_t)p * n + k];
+            sA[n + k] = q < n ? A[(size_t)q * n + k] : make_double2(0.0, 0.0);
+            sV[k] = make_double2(k == r0 ? 1.0 : 0.0, 0.0);
+            sV[n + k] = make_double2(k == r1 ? 1.0 : 0.0, 0.0);
+        }
+    }
+    __threadfence();
+    cluster.sync();
+    const double total = *(volatile double*)&scratch[0];
+    int sweep = 0;
+    bool converged = false;
+    for (; sweep < max_sweeps && !converged; ++sweep) {
+        for (int s = 0; s < nsteps; ++s) {
+            const int par = s & 1;
+            const int s2 = (s + 1) % nsteps;
+            // ---- phase 1: rotate this warp's pair, send X rows to their next owners
+            if (active) {
+                jac_pair(m, s, gw, p, q);
+                double c = 1.0, sn = 0.0, phr = 1.0, phi = 0.0;
+                if (q < n) {
+                    const double2 apq = sA[q];
+                    const double app = sA[p].x, aqq = sA[n + q].x;
+                    const double bm = hypot(apq.x, apq.y);
+                    if (bm > 1e-300 && bm > 1e-18 * sqrt(fabs(app * aqq))) {
+                        phr = apq.x / bm;
+                        phi = apq.y / bm;
+                        const double tau = (aqq - app) / (2.0 * bm);
+                        const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+                        c = 1.0 / sqrt(1.0 + t * t);
+                        sn = t * c;
+                    }
+                }
+                // destinations: the owners of rows p and q at step s + 1
+                double2* dst[2] = {nullptr, nullptr};
+                const int rows[2] = {p, q};
+                for (int h = 0; h < 2; ++h) {
+                    const int r = rows[h];
+                    if (r >= n) continue;
+                    int pi, partner;
+                    jac_partner(m, s2, r, pi, partner);
+                    const int owner_rank = pi / wpb, owner_w = pi % wpb;
+                    const int slot = r < partner ? 0 : 1;
+                    double2* local = csm + 4 * (size_t)npairs + (size_t)owner_w * 8 * n + 4 * n +
+                                     (size_t)par * 2 * n + (size_t)slot * n;
+                    dst[h] = cluster.map_shared_rank(local, owner_rank);
+                }
+                for (int k = lane; k < n; k += 32) {
+                    const double2 apk = sA[k];
+                    if (q < n) {
+                        const double2 aqk = sA[n + k];
+                        const double2 pa = make_double2(phr * aqk.x - phi * aqk.y, phr * aqk.y + phi * aqk.x);
+                        dst[0][k] = make_double2(c * apk.x - sn * pa.x, c * apk.y - sn * pa.y);
+                        dst[1][k] = make_double2(sn * apk.x + c * pa.x, sn * apk.y + c * pa.y);
+                    } else {
+                        dst[0][k] = apk;
+                    }
+                }
+                // broadcast the rotation to every block of the cluster
+                for (int b = lane; b < (int)cluster.num_blocks(); b += 32) {
+                    double* rp = cluster.map_shared_rank(prm + (size_t)par * 4 * npairs + 4 * gw, b);
+                    rp[0] = c; rp[1] = sn; rp[2] = phr; rp[3] = phi;
+                }
+            }
+            cluster.sync();
+            // ---- phase 2: rows of the next pair, A[r] = X[r] G(s); V <- V G(s)
+            if (active) {
+                const double* rs = prm + (size_t)par * 4 * npairs;
+                const double2* sT = stg + (size_t)par * 2 * n;
+                int p2, q2;
+                jac_pair(m, s2, gw, p2, q2);
+                auto mix = [&](const double2* src, int k) -> double2 {
+                    int pi, partner;
+                    jac_partner(m, s, k, pi, partner);
+                    const double2 xk = src[k];
+                    if (partner >= n) return xk;
+                    const double c = rs[4 * pi + 0], sn = rs[4 * pi + 1];
+                    const double phr = rs[4 * pi + 2], phi = rs[4 * pi + 3];
+                    const double2 xp = src[partner];
+                    if (k < partner) {
+                        const double2 qc = make_double2(phr * xp.x + phi * xp.y, phr * xp.y - phi * xp.x);
+                        return make_double2(c * xk.x - sn * qc.x, c * xk.y - sn * qc.y);
+                    }
+                    const double2 qc = make_double2(phr * xk.x + phi * xk.y, phr * xk.y - phi * xk.x);
+                    return make_double2(sn * xp.x + c * qc.x, sn * xp.y + c * qc.y);
+                };
+                for (int k = lane; k < n; k += 32) {
+                    sA[k] = mix(sT, k);
+                    if (q2 < n) sA[n + k] = mix(sT + n, k);
+                }
+                // V rows in place through registers (n <= 32 * kJacClusterMaxPerLane)
+                double2 v0[kJacClusterMaxPerLane], v1[kJacClusterMaxPerLane];
+#pragma unroll
+                for (int j = 0; j < kJacClusterMaxPerLane; ++j) {
+                    const int k = lane + 32 * j;
+                    if (k < n) {
+                        v0[j] = mix(sV, k);
+                        v1[j] = mix(sV + n, k);
+                    }
+                }
+                __syncwarp();
+#pragma unroll
+                for (int j = 0; j < kJacClusterMaxPerLane; ++j) {
+                    const int k = lane + 32 * j;
+                    if (k < n) {
+                        if (r0 < n) sV[k] = v0[j];
+                        if (r1 < n) sV[n + k] = v1[j];
+                    }
+                }
+                __syncwarp();
+            }
+        }
+        double off = 0.0;
+        if (active) {
+            jac_pair(m, 0, gw, p, q);
+            for (int k = lane; k < n; k += 32) {
+                if (k != p) off += sA[k].x * sA[k].x + sA[k].y * sA[k].y;
+                if (q < n && k != q) off += sA[n + k].x * sA[n + k].x + sA[n + k].y * sA[n + k].y;
+            }
+        }
+        off = block_sum(off, red);
+        if (threadIdx.x == 0) atomicAdd(&scratch[1 + sweep], off);
+        __threadfence();
+        cluster.sync();
+        converged = *(volatile double*)&scratch[1 + sweep] <= tol2 * total;
+    }
+    if (active) {
+        jac_pair(m, 0, gw, p, q);
+        for (int k = lane; k < n; k += 32) {
+            A[(size_t)p * n + k] = sA[k];
+            if (q < n) A[(size_t)q * n + k] = sA[n + k];
+            if (r0 < n) V[(size_t)r0 * n + k] = sV[k];
+            if (r1 < n) V[(size_t)r1 * n + k] = sV[n + k];
+        }
+    }
+    if (crank == 0 && threadIdx.x == 0) *sweeps_out = converged ? sweep : max_sweeps;
+    // no block may leave while others can still write into its shared memory
+    cluster.sync();
+}
+
 // Sort eigenvalues ascending (stable by index) and permute eigenvector columns.
 __global__ void __launch_bounds__(1024)
 k_sort_eig(const double2* __restrict__ A, const double2* __restrict__ V, int n,
@@ -804,6 +990,36 @@ cudaError_t jacobi(double2* A, double2* V, int n, int max_sweeps, double tol2, d
     double* rot = scratch + 1 + max_sweeps;
     double2* X = (double2*)(rot + 8 * (size_t)(npairs + 1));
     if (((uintptr_t)X) & 15) X = (double2*)(((uintptr_t)X + 15) & ~(uintptr_t)15);
+    // one thread-block cluster when its shared memory holds every pair's rows
+    if (n <= 32 * kJacClusterMaxPerLane) {
+        const int wpb = std::max(1, std::min(8, (npairs + 15) / 16));
+        const int nc = (npairs + wpb - 1) / wpb;
+        const size_t smc = (size_t)npairs * 8 * sizeof(double) + (size_t)wpb * 8 * n * sizeof(double2);
+        if (nc <= 16 && smc <= 200 * 1024) {
+            cudaFuncSetAttribute(k_jacobi_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smc);
+            if (nc > 8) cudaFuncSetAttribute(k_jacobi_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+            cudaLaunchConfig_t lc = {};
+            lc.gridDim = dim3(nc);
+            lc.blockDim = dim3(32 * wpb);
+            lc.dynamicSmemBytes = smc;
+            lc.stream = st;
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = nc;
+            at[0].val.clusterDim.y = 1;
+            at[0].val.clusterDim.z = 1;
+            lc.attrs = at;
+            lc.numAttrs = 1;
+            int clusters = 0;
+            if (cudaOccupancyMaxActiveClusters(&clusters, k_jacobi_cluster, &lc) == cudaSuccess &&
+                clusters >= 1) {
+                cudaError_t e = cudaLaunchKernelEx(&lc, k_jacobi_cluster, A, V, n, max_sweeps, tol2,
+                                                   scratch, sweeps_out);
+                if (e == cudaSuccess) return e;
+            }
+            cudaGetLastError();  // clear a refused configuration; fall through
+        }
+    }
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
