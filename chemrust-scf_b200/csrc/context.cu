@@ -2302,6 +2302,7 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
     if (s) return s;
     if (learned && (s = alloc_mix(ctx))) return s;
     MixRing ring;
+    bool prev_fp64 = false;  // the previous SCF iteration ran in FP64
     bool have_prev = false, fell_back = false;
     int rises = 0;
     double r_prev = -1.0;
@@ -2427,11 +2428,14 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
         // run only converges on FP64 iterations (the final filter passes are FP64)
         const double de = it > 1 ? std::fabs(etot - e_prev) / ctx->n_atoms : 1e300;
         if (ctx->mixed_active) ++r->n_iter_mixed;
-        if (de < p->tol_per_atom && !ctx->mixed_active) {
+        // convergence needs two FP64 iterations in a row: the change from the
+        // last mixed-precision iteration does not count
+        if (de < p->tol_per_atom && !ctx->mixed_active && prev_fp64) {
             status = CHFSI_OK;
             e_prev = etot;
             break;
         }
+        prev_fp64 = !ctx->mixed_active;
         if (ctx->mixed_active && (de < p->fp64_switch_per_atom || de < p->tol_per_atom))
             ctx->mixed_active = false;
         e_prev = etot;

@@ -77,20 +77,17 @@ __global__ void __launch_bounds__(1024) k_cholesky(double2* A, int n, int* info)
             a = make_double2(a.x * inv, a.y * inv);
         }
         __syncthreads();
-        // trailing update of the lower triangle: A[i][k] -= L[i][j] conj(L[k][j]), j < k <= i
-        const int m = n - j - 1;
-        const size_t tri = (size_t)m * (m + 1) / 2;
-        for (size_t t = threadIdx.x; t < tri; t += blockDim.x) {
-            // map t -> (ii, kk) with 0 <= kk <= ii < m
-            int ii = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
-            while ((size_t)(ii + 1) * (ii + 2) / 2 <= t) ++ii;
-            while ((size_t)ii * (ii + 1) / 2 > t) --ii;
-            const int kk = (int)(t - (size_t)ii * (ii + 1) / 2);
-            const int i = j + 1 + ii, k = j + 1 + kk;
-            const double2 lij = A[(size_t)i * n + j], lkj = A[(size_t)k * n + j];
-            double2& a = A[(size_t)i * n + k];
-            a.x -= lij.x * lkj.x + lij.y * lkj.y;
-            a.y -= lij.y * lkj.x - lij.x * lkj.y;
+        // trailing update of the lower triangle: A[i][k] -= L[i][j] conj(L[k][j]),
+        // j < k <= i; one warp per row, lanes along the row
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+        for (int i = j + 1 + warp; i < n; i += nw) {
+            const double2 lij = A[(size_t)i * n + j];
+            for (int k = j + 1 + lane; k <= i; k += 32) {
+                const double2 lkj = A[(size_t)k * n + j];
+                double2& a = A[(size_t)i * n + k];
+                a.x -= lij.x * lkj.x + lij.y * lkj.y;
+                a.y -= lij.y * lkj.x - lij.x * lkj.y;
+            }
         }
         __syncthreads();
     }
@@ -103,6 +100,39 @@ __global__ void __launch_bounds__(1024) k_cholesky(double2* A, int n, int* info)
 }
 
 // X = L^-1 by forward substitution, one column per thread.
+// X = L^-1 by forward substitution, one warp per column c: row i of the
+// column needs sum_{c <= k < i} L[i][k] X[k][c] (lanes along k, the column
+// kept in shared memory), then X[i][c] = (delta_ic - sum) / L[i][i].
+__global__ void __launch_bounds__(256)
+k_tri_inv_w(const double2* __restrict__ L, double2* __restrict__ X, int n) {
+    extern __shared__ double2 tri_cols[];  // 8 warps x n
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int c = blockIdx.x * 8 + wib;
+    if (c >= n) return;  // whole warps only; no block barrier below
+    double2* xc = tri_cols + (size_t)wib * n;
+    for (int i = lane; i < c; i += 32) X[(size_t)i * n + c] = make_double2(0.0, 0.0);
+    for (int i = c; i < n; ++i) {
+        const double2* Li = L + (size_t)i * n;
+        double sr = 0.0, si = 0.0;
+        for (int k = c + lane; k < i; k += 32) {
+            const double2 l = Li[k], x = xc[k];
+            sr += l.x * x.x - l.y * x.y;
+            si += l.x * x.y + l.y * x.x;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            sr += __shfl_xor_sync(0xffffffffu, sr, o);
+            si += __shfl_xor_sync(0xffffffffu, si, o);
+        }
+        const double d = Li[i].x;  // real diagonal
+        const double2 v = make_double2(((i == c ? 1.0 : 0.0) - sr) / d, -si / d);
+        if (lane == 0) {
+            xc[i] = v;
+            X[(size_t)i * n + c] = v;
+        }
+        __syncwarp();
+    }
+}
+
 __global__ void k_tri_inv(const double2* __restrict__ L, double2* __restrict__ X, int n) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= n) return;
@@ -967,7 +997,14 @@ void cholesky(double2* A, int n, int* info, cudaStream_t st) {
 }
 void tri_inv(const double2* L, double2* X, int n, cudaStream_t st) {
     count_launch();
-    k_tri_inv<<<(n + 63) / 64, 64, 0, st>>>(L, X, n);
+    const size_t sm = (size_t)8 * n * sizeof(double2);
+    if (sm <= 200 * 1024) {
+        if (sm > 48 * 1024)
+            cudaFuncSetAttribute(k_tri_inv_w, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_tri_inv_w<<<(n + 7) / 8, 256, sm, st>>>(L, X, n);
+    } else {
+        k_tri_inv<<<(n + 63) / 64, 64, 0, st>>>(L, X, n);
+    }
 }
 void small_gemm(int opa, int opb, const double2* A, const double2* B, double2* C, int n,
                 cudaStream_t st) {

@@ -291,7 +291,7 @@ typedef struct chfsi_scf_params {
     double kT;            /* Fermi-Dirac smearing (Ha); <= 0: fixed aufbau occupations */
     double fp64_switch_per_atom; /* mixed precision: switch the filter to FP64 once
                                     |dE|/atom < this (convergence is only declared on
-                                    FP64 steps)                                        */
+                                    the second of two FP64 steps in a row)            */
     int    mixer;         /* CHFSI_MIXER_PULAY / _LEARNED / _LEARNED_PULAY            */
     int    cg_steps;      /* band-CG steps per band after each filter (0: none)      */
     double* trace;        /* optional host buffer of 2 * max_iter * N^3 doubles: rho_in
