@@ -10,8 +10,9 @@
 //                    (W: K x M, X: K x N, N-contiguous; short K)
 //                    -> beta (D beta^H psi), psi V
 //
-// B200 FP64 has no tcgen05 kind; both run on the FP64 pipes with 4x4
-// complex register tiles per thread (64 FMA per 8 shared-memory loads).
+// B200 FP64 has no tcgen05 kind; both run on the FP64 tensor path
+// (mma.sync m8n8k4 .f64), the SIMT versions with 4x4 complex register tiles
+// per thread remain as the reference implementation of the same contract.
 #include "gemm.hpp"
 #include "launch_count.hpp"
 
@@ -97,6 +98,177 @@ k_gemm_cn_splitk(const double2* __restrict__ A, int lda, const double2* __restri
             const int n = n0 + tx + 16 * j;
             if (n < N) pp[(size_t)m * N + n] = acc[i][j];
         }
+    }
+}
+
+// ---- FP64 tensor-core (DMMA) versions: mma.sync m8n8k4 .f64, one warp
+// issues 256 FMAs per instruction.  Complex products as four real MMAs on
+// split (re, im) shared-memory planes.  Fragments (PTX m8n8k4 .f64): A row
+// (lane >> 2), col (lane & 3); B row (lane & 3), col (lane >> 2); C row
+// (lane >> 2), cols 2 (lane & 3) + {0, 1}.  CTA tile 64 x 64, 8 warps as
+// 2 (M) x 4 (N), warp tile 32 x 16 = 4 x 2 MMA tiles.
+__device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
+}
+
+constexpr int kDS = BK + 4;  // row stride (doubles) of K-contiguous planes
+constexpr int kDT = BM + 4;  // row stride (doubles) of M/N-contiguous planes
+
+// P[s][m][n] = sum_{k in chunk s} conj(A[m][k]) B[n][k]
+__global__ void __launch_bounds__(256, 2)
+k_zgemm_cn_dmma(const double2* __restrict__ A, int lda, const double2* __restrict__ B, int ldb,
+                int M, int N, int K, int kchunk, double2* __restrict__ part) {
+    __shared__ double Ar[BM][kDS], Ai[BM][kDS], Br[BN][kDS], Bi[BN][kDS];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int gid = lane >> 2, tig = lane & 3;
+    const int wm = warp & 1, wn = warp >> 1;
+    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    const int kb = blockIdx.z * kchunk;
+    const int ke = min(K, kb + kchunk);
+    double cr[4][2][2], ci[4][2][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) cr[i][j][0] = cr[i][j][1] = ci[i][j][0] = ci[i][j][1] = 0.0;
+    const int lr = threadIdx.x >> 2, lk = (threadIdx.x & 3) * 4;
+    const int am = m0 + lr, bn_ = n0 + lr;
+    const double2* ap = A + (size_t)am * lda;
+    const double2* bp = B + (size_t)bn_ * ldb;
+    double2 ra[4], rb[4];
+    auto fetch = [&](int k0) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int k = k0 + lk + i;
+            ra[i] = (am < M && k < ke) ? ap[k] : make_double2(0.0, 0.0);
+            rb[i] = (bn_ < N && k < ke) ? bp[k] : make_double2(0.0, 0.0);
+        }
+    };
+    if (kb < ke) fetch(kb);
+    for (int k0 = kb; k0 < ke; k0 += BK) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            Ar[lr][lk + i] = ra[i].x; Ai[lr][lk + i] = ra[i].y;
+            Br[lr][lk + i] = rb[i].x; Bi[lr][lk + i] = rb[i].y;
+        }
+        __syncthreads();
+        if (k0 + BK < ke) fetch(k0 + BK);
+#pragma unroll
+        for (int kk = 0; kk < BK; kk += 4) {
+            double br[2], bi[2];
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                const int n = wn * 16 + j * 8 + gid;
+                br[j] = Br[n][kk + tig];
+                bi[j] = Bi[n][kk + tig];
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int m = wm * 32 + i * 8 + gid;
+                const double ar = Ar[m][kk + tig], ai = Ai[m][kk + tig];
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    dmma(cr[i][j], ar, br[j]);
+                    dmma(cr[i][j], ai, bi[j]);
+                    dmma(ci[i][j], ar, bi[j]);
+                    dmma(ci[i][j], -ai, br[j]);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    double2* pp = part + (size_t)blockIdx.z * M * N;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int m = m0 + wm * 32 + i * 8 + gid;
+        if (m >= M) continue;
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const int n = n0 + wn * 16 + j * 8 + 2 * tig + e;
+                if (n < N) pp[(size_t)m * N + n] = make_double2(cr[i][j][e], ci[i][j][e]);
+            }
+    }
+}
+
+// O[m][n] = alpha sum_k W[k][m] X[k][n] + beta O[m][n]
+__global__ void __launch_bounds__(256, 2)
+k_zgemm_tn_dmma(const double2* __restrict__ W, int ldw, const double2* __restrict__ X, int ldx,
+                double2* O, int ldo, int M, int N, int K, double alpha, double beta) {
+    __shared__ double Wr[BK][kDT], Wi[BK][kDT], Xr[BK][kDT], Xi[BK][kDT];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int gid = lane >> 2, tig = lane & 3;
+    const int wm = warp & 1, wn = warp >> 1;
+    const int n0 = blockIdx.x * BN, m0 = blockIdx.y * BM;
+    double cr[4][2][2], ci[4][2][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) cr[i][j][0] = cr[i][j][1] = ci[i][j][0] = ci[i][j][1] = 0.0;
+    const int lk = threadIdx.x >> 4, lc = (threadIdx.x & 15) * 4;
+    double2 rw[4], rx[4];
+    auto fetch = [&](int k0) {
+        const int k = k0 + lk;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int m = m0 + lc + i, n = n0 + lc + i;
+            rw[i] = (k < K && m < M) ? W[(size_t)k * ldw + m] : make_double2(0.0, 0.0);
+            rx[i] = (k < K && n < N) ? X[(size_t)k * ldx + n] : make_double2(0.0, 0.0);
+        }
+    };
+    fetch(0);
+    for (int k0 = 0; k0 < K; k0 += BK) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            Wr[lk][lc + i] = rw[i].x; Wi[lk][lc + i] = rw[i].y;
+            Xr[lk][lc + i] = rx[i].x; Xi[lk][lc + i] = rx[i].y;
+        }
+        __syncthreads();
+        if (k0 + BK < K) fetch(k0 + BK);
+#pragma unroll
+        for (int kk = 0; kk < BK; kk += 4) {
+            double xr[2], xi[2];
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                const int n = wn * 16 + j * 8 + gid;
+                xr[j] = Xr[kk + tig][n];
+                xi[j] = Xi[kk + tig][n];
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int m = wm * 32 + i * 8 + gid;
+                const double wr = Wr[kk + tig][m], wi = Wi[kk + tig][m];
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    dmma(cr[i][j], wr, xr[j]);
+                    dmma(cr[i][j], -wi, xi[j]);
+                    dmma(ci[i][j], wr, xi[j]);
+                    dmma(ci[i][j], wi, xr[j]);
+                }
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int m = m0 + wm * 32 + i * 8 + gid;
+        if (m >= M) continue;
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const int n = n0 + wn * 16 + j * 8 + 2 * tig + e;
+                if (n >= N) continue;
+                double2* o = O + (size_t)m * ldo + n;
+                double2 r = make_double2(alpha * cr[i][j][e], alpha * ci[i][j][e]);
+                if (beta != 0.0) {
+                    r.x += beta * o->x;
+                    r.y += beta * o->y;
+                }
+                *o = r;
+            }
     }
 }
 
@@ -203,7 +375,7 @@ void gemm_cn(const double2* A, int lda, const double2* B, int ldb, int M, int N,
     kchunk = (kchunk + BK - 1) / BK * BK;
     const int used = (K + kchunk - 1) / kchunk;
     dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN, used);
-    k_gemm_cn_splitk<<<grid, 256, 0, st>>>(A, lda, B, ldb, M, N, K, kchunk, part);
+    k_zgemm_cn_dmma<<<grid, 256, 0, st>>>(A, lda, B, ldb, M, N, K, kchunk, part);
     const size_t mn = (size_t)M * N;
     int blocks = (int)((mn + 255) / 256);
     if (blocks > 148 * 8) blocks = 148 * 8;
@@ -214,7 +386,7 @@ void gemm_tn(const double2* W, int ldw, const double2* X, int ldx, double2* O, i
              int N, int K, double alpha, double beta, cudaStream_t st) {
     count_launch();
     dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
-    k_gemm_tn<<<grid, 256, 0, st>>>(W, ldw, X, ldx, O, ldo, M, N, K, alpha, beta);
+    k_zgemm_tn_dmma<<<grid, 256, 0, st>>>(W, ldw, X, ldx, O, ldo, M, N, K, alpha, beta);
 }
 
 }  // namespace chfsi
@@ -233,7 +405,7 @@ void gemm_cn_capped(const double2* A, int lda, const double2* B, int ldb, int M,
     kchunk = (kchunk + BK - 1) / BK * BK;
     const int used = (K + kchunk - 1) / kchunk;
     dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN, used);
-    k_gemm_cn_splitk<<<grid, 256, 0, st>>>(A, lda, B, ldb, M, N, K, kchunk, part);
+    k_zgemm_cn_dmma<<<grid, 256, 0, st>>>(A, lda, B, ldb, M, N, K, kchunk, part);
     const size_t mn = (size_t)M * N;
     int blocks = (int)((mn + 255) / 256);
     if (blocks > 148 * 8) blocks = 148 * 8;
