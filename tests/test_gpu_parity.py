@@ -187,3 +187,23 @@ def test_norm_guard_reports_divergence(chfsi, sys0):
     ctx.set_veff(ctx.get_vloc())
     with pytest.raises(chfsi.ChebyshevDiverged):
         ctx.chebyshev_filter(6, eigenvalues=np.linspace(0.0, 1e4, sys0.n_bands))
+
+
+@pytest.mark.parametrize("n_bands,z_val", [(1, 0.25), (21, 4.0), (261, 4.0)])
+def test_diagonalize_band_count_edges(chfsi, oracle, n_bands, z_val):
+    """Band counts that exercise the eigensolver's edge paths: one band, an
+    odd count (the round-robin Jacobi pads with a phantom index) and a count
+    above 256 (the grid-wide Jacobi instead of the cluster one), against the
+    oracle on the 8-atom cell."""
+    s = chfsi.SyntheticSystem(config_index=0, n_bands=n_bands, z_val=z_val)
+    assert s.n_bands == n_bands
+    ctx = chfsi.Context(s)
+    o = oracle.Oracle.from_system(s)
+    v = o.vloc_r()
+    ctx.set_veff(v)
+    o.set_veff(v)
+    wg = wc = None
+    for _ in range(1 if n_bands > 256 else 2):  # the oracle's 261-band pass takes ~20 s
+        wg = ctx.diagonalize(12, wg)
+        wc = o.diagonalize(12, wc)
+    np.testing.assert_allclose(wg, wc, atol=1e-9, rtol=0)
