@@ -228,7 +228,7 @@ def run_ours(args):
            "d2h_bytes_per_step": psi_bytes + 8 * nb,
            "api": "chfsi_set_psi + chfsi_diagonalize + chfsi_get_psi (pinned host buffers)"}
 
-    # ---- mixed precision: FP32 filter, tcgen05 BF16x3 GEMMs, FP64 RR eigensolve
+    # ---- mixed precision: FP32 filter (tcgen05 BF16x3 projector GEMMs), FP64 Rayleigh-Ritz
     mixed = None
     if not args.fp64_only:
         mctx = chfsi.Context(s, device=local, precision=chfsi.PREC_MIXED)
@@ -253,7 +253,7 @@ def run_ours(args):
             mms = float(t.item())
         mixed = {"value": round(applies_per_step * args.steps * world / (mms * 1e-3), 1),
                  "unit": UNIT, "ms_per_step": round(mms / args.steps, 3),
-                 "dtype": "f32 filter, bf16x3 tcgen05 GEMMs (fp32 accumulate), f64 eigensolve"}
+                 "dtype": "f32 filter (bf16x3 tcgen05 projector GEMMs, fp32 accumulate), f64 Rayleigh-Ritz"}
         mctx.close()
         if not args.no_scf:
             import learned_mixer

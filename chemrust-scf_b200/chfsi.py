@@ -662,9 +662,9 @@ class Context:
         return out
 
     def autotune(self):
-        """Time the local H|psi> launch configurations; returns (choice, 9 timings)."""
+        """Time the local H|psi> launch configurations; returns (choice, 18 timings)."""
         ch = C.c_int()
-        t = np.zeros(9, dtype=np.float32)
+        t = np.zeros(18, dtype=np.float32)
         self._c(lib().chfsi_autotune(self.handle, C.byref(ch), _ptr(t, C.c_float)))
         return ch.value, t
 

@@ -97,31 +97,6 @@ __global__ void k_f32_to_f64(const float2* __restrict__ a, double2* __restrict__
          i += (size_t)gridDim.x * blockDim.x)
         b[i] = make_double2((double)a[i].x, (double)a[i].y);
 }
-// Scale band b of x and y (FP32, band-major, n per band) by 1 / |x_b| (one
-// block per band; the norm is accumulated in FP64).
-__global__ void __launch_bounds__(256)
-k_normalize_bands32(float2* __restrict__ x, float2* __restrict__ y, int n) {
-    __shared__ double red[8];
-    __shared__ float inv;
-    float2* xb = x + (size_t)blockIdx.x * n;
-    float2* yb = y + (size_t)blockIdx.x * n;
-    double s = 0.0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) s += (double)xb[i].x * xb[i].x + (double)xb[i].y * xb[i].y;
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double t = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
-        inv = t > 0.0 ? (float)(1.0 / sqrt(t)) : 1.f;
-    }
-    __syncthreads();
-    const float f = inv;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        xb[i].x *= f; xb[i].y *= f;
-        yb[i].x *= f; yb[i].y *= f;
-    }
-}
 
 __global__ void __launch_bounds__(256) k_sumsq32(const float2* __restrict__ x, size_t n, double* acc) {
     __shared__ double red[8];
@@ -413,7 +388,7 @@ struct chfsi_ctx {
     float2* d_psi32a = nullptr; float2* d_psi32b = nullptr; float2* d_psi32 = nullptr;
     float2* d_hpsi32 = nullptr; float2* d_nl32 = nullptr; float2* d_work32 = nullptr;
     void* d_planes = nullptr;    // all bf16 plane storage
-    TcPlanes tp_beta_a, tp_betaT_b, tp_psi_b, tp_psi_a, tp_hpsi_b, tp_small_a, tp_psiT_b;
+    TcPlanes tp_beta_a, tp_betaT_b, tp_psi_b, tp_small_a;
     float* d_tc_part = nullptr; int* d_tc_err = nullptr;
     bool beta_planes_ready = false;
     bool last_pass_fp32 = false;  // the last filter ran in FP32
@@ -604,22 +579,38 @@ chfsi_status filter_dev(chfsi_ctx* ctx, int ndeg, const double* eig_dev, int n_e
 }
 
 // ---------------------------------------------------------------- Rayleigh-Ritz
-chfsi_status rr_dev(chfsi_ctx* ctx) {
-    const int n = ctx->nb;
+// fp32_block: the block comes from the FP32 filter, whose d_hpsi holds the
+// local part only; the non-local part enters the subspace matrix as C^H D C
+// (C = beta^H psi, shared with the ultrasoft overlap), which is how the
+// mixed-precision passes run their FP64 Rayleigh-Ritz.
+chfsi_status rr_dev(chfsi_ctx* ctx, bool fp32_block) {
+    const int n = ctx->nb, np = ctx->np;
     cudaStream_t st = ctx->st;
-    gemm_cn(ctx->d_psi, ctx->n_pw, ctx->d_hpsi, ctx->n_pw, n, n, ctx->n_pw, ctx->d_part, ctx->d_T1, st);
-    symmetrize(ctx->d_T1, ctx->d_H, n, st);
-    gemm_cn(ctx->d_psi, ctx->n_pw, ctx->d_psi, ctx->n_pw, n, n, ctx->n_pw, ctx->d_part, ctx->d_T1, st);
-    if (ctx->uspp) {
-        // S_sub = psi^H psi + C^H q C with C = beta^H psi
-        gemm_cn(ctx->d_beta, ctx->n_pw, ctx->d_psi, ctx->n_pw, ctx->np, n, ctx->n_pw, ctx->d_part,
+    const bool nl_sub = fp32_block && np > 0;
+    const bool aug_s = ctx->uspp && np > 0;
+    if (nl_sub || aug_s) {
+        // C = beta^H psi and its conjugate
+        gemm_cn(ctx->d_beta, ctx->n_pw, ctx->d_psi, ctx->n_pw, np, n, ctx->n_pw, ctx->d_part,
                 ctx->d_cp, st);
         count_launch();
-        k_apply_dmat<<<grid_for((size_t)ctx->np * n), 256, 0, st>>>(
-            ctx->d_cp, ctx->d_cd, ctx->np, n, ctx->d_proj_ion, ctx->d_poff, ctx->d_doff, ctx->d_qmat);
+        k_conj<<<grid_for((size_t)np * n), 256, 0, st>>>(ctx->d_cp, ctx->d_cq, (size_t)np * n);
+    }
+    gemm_cn(ctx->d_psi, ctx->n_pw, ctx->d_hpsi, ctx->n_pw, n, n, ctx->n_pw, ctx->d_part, ctx->d_T1, st);
+    if (nl_sub) {
+        // H_sub += C^H D C
         count_launch();
-        k_conj<<<grid_for((size_t)ctx->np * n), 256, 0, st>>>(ctx->d_cp, ctx->d_cq, (size_t)ctx->np * n);
-        gemm_tn(ctx->d_cq, n, ctx->d_cd, n, ctx->d_T1, n, n, n, ctx->np, 1.0, 1.0, st);
+        k_apply_dmat<<<grid_for((size_t)np * n), 256, 0, st>>>(
+            ctx->d_cp, ctx->d_cd, np, n, ctx->d_proj_ion, ctx->d_poff, ctx->d_doff, ctx->d_dmat);
+        gemm_tn(ctx->d_cq, n, ctx->d_cd, n, ctx->d_T1, n, n, n, np, 1.0, 1.0, st);
+    }
+    symmetrize(ctx->d_T1, ctx->d_H, n, st);
+    gemm_cn(ctx->d_psi, ctx->n_pw, ctx->d_psi, ctx->n_pw, n, n, ctx->n_pw, ctx->d_part, ctx->d_T1, st);
+    if (aug_s) {
+        // S_sub = psi^H psi + C^H q C
+        count_launch();
+        k_apply_dmat<<<grid_for((size_t)np * n), 256, 0, st>>>(
+            ctx->d_cp, ctx->d_cd, np, n, ctx->d_proj_ion, ctx->d_poff, ctx->d_doff, ctx->d_qmat);
+        gemm_tn(ctx->d_cq, n, ctx->d_cd, n, ctx->d_T1, n, n, n, np, 1.0, 1.0, st);
     }
     symmetrize(ctx->d_T1, ctx->d_S, n, st);
     cholesky(ctx->d_S, n, ctx->d_flags + 0, st);                   // S -> L
@@ -631,15 +622,26 @@ chfsi_status rr_dev(chfsi_ctx* ctx) {
     sort_eig(ctx->d_T2, ctx->d_V, n, ctx->d_eig, ctx->d_H, st);     // H = U (sorted)
     small_gemm(1, 0, ctx->d_T1, ctx->d_H, ctx->d_T2, n, st);        // T2 = Li^H U
     gemm_tn(ctx->d_T2, n, ctx->d_psi, ctx->n_pw, ctx->d_psi2, ctx->n_pw, n, ctx->n_pw, n, 1.0, 0.0, st);
-    std::swap(ctx->d_psi, ctx->d_psi2);
+    if (fp32_block) {
+        // copy back instead of swapping the pointers: a mixed pass captured
+        // into a CUDA graph (chfsi_batch_capture) replays on fixed buffers
+        CK(cudaMemcpyAsync(ctx->d_psi, ctx->d_psi2, sizeof(double2) * (size_t)n * ctx->n_pw,
+                           cudaMemcpyDeviceToDevice, st));
+    } else {
+        std::swap(ctx->d_psi, ctx->d_psi2);
+    }
     CK(cudaGetLastError());
     return CHFSI_OK;
 }
 
 // ---------------------------------------------------------------- mixed precision
 // FP32 filter with the projector GEMMs on tcgen05 (BF16 3-way split, FP32
-// accumulation in TMEM); Rayleigh-Ritz overlap / subspace matrices and the
-// psi V rotation on tcgen05, Cholesky and eigensolve in FP64.
+// accumulation in TMEM); the Rayleigh-Ritz of the filtered block runs in
+// FP64 (rr_dev with the non-local part as C^H D C).  Long-K sums accumulated
+// in the tensor core's FP32 accumulator drift low (the diagonal of psi^H psi
+// over n_pw terms loses ~1e-4 relative at n_pw ~ 1.7e5), which in an FP32
+// overlap shows up as a charge excess of ~0.1 electron and a total-energy
+// bias of ~1e-4 Ha/atom; the filter itself tolerates such errors.
 
 chfsi_status alloc_mixed(chfsi_ctx* ctx, int ncol) {
     const int nb = ctx->nb, np = ctx->np, npw = ctx->n_pw;
@@ -653,10 +655,7 @@ chfsi_status alloc_mixed(chfsi_ctx* ctx, int ncol) {
     const int kp_pw = tc_kpad(npw);
     std::vector<Spec> specs = {
         {&ctx->tp_psi_b, tc_rows_alloc(nb, false, nb), kp_pw},
-        {&ctx->tp_psi_a, tc_rows_alloc(2 * nb, true, 0), kp_pw},
-        {&ctx->tp_hpsi_b, tc_rows_alloc(nb, false, nb), kp_pw},
         {&ctx->tp_small_a, tc_rows_alloc(2 * nb, true, 0), std::max(tc_kpad(std::max(np, 1)), tc_kpad(nb))},
-        {&ctx->tp_psiT_b, tc_rows_alloc(npw, false, npw), tc_kpad(nb)},
     };
     if (np > 0) {
         specs.push_back({&ctx->tp_beta_a, tc_rows_alloc(2 * np, true, 0), kp_pw});
@@ -694,7 +693,7 @@ chfsi_status pack_beta_planes(chfsi_ctx* ctx) {
 }
 
 chfsi_status apply_h_dev32(chfsi_ctx* ctx, const float2* psi, float2* out, int nb, int mode,
-                           double* norm_acc) {
+                           double* norm_acc, bool local_only = false) {
     Epilogue e{};
     e.mode = mode;
     e.kin = ctx->d_kin;
@@ -703,7 +702,7 @@ chfsi_status apply_h_dev32(chfsi_ctx* ctx, const float2* psi, float2* out, int n
     e.norm_acc = norm_acc;
     e.inv_n = 1.0 / (double)ctx->ng;
     cudaStream_t st = ctx->st;
-    if (ctx->np > 0) {
+    if (ctx->np > 0 && !local_only) {
         // C = beta^H psi (tcgen05), C <- D C (FP64), nl = beta C (tcgen05, FP32 out)
         tc_pack<float2>(psi, ctx->n_pw, nb, ctx->n_pw, false, kSrcPlain, ctx->tp_psi_b, st);
         CK(tc_gemm(ctx->tp_beta_a, ctx->tp_psi_b, ctx->np, nb, ctx->n_pw, kTcOutPartial, ctx->d_cp,
@@ -776,60 +775,16 @@ chfsi_status filter_dev32(chfsi_ctx* ctx, int ndeg, const double* eig_dev, int n
     }
     float2* fin = ndeg >= 1 ? B : A;
     ctx->d_psi32 = fin;
-    s = apply_h_dev32(ctx, fin, ctx->d_hpsi32, ctx->nb, kEpiApply, nullptr);
+    // local H of the filtered block for the FP64 Rayleigh-Ritz (the non-local
+    // part enters its subspace matrix as C^H D C)
+    s = apply_h_dev32(ctx, fin, ctx->d_hpsi32, ctx->nb, kEpiApply, nullptr, true);
     if (s) return s;
-    // keep the FP64 master copy consistent with the filtered subspace
     count_launch();
     k_f32_to_f64<<<grid_for(n), 256, 0, st>>>(fin, ctx->d_psi, n);
+    count_launch();
+    k_f32_to_f64<<<grid_for(n), 256, 0, st>>>(ctx->d_hpsi32, ctx->d_hpsi, n);
     norm_guard(ctx->d_nsq, ndeg, ctx->d_flags + 1, st);
     ctx->last_ndeg = ndeg;
-    CK(cudaGetLastError());
-    return CHFSI_OK;
-}
-
-chfsi_status rr_dev32(chfsi_ctx* ctx) {
-    const int n = ctx->nb, npw = ctx->n_pw;
-    cudaStream_t st = ctx->st;
-    // unit-norm columns: the filter leaves band norms spread over orders of
-    // magnitude, and the FP32 / BF16x3 overlap of unscaled columns loses the
-    // weakly amplified top of the subspace; scaling changes neither the span
-    // nor the Ritz pairs
-    count_launch();
-    k_normalize_bands32<<<n, 256, 0, st>>>(ctx->d_psi32, ctx->d_hpsi32, npw);
-    const float2* psi = ctx->d_psi32;
-    tc_pack<float2>(psi, npw, n, npw, true, kSrcPlain, ctx->tp_psi_a, st);
-    tc_pack<float2>(psi, npw, n, npw, false, kSrcPlain, ctx->tp_psi_b, st);
-    tc_pack<float2>(ctx->d_hpsi32, npw, n, npw, false, kSrcPlain, ctx->tp_hpsi_b, st);
-    CK(tc_gemm(ctx->tp_psi_a, ctx->tp_hpsi_b, n, n, npw, kTcOutPartial, ctx->d_T1, n, ctx->d_tc_part,
-               ctx->d_tc_err, st));
-    symmetrize(ctx->d_T1, ctx->d_H, n, st);
-    CK(tc_gemm(ctx->tp_psi_a, ctx->tp_psi_b, n, n, npw, kTcOutPartial, ctx->d_T1, n, ctx->d_tc_part,
-               ctx->d_tc_err, st));
-    if (ctx->uspp) {
-        // S_sub += C^H q C, C = beta^H psi (tcgen05, FP64 out); the rest in FP64
-        CK(tc_gemm(ctx->tp_beta_a, ctx->tp_psi_b, ctx->np, n, npw, kTcOutPartial, ctx->d_cp, n,
-                   ctx->d_tc_part, ctx->d_tc_err, st));
-        count_launch();
-        k_apply_dmat<<<grid_for((size_t)ctx->np * n), 256, 0, st>>>(
-            ctx->d_cp, ctx->d_cd, ctx->np, n, ctx->d_proj_ion, ctx->d_poff, ctx->d_doff, ctx->d_qmat);
-        count_launch();
-        k_conj<<<grid_for((size_t)ctx->np * n), 256, 0, st>>>(ctx->d_cp, ctx->d_cq, (size_t)ctx->np * n);
-        gemm_tn(ctx->d_cq, n, ctx->d_cd, n, ctx->d_T1, n, n, n, ctx->np, 1.0, 1.0, st);
-    }
-    symmetrize(ctx->d_T1, ctx->d_S, n, st);
-    cholesky(ctx->d_S, n, ctx->d_flags + 0, st);
-    tri_inv(ctx->d_S, ctx->d_T1, n, st);
-    small_gemm(0, 0, ctx->d_T1, ctx->d_H, ctx->d_T2, n, st);
-    small_gemm(0, 1, ctx->d_T2, ctx->d_T1, ctx->d_H, n, st);
-    symmetrize(ctx->d_H, ctx->d_T2, n, st);
-    CK(jacobi(ctx->d_T2, ctx->d_V, n, ctx->jac_max_sweeps, 1e-26, ctx->d_jac, ctx->d_flags + 2, st));
-    sort_eig(ctx->d_T2, ctx->d_V, n, ctx->d_eig, ctx->d_H, st);
-    small_gemm(1, 0, ctx->d_T1, ctx->d_H, ctx->d_T2, n, st);  // Vf = Li^H U
-    // psi_new[i][g] = sum_j Vf[j][i] psi[j][g]  (tcgen05, FP64 output)
-    tc_pack<double2>(ctx->d_T2, n, n, n, true, kSrcConjT, ctx->tp_small_a, st);
-    tc_pack<float2>(psi, npw, npw, n, false, kSrcT, ctx->tp_psiT_b, st);
-    CK(tc_gemm(ctx->tp_small_a, ctx->tp_psiT_b, n, npw, n, kTcOutComplexF64, ctx->d_psi, npw, nullptr,
-               ctx->d_tc_err, st));
     CK(cudaGetLastError());
     return CHFSI_OK;
 }
@@ -846,12 +801,9 @@ chfsi_status filter_any(chfsi_ctx* ctx, int ndeg, const double* eig_dev, int n_e
 }
 
 chfsi_status rr_any(chfsi_ctx* ctx) {
-    if (ctx->mixed_active && ctx->d_psi32) {
-        chfsi_status s = rr_dev32(ctx);
-        ctx->d_psi32 = nullptr;
-        return s;
-    }
-    return rr_dev(ctx);
+    const bool fp32_block = ctx->mixed_active && ctx->d_psi32;
+    ctx->d_psi32 = nullptr;
+    return rr_dev(ctx, fp32_block);
 }
 
 // Read back eigenvalues, flags, bounds and norms; translate device flags into
@@ -1158,6 +1110,7 @@ chfsi_status alloc_all(chfsi_ctx* ctx) {
         CK(dalloc(&ctx->d_beta, (size_t)ctx->np * ctx->n_pw));
         CK(dalloc(&ctx->d_cp, (size_t)ctx->np * ctx->nb));
         CK(dalloc(&ctx->d_cd, (size_t)ctx->np * ctx->nb));
+        CK(dalloc(&ctx->d_cq, (size_t)ctx->np * ctx->nb));
         CK(dalloc(&ctx->d_proj_ion, ctx->np));
         CK(dalloc(&ctx->d_poff, ctx->nions + 1));
         CK(dalloc(&ctx->d_doff, ctx->nions));
@@ -2303,6 +2256,8 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
     if (learned && (s = alloc_mix(ctx))) return s;
     MixRing ring;
     bool prev_fp64 = false;  // the previous SCF iteration ran in FP64
+    constexpr int kMaxReverts = 3;
+    int reverts = 0;
     bool have_prev = false, fell_back = false;
     int rises = 0;
     double r_prev = -1.0;
@@ -2410,13 +2365,19 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
         r->e_total = etot;
         r->n_iter = it;
         if (p->verbose) {
+            // integrated charge of rho_out against the electron count
+            std::vector<double> h(ng);
+            CK(cudaMemcpyAsync(h.data(), ctx->d_rho_out, sizeof(double) * ng, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            double q = 0.0;
+            for (double v : h) q += v;
             std::fprintf(stderr,
                          "scf %3d %s E %.10f dE/atom %.3e eig [%.5f, %.5f] bounds lm %.4f cut %.4f "
-                         "retries %d learned %d\n",
+                         "retries %d learned %d charge-N %.3e eband %.8f\n",
                          it, ctx->mixed_active ? "mixed" : "fp64 ", etot,
                          it > 1 ? std::fabs(etot - e_prev) / ctx->n_atoms : 0.0, eig[0],
                          eig[ctx->nb - 1], ctx->h_coef[0], ctx->h_coef[1], r->n_fp64_retries,
-                         r->n_iter_learned);
+                         r->n_iter_learned, q * dv - n_elec, eband);
         }
         if (p->trace) {
             double* tr = p->trace + (size_t)2 * (it - 1) * ng;
@@ -2435,9 +2396,20 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
             e_prev = etot;
             break;
         }
-        prev_fp64 = !ctx->mixed_active;
-        if (ctx->mixed_active && (de < p->fp64_switch_per_atom || de < p->tol_per_atom))
+        // switch to FP64 once |dE| drops below the switch threshold; an FP64
+        // iteration that follows another FP64 iteration with |dE| still ten
+        // times above it hands the run back to mixed precision (at most
+        // kMaxReverts times, so the two can never alternate for ever)
+        const bool this_fp64 = !ctx->mixed_active;
+        const double sw = std::max(p->fp64_switch_per_atom, p->tol_per_atom);
+        if (ctx->mixed_active && de < sw) {
             ctx->mixed_active = false;
+        } else if (this_fp64 && ctx->mixed && prev_fp64 && de > 10.0 * sw && reverts < kMaxReverts) {
+            ctx->mixed_active = true;
+            ++reverts;
+            if (p->verbose) std::fprintf(stderr, "scf %3d: |dE| %.3e, back to mixed precision\n", it, de);
+        }
+        prev_fp64 = this_fp64;
         e_prev = etot;
         // mix (mixing.rs:24): Pulay over (rho_in, rho_out - rho_in)
         if (ps.m == p->max_hist) {
@@ -2769,9 +2741,16 @@ extern "C" chfsi_status chfsi_batch_run(chfsi_batch* b, double* eig_out, int* st
 
 // Launch configurations of the local H|psi> for this context's sizes: the
 // xy-plane kernel at 128, 256 or 512 threads per block and the z-stick
-// kernels at 16, 32 or 64 columns per block, each timed on the current psi
-// (all bands); the fastest is kept.  times_ms (optional, 9 entries) gets the
-// timing of every variant (planes variant * 3 + columns variant).
+// kernels at 16, 32 or 64 columns per block, each with the compile-time plane
+// kernel (choices 0-8, where the grid has one) and with the generic one
+// (9-17), timed on the current psi (all bands); the fastest is kept.
+// times_ms (optional, kLaunchConfigs entries) gets every timing.
+constexpr int kLaunchConfigs = 18;
+static void apply_launch_config(chfsi_ctx* ctx, int i) {
+    ctx->geo.fixed_planes = i < 9 ? 1 : 0;
+    ctx->geo.tune_planes = (i % 9) / 3;
+    ctx->geo.tune_cols = 16 << (i % 3);
+}
 extern "C" chfsi_status chfsi_autotune(chfsi_ctx* ctx, int* choice, float* times_ms) {
     chfsi_status s = ready(ctx);
     if (s) return s;
@@ -2784,9 +2763,8 @@ extern "C" chfsi_status chfsi_autotune(chfsi_ctx* ctx, int* choice, float* times
     ctx->np = 0;  // the launch configurations only concern the local part
     float best = 1e30f;
     int best_i = 0;
-    for (int i = 0; i < 9 && !s; ++i) {
-        ctx->geo.tune_planes = i / 3;
-        ctx->geo.tune_cols = 16 << (i % 3);
+    for (int i = 0; i < kLaunchConfigs && !s; ++i) {
+        apply_launch_config(ctx, i);
         for (int r = 0; r < 2 && !s; ++r) s = apply_h_dev(ctx, ctx->d_psi, ctx->d_hpsi, ctx->nb, kEpiApply, nullptr);
         cudaEventRecord(e0, ctx->st);
         for (int r = 0; r < 3 && !s; ++r) s = apply_h_dev(ctx, ctx->d_psi, ctx->d_hpsi, ctx->nb, kEpiApply, nullptr);
@@ -2801,8 +2779,7 @@ extern "C" chfsi_status chfsi_autotune(chfsi_ctx* ctx, int* choice, float* times
     ctx->np = np;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    ctx->geo.tune_planes = best_i / 3;
-    ctx->geo.tune_cols = 16 << (best_i % 3);
+    apply_launch_config(ctx, best_i);
     if (s) return s;
     CK(cudaGetLastError());
     if (choice) *choice = best_i;
@@ -2810,9 +2787,8 @@ extern "C" chfsi_status chfsi_autotune(chfsi_ctx* ctx, int* choice, float* times
 }
 
 extern "C" chfsi_status chfsi_set_launch_config(chfsi_ctx* ctx, int choice) {
-    if (!ctx || choice < 0 || choice >= 9) return CHFSI_ERR_BAD_INPUT;
-    ctx->geo.tune_planes = choice / 3;
-    ctx->geo.tune_cols = 16 << (choice % 3);
+    if (!ctx || choice < 0 || choice >= kLaunchConfigs) return CHFSI_ERR_BAD_INPUT;
+    apply_launch_config(ctx, choice);
     return CHFSI_OK;
 }
 

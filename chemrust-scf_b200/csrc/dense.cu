@@ -597,24 +597,30 @@ k_jacobi3(double2* __restrict__ A, double2* __restrict__ V, double2* __restrict_
 // grid barrier and the global round trip.  Staging rows and parameters are
 // double-buffered by step parity, so a block that runs ahead into step s + 1
 // never overwrites what a slower block still reads in step s.
-// Shared layout (double2): params [2][2 * npairs] | per warp: A rows [2n],
+// Each pair has two warps: one rotates the pair and rebuilds its A rows, the
+// other updates its two V rows in the same phase.
+// Shared layout (double2): params [2][2 * npairs] | per pair: A rows [2n],
 // V rows [2n], staging [2][2n].
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(512)
 k_jacobi_cluster(double2* __restrict__ A, double2* __restrict__ V, int n, int max_sweeps,
                  double tol2, double* scratch, int* sweeps_out) {
     cg::cluster_group cluster = cg::this_cluster();
     extern __shared__ double2 csm[];
     __shared__ double red[32];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    // two warps per pair: role 0 rotates and rebuilds the pair's A rows, role 1
+    // updates the pair's two V rows in the same phase
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 6;
+    const int role = wib / wpb, pw = wib - role * wpb;
     const int crank = (int)cluster.block_rank();
-    const int gw = crank * wpb + wib;
+    const int gw = crank * wpb + pw;
     const int m = n + (n & 1), npairs = m / 2, nsteps = m - 1;
     double* prm = reinterpret_cast<double*>(csm);  // [2][4 * npairs]
-    double2* wbase = csm + 4 * (size_t)npairs + (size_t)wib * 8 * n;
+    double2* wbase = csm + 4 * (size_t)npairs + (size_t)pw * 8 * n;
     double2* sA = wbase;
     double2* sV = wbase + 2 * n;
     double2* stg = wbase + 4 * n;  // [2][2n]
-    const bool active = gw < npairs;
+    const bool activeA = gw < npairs && role == 0;
+    const bool activeV = gw < npairs && role == 1;
     const int r0 = 2 * gw, r1 = 2 * gw + 1;
     // total |A|^2
     double tot = 0.0;
@@ -625,11 +631,15 @@ k_jacobi_cluster(double2* __restrict__ A, double2* __restrict__ V, int n, int ma
     tot = block_sum(tot, red);
     if (threadIdx.x == 0) atomicAdd(&scratch[0], tot);
     int p = 0, q = 0;
-    if (active) {
+    if (activeA) {
         jac_pair(m, 0, gw, p, q);
         for (int k = lane; k < n; k += 32) {
             sA[k] = A[(size_t)p * n + k];
             sA[n + k] = q < n ? A[(size_t)q * n + k] : make_double2(0.0, 0.0);
+        }
+    }
+    if (activeV) {
+        for (int k = lane; k < n; k += 32) {
             sV[k] = make_double2(k == r0 ? 1.0 : 0.0, 0.0);
             sV[n + k] = make_double2(k == r1 ? 1.0 : 0.0, 0.0);
         }
@@ -644,7 +654,7 @@ k_jacobi_cluster(double2* __restrict__ A, double2* __restrict__ V, int n, int ma
             const int par = s & 1;
             const int s2 = (s + 1) % nsteps;
             // ---- phase 1: rotate this warp's pair, send X rows to their next owners
-            if (active) {
+            if (activeA) {
                 jac_pair(m, s, gw, p, q);
                 double c = 1.0, sn = 0.0, phr = 1.0, phi = 0.0;
                 if (q < n) {
@@ -693,7 +703,7 @@ k_jacobi_cluster(double2* __restrict__ A, double2* __restrict__ V, int n, int ma
             }
             cluster.sync();
             // ---- phase 2: rows of the next pair, A[r] = X[r] G(s); V <- V G(s)
-            if (active) {
+            if (activeA || activeV) {
                 const double* rs = prm + (size_t)par * 4 * npairs;
                 const double2* sT = stg + (size_t)par * 2 * n;
                 int p2, q2;
@@ -713,34 +723,37 @@ k_jacobi_cluster(double2* __restrict__ A, double2* __restrict__ V, int n, int ma
                     const double2 qc = make_double2(phr * xk.x + phi * xk.y, phr * xk.y - phi * xk.x);
                     return make_double2(sn * xp.x + c * qc.x, sn * xp.y + c * qc.y);
                 };
-                for (int k = lane; k < n; k += 32) {
-                    sA[k] = mix(sT, k);
-                    if (q2 < n) sA[n + k] = mix(sT + n, k);
-                }
-                // V rows in place through registers (n <= 32 * kJacClusterMaxPerLane)
-                double2 v0[kJacClusterMaxPerLane], v1[kJacClusterMaxPerLane];
-#pragma unroll
-                for (int j = 0; j < kJacClusterMaxPerLane; ++j) {
-                    const int k = lane + 32 * j;
-                    if (k < n) {
-                        v0[j] = mix(sV, k);
-                        v1[j] = mix(sV + n, k);
+                if (activeA) {
+                    for (int k = lane; k < n; k += 32) {
+                        sA[k] = mix(sT, k);
+                        if (q2 < n) sA[n + k] = mix(sT + n, k);
                     }
-                }
-                __syncwarp();
+                } else {
+                    // V rows in place through registers (n <= 32 * kJacClusterMaxPerLane)
+                    double2 v0[kJacClusterMaxPerLane], v1[kJacClusterMaxPerLane];
 #pragma unroll
-                for (int j = 0; j < kJacClusterMaxPerLane; ++j) {
-                    const int k = lane + 32 * j;
-                    if (k < n) {
-                        if (r0 < n) sV[k] = v0[j];
-                        if (r1 < n) sV[n + k] = v1[j];
+                    for (int j = 0; j < kJacClusterMaxPerLane; ++j) {
+                        const int k = lane + 32 * j;
+                        if (k < n) {
+                            v0[j] = mix(sV, k);
+                            v1[j] = mix(sV + n, k);
+                        }
+                    }
+                    __syncwarp();
+#pragma unroll
+                    for (int j = 0; j < kJacClusterMaxPerLane; ++j) {
+                        const int k = lane + 32 * j;
+                        if (k < n) {
+                            if (r0 < n) sV[k] = v0[j];
+                            if (r1 < n) sV[n + k] = v1[j];
+                        }
                     }
                 }
                 __syncwarp();
             }
         }
         double off = 0.0;
-        if (active) {
+        if (activeA) {
             jac_pair(m, 0, gw, p, q);
             for (int k = lane; k < n; k += 32) {
                 if (k != p) off += sA[k].x * sA[k].x + sA[k].y * sA[k].y;
@@ -753,11 +766,15 @@ k_jacobi_cluster(double2* __restrict__ A, double2* __restrict__ V, int n, int ma
         cluster.sync();
         converged = *(volatile double*)&scratch[1 + sweep] <= tol2 * total;
     }
-    if (active) {
+    if (activeA) {
         jac_pair(m, 0, gw, p, q);
         for (int k = lane; k < n; k += 32) {
             A[(size_t)p * n + k] = sA[k];
             if (q < n) A[(size_t)q * n + k] = sA[n + k];
+        }
+    }
+    if (activeV) {
+        for (int k = lane; k < n; k += 32) {
             if (r0 < n) V[(size_t)r0 * n + k] = sV[k];
             if (r1 < n) V[(size_t)r1 * n + k] = sV[n + k];
         }
@@ -1037,7 +1054,7 @@ cudaError_t jacobi(double2* A, double2* V, int n, int max_sweeps, double tol2, d
             if (nc > 8) cudaFuncSetAttribute(k_jacobi_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
             cudaLaunchConfig_t lc = {};
             lc.gridDim = dim3(nc);
-            lc.blockDim = dim3(32 * wpb);
+            lc.blockDim = dim3(64 * wpb);  // two warps per pair
             lc.dynamicSmemBytes = smc;
             lc.stream = st;
             cudaLaunchAttribute at[1];

@@ -140,6 +140,141 @@ k_planes_vloc(C* __restrict__ work, const double* __restrict__ veff, HGeom g) {
     for (int c = threadIdx.x; c < g.ncol; c += blockDim.x) wp[c] = plane[g.col_pos[c]];
 }
 
+// ------------------------------------------ pass 2, two-radix compile-time plans
+// The same plane pipeline for axes whose plan has two radices, N = R0 R1
+// (DIF stage 0: radix R0 with span R1; stage 1: radix R1 on blocks of R1
+// consecutive elements, where every twiddle is 1).  Radices, spans and
+// twiddle indices are compile-time constants, and along x the last inverse
+// stage, the V(r) multiply and the first forward stage share registers:
+// lane n1 of a row's lane group holds the R0 elements n1 + m R1, which is
+// what those two stages read and write.
+
+// radix-R1 stage on block blk (elements blk R1 .. blk R1 + R1 - 1)
+template <int R0, int R1, int SIGN, typename C>
+__device__ __forceinline__ void p2_blocks(C* line, int es, int blk) {
+    constexpr int N = R0 * R1;
+    C x[R1];
+#pragma unroll
+    for (int j = 0; j < R1; ++j) x[j] = line[swz(blk * R1 + j, N) * es];
+    dft_r<R1, SIGN>(x);
+#pragma unroll
+    for (int m = 0; m < R1; ++m) line[swz(blk * R1 + m, N) * es] = x[m];
+}
+template <int R0, int R1, typename C>
+__device__ __forceinline__ void p2_load_span(const C* line, int es, int n1, C* x) {
+#pragma unroll
+    for (int j = 0; j < R0; ++j) x[j] = line[swz(n1 + j * R1, R0 * R1) * es];
+}
+template <int R0, int R1, typename C>
+__device__ __forceinline__ void p2_store_span(C* line, int es, int n1, const C* x) {
+#pragma unroll
+    for (int j = 0; j < R0; ++j) line[swz(n1 + j * R1, R0 * R1) * es] = x[j];
+}
+// DIT stage 0 on span n1: twiddle w^(n1 m), radix-R0 DFT (sign +1)
+template <int R0, typename C>
+__device__ __forceinline__ void p2_span_inverse(C* x, int n1, const C* tw) {
+#pragma unroll
+    for (int m = 1; m < R0; ++m) x[m] = cmul(tw[n1 * m], x[m]);
+    dft_r<R0, 1>(x);
+}
+// DIF stage 0 on span n1: radix-R0 DFT (sign -1), twiddle w^(-n1 m)
+template <int R0, typename C>
+__device__ __forceinline__ void p2_span_forward(C* x, int n1, const C* tw) {
+    dft_r<R0, -1>(x);
+#pragma unroll
+    for (int m = 1; m < R0; ++m) x[m] = cmulc(tw[n1 * m], x[m]);
+}
+// whole-line transforms by one lane group (lane i); every lane of the warp
+// calls them (act = false: idle)
+template <int R0, int R1, typename C>
+__device__ __forceinline__ void p2_line_inverse(C* line, bool act, int i, int es, const C* tw) {
+    if (act && i < R0) p2_blocks<R0, R1, 1>(line, es, i);
+    __syncwarp();
+    if (act && i < R1) {
+        C x[R0];
+        p2_load_span<R0, R1>(line, es, i, x);
+        p2_span_inverse<R0>(x, i, tw);
+        p2_store_span<R0, R1>(line, es, i, x);
+    }
+    __syncwarp();
+}
+template <int R0, int R1, typename C>
+__device__ __forceinline__ void p2_line_forward(C* line, bool act, int i, int es, const C* tw) {
+    if (act && i < R1) {
+        C x[R0];
+        p2_load_span<R0, R1>(line, es, i, x);
+        p2_span_forward<R0>(x, i, tw);
+        p2_store_span<R0, R1>(line, es, i, x);
+    }
+    __syncwarp();
+    if (act && i < R0) p2_blocks<R0, R1, -1>(line, es, i);
+    __syncwarp();
+}
+
+// Square planes (nx = ny = R0 R1, both axes on the same plan); shared memory
+// layout and launch shape as k_planes_vloc.
+template <typename C, int V, int R0, int R1>
+__global__ void __launch_bounds__(PlanesCfg<C, V>::threads, PlanesCfg<C, V>::min_blocks)
+k_planes_vloc_p2(C* __restrict__ work, const double* __restrict__ veff, HGeom g) {
+    constexpr int N = R0 * R1, LS = N | 1, T = R0 > R1 ? R0 : R1, PW = 32 / T;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* twx = reinterpret_cast<C*>(smem_raw);
+    C* twy = reinterpret_cast<C*>(smem_raw + align16<C>(N));
+    C* plane = reinterpret_cast<C*>(smem_raw + 2 * align16<C>(N));
+    int* xl = reinterpret_cast<int*>(plane + (size_t)N * LS);
+    const int z = blockIdx.x, b = blockIdx.y;
+    const int nxact = g.nxact;
+    copy_twiddles(twx, g.twd_x, g.twf_x, N);
+    copy_twiddles(twy, g.twd_y, g.twf_y, N);
+    for (int i = threadIdx.x; i < nxact; i += blockDim.x) xl[i] = g.xact[i];
+    for (int i = threadIdx.x; i < N * LS; i += blockDim.x) plane[i] = czero<C>();
+    __syncthreads();
+    C* wp = work + ((size_t)b * g.nz + z) * g.ncol;
+    for (int c = threadIdx.x; c < g.ncol; c += blockDim.x) plane[g.col_pos[c]] = wp[c];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, gi = lane / T, li = lane - gi * T;
+    const bool ing = gi < PW;
+    const int groups = (blockDim.x >> 5) * PW, gid = (threadIdx.x >> 5) * PW + gi;
+    // y lines through the active x positions
+    for (int l0 = 0; l0 < nxact; l0 += groups) {
+        const int l = l0 + gid;
+        const bool act = ing && l < nxact;
+        p2_line_inverse<R0, R1>(plane + (act ? xl[l] : 0), act, li, LS, twy);
+    }
+    __syncthreads();
+    // x rows: inverse, x V(r), forward
+    using R = typename RealOf<C>::type;
+    const double* vz = veff + (size_t)z * N * N;
+    for (int y0 = 0; y0 < N; y0 += groups) {
+        const int y = y0 + gid;
+        const bool act = ing && y < N;
+        C* row = plane + (act ? swz(y, N) * LS : 0);
+        if (act && li < R0) p2_blocks<R0, R1, 1>(row, 1, li);
+        __syncwarp();
+        if (act && li < R1) {
+            C x[R0];
+            p2_load_span<R0, R1>(row, 1, li, x);
+            p2_span_inverse<R0>(x, li, twx);
+            const double* vr = vz + (size_t)y * N + li;
+#pragma unroll
+            for (int m = 0; m < R0; ++m) x[m] = cscale(x[m], (R)vr[m * R1]);
+            p2_span_forward<R0>(x, li, twx);
+            p2_store_span<R0, R1>(row, 1, li, x);
+        }
+        __syncwarp();
+        if (act && li < R0) p2_blocks<R0, R1, -1>(row, 1, li);
+        __syncwarp();
+    }
+    __syncthreads();
+    for (int l0 = 0; l0 < nxact; l0 += groups) {
+        const int l = l0 + gid;
+        const bool act = ing && l < nxact;
+        p2_line_forward<R0, R1>(plane + (act ? xl[l] : 0), act, li, LS, twy);
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < g.ncol; c += blockDim.x) wp[c] = plane[g.col_pos[c]];
+}
+
 // ---------------------------------------------------------------- pass 3
 template <typename C, int MODE, int kColsPerBlock>
 __global__ void __launch_bounds__(256)
@@ -442,9 +577,52 @@ void planes_vloc_variant(C* work, const double* veff, int nb, const HGeom& g, cu
     k_planes_vloc<C, V><<<grid, PlanesCfg<C, V>::threads, sm, st>>>(work, veff, g);
 }
 
+template <typename C, int V, int R0, int R1>
+void planes_vloc_p2(C* work, const double* veff, int nb, const HGeom& g, cudaStream_t st) {
+    dim3 grid(g.nz, nb);
+    size_t sm = planes_smem_bytes(g, sizeof(C));
+    allow_smem(k_planes_vloc_p2<C, V, R0, R1>, sm);
+    k_planes_vloc_p2<C, V, R0, R1><<<grid, PlanesCfg<C, V>::threads, sm, st>>>(work, veff, g);
+}
+
+template <typename C, int R0, int R1>
+void planes_vloc_p2_variant(C* work, const double* veff, int nb, const HGeom& g, cudaStream_t st) {
+    switch (g.tune_planes) {
+    case 1: planes_vloc_p2<C, 1, R0, R1>(work, veff, nb, g, st); break;
+    case 2: planes_vloc_p2<C, 2, R0, R1>(work, veff, nb, g, st); break;
+    default: planes_vloc_p2<C, 0, R0, R1>(work, veff, nb, g, st); break;
+    }
+}
+
+// Radix pairs with a compile-time plane kernel (square planes only); other
+// plans run the generic kernel.
+static bool planes_vloc_fixed(void* work, const double* veff, int nb, const HGeom& g, cudaStream_t st,
+                       bool fp32) {
+    if (g.nx != g.ny || g.ax.nst != 2 || g.ay.nst != 2 || g.ax.r[0] != g.ay.r[0] ||
+        g.ax.r[1] != g.ay.r[1])
+        return false;
+    const int key = g.ax.r[0] * 100 + g.ax.r[1];
+#define CHFSI_P2(A, B)                                                                          \
+    case A * 100 + B:                                                                         \
+        if (fp32) planes_vloc_p2_variant<float2, A, B>((float2*)work, veff, nb, g, st);        \
+        else planes_vloc_p2_variant<double2, A, B>((double2*)work, veff, nb, g, st);           \
+        return true;
+    switch (key) {
+        CHFSI_P2(9, 8)    // 72
+        CHFSI_P2(12, 9)   // 108
+        CHFSI_P2(8, 5)    // 40
+        CHFSI_P2(12, 12)  // 144
+        CHFSI_P2(8, 8)    // 64
+        CHFSI_P2(8, 6)    // 48
+    default: return false;
+    }
+#undef CHFSI_P2
+}
+
 template <typename C>
 void launch_planes_vloc(C* work, const double* veff, int nb, const HGeom& g, cudaStream_t st) {
     count_launch();
+    if (g.fixed_planes && planes_vloc_fixed(work, veff, nb, g, st, sizeof(C) == 8)) return;
     switch (g.tune_planes) {
     case 1: planes_vloc_variant<C, 1>(work, veff, nb, g, st); break;
     case 2: planes_vloc_variant<C, 2>(work, veff, nb, g, st); break;

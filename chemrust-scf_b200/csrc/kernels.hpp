@@ -30,6 +30,9 @@ struct HGeom {
     // kernels at tune_cols (16, 32, 64) columns per block
     int tune_planes = 0;
     int tune_cols = 32;
+    // xy-plane kernels with compile-time radices where the plan has one
+    // (square planes, two radices); 0 = always the generic kernel
+    int fixed_planes = 1;
 };
 
 // Pass-3 epilogue: what to do with (H psi)_g once it is assembled.

@@ -3,8 +3,8 @@ Pulay and with the learned mixer, on one of the synthetic configurations.
 
     python chemrust-scf_b200/scf_compare.py --config 2 --max-iter 90
 
-Arms: FP64 filter + Pulay (alpha 0.3, history 6); FP32 filter / BF16x3
-tcgen05 GEMMs / FP64 eigensolve with Pulay; the same with the learned
+Arms: FP64 filter + Pulay (alpha 0.3, history 6); FP32 filter (BF16x3
+tcgen05 projector GEMMs) / FP64 Rayleigh-Ritz with Pulay; the same with the learned
 per-shell preconditioner inside Pulay.  The mixed runs switch to FP64 only
 for the confirming iterations (|dE| < tol) and only declare convergence on
 an FP64 iteration.  Times are device seconds of the SCF loop (CUDA events),

@@ -69,7 +69,8 @@ typedef enum chfsi_status {
 
 typedef struct chfsi_c128 { double re, im; } chfsi_c128;
 
-/* Precision of the filter (the Rayleigh-Ritz eigensolve is always FP64). */
+/* Precision of the filter (the Rayleigh-Ritz, its subspace matrices and the
+ * rotation of the block are FP64 in both modes). */
 enum { CHFSI_PREC_FP64 = 0, CHFSI_PREC_MIXED = 1 };
 /* Upper spectral bound used by the filter. */
 enum {
@@ -259,7 +260,7 @@ chfsi_status chfsi_zgemm_cn(const chfsi_c128* a_dev, int lda, const chfsi_c128* 
 chfsi_status chfsi_zgemm_cn_noalloc(const chfsi_c128* a_dev, int lda, const chfsi_c128* b_dev,
                                     int ldb, int m, int n, int k, chfsi_c128* c_dev, void* stream);
 /* Same product on the tcgen05 tensor cores in BF16 3-way split precision
- * with FP32 accumulation (the mixed-precision projector / overlap GEMM). */
+ * with FP32 accumulation (the mixed-precision filter's projector GEMM). */
 chfsi_status chfsi_zgemm_cn_bf16x3(const chfsi_c128* a_dev, int lda, const chfsi_c128* b_dev,
                                    int ldb, int m, int n, int k, chfsi_c128* c_dev, void* stream);
 
@@ -360,11 +361,13 @@ chfsi_status chfsi_batch_capture(chfsi_batch* b, int ndeg);
  * status_out: per member status (or NULL); returns the first failure */
 chfsi_status chfsi_batch_run(chfsi_batch* b, double* eig_out, int* status_out);
 chfsi_status chfsi_batch_graph_nodes(chfsi_batch* b, size_t* nodes);
-/* Autotuner: times the local H|psi> of this context at 3 x 3 launch
- * configurations (xy-plane kernel 256 / 128 / 512 threads per block; z-stick
- * kernels 16 / 32 / 64 columns per block) on its current psi and keeps the
- * fastest; choice = planes * 3 + columns, times_ms (9 floats) may be NULL.
- * chfsi_set_launch_config applies a choice (e.g. one tuned per size class). */
+/* Autotuner: times the local H|psi> of this context at 2 x 3 x 3 launch
+ * configurations (xy-plane kernel with compile-time radices where the grid's
+ * plan has one, or the generic kernel; 256 / 128 / 512 threads per block;
+ * z-stick kernels 16 / 32 / 64 columns per block) on its current psi and
+ * keeps the fastest; choice = generic * 9 + planes * 3 + columns, times_ms
+ * (18 floats) may be NULL.  chfsi_set_launch_config applies a choice (e.g.
+ * one tuned per size class). */
 chfsi_status chfsi_autotune(chfsi_ctx* ctx, int* choice, float* times_ms);
 chfsi_status chfsi_set_launch_config(chfsi_ctx* ctx, int choice);
 
