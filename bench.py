@@ -411,10 +411,28 @@ def run_reference(args):
 
 
 def run_profile(kind):
-    """Fixed workload of the 64-atom cell for profiler captures."""
+    """Fixed workloads for profiler captures: the 64-atom cell (local, fp64,
+    mixed), or two degree-16 passes of the 216-atom ultrasoft cell
+    (fp64-216, mixed-216) after one untraced pass from the random start;
+    only those two passes run between cudaProfilerStart / Stop (capture
+    them with ncu --profile-from-start off)."""
     import numpy as np
     import torch
     import chfsi
+    if kind.endswith("-216"):
+        s = chfsi.SyntheticSystem(config_index=2)
+        prec = chfsi.PREC_MIXED if kind.startswith("mixed") else chfsi.PREC_FP64
+        ctx = chfsi.Context(s, precision=prec)
+        ctx.build_v_eff(np.full(ctx.ng_density, s.n_elec / s.omega))
+        e = ctx.diagonalize(16)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        for _ in range(2):
+            e = ctx.diagonalize(16, e)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        print("profile %s: 2 traced diagonalisations, lowest eigenvalue %.8f" % (kind, e[0]))
+        return
     s = chfsi.SyntheticSystem(config_index=CONFIG_INDEX)
     prec = chfsi.PREC_MIXED if kind == "mixed" else chfsi.PREC_FP64
     ctx = chfsi.Context(s, precision=prec)
@@ -444,9 +462,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--fp64-only", action="store_true", help="skip the mixed-precision lines")
     ap.add_argument("--no-scf", action="store_true", help="skip the time-to-SCF comparison")
-    ap.add_argument("--profile", choices=["local", "fp64", "mixed"], default=None,
+    ap.add_argument("--profile", choices=["local", "fp64", "mixed", "fp64-216", "mixed-216"],
+                    default=None,
                     help="a short fixed workload for ncu captures (no JSON line): two local "
-                         "H|psi> launches, or six diagonalisations in one precision")
+                         "H|psi> launches, or six diagonalisations in one precision (64-atom "
+                         "cell), or two traced passes of the 216-atom ultrasoft cell")
     args = ap.parse_args()
     if args.profile:
         run_profile(args.profile)
