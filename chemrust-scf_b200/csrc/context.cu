@@ -674,8 +674,10 @@ chfsi_status alloc_mixed(chfsi_ctx* ctx, int ncol) {
         s.t->rows_alloc = s.rows_alloc;
         s.t->kp = s.kp;
     }
-    size_t pf = tc_partial_floats(nb, nb, npw);
-    if (np > 0) pf = std::max(pf, tc_partial_floats(np, nb, npw));
+    // the projector GEMM may see any band count 1..nb (chfsi_apply_h), and
+    // the K-split count depends on it: size for the largest
+    size_t pf = 1;
+    for (int b = 1; b <= nb && np > 0; ++b) pf = std::max(pf, tc_partial_floats(np, b, npw));
     CK(dalloc(&ctx->d_tc_part, pf));
     CK(dalloc(&ctx->d_tc_err, 4));
     CK(cudaMemsetAsync(ctx->d_tc_err, 0, 4 * sizeof(int), ctx->st));

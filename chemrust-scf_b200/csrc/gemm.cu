@@ -107,10 +107,12 @@ k_gemm_cn_splitk(const double2* __restrict__ A, int lda, const double2* __restri
 // (lane >> 2), col (lane & 3); B row (lane & 3), col (lane >> 2); C row
 // (lane >> 2), cols 2 (lane & 3) + {0, 1}.  CTA tile 64 x 64, 8 warps as
 // 2 (M) x 4 (N), warp tile 32 x 16 = 4 x 2 MMA tiles.
+// Not volatile: the MMA has no effect beyond its outputs, so the compiler may
+// interleave independent MMAs with the fragment loads.
 __device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
-                 : "+d"(d[0]), "+d"(d[1])
-                 : "d"(a), "d"(b));
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+        : "+d"(d[0]), "+d"(d[1])
+        : "d"(a), "d"(b));
 }
 
 constexpr int kDS = BK + 4;  // row stride (doubles) of K-contiguous planes
@@ -163,18 +165,29 @@ k_zgemm_cn_dmma(const double2* __restrict__ A, int lda, const double2* __restric
                 br[j] = Br[n][kk + tig];
                 bi[j] = Bi[n][kk + tig];
             }
+            double ar[4], ai[4];
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
                 const int m = wm * 32 + i * 8 + gid;
-                const double ar = Ar[m][kk + tig], ai = Ai[m][kk + tig];
+                ar[i] = Ar[m][kk + tig];
+                ai[i] = Ai[m][kk + tig];
+            }
+            // two rounds of 16 independent MMAs: each accumulator's second
+            // product comes 16 MMAs after its first
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
 #pragma unroll
                 for (int j = 0; j < 2; ++j) {
-                    dmma(cr[i][j], ar, br[j]);
-                    dmma(cr[i][j], ai, bi[j]);
-                    dmma(ci[i][j], ar, bi[j]);
-                    dmma(ci[i][j], -ai, br[j]);
+                    dmma(cr[i][j], ar[i], br[j]);
+                    dmma(ci[i][j], ar[i], bi[j]);
                 }
-            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    dmma(cr[i][j], ai[i], bi[j]);
+                    dmma(ci[i][j], -ai[i], br[j]);
+                }
         }
         __syncthreads();
     }
@@ -236,18 +249,27 @@ k_zgemm_tn_dmma(const double2* __restrict__ W, int ldw, const double2* __restric
                 xr[j] = Xr[kk + tig][n];
                 xi[j] = Xi[kk + tig][n];
             }
+            double wr[4], wi[4];
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
                 const int m = wm * 32 + i * 8 + gid;
-                const double wr = Wr[kk + tig][m], wi = Wi[kk + tig][m];
+                wr[i] = Wr[kk + tig][m];
+                wi[i] = Wi[kk + tig][m];
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
 #pragma unroll
                 for (int j = 0; j < 2; ++j) {
-                    dmma(cr[i][j], wr, xr[j]);
-                    dmma(cr[i][j], -wi, xi[j]);
-                    dmma(ci[i][j], wr, xi[j]);
-                    dmma(ci[i][j], wi, xr[j]);
+                    dmma(cr[i][j], wr[i], xr[j]);
+                    dmma(ci[i][j], wr[i], xi[j]);
                 }
-            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    dmma(cr[i][j], -wi[i], xi[j]);
+                    dmma(ci[i][j], wi[i], xr[j]);
+                }
         }
         __syncthreads();
     }

@@ -25,6 +25,7 @@
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <cstring>
 #include <mutex>
 
@@ -388,14 +389,34 @@ int grid_for(long long n) {
 
 int tc_kpad(int K) { return ((2 * K + kBK - 1) / kBK) * kBK; }
 
+// K-split count of the partial-output mode.  One CTA fits an SM, so the
+// grid runs in waves of 148; the split that fills the last wave best wins
+// (a larger split only when it fills it 2 % better), with at least 8 K-tiles
+// per split.  E.g. 81 tiles (the projector GEMM of 1,728 projectors x 576
+// bands) run as 9 splits, 729 CTAs in 4.93 waves, instead of 2 splits, 162
+// CTAs in 1.09 waves.
+int tc_splits(int tiles, int ktiles) {
+    const int smax = std::max(1, std::min(64, ktiles / 8));
+    int best = 1;
+    double best_eff = -1.0;
+    for (int s = 1; s <= smax; ++s) {
+        const int ctas = tiles * s;
+        const int waves = (ctas + 147) / 148;
+        const double eff = (double)ctas / (waves * 148.0);
+        if (eff > best_eff + 0.02) {
+            best_eff = eff;
+            best = s;
+        }
+    }
+    const int kps = (ktiles + best - 1) / best;
+    return (ktiles + kps - 1) / kps;
+}
+
 size_t tc_partial_floats(int M, int N, int K) {
     const int kp = tc_kpad(K);
     const int ktiles = kp / kBK;
     const int mt = (2 * M + kBM - 1) / kBM, nt = (N + pick_bn(N) - 1) / pick_bn(N);
-    int splits = (148 + mt * nt - 1) / (mt * nt);
-    if (splits > ktiles) splits = ktiles;
-    if (splits < 1) splits = 1;
-    return (size_t)splits * 2 * M * N;
+    return (size_t)tc_splits(mt * nt, ktiles) * 2 * M * N;
 }
 
 template <typename CIn>
@@ -442,11 +463,7 @@ cudaError_t tc_gemm(const TcPlanes& a, const TcPlanes& b, int M, int N, int K, i
     const int ktiles = a.kp / kBK;
     const int mt = (2 * M + kBM - 1) / kBM, nt = (N + bn - 1) / bn;
     int splits = 1;
-    if (out_mode == kTcOutPartial) {
-        splits = (148 + mt * nt - 1) / (mt * nt);
-        if (splits > ktiles) splits = ktiles;
-        if (splits < 1) splits = 1;
-    }
+    if (out_mode == kTcOutPartial) splits = tc_splits(mt * nt, ktiles);
     const int kps = (ktiles + splits - 1) / splits;
     splits = (ktiles + kps - 1) / kps;
     dim3 grid(mt, nt, splits);
