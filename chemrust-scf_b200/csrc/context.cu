@@ -2257,7 +2257,7 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
     if (s) return s;
     if (learned && (s = alloc_mix(ctx))) return s;
     MixRing ring;
-    bool prev_fp64 = false;  // the previous SCF iteration ran in FP64
+    int low_mixed = 0;  // mixed iterations in a row with |dE| below the switch
     constexpr int kMaxReverts = 3;
     int reverts = 0;
     bool have_prev = false, fell_back = false;
@@ -2387,31 +2387,35 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
             CK(cudaMemcpyAsync(tr + ng, ctx->d_rho_out, sizeof(double) * ng, cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
         }
-        // check (scf.rs:328): |dE| per atom below tolerance; a mixed-precision
-        // run only converges on FP64 iterations (the final filter passes are FP64)
+        // check (scf.rs:328): |dE| per atom below tolerance, declared on an
+        // FP64 iteration only (the last filter pass before convergence is
+        // FP64).  Mixed passes run an FP64 Rayleigh-Ritz, so their energies
+        // carry no precision bias and the change from a mixed iteration to
+        // the FP64 one after it counts.
         const double de = it > 1 ? std::fabs(etot - e_prev) / ctx->n_atoms : 1e300;
         if (ctx->mixed_active) ++r->n_iter_mixed;
-        // convergence needs two FP64 iterations in a row: the change from the
-        // last mixed-precision iteration does not count
-        if (de < p->tol_per_atom && !ctx->mixed_active && prev_fp64) {
+        if (de < p->tol_per_atom && !ctx->mixed_active) {
             status = CHFSI_OK;
             e_prev = etot;
             break;
         }
-        // switch to FP64 once |dE| drops below the switch threshold; an FP64
-        // iteration that follows another FP64 iteration with |dE| still ten
-        // times above it hands the run back to mixed precision (at most
-        // kMaxReverts times, so the two can never alternate for ever)
-        const bool this_fp64 = !ctx->mixed_active;
+        // switch to FP64 after two mixed iterations in a row with |dE| below
+        // the switch threshold (a single one falls below it by chance where
+        // the energy turns); an FP64 iteration whose |dE| is still ten times
+        // above it hands the run back to mixed precision (at most kMaxReverts
+        // times, so the two can never alternate for ever)
         const double sw = std::max(p->fp64_switch_per_atom, p->tol_per_atom);
-        if (ctx->mixed_active && de < sw) {
-            ctx->mixed_active = false;
-        } else if (this_fp64 && ctx->mixed && prev_fp64 && de > 10.0 * sw && reverts < kMaxReverts) {
+        if (ctx->mixed_active) {
+            low_mixed = de < sw ? low_mixed + 1 : 0;
+            if (low_mixed >= 2) {
+                ctx->mixed_active = false;
+                low_mixed = 0;
+            }
+        } else if (ctx->mixed && de > 10.0 * sw && reverts < kMaxReverts) {
             ctx->mixed_active = true;
             ++reverts;
             if (p->verbose) std::fprintf(stderr, "scf %3d: |dE| %.3e, back to mixed precision\n", it, de);
         }
-        prev_fp64 = this_fp64;
         e_prev = etot;
         // mix (mixing.rs:24): Pulay over (rho_in, rho_out - rho_in)
         if (ps.m == p->max_hist) {

@@ -449,23 +449,30 @@ k_jacobi2(double2* A, double2* V, double2* X, int n, int max_sweeps, double tol2
 // in phase 1 of step s + 1), and V rows 2w, 2w + 1 stay in shared memory for
 // the whole solve (V <- V G only mixes columns).  Per step the only global
 // traffic is the X rows of each pair and the rotation parameters: phase 1
-// writes them, one grid barrier, phase 2 reads them back.  Requires every
-// pair to have a resident warp (the host checks co-residency).
-__global__ void __launch_bounds__(256)
+// writes them, one grid barrier, phase 2 reads them back.  Each pair has two
+// warps: the A warp rotates, writes the X rows and rebuilds the next pair's A
+// rows; the V warp updates the pair's two V rows in the same phase.
+// Requires every pair to have its resident warps (the host checks
+// co-residency).  Shared memory per pair (double2): A rows [2n], X staging
+// [2n], V rows [2n], V ping-pong [2n].
+__global__ void __launch_bounds__(512)
 k_jacobi3(double2* __restrict__ A, double2* __restrict__ V, double2* __restrict__ X, int n,
           int max_sweeps, double tol2, double* scratch, double* rot, int* sweeps_out) {
     cg::grid_group grid = cg::this_grid();
     extern __shared__ double2 jsm[];
     __shared__ double red[32];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-    const int gw = blockIdx.x * wpb + wib;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 6;
+    const int role = wib / wpb, pw = wib - role * wpb;
+    const int gw = blockIdx.x * wpb + pw;
     const int m = n + (n & 1), npairs = m / 2, nsteps = m - 1;
     double* rs_s = reinterpret_cast<double*>(jsm);  // 4 * npairs doubles
-    double2* wbase = jsm + 2 * (size_t)npairs + (size_t)wib * 6 * n;
-    double2* sA = wbase;          // rows p, q of this warp's pair
-    double2* sV = wbase + 2 * n;  // V rows 2w, 2w + 1 (ping-pong with sT)
-    double2* sT = wbase + 4 * n;  // staging for X rows / next V rows
-    const bool active = gw < npairs;
+    double2* wbase = jsm + 2 * (size_t)npairs + (size_t)pw * 8 * n;
+    double2* sA = wbase;          // rows p, q of this pair
+    double2* sX = wbase + 2 * n;  // staging for the X rows of the next pair
+    double2* sV = wbase + 4 * n;  // V rows 2w, 2w + 1 (ping-pong with sT)
+    double2* sT = wbase + 6 * n;
+    const bool activeA = gw < npairs && role == 0;
+    const bool activeV = gw < npairs && role == 1;
     const int r0 = 2 * gw, r1 = 2 * gw + 1;
     const size_t nn = (size_t)n * n;
     const size_t gtid = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
@@ -475,11 +482,15 @@ k_jacobi3(double2* __restrict__ A, double2* __restrict__ V, double2* __restrict_
     tot = block_sum(tot, red);
     if (threadIdx.x == 0) atomicAdd(&scratch[0], tot);
     int p = 0, q = 0;
-    if (active) {
+    if (activeA) {
         jac_pair(m, 0, gw, p, q);
         for (int k = lane; k < n; k += 32) {
             sA[k] = A[(size_t)p * n + k];
             sA[n + k] = q < n ? A[(size_t)q * n + k] : make_double2(0.0, 0.0);
+        }
+    }
+    if (activeV) {
+        for (int k = lane; k < n; k += 32) {
             sV[k] = make_double2(k == r0 ? 1.0 : 0.0, 0.0);
             sV[n + k] = make_double2(k == r1 ? 1.0 : 0.0, 0.0);
         }
@@ -492,7 +503,7 @@ k_jacobi3(double2* __restrict__ A, double2* __restrict__ V, double2* __restrict_
         for (int s = 0; s < nsteps; ++s) {
             double* rs = rot + 4 * (size_t)npairs * (s & 1);
             // ---- phase 1: rotation of this warp's pair from its rows on chip
-            if (active) {
+            if (activeA) {
                 jac_pair(m, s, gw, p, q);
                 double c = 1.0, sn = 0.0, phr = 1.0, phi = 0.0;
                 if (q < n) {
@@ -524,16 +535,16 @@ k_jacobi3(double2* __restrict__ A, double2* __restrict__ V, double2* __restrict_
             // ---- phase 2: rows of the next pair, A[r] = X[r] G(s); V <- V G(s)
             const int s2 = (s + 1) % nsteps;
             int p2 = 0, q2 = 0;
-            if (active) {
+            if (activeA) {
                 jac_pair(m, s2, gw, p2, q2);
                 for (int k = lane; k < n; k += 32) {
-                    sT[k] = X[(size_t)p2 * n + k];
-                    if (q2 < n) sT[n + k] = X[(size_t)q2 * n + k];
+                    sX[k] = X[(size_t)p2 * n + k];
+                    if (q2 < n) sX[n + k] = X[(size_t)q2 * n + k];
                 }
             }
             for (int i = threadIdx.x; i < 4 * npairs; i += blockDim.x) rs_s[i] = rs[i];
             __syncthreads();
-            if (active) {
+            if (activeA || activeV) {
                 auto mix = [&](const double2* src, int k) -> double2 {
                     int pi, partner;
                     jac_partner(m, s, k, pi, partner);
@@ -550,22 +561,24 @@ k_jacobi3(double2* __restrict__ A, double2* __restrict__ V, double2* __restrict_
                     return make_double2(sn * xp.x + c * qc.x, sn * xp.y + c * qc.y);
                 };
                 __syncwarp();
-                for (int k = lane; k < n; k += 32) {
-                    sA[k] = mix(sT, k);
-                    if (q2 < n) sA[n + k] = mix(sT + n, k);
+                if (activeA) {
+                    for (int k = lane; k < n; k += 32) {
+                        sA[k] = mix(sX, k);
+                        if (q2 < n) sA[n + k] = mix(sX + n, k);
+                    }
+                } else {
+                    for (int k = lane; k < n; k += 32) {
+                        if (r0 < n) sT[k] = mix(sV, k);
+                        if (r1 < n) sT[n + k] = mix(sV + n, k);
+                    }
+                    double2* t = sV; sV = sT; sT = t;
                 }
                 __syncwarp();
-                for (int k = lane; k < n; k += 32) {
-                    if (r0 < n) sT[k] = mix(sV, k);
-                    if (r1 < n) sT[n + k] = mix(sV + n, k);
-                }
-                __syncwarp();
-                double2* t = sV; sV = sT; sT = t;
             }
         }
         // off-diagonal norm of this warp's rows (the pair of step 0)
         double off = 0.0;
-        if (active) {
+        if (activeA) {
             jac_pair(m, 0, gw, p, q);
             for (int k = lane; k < n; k += 32) {
                 if (k != p) off += sA[k].x * sA[k].x + sA[k].y * sA[k].y;
@@ -577,11 +590,15 @@ k_jacobi3(double2* __restrict__ A, double2* __restrict__ V, double2* __restrict_
         grid.sync();
         converged = scratch[1 + sweep] <= tol2 * total;
     }
-    if (active) {
+    if (activeA) {
         jac_pair(m, 0, gw, p, q);
         for (int k = lane; k < n; k += 32) {
             A[(size_t)p * n + k] = sA[k];
             if (q < n) A[(size_t)q * n + k] = sA[n + k];
+        }
+    }
+    if (activeV) {
+        for (int k = lane; k < n; k += 32) {
             if (r0 < n) V[(size_t)r0 * n + k] = sV[k];
             if (r1 < n) V[(size_t)r1 * n + k] = sV[n + k];
         }
@@ -1078,16 +1095,16 @@ cudaError_t jacobi(double2* A, double2* V, int n, int max_sweeps, double tol2, d
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     // on-chip variant: one warp per pair, all warps co-resident
-    for (int wpb = 8; wpb >= 1; wpb >>= 1) {
-        const size_t smem3 = (size_t)npairs * 4 * sizeof(double) + (size_t)wpb * 6 * n * sizeof(double2);
+    for (int wpb = 8; wpb >= 1; wpb >>= 1) {  // pairs per block, two warps each
+        const size_t smem3 = (size_t)npairs * 4 * sizeof(double) + (size_t)wpb * 8 * n * sizeof(double2);
         if (smem3 > 200 * 1024) continue;
         cudaFuncSetAttribute(k_jacobi3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem3);
         int per_sm3 = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm3, k_jacobi3, 32 * wpb, smem3);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm3, k_jacobi3, 64 * wpb, smem3);
         const int blocks3 = (npairs + wpb - 1) / wpb;
         if (per_sm3 < 1 || blocks3 > sms * per_sm3) continue;
         void* args3[] = {&A, &V, &X, &n, &max_sweeps, &tol2, &scratch, &rot, &sweeps_out};
-        return cudaLaunchCooperativeKernel((const void*)k_jacobi3, dim3(blocks3), dim3(32 * wpb),
+        return cudaLaunchCooperativeKernel((const void*)k_jacobi3, dim3(blocks3), dim3(64 * wpb),
                                            args3, smem3, st);
     }
     const int warps_per_block = 8;

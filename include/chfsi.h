@@ -290,9 +290,11 @@ typedef struct chfsi_scf_params {
     int    max_hist;      /* Pulay history length, 1..8 (1 = linear mixing)     */
     int    first_passes;  /* filter + Rayleigh-Ritz passes in the first step    */
     double kT;            /* Fermi-Dirac smearing (Ha); <= 0: fixed aufbau occupations */
-    double fp64_switch_per_atom; /* mixed precision: switch the filter to FP64 once
-                                    |dE|/atom < this (convergence is only declared on
-                                    the second of two FP64 steps in a row)            */
+    double fp64_switch_per_atom; /* mixed precision: switch the filter to FP64 after
+                                    two mixed steps in a row with |dE|/atom below
+                                    max(this, tol); convergence is declared on FP64
+                                    steps only; an FP64 step with |dE| ten times above
+                                    the switch returns to mixed (at most 3 times)      */
     int    mixer;         /* CHFSI_MIXER_PULAY / _LEARNED / _LEARNED_PULAY            */
     int    cg_steps;      /* band-CG steps per band after each filter (0: none)      */
     double* trace;        /* optional host buffer of 2 * max_iter * N^3 doubles: rho_in
