@@ -55,15 +55,23 @@ __global__ void k_symmetrize(const double2* __restrict__ in, double2* __restrict
 
 // Right-looking Cholesky of a Hermitian positive-definite matrix in place
 // (lower triangle = L, upper zeroed).  info = 0 or the failing column + 1.
+// A pivot fails when it is not above n * 2^-52 times its column's original
+// diagonal entry: such a matrix is singular to working precision (e.g. two
+// equal columns, whose pivot is a rounding residue of either sign) and its
+// factor would only amplify rounding.  The original diagonal is kept in row
+// 0 of the upper triangle, which the factorisation does not touch.
 __global__ void __launch_bounds__(1024) k_cholesky(double2* A, int n, int* info) {
     __shared__ double ljj;
     __shared__ int fail;
     if (threadIdx.x == 0) fail = 0;
+    for (int j = 1 + threadIdx.x; j < n; j += blockDim.x) A[j].x = A[(size_t)j * n + j].x;
     __syncthreads();
+    const double rel = (double)n * 2.220446049250313e-16;
     for (int j = 0; j < n; ++j) {
         if (threadIdx.x == 0) {
             const double d = A[(size_t)j * n + j].x;
-            if (!(d > 0.0)) { fail = j + 1; }
+            const double d0 = j == 0 ? d : A[j].x;
+            if (!(d > 0.0) || !(d > rel * d0)) { fail = j + 1; }
             else {
                 ljj = sqrt(d);
                 A[(size_t)j * n + j] = make_double2(ljj, 0.0);

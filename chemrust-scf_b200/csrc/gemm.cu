@@ -13,6 +13,7 @@
 // B200 FP64 has no tcgen05 kind; both run on the FP64 tensor path
 // (mma.sync m8n8k4 .f64), the SIMT versions with 4x4 complex register tiles
 // per thread remain as the reference implementation of the same contract.
+#include <algorithm>
 #include "gemm.hpp"
 #include "launch_count.hpp"
 
@@ -376,13 +377,28 @@ k_gemm_tn(const double2* __restrict__ W, int ldw, const double2* __restrict__ X,
 
 }  // namespace
 
+// Two CTAs of k_zgemm_cn_dmma fit an SM, so the grid runs in waves of 296.
+// The split count that fills the last wave best wins (a larger one only
+// when it fills it 2 % better), with at least 256 k per split and 64 splits
+// at most.  E.g. the 256-projector x 160-band product (12 tiles) runs as 49
+// splits, 588 CTAs in two full waves, not as 25 splits, 300 CTAs in 1.01
+// waves; psi^H psi of 576 bands (81 tiles) as 18 splits, 1,458 CTAs in 4.93
+// waves, not as 4 splits, 324 CTAs in 1.09 waves.
 int splitk_count(int M, int N, int K) {
     const int tiles = ((M + BM - 1) / BM) * ((N + BN - 1) / BN);
-    int splits = (2 * 148 + tiles - 1) / tiles;
-    const int max_splits = (K + 255) / 256;  // at least 256 k per split
-    if (splits > max_splits) splits = max_splits;
-    if (splits < 1) splits = 1;
-    return splits;
+    const int max_splits = std::min(64, std::max(1, (K + 255) / 256));
+    int best = 1;
+    double best_eff = -1.0;
+    for (int s = 1; s <= max_splits; ++s) {
+        const long long ctas = (long long)tiles * s;
+        const long long waves = (ctas + 295) / 296;
+        const double eff = (double)ctas / (waves * 296.0);
+        if (eff > best_eff + 0.02) {
+            best_eff = eff;
+            best = s;
+        }
+    }
+    return best;
 }
 
 size_t splitk_partial_elems(int M, int N, int K) {
