@@ -197,111 +197,6 @@ k_small_gemm(const double2* __restrict__ A, const double2* __restrict__ B, doubl
     if (i < n && j < n) C[(size_t)i * n + j] = acc;
 }
 
-// Parallel cyclic Jacobi for a Hermitian n x n matrix (row-major, in place).
-// On exit diag(A) holds the eigenvalues and V the eigenvectors (columns).
-// scratch: [0] |A|_F^2, [1 + s] off-diagonal |A|^2 after sweep s; rot: 4 doubles per pair.
-__global__ void __launch_bounds__(256)
-k_jacobi(double2* A, double2* V, int n, int max_sweeps, double tol2, double* scratch,
-         double* rot, int* sweeps_out) {
-    cg::grid_group grid = cg::this_grid();
-    __shared__ double red[32];
-    const int lane = threadIdx.x & 31;
-    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    const size_t nn = (size_t)n * n;
-    const size_t gtid = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-    const size_t gstride = (size_t)gridDim.x * blockDim.x;
-    for (size_t t = gtid; t < nn; t += gstride)
-        V[t] = make_double2((t / n) == (t % n) ? 1.0 : 0.0, 0.0);
-    double tot = 0.0;
-    for (size_t t = gtid; t < nn; t += gstride) tot += A[t].x * A[t].x + A[t].y * A[t].y;
-    tot = block_sum(tot, red);
-    if (threadIdx.x == 0) atomicAdd(&scratch[0], tot);
-    grid.sync();
-    const double total = scratch[0];
-    const int m = n + (n & 1);
-    const int npairs = m / 2;
-    int sweep = 0;
-    for (; sweep < max_sweeps; ++sweep) {
-        for (int s = 0; s < m - 1; ++s) {
-            // ---- phase 1: rotation parameters + row update (rows p, q)
-            for (int pi = gw; pi < npairs; pi += nwarps) {
-                int a = pi == 0 ? 0 : 1 + ((pi - 1 + s) % (m - 1));
-                int b = 1 + ((m - 2 - pi + s) % (m - 1));
-                int p = min(a, b), q = max(a, b);
-                double c = 1.0, sn = 0.0, phr = 1.0, phi = 0.0;
-                const bool live = q < n;
-                if (live) {
-                    const double2 apq = A[(size_t)p * n + q];
-                    const double app = A[(size_t)p * n + p].x, aqq = A[(size_t)q * n + q].x;
-                    const double bm = hypot(apq.x, apq.y);
-                    if (bm > 1e-300 && bm > 1e-18 * sqrt(fabs(app * aqq))) {
-                        phr = apq.x / bm;
-                        phi = apq.y / bm;
-                        const double tau = (aqq - app) / (2.0 * bm);
-                        const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
-                        c = 1.0 / sqrt(1.0 + t * t);
-                        sn = t * c;
-                    }
-                }
-                __syncwarp();
-                if (lane == 0) {
-                    rot[4 * pi + 0] = c; rot[4 * pi + 1] = sn;
-                    rot[4 * pi + 2] = phr; rot[4 * pi + 3] = phi;
-                }
-                if (live && sn != 0.0) {
-                    // conj(g_qp) = -s ph, conj(g_qq) = c ph ; row' = G^H row
-                    for (int k = lane; k < n; k += 32) {
-                        const double2 apk = A[(size_t)p * n + k], aqk = A[(size_t)q * n + k];
-                        // ph * aqk
-                        const double2 pa = make_double2(phr * aqk.x - phi * aqk.y, phr * aqk.y + phi * aqk.x);
-                        A[(size_t)p * n + k] = make_double2(c * apk.x - sn * pa.x, c * apk.y - sn * pa.y);
-                        A[(size_t)q * n + k] = make_double2(sn * apk.x + c * pa.x, sn * apk.y + c * pa.y);
-                    }
-                }
-            }
-            grid.sync();
-            // ---- phase 2: column update (columns p, q) of A and V
-            for (int pi = gw; pi < npairs; pi += nwarps) {
-                int a = pi == 0 ? 0 : 1 + ((pi - 1 + s) % (m - 1));
-                int b = 1 + ((m - 2 - pi + s) % (m - 1));
-                int p = min(a, b), q = max(a, b);
-                if (q >= n) continue;
-                const double c = rot[4 * pi + 0], sn = rot[4 * pi + 1];
-                const double phr = rot[4 * pi + 2], phi = rot[4 * pi + 3];
-                if (sn == 0.0) continue;
-                // g_qp = -s conj(ph), g_qq = c conj(ph); col' = col G
-                for (int k = lane; k < n; k += 32) {
-                    const double2 akp = A[(size_t)k * n + p], akq = A[(size_t)k * n + q];
-                    const double2 qc = make_double2(phr * akq.x + phi * akq.y, phr * akq.y - phi * akq.x);
-                    A[(size_t)k * n + p] = make_double2(c * akp.x - sn * qc.x, c * akp.y - sn * qc.y);
-                    A[(size_t)k * n + q] = make_double2(sn * akp.x + c * qc.x, sn * akp.y + c * qc.y);
-                    const double2 vkp = V[(size_t)k * n + p], vkq = V[(size_t)k * n + q];
-                    const double2 vc = make_double2(phr * vkq.x + phi * vkq.y, phr * vkq.y - phi * vkq.x);
-                    V[(size_t)k * n + p] = make_double2(c * vkp.x - sn * vc.x, c * vkp.y - sn * vc.y);
-                    V[(size_t)k * n + q] = make_double2(sn * vkp.x + c * vc.x, sn * vkp.y + c * vc.y);
-                }
-                __syncwarp();
-                if (lane == 0) {
-                    A[(size_t)p * n + q] = make_double2(0.0, 0.0);
-                    A[(size_t)q * n + p] = make_double2(0.0, 0.0);
-                    A[(size_t)p * n + p].y = 0.0;
-                    A[(size_t)q * n + q].y = 0.0;
-                }
-            }
-            grid.sync();
-        }
-        double off = 0.0;
-        for (size_t t = gtid; t < nn; t += gstride)
-            if ((t / n) != (t % n)) off += A[t].x * A[t].x + A[t].y * A[t].y;
-        off = block_sum(off, red);
-        if (threadIdx.x == 0) atomicAdd(&scratch[1 + sweep], off);
-        grid.sync();
-        if (scratch[1 + sweep] <= tol2 * total) { ++sweep; break; }
-    }
-    if (gtid == 0) *sweeps_out = sweep;
-}
-
 // Circle-method pairing of step s over m = n + (n & 1) indices: pair i of
 // step s is (min(a, b), max(a, b)).
 // Every argument reduced below lies in (-(m - 1), 2 (m - 1)), so one

@@ -2,17 +2,16 @@
 // ZGEMM calls: chebyshev.rs:432-497 projectors, rayleigh_ritz.rs:74-142
 // subspace matrices, rayleigh_ritz.rs:209-227 rotation).  Two shapes:
 //
-//   gemm_cn_splitk:  P[s][m][n] = sum_{k in chunk s} conj(A[m][k]) B[n][k]
-//                    (A: M x K, B: N x K, both K-contiguous; long K split
-//                    across CTAs, partials reduced deterministically)
-//                    -> beta^H psi, psi^H H psi, psi^H psi
-//   gemm_tn:         O[m][n] = alpha sum_k W[k][m] X[k][n] + beta O[m][n]
-//                    (W: K x M, X: K x N, N-contiguous; short K)
-//                    -> beta (D beta^H psi), psi V
+//   gemm_cn:  P[s][m][n] = sum_{k in chunk s} conj(A[m][k]) B[n][k]
+//             (A: M x K, B: N x K, both K-contiguous; long K split across
+//             CTAs, partials reduced deterministically)
+//             -> beta^H psi, psi^H H psi, psi^H psi
+//   gemm_tn:  O[m][n] = alpha sum_k W[k][m] X[k][n] + beta O[m][n]
+//             (W: K x M, X: K x N, N-contiguous; short K)
+//             -> beta (D beta^H psi), psi V
 //
 // B200 FP64 has no tcgen05 kind; both run on the FP64 tensor path
-// (mma.sync m8n8k4 .f64), the SIMT versions with 4x4 complex register tiles
-// per thread remain as the reference implementation of the same contract.
+// (mma.sync m8n8k4 .f64).
 #include <algorithm>
 #include "gemm.hpp"
 #include "launch_count.hpp"
@@ -22,85 +21,6 @@ namespace chfsi {
 namespace {
 
 constexpr int BM = 64, BN = 64, BK = 16;
-
-__device__ __forceinline__ void cfma_conj(double2& acc, double2 a, double2 b) {
-    // acc += conj(a) * b
-    acc.x = fma(a.x, b.x, acc.x);
-    acc.x = fma(a.y, b.y, acc.x);
-    acc.y = fma(a.x, b.y, acc.y);
-    acc.y = fma(-a.y, b.x, acc.y);
-}
-__device__ __forceinline__ void cfma(double2& acc, double2 a, double2 b) {
-    acc.x = fma(a.x, b.x, acc.x);
-    acc.x = fma(-a.y, b.y, acc.x);
-    acc.y = fma(a.x, b.y, acc.y);
-    acc.y = fma(a.y, b.x, acc.y);
-}
-
-__global__ void __launch_bounds__(256, 2)
-k_gemm_cn_splitk(const double2* __restrict__ A, int lda, const double2* __restrict__ B, int ldb,
-                 int M, int N, int K, int kchunk, double2* __restrict__ part) {
-    __shared__ double2 As[BK][BM + 1];
-    __shared__ double2 Bs[BK][BN + 1];
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
-    const int kb = blockIdx.z * kchunk;
-    const int ke = min(K, kb + kchunk);
-    double2 acc[4][4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = make_double2(0.0, 0.0);
-    // loader mapping: row r = t / 4, k offset (t % 4) * 4; the next tile is
-    // fetched into registers while the current one is consumed from smem
-    const int lr = threadIdx.x >> 2, lk = (threadIdx.x & 3) * 4;
-    const int am = m0 + lr, bn_ = n0 + lr;
-    const double2* ap = A + (size_t)am * lda;
-    const double2* bp = B + (size_t)bn_ * ldb;
-    double2 ra[4], rb[4];
-    auto fetch = [&](int k0) {
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const int k = k0 + lk + i;
-            ra[i] = (am < M && k < ke) ? ap[k] : make_double2(0.0, 0.0);
-            rb[i] = (bn_ < N && k < ke) ? bp[k] : make_double2(0.0, 0.0);
-        }
-    };
-    if (kb < ke) fetch(kb);
-    for (int k0 = kb; k0 < ke; k0 += BK) {
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            As[lk + i][lr] = ra[i];
-            Bs[lk + i][lr] = rb[i];
-        }
-        __syncthreads();
-        if (k0 + BK < ke) fetch(k0 + BK);
-#pragma unroll
-        for (int k = 0; k < BK; ++k) {
-            double2 a[4], b[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] = As[k][ty + 16 * i];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) b[j] = Bs[k][tx + 16 * j];
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) cfma_conj(acc[i][j], a[i], b[j]);
-        }
-        __syncthreads();
-    }
-    double2* pp = part + (size_t)blockIdx.z * M * N;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const int m = m0 + ty + 16 * i;
-        if (m >= M) continue;
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int n = n0 + tx + 16 * j;
-            if (n < N) pp[(size_t)m * N + n] = acc[i][j];
-        }
-    }
-}
 
 // ---- FP64 tensor-core (DMMA) versions: mma.sync m8n8k4 .f64, one warp
 // issues 256 FMAs per instruction.  Complex products as four real MMAs on
@@ -306,72 +226,6 @@ __global__ void k_reduce_partials(const double2* __restrict__ part, int splits, 
             s.y += v.y;
         }
         out[i] = s;
-    }
-}
-
-__global__ void __launch_bounds__(256, 2)
-k_gemm_tn(const double2* __restrict__ W, int ldw, const double2* __restrict__ X, int ldx,
-          double2* O, int ldo, int M, int N, int K, double alpha, double beta) {
-    __shared__ double2 Ws[BK][BM];
-    __shared__ double2 Xs[BK][BN];
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    const int n0 = blockIdx.x * BN, m0 = blockIdx.y * BM;
-    double2 acc[4][4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = make_double2(0.0, 0.0);
-    // loader: 16 x 64 tile, thread t loads row k = t / 16, cols (t % 16) * 4 .. +3
-    const int lk = threadIdx.x >> 4, lc = (threadIdx.x & 15) * 4;
-    double2 rw[4], rx[4];
-    auto fetch = [&](int k0) {
-        const int k = k0 + lk;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const int m = m0 + lc + i, n = n0 + lc + i;
-            rw[i] = (k < K && m < M) ? W[(size_t)k * ldw + m] : make_double2(0.0, 0.0);
-            rx[i] = (k < K && n < N) ? X[(size_t)k * ldx + n] : make_double2(0.0, 0.0);
-        }
-    };
-    fetch(0);
-    for (int k0 = 0; k0 < K; k0 += BK) {
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            Ws[lk][lc + i] = rw[i];
-            Xs[lk][lc + i] = rx[i];
-        }
-        __syncthreads();
-        if (k0 + BK < K) fetch(k0 + BK);
-#pragma unroll
-        for (int kk = 0; kk < BK; ++kk) {
-            double2 a[4], b[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] = Ws[kk][ty + 16 * i];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) b[j] = Xs[kk][tx + 16 * j];
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) cfma(acc[i][j], a[i], b[j]);
-        }
-        __syncthreads();
-    }
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const int m = m0 + ty + 16 * i;
-        if (m >= M) continue;
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int n = n0 + tx + 16 * j;
-            if (n >= N) continue;
-            double2* o = O + (size_t)m * ldo + n;
-            double2 r = make_double2(alpha * acc[i][j].x, alpha * acc[i][j].y);
-            if (beta != 0.0) {
-                r.x += beta * o->x;
-                r.y += beta * o->y;
-            }
-            *o = r;
-        }
     }
 }
 
