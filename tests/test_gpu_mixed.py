@@ -1,8 +1,8 @@
-"""Mixed-precision ChFSI (FP32 filter; projector, overlap, subspace and
-rotation GEMMs on tcgen05 in BF16 3-way split with FP32 accumulation; FP64
-Cholesky and eigensolve) against the FP64 oracle.  Errors are reported per
-result; the SCF test holds the north-star bar: converged energy and occupied
-eigenvalues within 1e-6 Ha of the FP64 run."""
+"""Mixed-precision ChFSI (FP32 filter with the projector GEMMs on tcgen05 in
+BF16 3-way split with FP32 accumulation; FP64 Rayleigh-Ritz, Cholesky and
+eigensolve) against the FP64 oracle.  Errors are reported per result; the SCF
+test holds the precision bar: converged energy and occupied eigenvalues within
+1e-6 Ha of the FP64 run."""
 import numpy as np
 import pytest
 

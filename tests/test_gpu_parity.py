@@ -1,7 +1,7 @@
 """Parity of the CUDA path (through the C ABI) against the CPU oracle.
 
 FP64 tolerances: H|psi> 1e-12 relative; filtered psi 1e-10 relative;
-eigenvalues and energies 1e-10 Ha (north-star bar for the plain FP64 method).
+eigenvalues and energies 1e-10 Ha (the bar for the plain FP64 method).
 """
 import json
 import os
