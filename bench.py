@@ -7,11 +7,21 @@ degree-16 Chebyshev filter (17 H|psi> applies per band incl. the final one
 for Rayleigh-Ritz) followed by Rayleigh-Ritz.  Metric: H|psi> band-applies
 per second (n_bands x 17 per step).
 
+At N = 1 the line also carries the time-to-SCF of the 216-atom ultrasoft
+cell (n_pw 173,925, 576 bands, 1,728 projectors, 108^3 / 144^3 grids):
+FP64 + Pulay, mixed precision + Pulay and mixed precision + the learned
+mixer, each stopped at |dE| < 1e-6 Ha/atom with the occupied eigenvalues
+changing by less than 1e-7 Ha, and each compared with the FP64 run
+continued (untimed) to tight convergence.
+
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 --impl reference times the reference's algorithm on the host CPU (the C++
-oracle restatement; the reference crate itself cannot be built here) on a
-bounded sample of the same workload, with all host threads.
+oracle restatement; the reference crate itself cannot be built here) on the
+same step: the degree-16 filter of one band per host thread (scaled by the
+per-band cost to all 160 bands) plus the Rayleigh-Ritz of all 160 bands.
+It loads only the oracle library (the inputs come from the oracle's copy of
+the seeded generator).
 For N > 1 (torchrun) every rank runs an independent replica of the workload
 (weak scaling, no collective on the data path); the value is the total over
 ranks divided by the slowest rank's time.
@@ -43,6 +53,15 @@ def peaks():
         return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except Exception:
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "fallback": True}
+
+
+def bench_config(s, world):
+    """The workload description shared by both arms (identical dicts)."""
+    return {"workload": "64-atom KB-projector cell, a=20.52 bohr, Ecut 20 Ha, n_pw=%d, grid "
+                        "72^3, 160 bands, 256 projectors, degree 16, FP64" % s.n_pw,
+            "n_pw": s.n_pw, "n_bands": s.n_bands, "ndeg": NDEG, "grid": list(s.ngrid),
+            "n_proj": s.n_proj, "parallelism": "replicas" if world > 1 else "single",
+            "l2": "working set (psi 95 MB + beta 152 MB + sticks 250 MB) exceeds the 126 MB L2"}
 
 
 class ClockSampler:
@@ -255,61 +274,28 @@ def run_ours(args):
                  "unit": UNIT, "ms_per_step": round(mms / args.steps, 3),
                  "dtype": "f32 filter (bf16x3 tcgen05 projector GEMMs, fp32 accumulate), f64 Rayleigh-Ritz"}
         mctx.close()
-        if not args.no_scf:
+        if not args.no_scf and world == 1:
             import learned_mixer
-            res = {}
-            arms = (("fp64", chfsi.PREC_FP64, chfsi.MIXER_PULAY),
-                    ("mixed", chfsi.PREC_MIXED, chfsi.MIXER_PULAY),
-                    ("mixed_learned", chfsi.PREC_MIXED, chfsi.MIXER_LEARNED_PULAY))
-            mixer_net = learned_mixer.load(device=local)
-            for name, prec, mode in arms:
-                sctx = chfsi.Context(s, device=local, precision=prec)
-                if mode != chfsi.MIXER_PULAY:
-                    sctx.set_mixer(mixer_net)
-                # FP64 only for the final confirming iterations of the mixed runs
-                r = sctx.run_scf(NDEG, tol_per_atom=1e-6, max_iter=60, kT=0.01, mixer=mode,
-                                 fp64_switch_per_atom=1e-6)
-                res[name] = r
-                sctx.close()
-            f = res["fp64"]
-            tts = {"criterion": "|dE| < 1e-6 Ha/atom (Fermi-Dirac kT = 0.01 Ha, Pulay 0.3/6)",
-                   "fp64_s": round(f["seconds"], 4), "fp64_iterations": f["n_iter"]}
-            for name in ("mixed", "mixed_learned"):
-                m = res[name]
-                tts.update({
-                    name + "_s": round(m["seconds"], 4), name + "_iterations": m["n_iter"],
-                    name + "_iterations_in_mixed_precision": m["n_iter_mixed"],
-                    name + "_speedup": round(f["seconds"] / m["seconds"], 3) if m["seconds"] > 0 else None,
-                    name + "_energy_diff_per_atom_Ha": abs(f["e_total"] - m["e_total"]) / s.n_atoms,
-                    name + "_max_occupied_eigenvalue_diff_Ha":
-                        float(np.abs(f["eigenvalues"][:s.n_occ] - m["eigenvalues"][:s.n_occ]).max()),
-                })
-            tts["converged"] = [bool(res[k]["converged"]) for k in ("fp64", "mixed", "mixed_learned")]
-            tts["note"] = ("runs stopped by the same |dE| rule end on different trajectories; "
-                           "precision_check compares them converged to 1e-9 Ha/atom")
-            mixed["time_to_scf"] = tts
-            # precision effect alone: FP64 and mixed, both with the learned mixer (which
-            # converges to 1e-9 Ha/atom where plain Pulay stalls), far below the SCF
-            # noise of the rule above
-            tight = {}
-            for name, prec, mode in (("fp64", chfsi.PREC_FP64, chfsi.MIXER_LEARNED_PULAY), arms[2]):
-                sctx = chfsi.Context(s, device=local, precision=prec)
-                if mode != chfsi.MIXER_PULAY:
-                    sctx.set_mixer(mixer_net)
-                tight[name] = sctx.run_scf(NDEG, tol_per_atom=1e-9, max_iter=80, kT=0.01,
-                                           mixer=mode, fp64_switch_per_atom=1e-6)
-                sctx.close()
-            a, b = tight["fp64"], tight["mixed_learned"]
-            mixed["precision_check"] = {
-                "tol_per_atom": 1e-9, "arms": "fp64 + learned mixer vs mixed + learned mixer", "converged": [bool(a["converged"]), bool(b["converged"])],
-                "energy_diff_per_atom_Ha": abs(a["e_total"] - b["e_total"]) / s.n_atoms,
-                "max_occupied_eigenvalue_diff_Ha":
-                    float(np.abs(a["eigenvalues"][:s.n_occ] - b["eigenvalues"][:s.n_occ]).max()),
-            }
+            net = learned_mixer.load(device=local)
+            mixed["time_to_scf"] = time_to_scf(chfsi, s, NDEG, local, net, max_iter=80,
+                                               tight_max_iter=80)
+
+    # ---- headline: time-to-SCF of the 216-atom ultrasoft cell (N = 1 only) ----
+    scf216 = None
+    if world == 1 and not args.no_scf and not args.no_scf_216:
+        import learned_mixer
+        s2 = chfsi.SyntheticSystem(config_index=2)
+        net = learned_mixer.load(device=local)
+        scf216 = time_to_scf(chfsi, s2, 16, local, net, max_iter=args.scf_216_max_iter,
+                             tight_max_iter=60)
+        scf216["workload"] = ("216-atom ultrasoft cell, a=30.78 bohr, Ecut 25 Ha, n_pw=%d, "
+                              "grid 108^3 (density 144^3), %d bands, %d projectors, degree 16"
+                              % (s2.n_pw, s2.n_bands, s2.n_proj))
+        del s2
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(s, seconds=args.cpu_seconds)
+        cpu = cpu_baseline(steps=2)
 
     if rank == 0:
         line = {
@@ -317,19 +303,15 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded 64-atom diamond cell; per-rank replica)",
-            "config": {"workload": "64-atom KB-projector cell, a=20.52 bohr, Ecut 20 Ha, "
-                                   "n_pw=%d, grid 72^3, 160 bands, 256 projectors, degree 16, FP64"
-                                   % s.n_pw,
-                       "n_pw": s.n_pw, "n_bands": nb, "ndeg": NDEG, "grid": list(s.ngrid),
-                       "n_proj": s.n_proj, "parallelism": "replicas" if world > 1 else "single",
-                       "launch_config": int(tune_choice),
-                       "l2": "working set (psi 95 MB + beta 152 MB + sticks 250 MB) exceeds the 126 MB L2"},
+            "config": bench_config(s, world),
+            "launch_config": int(tune_choice),
             "clocks": clk.summary(),
             "e2e": e2e,
             "gpu_launches": int(launches),
             "roofline": roofline,
             "cpu_baseline": cpu,
             "mixed_precision": mixed,
+            "time_to_scf_216atom": scf216,
         }
         print(json.dumps(line))
     if dist:
@@ -338,73 +320,134 @@ def run_ours(args):
     ctx.close()
 
 
+# time-to-SCF stopping rule of every timed arm, and the tight FP64 reference
+SCF_TOL_PER_ATOM = 1e-6   # |dE| per atom (Ha)
+SCF_TOL_EIG = 1e-7        # change of the occupied eigenvalues between iterations (Ha)
+TIGHT_TOL_PER_ATOM = 1e-10
+TIGHT_TOL_EIG = 1e-9
+
+
+def time_to_scf(chfsi, s, ndeg, device, net, max_iter, tight_max_iter):
+    """FP64 + Pulay, mixed + Pulay and mixed + learned-preconditioned Pulay,
+    each from the uniform density to the stopping rule (device seconds of the
+    SCF loop, context set-up excluded); the FP64 run is then continued,
+    untimed, to tight convergence, and every arm's energy and occupied
+    eigenvalues are compared with that reference."""
+    import numpy as np
+    arms = (("fp64", chfsi.PREC_FP64, chfsi.MIXER_PULAY),
+            ("mixed", chfsi.PREC_MIXED, chfsi.MIXER_PULAY),
+            ("mixed_learned", chfsi.PREC_MIXED, chfsi.MIXER_LEARNED_PULAY))
+    res, setup, tight = {}, {}, None
+    for name, prec, mode in arms:
+        t0 = time.time()
+        ctx = chfsi.Context(s, device=device, precision=prec)
+        setup[name] = time.time() - t0
+        if mode != chfsi.MIXER_PULAY:
+            ctx.set_mixer(net)
+        res[name] = ctx.run_scf(ndeg, tol_per_atom=SCF_TOL_PER_ATOM, tol_eig=SCF_TOL_EIG,
+                                max_iter=max_iter, kT=0.01, mixer=mode,
+                                fp64_switch_per_atom=SCF_TOL_PER_ATOM)
+        if name == "fp64":
+            tight = ctx.run_scf(ndeg, tol_per_atom=TIGHT_TOL_PER_ATOM, tol_eig=TIGHT_TOL_EIG,
+                                max_iter=tight_max_iter, kT=0.01, restart=True)
+        ctx.close()
+    n_occ = s.n_occ
+    out = {"criterion": "|dE| < %g Ha/atom and occupied eigenvalues changing by < %g Ha "
+                        "(Fermi-Dirac kT = 0.01 Ha; Pulay alpha 0.3, history 6)"
+                        % (SCF_TOL_PER_ATOM, SCF_TOL_EIG),
+           "reference": "FP64 run continued to |dE| < %g Ha/atom and eigenvalue changes < %g Ha"
+                        % (TIGHT_TOL_PER_ATOM, TIGHT_TOL_EIG),
+           "reference_converged": bool(tight["converged"]),
+           "reference_extra_iterations": tight["n_iter"],
+           "arms": {}}
+    f = res["fp64"]
+    for name, r in res.items():
+        a = {"seconds": round(r["seconds"], 3), "iterations": r["n_iter"],
+             "iterations_in_mixed_precision": r["n_iter_mixed"], "converged": bool(r["converged"]),
+             "setup_seconds": round(setup[name], 2),
+             "energy_error_per_atom_Ha": abs(r["e_total"] - tight["e_total"]) / s.n_atoms,
+             "max_occupied_eigenvalue_error_Ha":
+                 float(np.abs(r["eigenvalues"][:n_occ] - tight["eigenvalues"][:n_occ]).max()),
+             "fp64_retries": r["n_fp64_retries"]}
+        if name == "mixed_learned":
+            a["learned_steps"] = r["n_iter_learned"]
+            a["fell_back_to_pulay"] = bool(r["fell_back"])
+        if name != "fp64":
+            a["speedup_vs_fp64"] = round(f["seconds"] / r["seconds"], 3) if r["seconds"] > 0 else None
+        out["arms"][name] = a
+    return out
+
+
 def _get_psi_into(ctx, out):
     import ctypes as C
     import chfsi
     ctx._c(chfsi.lib().chfsi_get_psi(ctx.handle, out.ctypes.data_as(C.c_void_p)))
 
 
-def cpu_baseline(s, seconds=15.0, steps=1):
-    """Oracle (C++/OpenMP restatement) H|psi> band-applies/s on a bounded sample."""
+def reference_steps(steps, warmup):
+    """The reference's ChFSI iteration on the host cores (the C++/OpenMP
+    oracle restatement of chebyshev.rs:626-816 + rayleigh_ritz.rs:48-245),
+    inputs from the oracle's own copy of the seeded generator (the CUDA
+    library is not loaded).  Each step runs the degree-16 filter on one band
+    per host thread (the oracle parallelises over bands) and the
+    Rayleigh-Ritz of all 160 bands; the step time is the filter time scaled
+    by the per-band cost to 160 bands plus the Rayleigh-Ritz time.
+    Returns (seconds per full-step equivalent list, cores, sample text, system)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import numpy as np
     import oracle
-    o = oracle.Oracle.from_system(s)
+    import synth
+    s = synth.System(config_index=CONFIG_INDEX)
+    cores = oracle.lib().oracle_num_threads()
+    nb = s.n_bands
+    nb_s = max(1, min(nb, cores))
+    psi0 = s.psi0()
     rho0 = np.full(s.ng, s.n_elec / s.omega)
-    o.build_veff(rho0)
-    psi = s.psi0()
-    nb = 8
-    o.apply_h(psi[:nb])  # warm
-    done, t0 = 0, time.perf_counter()
-    while True:
-        o.apply_h(psi[:nb])
-        done += nb
-        el = time.perf_counter() - t0
-        if el >= seconds:
-            break
-    return {"value": round(done / el, 2), "unit": UNIT, "cores": oracle.lib().oracle_num_threads(),
-            "kind": "port",
-            "sample": "%d band-applies of full H|psi> (T + V_loc + V_NL) on the same 64-atom cell, "
-                      "%.1f s" % (done, el)}
+    args = (s.ngrid, s.miller(), s.kinetic(), s.beta(), s.proj_offsets(), s.dmat())
+    tail = (s.vloc_g(), s.omega, s.gmax, s.e_ewald, s.n_atoms)
+    o_f = oracle.Oracle(*args, psi0[:nb_s], s.occupations()[:nb_s], *tail)
+    o_rr = oracle.Oracle(*args, psi0, s.occupations(), *tail)
+    o_f.build_veff(rho0)
+    o_rr.build_veff(rho0)
+    o_rr.chebyshev_filter(0)  # H|psi> of all bands for the Rayleigh-Ritz (untimed set-up)
+    times = []
+    for i in range(warmup + steps):
+        o_f.set_psi(psi0[:nb_s])
+        t0 = time.perf_counter()
+        o_f.chebyshev_filter(NDEG)
+        t1 = time.perf_counter()
+        o_rr.rayleigh_ritz()
+        t2 = time.perf_counter()
+        if i >= warmup:
+            times.append((t1 - t0) * nb / nb_s + (t2 - t1))
+    sample = ("per step: degree-16 filter of %d of the %d bands (one per thread), scaled by "
+              "%d/%d, plus Rayleigh-Ritz of all %d bands, same 64-atom cell" % (nb_s, nb, nb, nb_s, nb))
+    return times, cores, sample, s
+
+
+def cpu_baseline(steps=2):
+    """The reference arm's measurement (reference_steps) on a short sample."""
+    times, cores, sample, s = reference_steps(steps, 1)
+    value = s.n_bands * (NDEG + 1) * len(times) / sum(times)
+    return {"value": round(value, 2), "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": sample + "; %d steps" % len(times)}
 
 
 def run_reference(args):
     rank, world, local = dist_env()
     if rank != 0:
         return
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import numpy as np
-    import chfsi
-    import oracle
-    s = chfsi.SyntheticSystem(config_index=CONFIG_INDEX)
-    # sample: a 16-band slice of the workload, degree-16 filter (17 applies/band)
-    nb = 16
-    o = oracle.Oracle(s.ngrid, s.miller(), s.kinetic(), s.beta(), s.proj_offsets(), s.dmat(),
-                      s.psi0()[:nb], s.occupations()[:nb], s.vloc_g(), s.omega, s.gmax,
-                      s.e_ewald, s.n_atoms)
-    o.build_veff(np.full(s.ng, s.n_elec / s.omega))
-    for _ in range(args.warmup):
-        o.set_psi(s.psi0()[:nb])
-        o.chebyshev_filter(NDEG)
-    t = []
-    for _ in range(args.steps):
-        o.set_psi(s.psi0()[:nb])
-        t0 = time.perf_counter()
-        o.chebyshev_filter(NDEG)
-        t.append(time.perf_counter() - t0)
-    tot = sum(t)
-    value = nb * (NDEG + 1) * args.steps / tot
-    cores = oracle.lib().oracle_num_threads()
+    times, cores, sample, s = reference_steps(args.steps, args.warmup)
+    tot = sum(times)
+    value = s.n_bands * (NDEG + 1) * args.steps / tot
     line = {"impl": "reference", "metric": METRIC, "value": round(value, 2), "unit": UNIT,
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(tot / args.steps * 1e3, 1), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded 64-atom diamond cell)",
-            "config": {"workload": "64-atom KB-projector cell, a=20.52 bohr, Ecut 20 Ha, "
-                                   "n_pw=%d, grid 72^3, 160 bands, 256 projectors, degree 16, FP64"
-                                   % s.n_pw, "parallelism": "host CPU"},
+            "data": "synthetic (seeded 64-atom diamond cell; per-rank replica)",
+            "config": bench_config(s, world),
             "cpu_baseline": {"value": round(value, 2), "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": "degree-16 Chebyshev filter of a 16-band slice per step"},
+                             "sample": sample},
             "e2e": {"value": round(value, 2), "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -458,10 +501,12 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--fp64-only", action="store_true", help="skip the mixed-precision lines")
-    ap.add_argument("--no-scf", action="store_true", help="skip the time-to-SCF comparison")
+    ap.add_argument("--no-scf", action="store_true", help="skip every time-to-SCF comparison")
+    ap.add_argument("--no-scf-216", action="store_true",
+                    help="skip the 216-atom time-to-SCF comparison (about ten minutes)")
+    ap.add_argument("--scf-216-max-iter", type=int, default=120)
     ap.add_argument("--profile", choices=["local", "fp64", "mixed", "fp64-216", "mixed-216"],
                     default=None,
                     help="a short fixed workload for ncu captures (no JSON line): two local "

@@ -25,7 +25,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libchfsi_b200.so")
 
 OK, NOT_CONVERGED, NOT_IMPLEMENTED, CHEB_DIVERGED, RR_FAILED, CUDA_ERROR, BAD_INPUT, \
-    NO_DEVICE, OUT_OF_MEMORY, NUMERIC = 0, -1, -2, -3, -4, -5, -6, -7, -8, -9
+    NO_DEVICE, OUT_OF_MEMORY, NUMERIC, TIMEOUT = 0, -1, -2, -3, -4, -5, -6, -7, -8, -9, -10
+INJECT_NONE, INJECT_TC_NO_LOADS, INJECT_ALLOC_FAIL = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
 BOUND_HEURISTIC, BOUND_LANCZOS = 0, 1
 MIXER_PULAY, MIXER_LEARNED, MIXER_LEARNED_PULAY = 0, 1, 2
@@ -72,9 +73,15 @@ class NumericError(ChfsiError):
     status = NUMERIC
 
 
+class Timeout(ChfsiError):
+    """A bounded device-side wait ran out; the kernel retired what it had
+    issued and returned, so the context stays usable."""
+    status = TIMEOUT
+
+
 _ERRORS = {c.status: c for c in (NotConverged, NotImplementedErr, ChebyshevDiverged,
                                   RayleighRitzFailed, CudaError, BadInput, NoDevice, OutOfMemory,
-                                  NumericError)}
+                                  NumericError, Timeout)}
 
 
 class SynthParams(C.Structure):
@@ -111,7 +118,7 @@ class ScfParams(C.Structure):
                 ("alpha", C.c_double), ("max_hist", C.c_int), ("first_passes", C.c_int),
                 ("kT", C.c_double), ("fp64_switch_per_atom", C.c_double),
                 ("mixer", C.c_int), ("cg_steps", C.c_int), ("trace", C.POINTER(C.c_double)),
-                ("verbose", C.c_int), ("reserved", C.c_int)]
+                ("verbose", C.c_int), ("restart", C.c_int), ("tol_eig", C.c_double)]
 
 
 class ScfResult(C.Structure):
@@ -164,6 +171,7 @@ def lib():
         "chfsi_get_psi": [vp, vp],
         "chfsi_apply_h": [vp, vp, vp, C.c_int],
         "chfsi_apply_h_local": [vp, vp, vp, C.c_int],
+        "chfsi_apply_sinv_h": [vp, vp, vp, C.c_int],
         "chfsi_get_stream": [vp, C.POINTER(vp)],
         "chfsi_zgemm_cn": [vp, C.c_int, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp],
         "chfsi_zgemm_cn_bf16x3": [vp, C.c_int, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp],
@@ -202,6 +210,7 @@ def lib():
         "chfsi_batch_graph_nodes": [vp, C.POINTER(C.c_size_t)],
         "chfsi_autotune": [vp, C.POINTER(C.c_int), fp],
         "chfsi_set_launch_config": [vp, C.c_int],
+        "chfsi_test_inject": [C.c_int, C.c_longlong],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -334,6 +343,13 @@ def zgemm_cn_bf16x3(a_dev, lda, b_dev, ldb, m, n, k, c_dev, stream=0):
                                        C.c_void_p(c_dev), C.c_void_p(stream)))
 
 
+def inject_fault(what, arg=0):
+    """Host-side fault injection for error-path tests (INJECT_TC_NO_LOADS:
+    the next `arg` tensor-core GEMM launches issue no loads and time out;
+    INJECT_ALLOC_FAIL: the arg-th device allocation fails; INJECT_NONE clears)."""
+    _check(lib().chfsi_test_inject(what, arg))
+
+
 def launch_count():
     """Kernels launched by the library since it was loaded."""
     return int(lib().chfsi_launch_count())
@@ -359,12 +375,21 @@ def _ptr(a, ctype=None):
 class SyntheticSystem:
     """Seeded synthetic plane-wave system (lattice, G-sphere, V_loc, projectors, psi0)."""
 
+    @staticmethod
+    def _L():
+        """The library whose generator builds the system."""
+        return lib()
+
+    @staticmethod
+    def _chk(st):
+        _check(st)
+
     def __init__(self, params=None, config_index=None, **overrides):
-        L = lib()
+        L = self._L()
         if params is None:
             params = SynthParams()
-            _check(L.chfsi_synth_defaults(0 if config_index is None else config_index,
-                                          C.byref(params)))
+            self._chk(L.chfsi_synth_defaults(0 if config_index is None else config_index,
+                                             C.byref(params)))
         for k, v in overrides.items():
             if k in ("ngrid", "rc_proj", "kpt", "ngrid_density"):
                 arr = getattr(params, k)
@@ -374,10 +399,10 @@ class SyntheticSystem:
                 setattr(params, k, v)
         self.params = params
         h = C.c_void_p()
-        _check(L.chfsi_system_generate(C.byref(params), C.byref(h)))
+        self._chk(L.chfsi_system_generate(C.byref(params), C.byref(h)))
         self.handle = h
         info = SystemInfo()
-        _check(L.chfsi_system_get_info(h, C.byref(info)))
+        self._chk(L.chfsi_system_get_info(h, C.byref(info)))
         self.info = info
         self.ngrid = tuple(info.ngrid)
         self.n_pw, self.n_bands, self.n_occ = info.n_pw, info.n_bands, info.n_occ
@@ -395,7 +420,7 @@ class SyntheticSystem:
 
     def _get(self, fn, shape, dtype, ctype=None):
         a = np.zeros(shape, dtype=dtype)
-        _check(getattr(lib(), fn)(self.handle, _ptr(a, ctype)))
+        self._chk(getattr(self._L(), fn)(self.handle, _ptr(a, ctype)))
         return a
 
     @property
@@ -566,6 +591,11 @@ class Context:
         self._c(lib().chfsi_apply_h(self.handle, C.c_void_p(psi_dev_ptr),
                                     C.c_void_p(hpsi_dev_ptr), nb))
 
+    def apply_sinv_h(self, psi_dev_ptr, out_dev_ptr, nb):
+        """S^-1 H|psi> (ultrasoft; H|psi> without q) on device pointers."""
+        self._c(lib().chfsi_apply_sinv_h(self.handle, C.c_void_p(psi_dev_ptr),
+                                         C.c_void_p(out_dev_ptr), nb))
+
     def apply_h_local(self, psi_dev_ptr, hpsi_dev_ptr, nb):
         """T + V_loc only, on device pointers."""
         self._c(lib().chfsi_apply_h_local(self.handle, C.c_void_p(psi_dev_ptr),
@@ -629,12 +659,16 @@ class Context:
 
     def run_scf(self, ndeg, tol_per_atom=1e-6, max_iter=30, alpha=0.3, max_hist=6,
                 first_passes=4, kT=0.01, fp64_switch_per_atom=1e-4, raise_not_converged=False,
-                mixer=MIXER_PULAY, trace=False, cg_steps=0, verbose=False):
+                mixer=MIXER_PULAY, trace=False, cg_steps=0, verbose=False, tol_eig=0.0,
+                restart=False):
         """Full SCF; mixer is MIXER_PULAY or, after set_mixer(), MIXER_LEARNED /
-        MIXER_LEARNED_PULAY.  trace=True also returns rho_in and rho_out of every
-        iteration (n_iter x N^3 each) as 'trace_in' / 'trace_out'."""
+        MIXER_LEARNED_PULAY.  tol_eig > 0 adds the occupied-eigenvalue change test;
+        restart=True continues from this context's last state.  trace=True also
+        returns rho_in and rho_out of every iteration (n_iter x N^3 each) as
+        'trace_in' / 'trace_out'."""
         p = ScfParams(ndeg, max_iter, tol_per_atom, alpha, max_hist, first_passes, kT,
-                      fp64_switch_per_atom, mixer, cg_steps, None, int(verbose), 0)
+                      fp64_switch_per_atom, mixer, cg_steps, None, int(verbose), int(restart),
+                      tol_eig)
         tr = None
         if trace:
             tr = np.zeros((max_iter, 2, self.ng_density))

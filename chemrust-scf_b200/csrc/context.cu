@@ -22,6 +22,7 @@
 #include "system.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <complex>
 #include <cstdio>
@@ -138,7 +139,8 @@ k_cheb_combine(const C* __restrict__ hx, const C* __restrict__ corr, const C* __
         const C p = x[i];
         const R sr = hr * ie + nc * p.x, si = hi * ie + nc * p.y;
         R orr, oi;
-        if (mode == 1) { orr = sr; oi = si; }
+        if (mode == 0) { orr = hr; oi = hi; }  // plain S^-1 H x
+        else if (mode == 1) { orr = sr; oi = si; }
         else {
             const C prev = out[i];
             orr = (R)2 * sr - prev.x;
@@ -276,9 +278,15 @@ void digit_reversal(const AxisPlan& P, std::vector<int>& pos) {
     }
 }
 
+// Test hook (chfsi_test_inject): device allocations left before one fails
+// with cudaErrorMemoryAllocation; negative = no failure planned.
+std::atomic<long long> g_alloc_fail_in{-1};
+
 template <typename T> cudaError_t dalloc(T** p, size_t n) {
     *p = nullptr;
     if (n == 0) return cudaSuccess;
+    if (g_alloc_fail_in.load() >= 0 && g_alloc_fail_in.fetch_sub(1) == 0)
+        return cudaErrorMemoryAllocation;
     return cudaMalloc((void**)p, n * sizeof(T));
 }
 
@@ -384,6 +392,8 @@ struct chfsi_ctx {
     double2* d_sx = nullptr;     // n_bands x n_pw scratch
     // mixed precision (FP32 filter, tcgen05 BF16x3 GEMMs)
     bool mixed = false;          // configured precision
+    bool scf_done = false;       // a chfsi_scf_run left density, psi and eigenvalues
+    double scf_e_last = 0.0;     // its last total energy (restart reference)
     bool mixed_active = false;   // current filter precision (SCF may switch to FP64)
     float2* d_psi32a = nullptr; float2* d_psi32b = nullptr; float2* d_psi32 = nullptr;
     float2* d_hpsi32 = nullptr; float2* d_nl32 = nullptr; float2* d_work32 = nullptr;
@@ -824,7 +834,10 @@ chfsi_status finish_diag(chfsi_ctx* ctx, double* eig_out, bool have_rr) {
     if (ctx->d_tc_err)
         CK(cudaMemcpyAsync(&tc_err, ctx->d_tc_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
-    if (tc_err) return ctx->fail(CHFSI_ERR_CUDA, "tensor-core GEMM pipeline wait timed out");
+    if (tc_err) {
+        CK(cudaMemsetAsync(ctx->d_tc_err, 0, sizeof(int), ctx->st));
+        return ctx->fail(CHFSI_ERR_TIMEOUT, "tensor-core GEMM pipeline wait timed out");
+    }
     std::memcpy(ctx->h_coef, h + n, sizeof(double) * 6);
     int flags[4];
     std::memcpy(flags, h + n + 6, sizeof(flags));
@@ -1902,6 +1915,38 @@ chfsi_status chfsi_get_stream(chfsi_ctx* ctx, void** out) {
 
 long long chfsi_launch_count(void) { return g_launch_count.load(); }
 
+// S^-1 H x of the generalised (ultrasoft) problem, the operator the filter
+// applies (Woodbury inverse S^-1 = 1 - beta M beta^H); H x alone without q.
+chfsi_status chfsi_apply_sinv_h(chfsi_ctx* ctx, const chfsi_c128* psi_dev, chfsi_c128* out_dev,
+                                int nb) {
+    chfsi_status s = ready(ctx);
+    if (s) return s;
+    if (!psi_dev || !out_dev || nb <= 0 || nb > ctx->nb) return CHFSI_ERR_BAD_INPUT;
+    const double2* x = reinterpret_cast<const double2*>(psi_dev);
+    double2* out = reinterpret_cast<double2*>(out_dev);
+    if (!ctx->uspp) {
+        s = apply_h_dev(ctx, x, out, nb, kEpiApply, nullptr);
+    } else {
+        s = apply_h_dev(ctx, x, ctx->d_hpsi, nb, kEpiApply, nullptr);
+        if (s) return s;
+        cudaStream_t st = ctx->st;
+        gemm_cn(ctx->d_beta, ctx->n_pw, ctx->d_hpsi, ctx->n_pw, ctx->np, nb, ctx->n_pw,
+                ctx->d_part, ctx->d_cp, st);
+        gemm_tn(ctx->d_sinvT, ctx->np, ctx->d_cp, nb, ctx->d_cq, nb, ctx->np, nb, ctx->np, 1.0,
+                0.0, st);
+        gemm_tn(ctx->d_cq, nb, ctx->d_beta, ctx->n_pw, ctx->d_sx, ctx->n_pw, nb, ctx->n_pw,
+                ctx->np, 1.0, 0.0, st);
+        const size_t n = (size_t)nb * ctx->n_pw;
+        count_launch();
+        k_cheb_combine<double2><<<grid_for(n), 256, 0, st>>>(ctx->d_hpsi, ctx->d_sx, x, out, n,
+                                                             ctx->d_coef, 0, nullptr);
+        CK(cudaGetLastError());
+    }
+    if (s) return s;
+    CK(cudaStreamSynchronize(ctx->st));
+    return CHFSI_OK;
+}
+
 chfsi_status chfsi_apply_h(chfsi_ctx* ctx, const chfsi_c128* psi_dev, chfsi_c128* hpsi_dev, int nb) {
     chfsi_status s = ready(ctx);
     if (s) return s;
@@ -2250,8 +2295,11 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
     const double dv = ctx->omega / (double)ng;
     cudaStream_t st = ctx->st;
     const double n_elec = ctx->n_elec;
-    count_launch();
-    k_fill<<<grid_for(ng), 256, 0, st>>>(ctx->d_rho_in, ng, n_elec / ctx->omega);
+    const bool restart = p->restart != 0 && ctx->scf_done;
+    if (!restart) {
+        count_launch();
+        k_fill<<<grid_for(ng), 256, 0, st>>>(ctx->d_rho_in, ng, n_elec / ctx->omega);
+    }
     PulayState ps;
     chfsi_status s = ensure_pinned(ctx, (size_t)ctx->nb + 64 + ctx->max_deg);
     if (s) return s;
@@ -2263,9 +2311,12 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
     bool have_prev = false, fell_back = false;
     int rises = 0;
     double r_prev = -1.0;
-    std::vector<double> eig(ctx->nb);
-    bool have_eig = false;
-    double e_prev = 0.0;
+    std::vector<double> eig(ctx->nb), eig_prev(ctx->nb);
+    bool have_eig = restart;
+    if (restart)
+        CK(copy_sync(eig.data(), ctx->d_eig, sizeof(double) * ctx->nb, cudaMemcpyDeviceToHost, st));
+    eig_prev = eig;
+    double e_prev = restart ? ctx->scf_e_last : 0.0;
     chfsi_status status = CHFSI_NOT_CONVERGED;
     cudaEvent_t t0, t1;
     cudaEventCreate(&t0);
@@ -2280,7 +2331,7 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
         if (s) { status = s; break; }
         ctx->veff_set = true;
         // diagonalize (scf.rs:169)
-        const int passes = it == 1 ? std::max(1, p->first_passes) : 1;
+        const int passes = it == 1 && !restart ? std::max(1, p->first_passes) : 1;
         for (int q = 0; q < passes; ++q) {
             const bool mixed_pass = ctx->mixed_active;
             const size_t npsi = (size_t)ctx->nb * ctx->n_pw;
@@ -2392,9 +2443,25 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
         // FP64).  Mixed passes run an FP64 Rayleigh-Ritz, so their energies
         // carry no precision bias and the change from a mixed iteration to
         // the FP64 one after it counts.
-        const double de = it > 1 ? std::fabs(etot - e_prev) / ctx->n_atoms : 1e300;
+        const double de = it > 1 || restart ? std::fabs(etot - e_prev) / ctx->n_atoms : 1e300;
+        // largest change of an occupied eigenvalue since the previous iteration
+        double deig = 0.0;
+        if (it > 1 || restart) {
+            for (int b = 0; b < ctx->nb; ++b)
+                if (ctx->occ[b] > 0.01) deig = std::max(deig, std::fabs(eig[b] - eig_prev[b]));
+        } else {
+            deig = 1e300;
+        }
+        eig_prev = eig;
+        const bool eig_ok = p->tol_eig <= 0.0 || deig < p->tol_eig;
+        // the FP32 filter leaves ~1e-7 Ha of noise in the eigenvalue changes:
+        // the switch to FP64 takes ten times the tolerance, the FP64 steps
+        // after it meet the tolerance itself
+        const bool eig_near = p->tol_eig <= 0.0 || deig < 10.0 * p->tol_eig;
         if (ctx->mixed_active) ++r->n_iter_mixed;
-        if (de < p->tol_per_atom && !ctx->mixed_active) {
+        if (p->verbose && p->tol_eig > 0.0)
+            std::fprintf(stderr, "scf %3d max |d eig_occ| %.3e\n", it, deig);
+        if (de < p->tol_per_atom && eig_ok && !ctx->mixed_active) {
             status = CHFSI_OK;
             e_prev = etot;
             break;
@@ -2406,7 +2473,7 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
         // times, so the two can never alternate for ever)
         const double sw = std::max(p->fp64_switch_per_atom, p->tol_per_atom);
         if (ctx->mixed_active) {
-            low_mixed = de < sw ? low_mixed + 1 : 0;
+            low_mixed = de < sw && eig_near ? low_mixed + 1 : 0;
             if (low_mixed >= 2) {
                 ctx->mixed_active = false;
                 low_mixed = 0;
@@ -2462,11 +2529,8 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
         }
         r_prev = rnorm;
         if (learned) ring_push(ctx, ring, ctx->d_rho_out, ctx->d_rho_in);
-        if (!learned || fell_back) {
-            pulay_combine(ctx->d_hist_ptrs + kPulayMax, ctx->d_hist_ptrs, ps.m, c, p->alpha, ng,
-                          ctx->d_rho_next, st);
-        } else {
-            double2* Dg = nullptr;
+        double2* Dg = nullptr;
+        if (learned && !fell_back) {
             if (have_prev) {
                 Dg = mix_grid(ctx, kGridD);
                 launch_diff_complex(ctx->d_rho_in, mix_real(ctx, 0), Dg, ng, st);
@@ -2474,6 +2538,23 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
             }
             if ((s = mix_features(ctx, ring, Dg, nullptr))) { status = s; break; }
             mlp_forward(ctx->mixer->mlp, ctx->d_mix_x, 1, mix_y(ctx), st);
+            // a network whose output is not finite (diverged weights, a NaN in
+            // the residual history) hands the run to Pulay like a residual rise
+            float yh[kMixOut];
+            CK(cudaMemcpyAsync(yh, mix_y(ctx), sizeof(yh), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            for (float v : yh)
+                if (!std::isfinite(v)) {
+                    fell_back = true;
+                    if (p->verbose)
+                        std::fprintf(stderr, "scf %3d: learned mixer output not finite, Pulay from here\n", it);
+                    break;
+                }
+        }
+        if (!learned || fell_back) {
+            pulay_combine(ctx->d_hist_ptrs + kPulayMax, ctx->d_hist_ptrs, ps.m, c, p->alpha, ng,
+                          ctx->d_rho_next, st);
+        } else {
             double2* W = mix_grid(ctx, kGridW);
             if (p->mixer == CHFSI_MIXER_LEARNED) {
                 // rho_in + a_s R_0 + b_s D per shell
@@ -2507,6 +2588,8 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
         CK(cudaGetLastError());
     }
     ctx->mixed_active = ctx->mixed;
+    ctx->scf_done = have_eig;
+    ctx->scf_e_last = e_prev;
     r->fell_back = fell_back ? 1 : 0;
     cudaEventRecord(t1, st);
     cudaEventSynchronize(t1);
@@ -2869,6 +2952,9 @@ extern "C" chfsi_status chfsi_mixer_samples(chfsi_ctx* ctx, const double* rho_in
     return CHFSI_OK;
 }
 
+// Largest K of the GEMM entry points: the split-K chunk arithmetic is 32-bit.
+constexpr int kGemmMaxK = 1 << 30;
+
 // C[m][n] = sum_k conj(A[m][k]) B[n][k] on device pointers (row-major,
 // leading dimensions lda, ldb; C dense m x n) — the op::C ZGEMM of the
 // reference's BlasHandle::gemm_c64 (src/device/blas.rs:79-102) as used for
@@ -2877,8 +2963,11 @@ extern "C" chfsi_status chfsi_mixer_samples(chfsi_ctx* ctx, const double* rho_in
 extern "C" chfsi_status chfsi_zgemm_cn(const chfsi_c128* a_dev, int lda, const chfsi_c128* b_dev,
                                        int ldb, int m, int n, int k, chfsi_c128* c_dev,
                                        void* stream) {
-    if (!a_dev || !b_dev || !c_dev || m <= 0 || n <= 0 || k <= 0 || lda < k || ldb < k)
+    if (!a_dev || !b_dev || !c_dev || m <= 0 || n <= 0 || k <= 0 || lda < k || ldb < k ||
+        k > kGemmMaxK) {
+        g_last_error = "chfsi_zgemm_cn: null pointer, size outside 1..2^30 or lda/ldb < k";
         return CHFSI_ERR_BAD_INPUT;
+    }
     cudaStream_t st = (cudaStream_t)stream;
     double2* part = nullptr;
     const size_t pe = splitk_partial_elems(m, n, k);
@@ -2900,8 +2989,11 @@ extern "C" chfsi_status chfsi_zgemm_cn(const chfsi_c128* a_dev, int lda, const c
 extern "C" chfsi_status chfsi_zgemm_cn_bf16x3(const chfsi_c128* a_dev, int lda,
                                               const chfsi_c128* b_dev, int ldb, int m, int n,
                                               int k, chfsi_c128* c_dev, void* stream) {
-    if (!a_dev || !b_dev || !c_dev || m <= 0 || n <= 0 || k <= 0 || lda < k || ldb < k)
+    if (!a_dev || !b_dev || !c_dev || m <= 0 || n <= 0 || k <= 0 || lda < k || ldb < k ||
+        k > kGemmMaxK) {
+        g_last_error = "chfsi_zgemm_cn_bf16x3: null pointer, size outside 1..2^30 or lda/ldb < k";
         return CHFSI_ERR_BAD_INPUT;
+    }
     cudaStream_t st = (cudaStream_t)stream;
     const int kp = tc_kpad(k);
     TcPlanes pa, pb;
@@ -2930,7 +3022,28 @@ extern "C" chfsi_status chfsi_zgemm_cn_bf16x3(const chfsi_c128* a_dev, int lda,
     if (e != cudaSuccess) return cuda_fail(e, "tc_gemm", __FILE__, __LINE__);
     if (herr) {
         g_last_error = "tensor-core GEMM pipeline wait timed out";
-        return CHFSI_ERR_CUDA;
+        return CHFSI_ERR_TIMEOUT;
     }
     return CHFSI_OK;
+}
+
+// Host-side fault injection for the error-path tests (no GPU fault is made:
+// an injected tensor-core timeout is a producer that issues no loads, so the
+// consumer's bounded wait runs out with nothing in flight).
+extern "C" chfsi_status chfsi_test_inject(int what, long long arg) {
+    switch (what) {
+        case CHFSI_INJECT_NONE:
+            tc_inject_no_loads(0);
+            g_alloc_fail_in.store(-1);
+            return CHFSI_OK;
+        case CHFSI_INJECT_TC_NO_LOADS:
+            if (arg < 0 || arg > (1 << 20)) return CHFSI_ERR_BAD_INPUT;
+            tc_inject_no_loads((int)arg);
+            return CHFSI_OK;
+        case CHFSI_INJECT_ALLOC_FAIL:
+            g_alloc_fail_in.store(arg < 0 ? -1 : arg);
+            return CHFSI_OK;
+        default:
+            return CHFSI_ERR_BAD_INPUT;
+    }
 }

@@ -16,8 +16,10 @@
 //   warp 1 lane 0: MMA issuer, 4 x tcgen05.mma (M128 x N BN x K16) per
 //                  stage, tcgen05.commit frees the stage
 //   all 4 warps  : epilogue, tcgen05.ld 32 lanes x 16 columns per step
-// Every wait is bounded; on timeout the kernel records the failure in an
-// error word and skips the remaining work instead of spinning forever.
+// Every wait is bounded in time (%globaltimer) and in iterations; on timeout
+// the kernel records the failure in an error word, stops issuing work, waits
+// (again bounded) for the TMA loads and MMAs it has already issued, frees its
+// TMEM and returns, so the context stays usable and the host reads the error.
 #include "gemm_tc.hpp"
 #include "launch_count.hpp"
 
@@ -26,6 +28,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <mutex>
 
@@ -37,7 +40,20 @@ constexpr int kBM = 128;
 constexpr int kBK = 64;          // one 128-byte swizzle atom of bf16
 constexpr int kStages = 4;
 constexpr int kThreads = 128;
-constexpr long long kSpinLimit = 1LL << 28;
+// hard cap on polls of one wait, whatever the clock says
+constexpr long long kSpinLimit = 1LL << 30;
+// time limit of one wait in normal operation (a whole GEMM takes milliseconds)
+constexpr unsigned long long kWaitNs = 4000000000ULL;
+// time limit while a test has switched the producer's loads off
+constexpr unsigned long long kInjectedWaitNs = 20000000ULL;
+
+std::atomic<int> g_inject_no_loads{0};
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return (uint32_t)__cvta_generic_to_shared(p);
@@ -53,9 +69,12 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
                  : "memory");
 }
 
-// Bounded parity wait; returns false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Parity wait bounded by wait_ns of device time (and kSpinLimit polls);
+// returns false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
+                                          unsigned long long wait_ns) {
     const uint32_t a = smem_u32(bar);
+    const unsigned long long t0 = global_ns();
     for (long long i = 0; i < kSpinLimit; ++i) {
         uint32_t ok;
         asm volatile(
@@ -66,6 +85,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
             : "r"(a), "r"(parity)
             : "memory");
         if (ok) return true;
+        if ((i & 63) == 63 && global_ns() - t0 > wait_ns) return false;
     }
     return false;
 }
@@ -134,7 +154,8 @@ enum { kOutPartialF32 = 0, kOutComplexF32 = 1, kOutComplexF64 = 2 };
 template <int MODE>
 __global__ void __launch_bounds__(kThreads, 1)
 k_umma_split3(const __grid_constant__ TcMaps maps, int M2, int N, int bn, int ktiles_total,
-              int ktiles_per_split, void* out, long long ldo, int* err) {
+              int ktiles_per_split, void* out, long long ldo, int* err,
+              unsigned long long wait_ns, int no_loads) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     // 1024-byte aligned stage ring
     unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -179,22 +200,36 @@ k_umma_split3(const __grid_constant__ TcMaps maps, int M2, int N, int bn, int kt
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
 
-    if (warp == 0 && lane == 0 && iters > 0) {
-        // ---- TMA producer
+    if (warp == 0 && lane == 0 && iters > 0 && !no_loads) {
+        // ---- TMA producer (no_loads: a test switch under which nothing is
+        // issued, so the MMA warp's first wait runs out with nothing in flight)
+        int issued = 0;
+        bool aborted = false;
         for (int it = 0; it < iters; ++it) {
             const int s = it % kStages;
             const uint32_t ph = (it / kStages) & 1;
-            if (it >= kStages && !mbar_wait(&empty[s], ph ^ 1)) {
+            if (it >= kStages && !mbar_wait(&empty[s], ph ^ 1, wait_ns)) {
                 atomicExch(err, 1);
                 *(volatile int*)abort_flag = 1;
+                aborted = true;
                 break;
             }
-            if (*(volatile int*)abort_flag) break;
+            if (*(volatile int*)abort_flag) { aborted = true; break; }
             const int t = it / nk, kk = it - t * nk;
             const int kx = (kt0 + kk) * kBK;
             mbar_expect_tx(&full[s], a_bytes + b_bytes);
             tma_load_2d(sa + s * a_bytes, &maps.a[pa[t]], &full[s], kx, m0);
             tma_load_2d(sb + s * b_bytes, &maps.b[pb[t]], &full[s], kx, n0);
+            ++issued;
+        }
+        if (aborted) {
+            // retire the loads still in flight (the last kStages issued)
+            // before the CTA releases its shared memory
+            for (int j = issued > kStages ? issued - kStages : 0; j < issued; ++j)
+                if (!mbar_wait(&full[j % kStages], (j / kStages) & 1, wait_ns)) {
+                    atomicExch(err, 4);
+                    break;
+                }
         }
     } else if (warp == 1 && lane == 0 && iters > 0) {
         // ---- MMA issuer
@@ -203,7 +238,7 @@ k_umma_split3(const __grid_constant__ TcMaps maps, int M2, int N, int bn, int kt
         for (int it = 0; it < iters; ++it) {
             const int s = it % kStages;
             const uint32_t ph = (it / kStages) & 1;
-            if (!mbar_wait(&full[s], ph)) {
+            if (!mbar_wait(&full[s], ph, wait_ns)) {
                 atomicExch(err, 2);
                 *(volatile int*)abort_flag = 1;
                 ok = false;
@@ -218,13 +253,14 @@ k_umma_split3(const __grid_constant__ TcMaps maps, int M2, int N, int bn, int kt
             umma_commit(&empty[s]);
         }
         (void)ok;
+        // arrives once every MMA issued above has completed (also on abort)
         umma_commit(done);
     }
     __syncwarp();
     // ---- epilogue: every warp reads its 32 TMEM lanes
     bool have = iters > 0;
     if (have) {
-        if (!mbar_wait(done, 0)) {
+        if (!mbar_wait(done, 0, wait_ns)) {
             atomicExch(err, 3);
             have = false;
         }
@@ -468,24 +504,36 @@ cudaError_t tc_gemm(const TcPlanes& a, const TcPlanes& b, int M, int N, int K, i
     splits = (ktiles + kps - 1) / kps;
     dim3 grid(mt, nt, splits);
     const size_t sm = smem_bytes(bn);
+    int no_loads = 0;
+    unsigned long long wait_ns = kWaitNs;
+    for (int left = g_inject_no_loads.load(); left > 0; left = g_inject_no_loads.load())
+        if (g_inject_no_loads.compare_exchange_weak(left, left - 1)) {
+            no_loads = 1;
+            wait_ns = kInjectedWaitNs;
+            break;
+        }
     count_launch();
     if (out_mode == kTcOutPartial) {
         cudaFuncSetAttribute(k_umma_split3<kOutPartialF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         k_umma_split3<kOutPartialF32><<<grid, kThreads, sm, st>>>(maps, 2 * M, N, bn, ktiles, kps,
-                                                                  part, N, err);
+                                                                  part, N, err, wait_ns, no_loads);
         count_launch();
         k_reduce_tc<<<grid_for((long long)M * N), 256, 0, st>>>(part, splits, M, N, (double2*)out);
     } else if (out_mode == kTcOutComplexF32) {
         cudaFuncSetAttribute(k_umma_split3<kOutComplexF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         k_umma_split3<kOutComplexF32><<<grid, kThreads, sm, st>>>(maps, 2 * M, N, bn, ktiles, kps,
-                                                                  out, ldo, err);
+                                                                  out, ldo, err, wait_ns,
+                                                                  no_loads);
     } else {
         cudaFuncSetAttribute(k_umma_split3<kOutComplexF64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         k_umma_split3<kOutComplexF64><<<grid, kThreads, sm, st>>>(maps, 2 * M, N, bn, ktiles, kps,
-                                                                  out, ldo, err);
+                                                                  out, ldo, err, wait_ns,
+                                                                  no_loads);
     }
     return cudaGetLastError();
 }
+
+void tc_inject_no_loads(int launches) { g_inject_no_loads.store(launches < 0 ? 0 : launches); }
 
 template void tc_pack<double2>(const double2*, long long, int, int, bool, int, TcPlanes&, cudaStream_t);
 template void tc_pack<float2>(const float2*, long long, int, int, bool, int, TcPlanes&, cudaStream_t);

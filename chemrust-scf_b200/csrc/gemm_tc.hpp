@@ -35,6 +35,11 @@ void tc_pack(const CIn* x, long long ldx, int rows, int K, bool doubled, int src
 // b: plain planes (N rows).  kTcOutPartial writes double2 C (M x N dense)
 // through `part` scratch; the complex modes write float2 / double2 rows of
 // leading dimension ldo directly.  err: device word set on a wait timeout.
+// Test hook: the next `launches` tcgen05 GEMM launches run with a producer
+// that issues no loads and a 20 ms wait limit (their waits run out, the
+// error word is set, nothing is left in flight).
+void tc_inject_no_loads(int launches);
+
 cudaError_t tc_gemm(const TcPlanes& a, const TcPlanes& b, int M, int N, int K, int out_mode,
                     void* out, long long ldo, float* part, int* err, cudaStream_t st);
 

@@ -10,9 +10,12 @@
 //
 // Set-up: the first call on a device (with that device current) looks the
 // array's device address up with cudaGetSymbolAddress and caches it per
-// device; make that first call before any stream capture.  Calls share the
-// array, so calls that overlap on the GPU (different streams, or different
-// host threads on one device) race; serialise them.  Nothing needs clearing
+// device; make that first call before any stream capture.  The cached address
+// belongs to the device's primary context: cudaDeviceReset while the library
+// is loaded is not supported (the next call would write to a stale address).
+// Calls share the array, so calls that overlap on the GPU (different streams,
+// or different host threads on one device) race; serialise them.  Nothing
+// needs clearing
 // between calls: every partial the reduction reads is written earlier in the
 // same call.
 #include "chfsi.h"
@@ -33,6 +36,8 @@ namespace {
 constexpr size_t kNoAllocScratchBytes = (size_t)CHFSI_NOALLOC_SCRATCH_BYTES;
 constexpr size_t kNoAllocScratchElems = kNoAllocScratchBytes / sizeof(double2);
 constexpr int kMaxDevices = 64;
+// split-K chunk arithmetic is 32-bit; this bound keeps it far from overflow
+constexpr int kMaxK = 1 << 30;
 
 static __device__ __align__(256) double2 g_noalloc_scratch[kNoAllocScratchElems];
 
@@ -45,7 +50,10 @@ chfsi_status scratch_for_current_device(double2** out) {
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return chfsi::cuda_fail(e, "cudaGetDevice", __FILE__, __LINE__);
-    if (dev < 0 || dev >= kMaxDevices) return CHFSI_ERR_BAD_INPUT;
+    if (dev < 0 || dev >= kMaxDevices) {
+        chfsi::set_last_error("chfsi_zgemm_cn_noalloc: device ordinal above 63");
+        return CHFSI_ERR_BAD_INPUT;
+    }
     std::lock_guard<std::mutex> lock(g_setup_mutex);
     if (!g_scratch_addr[dev]) {
         void* p = nullptr;
@@ -63,8 +71,18 @@ chfsi_status scratch_for_current_device(double2** out) {
 extern "C" chfsi_status chfsi_zgemm_cn_noalloc(const chfsi_c128* a_dev, int lda,
                                                const chfsi_c128* b_dev, int ldb, int m, int n,
                                                int k, chfsi_c128* c_dev, void* stream) {
-    if (!a_dev || !b_dev || !c_dev || m <= 0 || n <= 0 || k <= 0 || lda < k || ldb < k)
+    if (!a_dev || !b_dev || !c_dev) {
+        chfsi::set_last_error("chfsi_zgemm_cn_noalloc: null device pointer");
         return CHFSI_ERR_BAD_INPUT;
+    }
+    if (m <= 0 || n <= 0 || k <= 0 || k > kMaxK) {
+        chfsi::set_last_error("chfsi_zgemm_cn_noalloc: m, n and k must be in 1..2^30");
+        return CHFSI_ERR_BAD_INPUT;
+    }
+    if (lda < k || ldb < k) {
+        chfsi::set_last_error("chfsi_zgemm_cn_noalloc: lda and ldb must be at least k");
+        return CHFSI_ERR_BAD_INPUT;
+    }
     const size_t mn = (size_t)m * (size_t)n;
     if (mn > kNoAllocScratchElems) {
         // one split needs m*n partials; larger outputs need the allocating entry point

@@ -64,7 +64,10 @@ typedef enum chfsi_status {
     CHFSI_ERR_BAD_INPUT       = -6,  /* shape / pointer / range violation    */
     CHFSI_ERR_NO_DEVICE       = -7,  /* no CUDA device visible               */
     CHFSI_ERR_OUT_OF_MEMORY   = -8,
-    CHFSI_ERR_NUMERIC         = -9   /* NaN/Inf detected on device           */
+    CHFSI_ERR_NUMERIC         = -9,  /* NaN/Inf detected on device           */
+    CHFSI_ERR_TIMEOUT         = -10  /* a bounded device-side wait ran out
+                                        (the kernel stopped, retired what it
+                                        had issued and returned)             */
 } chfsi_status;
 
 typedef struct chfsi_c128 { double re, im; } chfsi_c128;
@@ -230,6 +233,14 @@ chfsi_status chfsi_get_bounds(chfsi_ctx* ctx, double* out4);
 /* Frobenius norms |psi_k| per filter degree k = 0..ndeg of the last filter. */
 chfsi_status chfsi_get_filter_norms(chfsi_ctx* ctx, double* out, int n);
 
+/* S^-1 H |psi> of the generalised (ultrasoft) problem after chfsi_set_qmat,
+ * the operator the filter applies (the reference's ChFSI has no S; the
+ * operator pair is tests/phase0_gate2_convergence.rs:279-322 apply_hs with
+ * the Woodbury inverse noted at cg_helpers.rs:86-92); H |psi> without q.
+ * Device pointers as chfsi_apply_h; overwrites the context's H|psi> buffer. */
+chfsi_status chfsi_apply_sinv_h(chfsi_ctx* ctx, const chfsi_c128* psi_dev, chfsi_c128* out_dev,
+                                int nb);
+
 /* Local part only, T + V_loc (apply_v_loc_hamiltonian, chebyshev.rs:279-365). */
 chfsi_status chfsi_apply_h_local(chfsi_ctx* ctx, const chfsi_c128* psi_dev,
                                  chfsi_c128* hpsi_dev, int nb);
@@ -300,7 +311,14 @@ typedef struct chfsi_scf_params {
     double* trace;        /* optional host buffer of 2 * max_iter * N^3 doubles: rho_in
                              and rho_out of every iteration (training trajectories)   */
     int    verbose;       /* 1: one line per iteration on stderr                       */
-    int    reserved;
+    int    restart;       /* 1: continue from the context's current input density,
+                             wavefunctions and eigenvalues (one pass in the first
+                             step, fresh mixing history) instead of a uniform density */
+    double tol_eig;       /* > 0: convergence also needs the occupied eigenvalues
+                             (f > 0.01) to change by less than this (Ha) from the
+                             previous iteration; mixed runs switch to FP64 only after
+                             two mixed iterations with |dE| below the switch and
+                             eigenvalue changes below 10 x tol_eig                   */
 } chfsi_scf_params;
 
 /* Density mixers of chfsi_scf_run.  PULAY: Pulay/DIIS over (rho_in,
@@ -409,6 +427,16 @@ chfsi_status chfsi_set_mixer(chfsi_ctx* ctx, chfsi_mixer* m);
  * this context's grid: rho_in / rho_out are n_iter x N^3, rho_star N^3 */
 chfsi_status chfsi_mixer_samples(chfsi_ctx* ctx, const double* rho_in, const double* rho_out,
                                  int n_iter, const double* rho_star, float* x, float* t);
+
+/* ---- test hooks (host-side fault injection; no counterpart in the crate) --
+ * CHFSI_INJECT_TC_NO_LOADS: the next `arg` tensor-core GEMM launches run with
+ *   a producer that issues no loads; the consumer's wait runs out after 20 ms
+ *   and the call returns CHFSI_ERR_TIMEOUT (no GPU fault, nothing in flight).
+ * CHFSI_INJECT_ALLOC_FAIL: the arg-th device allocation of a context from now
+ *   (0 = the next) fails as out of memory.
+ * CHFSI_INJECT_NONE clears both. */
+enum { CHFSI_INJECT_NONE = 0, CHFSI_INJECT_TC_NO_LOADS = 1, CHFSI_INJECT_ALLOC_FAIL = 2 };
+chfsi_status chfsi_test_inject(int what, long long arg);
 
 #ifdef __cplusplus
 }

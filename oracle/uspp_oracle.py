@@ -92,8 +92,8 @@ class UsppScf:
         self.G = G
         self.g2 = (G * G).sum(-1)
         self.ghat = np.exp(-0.25 * self.g2 * self.width ** 2)
-        # e^{-i G.R_I} per ion on the density grid
-        self.sf = np.exp(-1j * np.einsum("zyxd,id->izyx", G, self.pos))
+        # phases e^{-i G.R_I} are formed one ion at a time (a table over all
+        # ions of the 216-atom cell on its 144^3 grid would take 10 GB)
         # blocks of q and D0 per ion
         self.blocks = []
         off = 0
@@ -102,6 +102,16 @@ class UsppScf:
             self.blocks.append((self.poff[i], ne, off))
             off += ne * ne
         self.vloc = self.up_coeffs(self.wave_coeffs_vloc()).real.ravel()
+
+    def _phase(self, i):
+        return np.exp(-1j * (self.G @ self.pos[i]))
+
+    def _phase_sum(self, c):
+        """sum_I c_I e^{-i G.R_I} on the density grid."""
+        out = np.zeros(self.g2.shape, dtype=complex)
+        for i, ci in enumerate(c):
+            out += ci * self._phase(i)
+        return out
 
     # --- grids
     def _wave_idx(self):
@@ -150,8 +160,8 @@ class UsppScf:
     def screened_d(self, vf):
         nx, ny, nz = self.nf
         Vg = np.fft.fftn(vf.reshape(nz, ny, nx)) / vf.size
-        v = np.array([np.sum(Vg * self.ghat * np.conj(self.sf[I])).real
-                      for I in range(len(self.pos))])
+        vq = Vg * self.ghat
+        v = np.array([np.sum(vq * np.conj(self._phase(I))).real for I in range(len(self.pos))])
         d = self.d0.copy()
         for I, (p0, ne, off) in enumerate(self.blocks):
             d[off:off + ne * ne] += v[I] * self.q[off:off + ne * ne]
@@ -173,7 +183,7 @@ class UsppScf:
         (hx, fx), (hy, fy), (hz, fz) = self._wave_idx()
         F = np.zeros(self.nf[::-1], dtype=complex)
         F[np.ix_(fz, fy, fx)] = cw[np.ix_(hz, hy, hx)]
-        F += self.ghat / self.omega * np.tensordot(c, self.sf, axes=1)
+        F += self.ghat / self.omega * self._phase_sum(c)
         return (np.fft.ifftn(F) * F.size).real.ravel(), c
 
     def run_scf(self, ndeg, max_iter=30, tol_per_atom=1e-6, alpha=0.3, max_hist=6,

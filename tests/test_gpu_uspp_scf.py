@@ -27,7 +27,8 @@ def test_uspp_scf_energies_match_oracle(chfsi, dens):
     assert ctx.ngrid_density == s.ngrid_density
     r = ctx.run_scf(12, max_iter=4, kT=0.01)
     print("density grid %s: device %s oracle %s" % (s.ngrid_density, r["energies"], ref["energies"]))
-    np.testing.assert_allclose(r["energies"], ref["energies"], rtol=0, atol=1e-8)
+    print("max energy difference %.3e Ha" % np.abs(r["energies"] - ref["energies"]).max())
+    np.testing.assert_allclose(r["energies"], ref["energies"], rtol=0, atol=1e-10)
     rho = ctx.get_density()
     assert abs(rho.sum() * s.omega / rho.size - s.n_elec) < 1e-8
     np.testing.assert_allclose(rho, ref["rho"], rtol=0, atol=1e-8 * np.abs(ref["rho"]).max())
@@ -48,16 +49,18 @@ def test_uspp_scf_converges_to_oracle(chfsi):
 def test_mixed_precision_uspp_scf_matches_fp64(chfsi):
     """FP32 filter of S^-1 H with tcgen05 projections, FP64 Rayleigh-Ritz with
     the ultrasoft overlap, final FP64 passes: same converged energy and
-    occupied eigenvalues as the FP64 run."""
+    occupied eigenvalues (within 1e-6 Ha) as the FP64 run, both converged to
+    1e-9 Ha/atom so that the comparison measures precision, not the SCF stop."""
     s = _system(chfsi, (32, 32, 32))
-    rf = chfsi.Context(s).run_scf(12, max_iter=40, kT=0.01)
-    rm = chfsi.Context(s, precision=chfsi.PREC_MIXED).run_scf(12, max_iter=40, kT=0.01,
-                                                              fp64_switch_per_atom=1e-4)
+    rf = chfsi.Context(s).run_scf(12, max_iter=80, kT=0.01, tol_per_atom=1e-9)
+    rm = chfsi.Context(s, precision=chfsi.PREC_MIXED).run_scf(12, max_iter=80, kT=0.01,
+                                                              tol_per_atom=1e-9,
+                                                              fp64_switch_per_atom=1e-6)
     n_occ = int(round(s.n_elec / 2))
     de = abs(rm["e_total"] - rf["e_total"]) / s.n_atoms
     docc = np.abs(rm["eigenvalues"][:n_occ] - rf["eigenvalues"][:n_occ]).max()
     print("mixed ultrasoft SCF: %d iterations (%d mixed) vs %d; dE/atom %.2e, occupied eig %.2e"
           % (rm["n_iter"], rm["n_iter_mixed"], rf["n_iter"], de, docc))
     assert rf["converged"] and rm["converged"] and rm["n_iter_mixed"] >= 1
-    assert de < 1e-6
-    assert docc < 1e-5
+    assert de < 1e-8
+    assert docc < 1e-6
