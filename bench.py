@@ -462,6 +462,30 @@ def run_profile(kind):
     import numpy as np
     import torch
     import chfsi
+    if kind == "gemm":
+        # the FP64 tensor-path op::C GEMM at the 216-atom shapes, on random
+        # operands of a few GB: psi^H psi (576 x 576, K = 173,925) and a
+        # projector product (1,728 x 576) with K cut to 43,000
+        g = torch.Generator(device="cuda").manual_seed(0)
+        st = torch.cuda.current_stream().cuda_stream
+        for m, n, k in ((576, 576, 173925), (1728, 576, 43000)):
+            a = torch.randn((m, k), dtype=torch.complex128, device="cuda", generator=g)
+            b = a if m == n else torch.randn((n, k), dtype=torch.complex128, device="cuda",
+                                             generator=g)
+            c = torch.empty((m, n), dtype=torch.complex128, device="cuda")
+            for _ in range(2):
+                chfsi.zgemm_cn(a.data_ptr(), k, b.data_ptr(), k, m, n, k, c.data_ptr(), st)
+            torch.cuda.synchronize()
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record()
+            chfsi.zgemm_cn(a.data_ptr(), k, b.data_ptr(), k, m, n, k, c.data_ptr(), st)
+            ev1.record()
+            ev1.synchronize()
+            ms = ev0.elapsed_time(ev1)
+            print("profile gemm %d x %d x %d: %.3f ms, %.1f TFLOP/s" % (m, n, k, ms,
+                                                                       8.0 * m * n * k / ms / 1e9))
+            del a, b, c
+        return
     if kind.endswith("-216"):
         s = chfsi.SyntheticSystem(config_index=2)
         prec = chfsi.PREC_MIXED if kind.startswith("mixed") else chfsi.PREC_FP64
@@ -507,7 +531,7 @@ def main():
     ap.add_argument("--no-scf-216", action="store_true",
                     help="skip the 216-atom time-to-SCF comparison (about ten minutes)")
     ap.add_argument("--scf-216-max-iter", type=int, default=120)
-    ap.add_argument("--profile", choices=["local", "fp64", "mixed", "fp64-216", "mixed-216"],
+    ap.add_argument("--profile", choices=["local", "fp64", "mixed", "fp64-216", "mixed-216", "gemm"],
                     default=None,
                     help="a short fixed workload for ncu captures (no JSON line): two local "
                          "H|psi> launches, or six diagonalisations in one precision (64-atom "

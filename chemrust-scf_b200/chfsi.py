@@ -28,7 +28,8 @@ OK, NOT_CONVERGED, NOT_IMPLEMENTED, CHEB_DIVERGED, RR_FAILED, CUDA_ERROR, BAD_IN
     NO_DEVICE, OUT_OF_MEMORY, NUMERIC, TIMEOUT = 0, -1, -2, -3, -4, -5, -6, -7, -8, -9, -10
 INJECT_NONE, INJECT_TC_NO_LOADS, INJECT_ALLOC_FAIL = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
-BOUND_HEURISTIC, BOUND_LANCZOS = 0, 1
+BOUND_HEURISTIC, BOUND_LANCZOS, BOUND_LANCZOS_FUSED = 0, 1, 2
+FILTER_CHEBYSHEV, FILTER_RESIDUAL = 0, 1
 MIXER_PULAY, MIXER_LEARNED, MIXER_LEARNED_PULAY = 0, 1, 2
 MIXER_FEATURES, MIXER_OUTPUTS, MIXER_TARGETS, MIXER_SHELLS = 512, 128, 320, 64
 
@@ -110,7 +111,8 @@ class Dims(C.Structure):
 
 class Config(C.Structure):
     _fields_ = [("device", C.c_int), ("precision", C.c_int), ("bound_mode", C.c_int),
-                ("lanczos_steps", C.c_int), ("check_norms", C.c_int), ("reserved", C.c_int * 3)]
+                ("lanczos_steps", C.c_int), ("check_norms", C.c_int), ("filter_form", C.c_int),
+                ("reserved", C.c_int * 2)]
 
 
 class ScfParams(C.Structure):
@@ -470,12 +472,13 @@ class Context:
     """Device-resident ChFSI state (one CUDA stream, all buffers on the GPU)."""
 
     def __init__(self, system=None, dims=None, precision=PREC_FP64, bound_mode=BOUND_HEURISTIC,
-                 lanczos_steps=10, device=0):
+                 lanczos_steps=10, device=0, filter_form=FILTER_CHEBYSHEV):
         L = lib()
         cfg = Config()
         _check(L.chfsi_default_config(C.byref(cfg)))
         cfg.device, cfg.precision, cfg.bound_mode, cfg.lanczos_steps = \
             device, precision, bound_mode, lanczos_steps
+        cfg.filter_form = filter_form
         h = C.c_void_p()
         if system is not None:
             _check(L.chfsi_create_from_system(system.handle, C.byref(cfg), C.byref(h)))

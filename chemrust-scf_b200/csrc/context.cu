@@ -125,10 +125,14 @@ __global__ void k_conj(const double2* __restrict__ a, double2* __restrict__ b, s
 // Chebyshev step of the generalised problem: y = S^-1 H x = hx - corr, then
 // the recurrence epilogue of the local pass (first degree / later degrees).
 // C = double2 (FP64 filter) or float2 (FP32 filter; norms still summed in FP64).
+// mode 3: residual step of R-ChFSI, out = a S^-1 H x + b x + c out + a lam[band] y
+// with {a, b, c} = rc[0..2] (bands of npw elements).
 template <typename C>
 __global__ void __launch_bounds__(256)
 k_cheb_combine(const C* __restrict__ hx, const C* __restrict__ corr, const C* __restrict__ x,
-               C* out, size_t n, const double* coef, int mode, double* norm_acc) {
+               C* out, size_t n, const double* coef, int mode, double* norm_acc,
+               const C* __restrict__ yres = nullptr, const double* __restrict__ lam = nullptr,
+               const double* __restrict__ rc = nullptr, int npw = 1) {
     using R = decltype(C{}.x);
     __shared__ double red[8];
     const R ie = (R)coef[4], nc = (R)coef[5];
@@ -140,6 +144,14 @@ k_cheb_combine(const C* __restrict__ hx, const C* __restrict__ corr, const C* __
         const R sr = hr * ie + nc * p.x, si = hi * ie + nc * p.y;
         R orr, oi;
         if (mode == 0) { orr = hr; oi = hi; }  // plain S^-1 H x
+        else if (mode == 3) {
+            const R a = (R)rc[0], b = (R)rc[1], c = (R)rc[2];
+            const R ly = (R)(rc[0] * lam[i / (size_t)npw]);
+            const C prev = out[i];
+            const C y = yres[i];
+            orr = a * hr + b * p.x + c * prev.x + ly * y.x;
+            oi = a * hi + b * p.y + c * prev.y + ly * y.y;
+        }
         else if (mode == 1) { orr = sr; oi = si; }
         else {
             const C prev = out[i];
@@ -158,6 +170,86 @@ k_cheb_combine(const C* __restrict__ hx, const C* __restrict__ corr, const C* __
         double t = 0.0;
         for (int w = 0; w < 8; ++w) t += red[w];
         atomicAdd(norm_acc, t);
+    }
+}
+
+// ---- R-ChFSI (reference_paper/2025 main.tex Algorithm 3) coefficient tables:
+// sigma-scaled Chebyshev steps {a_k, b_k, c_k} (k = 2..p) and the filtered
+// Ritz values L_k(lambda_b) (k = 0..p) of every band; rc[0] = sigma_1 / e.
+// coef: [lambda_max, cut, c, e, ..]; lambda_min = eig[0].
+__global__ void k_rc_tables(const double* __restrict__ coef, const double* __restrict__ eig,
+                            int nb, int p, double* __restrict__ rc, double* __restrict__ lam) {
+    __shared__ double s_rc[3 * 65];
+    const double c = coef[2], e = coef[3];
+    if (threadIdx.x == 0) {
+        double sigma = e / (eig[0] - c);
+        const double sigma1 = sigma, gamma = 2.0 / sigma1;
+        s_rc[0] = sigma1 / e;
+        s_rc[1] = s_rc[2] = 0.0;
+        for (int k = 2; k <= p; ++k) {
+            const double s2 = 1.0 / (gamma - sigma);
+            const double a = 2.0 * s2 / e;
+            s_rc[3 * k] = a;
+            s_rc[3 * k + 1] = -a * c;
+            s_rc[3 * k + 2] = -sigma * s2;
+            sigma = s2;
+        }
+        s_rc[3] = s_rc[4] = s_rc[5] = 0.0;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 3 * (p + 1); i += blockDim.x) rc[i] = s_rc[i];
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+        const double l = eig[b];
+        double l0 = 1.0, l1 = s_rc[0] * (l - c);
+        lam[b] = l0;
+        if (p >= 1) lam[nb + b] = l1;
+        for (int k = 2; k <= p; ++k) {
+            const double l2 = s_rc[3 * k] * l1 * l + s_rc[3 * k + 1] * l1 + s_rc[3 * k + 2] * l0;
+            lam[(size_t)k * nb + b] = l2;
+            l0 = l1;
+            l1 = l2;
+        }
+    }
+}
+
+// t = hx - (x + sx_extra) lam[band]   (residual H X - S X Lam; sx_extra = S X - X or null)
+__global__ void k_rc_resid(const double2* __restrict__ hx, const double2* __restrict__ x,
+                           const double2* __restrict__ sx_extra, const double* __restrict__ lam,
+                           int npw, size_t n, double2* __restrict__ t) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const double l = lam[i / (size_t)npw];
+        double2 v = x[i];
+        if (sx_extra) { v.x += sx_extra[i].x; v.y += sx_extra[i].y; }
+        t[i] = make_double2(hx[i].x - v.x * l, hx[i].y - v.y * l);
+    }
+}
+
+// out = s y (precision of out)
+template <typename C>
+__global__ void k_rc_scale(const double2* __restrict__ y, const double* __restrict__ s, size_t n,
+                           C* __restrict__ out, C* __restrict__ ycopy) {
+    using R = decltype(C{}.x);
+    const double f = *s;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        out[i].x = (R)(f * y[i].x);
+        out[i].y = (R)(f * y[i].y);
+        if (ycopy) { ycopy[i].x = (R)y[i].x; ycopy[i].y = (R)y[i].y; }
+    }
+}
+
+// X_new = R + X lam[band], HX_new = HR + HX lam[band]  (FP64 out)
+template <typename C>
+__global__ void k_rc_final(const C* __restrict__ r, const C* __restrict__ hr,
+                           const double2* __restrict__ x, const double2* __restrict__ hx,
+                           const double* __restrict__ lam, int npw, size_t n,
+                           double2* __restrict__ xo, double2* __restrict__ hxo) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const double l = lam[i / (size_t)npw];
+        xo[i] = make_double2((double)r[i].x + x[i].x * l, (double)r[i].y + x[i].y * l);
+        hxo[i] = make_double2((double)hr[i].x + hx[i].x * l, (double)hr[i].y + hx[i].y * l);
     }
 }
 
@@ -364,6 +456,8 @@ struct chfsi_ctx {
     // Lanczos
     double2* d_lz_v = nullptr; double2* d_lz_v0 = nullptr; double2* d_lz_f = nullptr;
     double2* d_lz_start = nullptr; double* d_lz = nullptr;
+    bool lz_carry = false;       // d_lz holds the tridiagonal of a Lanczos run carried by a filter
+    int lz_carry_k = 0;
     // density / SCF
     double* d_occ = nullptr; std::vector<double> occ;
     std::vector<double> kin_host;  // 1/2 |G+k|^2 in the internal plane-wave order
@@ -378,6 +472,10 @@ struct chfsi_ctx {
     double* d_cgdot = nullptr;     // 16 dot-product accumulators
     bool cg_ready = false;
     double2* d_psi_save = nullptr; // start of a mixed-precision pass (FP64 retry)
+    // R-ChFSI (residual filter): H X, residual, FP64 recurrence pair, FP32 residual copy
+    double2* d_rc_hx = nullptr; double2* d_rc_y = nullptr;
+    double2* d_rc_r0 = nullptr; double2* d_rc_r1 = nullptr;
+    float2* d_rc_y32 = nullptr; double* d_rc_coef = nullptr; double* d_rc_lam = nullptr;
     double* d_rho_in = nullptr; double* d_rho_out = nullptr; double* d_rho_next = nullptr;
     double2* d_cgrid = nullptr; double* d_acc = nullptr;
     double* d_hist = nullptr;  // 2 * kPulayMax * ng
@@ -464,10 +562,21 @@ chfsi_status ensure_pinned(chfsi_ctx* ctx, size_t n) {
 
 // ---------------------------------------------------------------- H|psi>
 // out = epilogue(H psi) for nb bands of psi (ld n_pw, context PW order).
+// Coefficients of one residual (R-ChFSI) step for the kEpiResid epilogue.
+struct ResidStep {
+    const double* rc;   // {a, b, c}
+    const double* lam;  // per band
+    const void* y;      // residual, ld n_pw
+};
+
 chfsi_status apply_h_dev(chfsi_ctx* ctx, const double2* psi, double2* out, int nb, int mode,
-                         double* norm_acc) {
+                         double* norm_acc, int plain_band = -1, double2* plain_out = nullptr,
+                         const ResidStep* rs = nullptr) {
     Epilogue e{};
     e.mode = mode;
+    e.plain_band = plain_band;
+    e.plain_out = plain_out;
+    if (rs) { e.rc = rs->rc; e.lam = rs->lam; e.yres = rs->y; }
     e.kin = ctx->d_kin;
     e.coef = ctx->d_coef;
     e.nl = nullptr;
@@ -496,11 +605,20 @@ chfsi_status apply_h_dev(chfsi_ctx* ctx, const double2* psi, double2* out, int n
 // One filter operator application: H x, or S^-1 H x for the generalised
 // (ultrasoft) problem, where S^-1 = 1 - beta M beta^H is applied to H x by
 // three GEMMs and the recurrence epilogue runs in k_cheb_combine.
+// lz_col: row nb of x holds the carried Lanczos vector v; H v goes to d_lz_f
+// (the H of the generalised problem's pencil, without S^-1, like the
+// separate Lanczos run).
 chfsi_status apply_op_dev(chfsi_ctx* ctx, const double2* x, double2* out, int nb, int mode,
-                          double* norm_acc) {
-    if (!ctx->uspp || mode == kEpiApply) return apply_h_dev(ctx, x, out, nb, mode, norm_acc);
-    chfsi_status s = apply_h_dev(ctx, x, ctx->d_hpsi, nb, kEpiApply, nullptr);
+                          double* norm_acc, bool lz_col = false) {
+    if (!ctx->uspp || mode == kEpiApply) {
+        if (!lz_col) return apply_h_dev(ctx, x, out, nb, mode, norm_acc);
+        return apply_h_dev(ctx, x, out, nb + 1, mode, norm_acc, nb, ctx->d_lz_f);
+    }
+    chfsi_status s = apply_h_dev(ctx, x, ctx->d_hpsi, nb + (lz_col ? 1 : 0), kEpiApply, nullptr);
     if (s) return s;
+    if (lz_col)
+        CK(cudaMemcpyAsync(ctx->d_lz_f, ctx->d_hpsi + (size_t)nb * ctx->n_pw,
+                           sizeof(double2) * ctx->n_pw, cudaMemcpyDeviceToDevice, ctx->st));
     cudaStream_t st = ctx->st;
     gemm_cn(ctx->d_beta, ctx->n_pw, ctx->d_hpsi, ctx->n_pw, ctx->np, nb, ctx->n_pw, ctx->d_part,
             ctx->d_cp, st);
@@ -541,7 +659,16 @@ chfsi_status lanczos_bound(chfsi_ctx* ctx) {
 }
 
 chfsi_status compute_bounds(chfsi_ctx* ctx, const double* eig_dev, int n_eig) {
-    if (ctx->cfg.bound_mode == CHFSI_BOUND_LANCZOS) {
+    if (ctx->cfg.bound_mode == CHFSI_BOUND_LANCZOS_FUSED && ctx->lz_carry) {
+        // tridiagonal left by the Lanczos vector the previous filter carried
+        bounds(ctx->kin_max, ctx->d_minmax, eig_dev, n_eig, ctx->d_lz, ctx->lz_carry_k,
+               1.0 / ctx->s_min, ctx->d_coef, ctx->st);
+        ctx->lz_carry = false;
+        CK(cudaGetLastError());
+        return CHFSI_OK;
+    }
+    if (ctx->cfg.bound_mode == CHFSI_BOUND_LANCZOS ||
+        ctx->cfg.bound_mode == CHFSI_BOUND_LANCZOS_FUSED) {
         chfsi_status s = lanczos_bound(ctx);
         if (s) return s;
         // the cut still comes from the previous eigenvalues
@@ -566,15 +693,50 @@ chfsi_status filter_dev(chfsi_ctx* ctx, int ndeg, const double* eig_dev, int n_e
     sumsq(ctx->d_psi, n, ctx->d_nsq, ctx->st);
     double2* A = ctx->d_psi;   // psi_{k-2}
     double2* B = ctx->d_psi2;  // psi_{k-1}
+    // k-step Lanczos carried as column nb of the first k applies (its bound
+    // serves the next filter): v_0 is the shared start vector, normalised
+    const int klz = ctx->cfg.bound_mode == CHFSI_BOUND_LANCZOS_FUSED
+                        ? std::min(std::max(2, std::min(ctx->cfg.lanczos_steps, 60)), ndeg) : 0;
+    const size_t npw = ctx->n_pw;
+    if (klz >= 2) {
+        CK(cudaMemsetAsync(ctx->d_lz, 0, sizeof(double) * 2 * klz, ctx->st));
+        CK(cudaMemcpyAsync(ctx->d_lz_v, ctx->d_lz_start, npw * sizeof(double2),
+                           cudaMemcpyDeviceToDevice, ctx->st));
+        double* fn0 = ctx->d_lz + 2 * klz - 1;
+        sumsq(ctx->d_lz_v, npw, fn0, ctx->st);
+        scale_by_rsqrt(ctx->d_lz_v, npw, fn0, ctx->st);
+        CK(cudaMemsetAsync(fn0, 0, sizeof(double), ctx->st));
+        CK(cudaMemcpyAsync(A + (size_t)ctx->nb * npw, ctx->d_lz_v, npw * sizeof(double2),
+                           cudaMemcpyDeviceToDevice, ctx->st));
+    }
+    // Lanczos step j on H v_j (in d_lz_f); v_{j+1} goes to row nb of `next`
+    auto lz_step = [&](int j, double2* next) {
+        lanczos_a(ctx->d_lz_f, ctx->d_lz_v, ctx->d_lz_v0, j > 0 ? ctx->d_lz + klz + j - 1 : nullptr,
+                  npw, ctx->d_lz + j, ctx->st);
+        lanczos_b(ctx->d_lz_f, ctx->d_lz_v, ctx->d_lz + j, npw, ctx->d_lz + klz + j, ctx->st);
+        if (j < klz - 1) {
+            lanczos_c(ctx->d_lz_f, ctx->d_lz_v, ctx->d_lz_v0, npw, ctx->d_lz + klz + j, ctx->st);
+            return cudaMemcpyAsync(next + (size_t)ctx->nb * npw, ctx->d_lz_v, npw * sizeof(double2),
+                                   cudaMemcpyDeviceToDevice, ctx->st);
+        }
+        return cudaSuccess;
+    };
     if (ndeg >= 1) {
-        s = apply_op_dev(ctx, A, B, ctx->nb, kEpiChebFirst, ctx->d_nsq + 1);
+        s = apply_op_dev(ctx, A, B, ctx->nb, kEpiChebFirst, ctx->d_nsq + 1, klz > 0);
         if (s) return s;
+        if (klz > 0) CK(lz_step(0, B));
     }
     for (int k = 2; k <= ndeg; ++k) {
         // psi_k = 2 sigma(H) psi_{k-1} - psi_{k-2}, written over psi_{k-2}
-        s = apply_op_dev(ctx, B, A, ctx->nb, kEpiCheb, ctx->d_nsq + k);
+        const bool lz = k - 1 < klz;
+        s = apply_op_dev(ctx, B, A, ctx->nb, kEpiCheb, ctx->d_nsq + k, lz);
         if (s) return s;
+        if (lz) CK(lz_step(k - 1, A));
         std::swap(A, B);
+    }
+    if (klz >= 2) {
+        ctx->lz_carry = true;
+        ctx->lz_carry_k = klz;
     }
     double2* fin = ndeg >= 1 ? B : A;
     double2* other = fin == ctx->d_psi ? ctx->d_psi2 : ctx->d_psi;
@@ -705,9 +867,11 @@ chfsi_status pack_beta_planes(chfsi_ctx* ctx) {
 }
 
 chfsi_status apply_h_dev32(chfsi_ctx* ctx, const float2* psi, float2* out, int nb, int mode,
-                           double* norm_acc, bool local_only = false) {
+                           double* norm_acc, bool local_only = false,
+                           const ResidStep* rs = nullptr) {
     Epilogue e{};
     e.mode = mode;
+    if (rs) { e.rc = rs->rc; e.lam = rs->lam; e.yres = rs->y; }
     e.kin = ctx->d_kin;
     e.coef = ctx->d_coef;
     e.nl = nullptr;
@@ -801,12 +965,166 @@ chfsi_status filter_dev32(chfsi_ctx* ctx, int ndeg, const double* eig_dev, int n
     return CHFSI_OK;
 }
 
+// ---------------------------------------------------------------- R-ChFSI
+// Residual-based Chebyshev filter (reference_paper/2025 main.tex Algorithm 3)
+// of the current Ritz pairs (X = d_psi, S-orthonormal; Lam = eig_dev), with
+// the exact Woodbury S^-1 as the approximate inverse, in the form with the
+// operator S^-1 H on unweighted residuals:
+//   Y = S^-1 (H X - S X Lam)                                   (FP64)
+//   R_1 = (s_1/e) Y, R_0 = 0
+//   R_k = a_k S^-1 H R_{k-1} + b_k R_{k-1} + c_k R_{k-2} + a_k Y L_{k-1}
+//   X_p = R_p + X L_p,  H X_p = H R_p + (H X) L_p              (FP64 out)
+// The recurrence runs in FP32 (tcgen05 projector products) when fp32: its
+// rounding enters through R, whose size falls with the residual of the Ritz
+// pairs, so the filtered block keeps FP64 accuracy as the SCF converges
+// (the plain FP32 filter stalls at its rounding level).  The Rayleigh-Ritz
+// that follows gets the full H X_p in FP64.
+chfsi_status alloc_rchfsi(chfsi_ctx* ctx, bool fp32) {
+    const size_t n = (size_t)ctx->nb * ctx->n_pw;
+    if (!ctx->d_rc_hx) CK(dalloc(&ctx->d_rc_hx, n));
+    if (!ctx->d_rc_y) CK(dalloc(&ctx->d_rc_y, n));
+    if (!ctx->d_rc_coef) CK(dalloc(&ctx->d_rc_coef, (size_t)3 * (ctx->max_deg + 1)));
+    if (!ctx->d_rc_lam) CK(dalloc(&ctx->d_rc_lam, (size_t)(ctx->max_deg + 1) * ctx->nb));
+    if (fp32) {
+        if (!ctx->d_rc_y32) CK(dalloc(&ctx->d_rc_y32, n));
+    } else {
+        if (!ctx->d_rc_r0) CK(dalloc(&ctx->d_rc_r0, n));
+        if (!ctx->d_rc_r1) CK(dalloc(&ctx->d_rc_r1, n));
+    }
+    return CHFSI_OK;
+}
+
+// out = a op(x) + b x + c out + a L y  (op = H, or S^-1 H when ultrasoft)
+chfsi_status rc_step64(chfsi_ctx* ctx, const double2* x, double2* out, const ResidStep& rs) {
+    const int nb = ctx->nb;
+    if (!ctx->uspp) return apply_h_dev(ctx, x, out, nb, kEpiResid, nullptr, -1, nullptr, &rs);
+    chfsi_status s = apply_h_dev(ctx, x, ctx->d_hpsi, nb, kEpiApply, nullptr);
+    if (s) return s;
+    cudaStream_t st = ctx->st;
+    gemm_cn(ctx->d_beta, ctx->n_pw, ctx->d_hpsi, ctx->n_pw, ctx->np, nb, ctx->n_pw, ctx->d_part,
+            ctx->d_cp, st);
+    gemm_tn(ctx->d_sinvT, ctx->np, ctx->d_cp, nb, ctx->d_cq, nb, ctx->np, nb, ctx->np, 1.0, 0.0, st);
+    gemm_tn(ctx->d_cq, nb, ctx->d_beta, ctx->n_pw, ctx->d_sx, ctx->n_pw, nb, ctx->n_pw, ctx->np, 1.0,
+            0.0, st);
+    const size_t n = (size_t)nb * ctx->n_pw;
+    count_launch();
+    k_cheb_combine<double2><<<grid_for(n), 256, 0, st>>>(
+        ctx->d_hpsi, ctx->d_sx, x, out, n, ctx->d_coef, 3, nullptr,
+        reinterpret_cast<const double2*>(rs.y), rs.lam, rs.rc, ctx->n_pw);
+    CK(cudaGetLastError());
+    return CHFSI_OK;
+}
+
+chfsi_status rc_step32(chfsi_ctx* ctx, const float2* x, float2* out, const ResidStep& rs) {
+    const int nb = ctx->nb;
+    if (!ctx->uspp) return apply_h_dev32(ctx, x, out, nb, kEpiResid, nullptr, false, &rs);
+    chfsi_status s = apply_h_dev32(ctx, x, ctx->d_hpsi32, nb, kEpiApply, nullptr);
+    if (s) return s;
+    cudaStream_t st = ctx->st;
+    tc_pack<float2>(ctx->d_hpsi32, ctx->n_pw, nb, ctx->n_pw, false, kSrcPlain, ctx->tp_psi_b, st);
+    CK(tc_gemm(ctx->tp_beta_a, ctx->tp_psi_b, ctx->np, nb, ctx->n_pw, kTcOutPartial, ctx->d_cp, nb,
+               ctx->d_tc_part, ctx->d_tc_err, st));
+    gemm_tn(ctx->d_sinvT, ctx->np, ctx->d_cp, nb, ctx->d_cq, nb, ctx->np, nb, ctx->np, 1.0, 0.0, st);
+    tc_pack<double2>(ctx->d_cq, nb, nb, ctx->np, true, kSrcConjT, ctx->tp_small_a, st);
+    CK(tc_gemm(ctx->tp_small_a, ctx->tp_betaT_b, nb, ctx->n_pw, ctx->np, kTcOutComplexF32,
+               ctx->d_nl32, ctx->n_pw, nullptr, ctx->d_tc_err, st));
+    const size_t n = (size_t)nb * ctx->n_pw;
+    count_launch();
+    k_cheb_combine<float2><<<grid_for(n), 256, 0, st>>>(
+        ctx->d_hpsi32, ctx->d_nl32, x, out, n, ctx->d_coef, 3, nullptr,
+        reinterpret_cast<const float2*>(rs.y), rs.lam, rs.rc, ctx->n_pw);
+    CK(cudaGetLastError());
+    return CHFSI_OK;
+}
+
+chfsi_status filter_rchfsi(chfsi_ctx* ctx, int ndeg, const double* eig_dev, int n_eig, bool fp32) {
+    const int nb = ctx->nb, npw = ctx->n_pw, np = ctx->np;
+    if (!eig_dev || n_eig != nb || ndeg < 1 || ndeg > ctx->max_deg)
+        return ctx->fail(CHFSI_ERR_BAD_INPUT, "R-ChFSI needs the Ritz values of every band");
+    chfsi_status s = alloc_rchfsi(ctx, fp32);
+    if (s) return s;
+    if (fp32 && np > 0 && !ctx->beta_planes_ready && (s = pack_beta_planes(ctx))) return s;
+    if ((s = compute_bounds(ctx, eig_dev, n_eig))) return s;
+    cudaStream_t st = ctx->st;
+    const size_t n = (size_t)nb * npw;
+    CK(cudaMemsetAsync(ctx->d_flags + 1, 0, sizeof(int), st));
+    CK(cudaMemsetAsync(ctx->d_nsq, 0, sizeof(double) * (ndeg + 1), st));
+    count_launch();
+    k_rc_tables<<<1, 256, 0, st>>>(ctx->d_coef, eig_dev, nb, ndeg, ctx->d_rc_coef, ctx->d_rc_lam);
+    // residual of the Ritz pairs, FP64
+    if ((s = apply_h_dev(ctx, ctx->d_psi, ctx->d_rc_hx, nb, kEpiApply, nullptr))) return s;
+    if (ctx->uspp) {
+        // S X - X = beta q beta^H X, then Y = S^-1 (H X - S X Lam)
+        gemm_cn(ctx->d_beta, npw, ctx->d_psi, npw, np, nb, npw, ctx->d_part, ctx->d_cp, st);
+        count_launch();
+        k_apply_dmat<<<grid_for((size_t)np * nb), 256, 0, st>>>(
+            ctx->d_cp, ctx->d_cd, np, nb, ctx->d_proj_ion, ctx->d_poff, ctx->d_doff, ctx->d_qmat);
+        gemm_tn(ctx->d_cd, nb, ctx->d_beta, npw, ctx->d_sx, npw, nb, npw, np, 1.0, 0.0, st);
+        count_launch();
+        k_rc_resid<<<grid_for(n), 256, 0, st>>>(ctx->d_rc_hx, ctx->d_psi, ctx->d_sx, eig_dev, npw, n,
+                                                ctx->d_rc_y);
+        gemm_cn(ctx->d_beta, npw, ctx->d_rc_y, npw, np, nb, npw, ctx->d_part, ctx->d_cp, st);
+        gemm_tn(ctx->d_sinvT, np, ctx->d_cp, nb, ctx->d_cq, nb, np, nb, np, 1.0, 0.0, st);
+        gemm_tn(ctx->d_cq, nb, ctx->d_beta, npw, ctx->d_sx, npw, nb, npw, np, 1.0, 0.0, st);
+        count_launch();
+        k_cheb_combine<double2><<<grid_for(n), 256, 0, st>>>(ctx->d_rc_y, ctx->d_sx, ctx->d_rc_y,
+                                                             ctx->d_rc_y, n, ctx->d_coef, 0, nullptr);
+    } else {
+        count_launch();
+        k_rc_resid<<<grid_for(n), 256, 0, st>>>(ctx->d_rc_hx, ctx->d_psi, nullptr, eig_dev, npw, n,
+                                                ctx->d_rc_y);
+    }
+    const double* lam = ctx->d_rc_lam;
+    if (fp32) {
+        float2* A = ctx->d_psi32a;  // R_{k-2}
+        float2* B = ctx->d_psi32b;  // R_{k-1}
+        count_launch();
+        k_rc_scale<float2><<<grid_for(n), 256, 0, st>>>(ctx->d_rc_y, ctx->d_rc_coef, n, B, ctx->d_rc_y32);
+        CK(cudaMemsetAsync(A, 0, n * sizeof(float2), st));
+        for (int k = 2; k <= ndeg; ++k) {
+            const ResidStep rs{ctx->d_rc_coef + 3 * k, lam + (size_t)(k - 1) * nb, ctx->d_rc_y32};
+            if ((s = rc_step32(ctx, B, A, rs))) return s;
+            std::swap(A, B);
+        }
+        if ((s = apply_h_dev32(ctx, B, ctx->d_hpsi32, nb, kEpiApply, nullptr))) return s;
+        count_launch();
+        k_rc_final<float2><<<grid_for(n), 256, 0, st>>>(B, ctx->d_hpsi32, ctx->d_psi, ctx->d_rc_hx,
+                                                        lam + (size_t)ndeg * nb, npw, n,
+                                                        ctx->d_psi2, ctx->d_hpsi);
+    } else {
+        double2* A = ctx->d_rc_r0;
+        double2* B = ctx->d_rc_r1;
+        count_launch();
+        k_rc_scale<double2><<<grid_for(n), 256, 0, st>>>(ctx->d_rc_y, ctx->d_rc_coef, n, B, nullptr);
+        CK(cudaMemsetAsync(A, 0, n * sizeof(double2), st));
+        for (int k = 2; k <= ndeg; ++k) {
+            const ResidStep rs{ctx->d_rc_coef + 3 * k, lam + (size_t)(k - 1) * nb, ctx->d_rc_y};
+            if ((s = rc_step64(ctx, B, A, rs))) return s;
+            std::swap(A, B);
+        }
+        if ((s = apply_h_dev(ctx, B, A, nb, kEpiApply, nullptr))) return s;
+        count_launch();
+        k_rc_final<double2><<<grid_for(n), 256, 0, st>>>(B, A, ctx->d_psi, ctx->d_rc_hx,
+                                                         lam + (size_t)ndeg * nb, npw, n,
+                                                         ctx->d_psi2, ctx->d_hpsi);
+    }
+    // copy back (fixed buffers, as a captured mixed pass needs)
+    CK(cudaMemcpyAsync(ctx->d_psi, ctx->d_psi2, n * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+    ctx->last_ndeg = ndeg;
+    CK(cudaGetLastError());
+    return CHFSI_OK;
+}
+
 // A pass without previous eigenvalues (the random start) filters with the
 // cut at lambda_max / 3, where the deepest states grow by ~1e9 over degree
 // 16 relative to the cut: FP32 rounding of the weakly amplified top bands
 // would swamp them, so such passes always run in FP64.
 chfsi_status filter_any(chfsi_ctx* ctx, int ndeg, const double* eig_dev, int n_eig) {
     ctx->last_pass_fp32 = ctx->mixed_active && eig_dev != nullptr && n_eig > 0;
+    if (ctx->cfg.filter_form == CHFSI_FILTER_RESIDUAL && eig_dev && n_eig == ctx->nb && ndeg >= 1) {
+        ctx->d_psi32 = nullptr;  // the Rayleigh-Ritz gets the full H psi in FP64
+        return filter_rchfsi(ctx, ndeg, eig_dev, n_eig, ctx->last_pass_fp32);
+    }
     if (ctx->last_pass_fp32) return filter_dev32(ctx, ndeg, eig_dev, n_eig);
     ctx->d_psi32 = nullptr;
     return filter_dev(ctx, ndeg, eig_dev, n_eig);
@@ -1108,7 +1426,10 @@ chfsi_status mix_features(chfsi_ctx* ctx, const MixRing& r, const double2* D, co
 }
 
 chfsi_status alloc_all(chfsi_ctx* ctx) {
-    const size_t nbpw = (size_t)ctx->nb * ctx->n_pw;
+    // band buffers keep one spare row: the Lanczos vector that the filter
+    // carries along as an extra column (CHFSI_BOUND_LANCZOS_FUSED)
+    const int nbx = ctx->nb + 1;
+    const size_t nbpw = (size_t)nbx * ctx->n_pw;
     CK(dalloc(&ctx->d_kin, ctx->n_pw));
     CK(dalloc(&ctx->d_perm, ctx->n_pw));
     CK(dalloc(&ctx->d_pw_col, ctx->n_pw));
@@ -1123,9 +1444,9 @@ chfsi_status alloc_all(chfsi_ctx* ctx) {
     if (ctx->np > 0) {
         CK(dalloc(&ctx->d_nl, nbpw));
         CK(dalloc(&ctx->d_beta, (size_t)ctx->np * ctx->n_pw));
-        CK(dalloc(&ctx->d_cp, (size_t)ctx->np * ctx->nb));
-        CK(dalloc(&ctx->d_cd, (size_t)ctx->np * ctx->nb));
-        CK(dalloc(&ctx->d_cq, (size_t)ctx->np * ctx->nb));
+        CK(dalloc(&ctx->d_cp, (size_t)ctx->np * nbx));
+        CK(dalloc(&ctx->d_cd, (size_t)ctx->np * nbx));
+        CK(dalloc(&ctx->d_cq, (size_t)ctx->np * nbx));
         CK(dalloc(&ctx->d_proj_ion, ctx->np));
         CK(dalloc(&ctx->d_poff, ctx->nions + 1));
         CK(dalloc(&ctx->d_doff, ctx->nions));
@@ -1150,7 +1471,7 @@ chfsi_status alloc_all(chfsi_ctx* ctx) {
     // (any band count 1..nb may reach the projector GEMM through chfsi_apply_h)
     size_t pe = splitk_partial_elems(ctx->nb, ctx->nb, ctx->n_pw);
     if (ctx->np > 0)
-        for (int n = 1; n <= ctx->nb; ++n)
+        for (int n = 1; n <= nbx; ++n)
             pe = std::max(pe, splitk_partial_elems(ctx->np, n, ctx->n_pw));
     ctx->part_elems = pe;
     CK(dalloc(&ctx->d_part, pe));
@@ -1196,7 +1517,8 @@ void free_all(chfsi_ctx* ctx) {
                   ctx->d_gmap_w, ctx->d_gmap_f, ctx->d_veff_d, ctx->d_rho_w, ctx->d_wgrid,
                   ctx->d_phase, ctx->d_dmat0, ctx->d_cion, ctx->d_vion, ctx->d_tpa, ctx->d_cgR,
                   ctx->d_cgv, ctx->d_cgc, ctx->d_cgov, ctx->d_cgpart, ctx->d_cgdot, ctx->d_cgG,
-                  ctx->d_psi_save};
+                  ctx->d_psi_save, ctx->d_rc_hx, ctx->d_rc_y, ctx->d_rc_r0, ctx->d_rc_r1,
+                  ctx->d_rc_y32, ctx->d_rc_coef, ctx->d_rc_lam};
     for (void* p : mp)
         if (p) cudaFree(p);
     if (ctx->h_pin) cudaFreeHost(ctx->h_pin);
@@ -1555,6 +1877,16 @@ chfsi_status chfsi_create(const chfsi_dims* dims, const chfsi_config* cfg, chfsi
     if (!ctx) return CHFSI_ERR_OUT_OF_MEMORY;
     ctx->dims = *dims;
     if (cfg) ctx->cfg = *cfg; else chfsi_default_config(&ctx->cfg);
+    if (ctx->cfg.filter_form != CHFSI_FILTER_CHEBYSHEV && ctx->cfg.filter_form != CHFSI_FILTER_RESIDUAL) {
+        delete ctx;
+        g_last_error = "unknown filter form";
+        return CHFSI_ERR_BAD_INPUT;
+    }
+    if (ctx->cfg.bound_mode < CHFSI_BOUND_HEURISTIC || ctx->cfg.bound_mode > CHFSI_BOUND_LANCZOS_FUSED) {
+        delete ctx;
+        g_last_error = "unknown bound mode";
+        return CHFSI_ERR_BAD_INPUT;
+    }
     if (ctx->cfg.precision != CHFSI_PREC_FP64 && ctx->cfg.precision != CHFSI_PREC_MIXED) {
         delete ctx;
         g_last_error = "unknown precision mode";
@@ -1666,7 +1998,7 @@ chfsi_status chfsi_set_basis(chfsi_ctx* ctx, const int32_t* miller, const double
     CK(dalloc(&ctx->d_col_start, ncol + 1));
     CK(dalloc(&ctx->d_col_pos, ncol));
     CK(dalloc(&ctx->d_xact, xact.size()));
-    CK(dalloc(&ctx->d_work, (size_t)ctx->nb * nz * ncol));
+    CK(dalloc(&ctx->d_work, (size_t)(ctx->nb + 1) * nz * ncol));
     CK(copy_sync(ctx->d_col_start, col_start.data(), sizeof(int) * (ncol + 1), cudaMemcpyHostToDevice, ctx->st));
     CK(copy_sync(ctx->d_col_pos, col_pos.data(), sizeof(int) * ncol, cudaMemcpyHostToDevice, ctx->st));
     CK(copy_sync(ctx->d_xact, xact.data(), sizeof(int) * xact.size(), cudaMemcpyHostToDevice, ctx->st));

@@ -302,11 +302,23 @@ k_zsticks_forward(const C* __restrict__ work, const C* __restrict__ psi, int ldp
     C* ob = out + (size_t)b * ldo;
     const C* nlb = e.nl ? reinterpret_cast<const C*>(e.nl) + (size_t)b * ldp : nullptr;
     R ie = 0, nc = 0;
-    if (MODE != kEpiApply) {
+    if (MODE == kEpiChebFirst || MODE == kEpiCheb) {
         ie = (R)e.coef[4];
         nc = (R)e.coef[5];
     }
+    R ra = 0, rb = 0, rcc = 0, rly = 0;
+    const C* yb = nullptr;
+    if (MODE == kEpiResid) {
+        ra = (R)e.rc[0];
+        rb = (R)e.rc[1];
+        rcc = (R)e.rc[2];
+        rly = (R)(e.rc[0] * e.lam[b]);
+        yb = reinterpret_cast<const C*>(e.yres) + (size_t)b * ldp;
+    }
     const R inv_n = (R)e.inv_n;
+    // the Lanczos vector carried in the batch: plain H x, no recurrence
+    const bool plain = b == e.plain_band;
+    C* pob = plain ? reinterpret_cast<C*>(e.plain_out) : nullptr;
     double nacc = 0.0;
     for (int q = g0 + threadIdx.x; q < g1; q += blockDim.x) {
         const C v = lines[(g.pw_col[q] - c0) * g.lsz + swz(g.pw_zpos[q], g.nz)];
@@ -315,8 +327,15 @@ k_zsticks_forward(const C* __restrict__ work, const C* __restrict__ psi, int ldp
         C h = mk(p.x * k, p.y * k);
         h = mk(h.x + v.x * inv_n, h.y + v.y * inv_n);
         if (nlb) h = cadd(h, nlb[q]);
-        if (MODE == kEpiApply) {
+        if (plain) {
+            pob[q] = h;
+        } else if (MODE == kEpiApply) {
             ob[q] = h;
+        } else if (MODE == kEpiResid) {
+            const C prev = ob[q];
+            const C y = yb[q];
+            ob[q] = mk(ra * h.x + rb * p.x + rcc * prev.x + rly * y.x,
+                       ra * h.y + rb * p.y + rcc * prev.y + rly * y.y);
         } else {
             C s = mk(h.x * ie + nc * p.x, h.y * ie + nc * p.y);
             C o;
@@ -643,6 +662,10 @@ void zsticks_forward_cols(const C* work, const C* psi, int ldp, C* out, int ldo,
     case kEpiChebFirst:
         allow_smem(k_zsticks_forward<C, kEpiChebFirst, COLS>, sm);
         k_zsticks_forward<C, kEpiChebFirst, COLS><<<grid, 256, sm, st>>>(work, psi, ldp, out, ldo, g, e);
+        break;
+    case kEpiResid:
+        allow_smem(k_zsticks_forward<C, kEpiResid, COLS>, sm);
+        k_zsticks_forward<C, kEpiResid, COLS><<<grid, 256, sm, st>>>(work, psi, ldp, out, ldo, g, e);
         break;
     default:
         allow_smem(k_zsticks_forward<C, kEpiCheb, COLS>, sm);

@@ -36,7 +36,7 @@ struct HGeom {
 };
 
 // Pass-3 epilogue: what to do with (H psi)_g once it is assembled.
-enum EpiMode { kEpiApply = 0, kEpiChebFirst = 1, kEpiCheb = 2 };
+enum EpiMode { kEpiApply = 0, kEpiChebFirst = 1, kEpiCheb = 2, kEpiResid = 3 };
 
 struct Epilogue {
     int mode;
@@ -45,6 +45,16 @@ struct Epilogue {
     const void* nl;        // non-local contribution (same type as psi), ld n_pw; may be null
     double* norm_acc;      // += sum |out|^2 (may be null)
     double inv_n;          // 1 / N^3
+    // one band of the batch that gets plain H x written to plain_out instead
+    // of the recurrence (the Lanczos vector carried along by the filter);
+    // -1: none
+    int plain_band = -1;
+    void* plain_out = nullptr;
+    // kEpiResid (residual Chebyshev step, R-ChFSI):
+    //   out = a H p + b p + c prev + a lam[band] y,  {a, b, c} = rc[0..2]
+    const double* rc = nullptr;
+    const double* lam = nullptr;   // per band
+    const void* yres = nullptr;    // residual Y (same type as psi), ld n_pw
 };
 
 // density accumulation keeps 24 plane points per thread x 512 threads

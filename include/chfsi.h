@@ -78,8 +78,23 @@ enum { CHFSI_PREC_FP64 = 0, CHFSI_PREC_MIXED = 1 };
 /* Upper spectral bound used by the filter. */
 enum {
     CHFSI_BOUND_HEURISTIC = 0, /* chebyshev.rs:225-254: 1/2 Gmax^2 + (maxV - minV) */
-    CHFSI_BOUND_LANCZOS   = 1  /* k-step Lanczos: lambda_max(T_k) + |f_k| (Zhou 2010) */
+    CHFSI_BOUND_LANCZOS   = 1, /* k-step Lanczos: lambda_max(T_k) + |f_k| (Zhou 2010) */
+    CHFSI_BOUND_LANCZOS_FUSED = 2 /* the same k-step Lanczos carried as one extra column of
+                                     the filter's own H applies (FP64 filter): each filter
+                                     leaves the bound for the next, no separate passes; the
+                                     first filter of a context, and mixed-precision filters,
+                                     run the k steps separately */
 };
+
+/* Form of the filter once Ritz values of the current block are known.
+ * CHEBYSHEV: the reference's three-term recurrence on the block itself
+ * (chebyshev.rs:626-816).  RESIDUAL: R-ChFSI (reference_paper/2025
+ * Algorithm 3), the sigma-scaled recurrence on the residuals H X - S X Lam of
+ * the Ritz pairs with the Woodbury S^-1 as approximate inverse: the same
+ * span in exact arithmetic, and in the mixed-precision mode an FP32/BF16x3
+ * filter whose error falls with the residual instead of stalling at FP32
+ * rounding.  The norm guard does not apply to the residual recurrence. */
+enum { CHFSI_FILTER_CHEBYSHEV = 0, CHFSI_FILTER_RESIDUAL = 1 };
 
 /* ------------------------------------------------------------------------ */
 /* Synthetic systems (the seeded inputs of the benchmark configurations).   */
@@ -175,7 +190,8 @@ typedef struct chfsi_config {
     int    bound_mode;      /* CHFSI_BOUND_*                                    */
     int    lanczos_steps;   /* k for CHFSI_BOUND_LANCZOS (default 10)          */
     int    check_norms;     /* 1: 10x norm-growth guard (chebyshev.rs:552-563) */
-    int    reserved[3];
+    int    filter_form;     /* CHFSI_FILTER_*                                  */
+    int    reserved[2];
 } chfsi_config;
 
 chfsi_status chfsi_default_config(chfsi_config* out);

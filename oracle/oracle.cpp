@@ -1043,6 +1043,73 @@ int oracle_chebyshev_filter(OracleCtx* c, int ndeg, const double* eig, int n_eig
     return status;
 }
 
+// Residual-based Chebyshev filter, R-ChFSI (reference_paper/2025 main.tex
+// Algorithm 3), for H x = e S x with the approximate inverse D^-1 taken as
+// the exact S^-1 (Woodbury), written for the operator S^-1 H on unweighted
+// residuals (R~ = D^-1 Z of the paper, which is the same recurrence after the
+// similarity D^-1 (.) D):
+//   Y   = S^-1 (H X - S X Lam)                     (residual of the Ritz pairs)
+//   R_0 = 0, R_1 = (s1/e) Y;  L_0 = 1, L_1 = (s1/e)(Lam - c)
+//   R_k = a_k S^-1 H R_{k-1} - a_k c R_{k-1} - s_{k-1} s_k R_{k-2} + a_k Y L_{k-1}
+//   L_k = a_k L_{k-1} Lam - a_k c L_{k-1} - s_{k-1} s_k L_{k-2}
+//   a_k = 2 s_k / e,  s_1 = e / (lambda_min - c),  s_k = 1 / (2 / s_1 - s_{k-1})
+//   X_p = R_p + X L_p
+// with the bounds of oracle_spectral_bounds and lambda_min = the lowest Ritz
+// value.  In exact arithmetic X_p = C_p(S^-1 H) X / C_p(s_1^-1 ...), the
+// sigma-scaled Chebyshev filter of X: the same span as the unscaled filter of
+// oracle_chebyshev_filter.  Needs the Ritz values of X (n_eig = n_bands).
+int oracle_rchfsi_filter(OracleCtx* c, int ndeg, const double* eig, int n_eig) {
+    const int nb = c->n_bands, npw = c->n_pw;
+    if (!eig || n_eig != nb || ndeg < 1) return -6;
+    double b4[4];
+    oracle_spectral_bounds(c, eig, n_eig, b4);
+    c->bounds.assign(b4, b4 + 4);
+    c->norms.clear();
+    const double cc = b4[2], e = b4[3];
+    double sigma = e / (eig[0] - cc);
+    const double sigma1 = sigma, gamma = 2.0 / sigma1;
+    const size_t n = c->psi.size();
+    std::vector<cplx> hx(n), sx(n), y(n), t(n), rx(n, 0.0), ry(n), tmp(n);
+    apply_h(*c, c->psi.data(), hx.data(), nb);
+    apply_s(*c, c->psi.data(), sx.data(), nb);
+#pragma omp parallel for
+    for (int b = 0; b < nb; ++b)
+        for (int g = 0; g < npw; ++g) {
+            const size_t i = (size_t)b * npw + g;
+            tmp[i] = hx[i] - sx[i] * eig[b];
+        }
+    apply_sinv(*c, tmp.data(), y.data(), nb);
+    std::vector<double> lx(nb, 1.0), ly(nb);
+    for (int b = 0; b < nb; ++b) ly[b] = sigma1 / e * (eig[b] - cc);
+#pragma omp parallel for
+    for (size_t i = 0; i < n; ++i) ry[i] = (sigma1 / e) * y[i];
+    for (int k = 2; k <= ndeg; ++k) {
+        const double s2 = 1.0 / (gamma - sigma);
+        const double a = 2.0 * s2 / e;
+        apply_h(*c, ry.data(), tmp.data(), nb);
+        apply_sinv(*c, tmp.data(), t.data(), nb);
+#pragma omp parallel for
+        for (int b = 0; b < nb; ++b)
+            for (int g = 0; g < npw; ++g) {
+                const size_t i = (size_t)b * npw + g;
+                rx[i] = a * t[i] - a * cc * ry[i] - sigma * s2 * rx[i] + a * y[i] * ly[b];
+            }
+        for (int b = 0; b < nb; ++b) lx[b] = a * ly[b] * eig[b] - a * cc * ly[b] - sigma * s2 * lx[b];
+        std::swap(rx, ry);
+        std::swap(lx, ly);
+        sigma = s2;
+    }
+#pragma omp parallel for
+    for (int b = 0; b < nb; ++b)
+        for (int g = 0; g < npw; ++g) {
+            const size_t i = (size_t)b * npw + g;
+            c->psi[i] = ry[i] + c->psi[i] * ly[b];
+        }
+    c->hpsi.resize(n);
+    apply_h(*c, c->psi.data(), c->hpsi.data(), nb);
+    return 0;
+}
+
 // Rayleigh-Ritz by Cholesky reduction (subspace_diag.rs:71-391):
 // H_sub, S_sub upper triangles + Hermitian fill + symmetrise; S = L L^H;
 // B = L^-1 H L^-H (symmetrised); B U = U diag(eps); V = L^-H U;

@@ -47,6 +47,7 @@ def lib():
         "oracle_apply_h": ([vp, vp, vp, C.c_int], None),
         "oracle_spectral_bounds": ([vp, dp, C.c_int, dp], None),
         "oracle_chebyshev_filter": ([vp, C.c_int, dp, C.c_int, ip], C.c_int),
+        "oracle_rchfsi_filter": ([vp, C.c_int, dp, C.c_int], C.c_int),
         "oracle_rayleigh_ritz": ([vp, dp, ip], C.c_int),
         "oracle_diagonalize": ([vp, C.c_int, dp, C.c_int, dp], C.c_int),
         "oracle_hegv": ([C.c_int, vp, vp, dp, vp], C.c_int),
@@ -244,6 +245,21 @@ class Oracle:
             e = np.ascontiguousarray(eigenvalues, dtype=np.float64)
             st = lib().oracle_chebyshev_filter(self.h, ndeg, _p(e, C.c_double), len(e), C.byref(fk))
         return st, fk.value
+
+    def rchfsi_filter(self, ndeg, eigenvalues):
+        """Residual-based Chebyshev filter (R-ChFSI) of the current Ritz pairs."""
+        e = np.ascontiguousarray(eigenvalues, dtype=np.float64)
+        st = lib().oracle_rchfsi_filter(self.h, ndeg, _p(e, C.c_double), len(e))
+        if st != 0:
+            raise RuntimeError("oracle R-ChFSI filter failed: %d" % st)
+
+    def rchfsi_diagonalize(self, ndeg, eigenvalues):
+        """R-ChFSI filter + Rayleigh-Ritz."""
+        self.rchfsi_filter(ndeg, eigenvalues)
+        st, w = self.rayleigh_ritz()
+        if st != 0:
+            raise RuntimeError("oracle Rayleigh-Ritz failed: %d" % st)
+        return w
 
     def rayleigh_ritz(self):
         w = np.zeros(self.n_bands)

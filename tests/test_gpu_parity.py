@@ -290,3 +290,31 @@ def test_diagonalize_band_count_edges(chfsi, oracle, n_bands, z_val):
         wc = o.diagonalize(12, wc)
     print("%d bands: %.3e Ha" % (n_bands, np.abs(wg - wc).max()))
     np.testing.assert_allclose(wg, wc, atol=1e-10, rtol=0)
+
+
+def test_fused_lanczos_bound_parity(chfsi, oracle, sys1s):
+    """Lanczos bound carried as one extra column of the filter's own H
+    applies (Zhou 2010; notes/pr-reviews/phase-2/deferred.md:131-161): the
+    bound a filter leaves for the next one equals the oracle's separate
+    k-step Lanczos bound on the same V_eff, and the filter that carries it
+    launches no H|psi> pass beyond the heuristic-bound filter's (only the
+    3k + 1 vector kernels of the Lanczos recurrence)."""
+    k = 10
+    fused = chfsi.Context(sys1s, bound_mode=chfsi.BOUND_LANCZOS_FUSED, lanczos_steps=k)
+    plain = chfsi.Context(sys1s)
+    o = oracle.Oracle.from_system(sys1s)
+    o.set_bound_mode(1, k)
+    v = o.vloc_r()
+    for c in (fused, plain):
+        c.set_veff(v)
+    o.set_veff(v)
+    fused.chebyshev_filter(16)   # first filter: separate Lanczos, carries the next one
+    plain.chebyshev_filter(16)
+    l0 = chfsi.launch_count()
+    fused.chebyshev_filter(16)   # bound from the carried column
+    l1 = chfsi.launch_count()
+    plain.chebyshev_filter(16)
+    l2 = chfsi.launch_count()
+    o.chebyshev_filter(16)
+    np.testing.assert_allclose(fused.bounds(), o.bounds(), rtol=1e-10)
+    assert (l1 - l0) - (l2 - l1) == 3 * k + 1
