@@ -213,6 +213,10 @@ def lib():
         "chfsi_autotune": [vp, C.POINTER(C.c_int), fp],
         "chfsi_set_launch_config": [vp, C.c_int],
         "chfsi_test_inject": [C.c_int, C.c_longlong],
+        "chfsi_zgemm_tn": [vp, C.c_int, vp, C.c_int, vp, C.c_int, C.c_int, C.c_int, C.c_int,
+                           C.c_double, C.c_double, vp],
+        "chfsi_hegv_dev": [vp, vp, C.c_int, dp, vp, vp],
+        "chfsi_hpsi_device_ptr": [vp, C.POINTER(vp)],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -337,6 +341,21 @@ def zgemm_cn_noalloc(a_dev, lda, b_dev, ldb, m, n, k, c_dev, stream=0):
     """zgemm_cn without device allocation (static 4 MiB scratch; m * n <= 262144)."""
     _check(lib().chfsi_zgemm_cn_noalloc(C.c_void_p(a_dev), lda, C.c_void_p(b_dev), ldb, m, n, k,
                                         C.c_void_p(c_dev), C.c_void_p(stream)))
+
+
+def zgemm_tn(w_dev, ldw, x_dev, ldx, o_dev, ldo, m, n, k, alpha=1.0, beta=0.0, stream=0):
+    """O[m][n] = alpha sum_k W[k][m] X[k][n] + beta O[m][n] (device pointers)."""
+    _check(lib().chfsi_zgemm_tn(C.c_void_p(w_dev), ldw, C.c_void_p(x_dev), ldx, C.c_void_p(o_dev),
+                                ldo, m, n, k, alpha, beta, C.c_void_p(stream)))
+
+
+def hegv_dev(h_dev, s_dev, n, v_dev, stream=0):
+    """H x = e S x on device n x n matrices; returns the eigenvalues (host),
+    eigenvectors as the columns of v_dev."""
+    w = np.zeros(n)
+    _check(lib().chfsi_hegv_dev(C.c_void_p(h_dev), C.c_void_p(s_dev), n, _ptr(w, C.c_double),
+                                C.c_void_p(v_dev), C.c_void_p(stream)))
+    return w
 
 
 def zgemm_cn_bf16x3(a_dev, lda, b_dev, ldb, m, n, k, c_dev, stream=0):
@@ -582,6 +601,11 @@ class Context:
         v = np.zeros(self.ng)
         self._c(lib().chfsi_get_veff(self.handle, _ptr(v, C.c_double)))
         return v
+
+    def hpsi_device_ptr(self):
+        p = C.c_void_p()
+        self._c(lib().chfsi_hpsi_device_ptr(self.handle, C.byref(p)))
+        return p.value
 
     def psi_device_ptr(self):
         p = C.c_void_p()

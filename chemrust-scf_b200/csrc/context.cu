@@ -3359,6 +3359,96 @@ extern "C" chfsi_status chfsi_zgemm_cn_bf16x3(const chfsi_c128* a_dev, int lda,
     return CHFSI_OK;
 }
 
+// O[m][n] = alpha sum_k W[k][m] X[k][n] + beta O[m][n] on device pointers: the
+// ZGEMM of the subspace rotation psi <- psi V (rayleigh_ritz.rs:209-227) and
+// the projector back-substitution beta (D C) (chebyshev.rs:480-497).
+extern "C" chfsi_status chfsi_zgemm_tn(const chfsi_c128* w_dev, int ldw, const chfsi_c128* x_dev,
+                                       int ldx, chfsi_c128* o_dev, int ldo, int m, int n, int k,
+                                       double alpha, double beta, void* stream) {
+    if (!w_dev || !x_dev || !o_dev || m <= 0 || n <= 0 || k <= 0 || k > kGemmMaxK || ldw < m ||
+        ldx < n || ldo < n) {
+        g_last_error = "chfsi_zgemm_tn: null pointer, size outside 1..2^30 or leading dimension too small";
+        return CHFSI_ERR_BAD_INPUT;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    gemm_tn(reinterpret_cast<const double2*>(w_dev), ldw, reinterpret_cast<const double2*>(x_dev),
+            ldx, reinterpret_cast<double2*>(o_dev), ldo, m, n, k, alpha, beta, st);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(e, "gemm_tn", __FILE__, __LINE__);
+    return CHFSI_OK;
+}
+
+// Generalised Hermitian eigenproblem H x = e S x of an n x n subspace pair on
+// the device (the ZHEGVD itype-1 contract of src/device/solver.rs:47-95, by
+// the Cholesky reduction of subspace_diag.rs:275-363): S = L L^H,
+// B = L^-1 H L^-H, B U = U diag(w), V = L^-H U.  h_dev, s_dev: row-major
+// n x n (read only); w_host: n eigenvalues ascending; v_dev: n x n with
+// column i the eigenvector of w[i] (row-major, V[j][i]).  Scratch is a
+// stream-ordered allocation on `stream`.  CHFSI_ERR_RR_FAILED when S is not
+// positive definite or the eigensolver does not converge.
+extern "C" chfsi_status chfsi_hegv_dev(const chfsi_c128* h_dev, const chfsi_c128* s_dev, int n,
+                                       double* w_host, chfsi_c128* v_dev, void* stream) {
+    if (!h_dev || !s_dev || !w_host || !v_dev || n <= 0 || n > 4096) {
+        g_last_error = "chfsi_hegv_dev: null pointer or n outside 1..4096";
+        return CHFSI_ERR_BAD_INPUT;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t nn = (size_t)n * n;
+    const int max_sweeps = 60;
+    const size_t jac = jacobi_scratch_doubles(n, max_sweeps);
+    char* buf = nullptr;
+    const size_t bytes = 5 * nn * sizeof(double2) + (jac + n) * sizeof(double) + 64;
+    cudaError_t e = cudaMallocAsync((void**)&buf, bytes, st);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMallocAsync", __FILE__, __LINE__);
+    double2* H = (double2*)buf;
+    double2* S = H + nn;
+    double2* T1 = S + nn;
+    double2* T2 = T1 + nn;
+    double2* V = T2 + nn;
+    double* w = (double*)(V + nn);
+    double* js = w + n;
+    int* flags = (int*)(js + jac);
+    cudaMemsetAsync(flags, 0, 4 * sizeof(int), st);
+    symmetrize(reinterpret_cast<const double2*>(h_dev), H, n, st);
+    symmetrize(reinterpret_cast<const double2*>(s_dev), S, n, st);
+    cholesky(S, n, flags + 0, st);
+    tri_inv(S, T1, n, st);                       // T1 = L^-1
+    small_gemm(0, 0, T1, H, T2, n, st);          // T2 = L^-1 H
+    small_gemm(0, 1, T2, T1, H, n, st);          // H = L^-1 H L^-H
+    symmetrize(H, T2, n, st);
+    e = jacobi(T2, V, n, max_sweeps, 1e-26, js, flags + 2, st);
+    if (e == cudaSuccess) {
+        sort_eig(T2, V, n, w, H, st);            // H = U (sorted)
+        small_gemm(1, 0, T1, H, reinterpret_cast<double2*>(v_dev), n, st);  // V = L^-H U
+        e = cudaGetLastError();
+    }
+    int fl[4] = {0, 0, 0, 0};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(w_host, w, sizeof(double) * n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(fl, flags, sizeof(fl), cudaMemcpyDeviceToHost, st);
+    cudaFreeAsync(buf, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(e, "chfsi_hegv_dev", __FILE__, __LINE__);
+    if (fl[0] != 0) {
+        g_last_error = "Rayleigh-Ritz failed: overlap not positive definite";
+        return CHFSI_ERR_RR_FAILED;
+    }
+    if (fl[2] >= max_sweeps) {
+        g_last_error = "Rayleigh-Ritz failed: eigensolver did not converge";
+        return CHFSI_ERR_RR_FAILED;
+    }
+    return CHFSI_OK;
+}
+
+// Device pointer of the context's H|psi> (n_bands x n_pw): after
+// chfsi_chebyshev_filter it holds H of the filtered block (the second output
+// of the reference's chebyshev_filter, chebyshev.rs:626-643).
+extern "C" chfsi_status chfsi_hpsi_device_ptr(chfsi_ctx* ctx, chfsi_c128** out) {
+    if (!ctx || !out) return CHFSI_ERR_BAD_INPUT;
+    *out = reinterpret_cast<chfsi_c128*>(ctx->d_hpsi);
+    return CHFSI_OK;
+}
+
 // Host-side fault injection for the error-path tests (no GPU fault is made:
 // an injected tensor-core timeout is a producer that issues no loads, so the
 // consumer's bounded wait runs out with nothing in flight).

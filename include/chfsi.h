@@ -444,6 +444,22 @@ chfsi_status chfsi_set_mixer(chfsi_ctx* ctx, chfsi_mixer* m);
 chfsi_status chfsi_mixer_samples(chfsi_ctx* ctx, const double* rho_in, const double* rho_out,
                                  int n_iter, const double* rho_star, float* x, float* t);
 
+/* O[m][n] = alpha sum_k W[k][m] X[k][n] + beta O[m][n] (device pointers,
+ * row-major): the rotation psi <- psi V of rayleigh_ritz.rs:209-227 and the
+ * projector back-substitution of chebyshev.rs:480-497.  Blocks until done. */
+chfsi_status chfsi_zgemm_tn(const chfsi_c128* w_dev, int ldw, const chfsi_c128* x_dev, int ldx,
+                            chfsi_c128* o_dev, int ldo, int m, int n, int k, double alpha,
+                            double beta, void* stream);
+/* Subspace eigenproblem H x = e S x (n x n, device, row-major), the ZHEGVD
+ * itype-1 contract of src/device/solver.rs:47-95 solved by Cholesky
+ * reduction and the library's Jacobi eigensolver: eigenvalues ascending to
+ * w_host, eigenvectors as the columns of v_dev (V[j][i]).  Blocks until done. */
+chfsi_status chfsi_hegv_dev(const chfsi_c128* h_dev, const chfsi_c128* s_dev, int n,
+                            double* w_host, chfsi_c128* v_dev, void* stream);
+/* Device pointer of the context's H|psi> (after chfsi_chebyshev_filter: H of
+ * the filtered block, the second output of chebyshev.rs:626-643). */
+chfsi_status chfsi_hpsi_device_ptr(chfsi_ctx* ctx, chfsi_c128** out);
+
 /* ---- test hooks (host-side fault injection; no counterpart in the crate) --
  * CHFSI_INJECT_TC_NO_LOADS: the next `arg` tensor-core GEMM launches run with
  *   a producer that issues no loads; the consumer's wait runs out after 20 ms
