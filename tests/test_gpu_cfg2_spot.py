@@ -4,8 +4,8 @@ against the oracle: H|psi> and S^-1 H|psi> of 8 bands (chebyshev.rs:279-500
 with the Woodbury S^-1 of the generalised problem), and one density build with
 augmentation charges on the 144^3 grid (construct_density, scf.rs:275-279,
 against oracle/uspp_oracle.py).  The system carries 16 bands instead of 576
-so that the oracle side stays within seconds; every grid, basis and
-projector set is the configuration's own."""
+(valence charge 1/8 per atom) so that the oracle side stays within seconds;
+every grid, the basis and the projector set are the configuration's own."""
 import os
 import sys
 
@@ -21,7 +21,9 @@ NB = 8
 
 @pytest.fixture(scope="module")
 def sys2(chfsi):
-    s = chfsi.SyntheticSystem(config_index=2, n_bands=16)
+    # valence charge 1/8 per atom so that 16 bands hold the 27 electrons; the
+    # grids, the plane-wave basis, the projectors and q are the configuration's
+    s = chfsi.SyntheticSystem(config_index=2, n_bands=16, z_val=0.125)
     assert s.ngrid == (108, 108, 108) and s.ngrid_density == (144, 144, 144)
     assert s.n_proj == 1728 and s.uspp
     return s

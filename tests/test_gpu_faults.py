@@ -39,15 +39,20 @@ def test_tensor_core_wait_timeout_is_reported_and_recoverable(chfsi, sys_kb):
     v = ref.get_vloc()
     ctx.set_veff(v)
     ref.set_veff(v)
-    psi0 = sys_kb.psi0()
+    # the first pass (no Ritz values yet) is FP64; the second is mixed and
+    # runs the projector products on the tensor cores
+    w = ctx.diagonalize(8)
+    wr = ref.diagonalize(8)
+    psi1 = ctx.get_psi()
     chfsi.inject_fault(chfsi.INJECT_TC_NO_LOADS, 1)
     with pytest.raises(chfsi.Timeout, match="timed out"):
-        ctx.diagonalize(8)
+        ctx.diagonalize(8, w)
     chfsi.inject_fault(chfsi.INJECT_NONE)
-    # the context is usable: same pass from the same start as a fresh context
-    ctx.set_psi(psi0)
-    w1 = ctx.diagonalize(8)
-    w2 = ref.diagonalize(8)
+    # the context is usable: the same mixed pass from the same start as the
+    # context that saw no fault
+    ctx.set_psi(psi1)
+    w1 = ctx.diagonalize(8, w)
+    w2 = ref.diagonalize(8, wr)
     np.testing.assert_allclose(w1, w2, atol=1e-12, rtol=0)
 
 
