@@ -30,6 +30,7 @@ INJECT_NONE, INJECT_TC_NO_LOADS, INJECT_ALLOC_FAIL = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
 BOUND_HEURISTIC, BOUND_LANCZOS, BOUND_LANCZOS_FUSED = 0, 1, 2
 FILTER_CHEBYSHEV, FILTER_RESIDUAL = 0, 1
+XC_LDA_PZ, XC_PBE = 0, 1
 MIXER_PULAY, MIXER_LEARNED, MIXER_LEARNED_PULAY = 0, 1, 2
 MIXER_FEATURES, MIXER_OUTPUTS, MIXER_TARGETS, MIXER_SHELLS = 512, 128, 320, 64
 
@@ -213,6 +214,10 @@ def lib():
         "chfsi_autotune": [vp, C.POINTER(C.c_int), fp],
         "chfsi_set_launch_config": [vp, C.c_int],
         "chfsi_test_inject": [C.c_int, C.c_longlong],
+        "chfsi_set_xc": [vp, C.c_int],
+        "chfsi_set_ions": [vp, C.c_int, dp, dp, dp, dp],
+        "chfsi_forces": [vp, dp],
+        "chfsi_system_generate_at": [C.POINTER(SynthParams), dp, C.POINTER(vp)],
         "chfsi_zgemm_tn": [vp, C.c_int, vp, C.c_int, vp, C.c_int, C.c_int, C.c_int, C.c_int,
                            C.c_double, C.c_double, vp],
         "chfsi_hegv_dev": [vp, vp, C.c_int, dp, vp, vp],
@@ -405,7 +410,9 @@ class SyntheticSystem:
     def _chk(st):
         _check(st)
 
-    def __init__(self, params=None, config_index=None, **overrides):
+    def __init__(self, params=None, config_index=None, positions=None, **overrides):
+        """positions: Cartesian atom positions (n_atoms x 3, bohr) in place of
+        the seeded jittered lattice."""
         L = self._L()
         if params is None:
             params = SynthParams()
@@ -420,7 +427,12 @@ class SyntheticSystem:
                 setattr(params, k, v)
         self.params = params
         h = C.c_void_p()
-        self._chk(L.chfsi_system_generate(C.byref(params), C.byref(h)))
+        if positions is None:
+            self._chk(L.chfsi_system_generate(C.byref(params), C.byref(h)))
+        else:
+            pos = np.ascontiguousarray(positions, dtype=np.float64).ravel()
+            self._chk(L.chfsi_system_generate_at(C.byref(params), _ptr(pos, C.c_double),
+                                                 C.byref(h)))
         self.handle = h
         info = SystemInfo()
         self._chk(L.chfsi_system_get_info(h, C.byref(info)))
@@ -512,6 +524,8 @@ class Context:
             self.ngrid, self.n_pw, self.n_bands = tuple(dims["ngrid"]), d.n_pw, d.n_bands
         self.handle = h
         self.ng = int(np.prod(self.ngrid))
+        if system is not None:
+            self._n_atoms = system.n_atoms
         self._refresh_density_grid()
 
     def _refresh_density_grid(self):
@@ -678,6 +692,28 @@ class Context:
         e2 = np.zeros(2)
         self._c(lib().chfsi_build_veff(self.handle, _ptr(r, C.c_double), _ptr(e2, C.c_double)))
         return e2
+
+    def set_xc(self, functional):
+        """XC_LDA_PZ (default) or XC_PBE for build_v_eff and run_scf."""
+        self._c(lib().chfsi_set_xc(self.handle, functional))
+
+    def set_ions(self, positions, zion, rc_loc, kpt=(0.0, 0.0, 0.0)):
+        pos = np.ascontiguousarray(positions, dtype=np.float64).ravel()
+        z = np.ascontiguousarray(zion, dtype=np.float64)
+        rc = np.ascontiguousarray(rc_loc, dtype=np.float64)
+        k = np.ascontiguousarray(kpt, dtype=np.float64)
+        self._c(lib().chfsi_set_ions(self.handle, len(z), _ptr(pos, C.c_double), _ptr(z, C.c_double),
+                                     _ptr(rc, C.c_double), _ptr(k, C.c_double)))
+        self._n_atoms = len(z)
+
+    def forces(self):
+        """Hellmann-Feynman forces (n_atoms x 3, Ha/bohr) of the current state."""
+        n = getattr(self, "_n_atoms", None)
+        if n is None:
+            raise BadInput("ions not set")
+        f = np.zeros((n, 3))
+        self._c(lib().chfsi_forces(self.handle, _ptr(f, C.c_double)))
+        return f
 
     def get_density(self):
         r = np.zeros(self.ng_density)

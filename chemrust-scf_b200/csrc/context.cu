@@ -422,6 +422,7 @@ struct chfsi_ctx {
     bool have_vloc = false;
     double kin_max = 0.0, omega = 0.0, n_elec = 0.0, e_ewald = 0.0, n_atoms = 1.0;
     double recip[9] = {};
+    double lattice[9] = {};
     // geometry
     HGeom geo{};
     AxisPlan ax{}, ay{}, az{};
@@ -512,6 +513,18 @@ struct chfsi_ctx {
     bool fine = false;
     int* d_gmap_w = nullptr; int* d_gmap_f = nullptr; int n_gmap = 0;  // shared G vectors
     double* d_veff_d = nullptr;   // V_eff on the density grid
+    // exchange-correlation functional; PBE scratch: three complex density
+    // grids (gradient, then 2 de/dsigma grad rho) and de/drho
+    int xc = CHFSI_XC_LDA_PZ;
+    double2* d_gga = nullptr; double* d_gga_v1 = nullptr;
+    // ions for forces (chfsi_set_ions)
+    int n_ion_atoms = 0;
+    std::vector<double> atom_pos, atom_z, atom_rc;
+    double ion_kpt[3] = {0.0, 0.0, 0.0};
+    double* d_ion = nullptr;      // positions (3n), z (n), rc (n), forces (3n)
+    double* d_qvec = nullptr;     // Cartesian G + k per plane wave, 3 x n_pw
+    int* d_atom_of_ion = nullptr;
+    std::vector<int32_t> miller_ctx;  // Miller indices in the context's plane-wave order
     double* d_rho_w = nullptr;    // smooth density on the wavefunction grid
     double2* d_wgrid = nullptr;   // wavefunction-grid complex scratch
     // ultrasoft augmentation Q_ij(r) = q_ij g(|r - R_I|)
@@ -1248,14 +1261,35 @@ chfsi_status screen_dmat(chfsi_ctx* ctx) {
 }
 
 // veff = vloc + V_H[rho] + V_xc[rho]; acc[0] += E_H[rho], acc[1] += E_xc[rho]
+// grad rho of the density whose forward FFT is in d_cgrid: real parts of the
+// three d_gga grids (PBE)
+void gga_gradient(chfsi_ctx* ctx) {
+    const size_t ng = ctx->fng;
+    double2* g0 = ctx->d_gga;
+    launch_grad_gspace(ctx->d_cgrid, grid_recip(ctx), g0, g0 + ng, g0 + 2 * ng, ctx->st);
+    for (int a = 0; a < 3; ++a) grid_fft3(ctx, g0 + a * ng, false);
+}
+
 chfsi_status build_veff_dev(chfsi_ctx* ctx, const double* rho, double* acc) {
     const size_t ng = ctx->fng;
+    const double dv = ctx->omega / (double)ng;
     launch_real_to_complex(rho, ctx->d_cgrid, ng, ctx->st);
     grid_fft3(ctx, ctx->d_cgrid, true);
+    const bool gga = ctx->xc == CHFSI_XC_PBE;
+    if (gga) gga_gradient(ctx);
     launch_hartree_gspace(ctx->d_cgrid, grid_recip(ctx), ctx->omega, acc + 0, ctx->st);
     grid_fft3(ctx, ctx->d_cgrid, false);
-    launch_assemble_veff(ctx->d_vloc, ctx->d_cgrid, rho, ctx->d_veff_d, ng,
-                         ctx->omega / (double)ng, acc + 1, ctx->st);
+    if (!gga) {
+        launch_assemble_veff(ctx->d_vloc, ctx->d_cgrid, rho, ctx->d_veff_d, ng, dv, acc + 1, ctx->st);
+    } else {
+        // V_xc = de/drho - div(2 de/dsigma grad rho)
+        double2* g0 = ctx->d_gga;
+        launch_pbe_point(rho, g0, g0 + ng, g0 + 2 * ng, ctx->d_gga_v1, ng, dv, acc + 1, true, ctx->st);
+        for (int a = 0; a < 3; ++a) grid_fft3(ctx, g0 + a * ng, true);
+        launch_div_gspace(g0, g0 + ng, g0 + 2 * ng, grid_recip(ctx), g0, ctx->st);
+        grid_fft3(ctx, g0, false);
+        launch_assemble_gga(ctx->d_vloc, ctx->d_cgrid, ctx->d_gga_v1, g0, ctx->d_veff_d, ng, ctx->st);
+    }
     project_veff(ctx);
     CK(cudaGetLastError());
     return CHFSI_OK;
@@ -1518,7 +1552,8 @@ void free_all(chfsi_ctx* ctx) {
                   ctx->d_phase, ctx->d_dmat0, ctx->d_cion, ctx->d_vion, ctx->d_tpa, ctx->d_cgR,
                   ctx->d_cgv, ctx->d_cgc, ctx->d_cgov, ctx->d_cgpart, ctx->d_cgdot, ctx->d_cgG,
                   ctx->d_psi_save, ctx->d_rc_hx, ctx->d_rc_y, ctx->d_rc_r0, ctx->d_rc_r1,
-                  ctx->d_rc_y32, ctx->d_rc_coef, ctx->d_rc_lam};
+                  ctx->d_rc_y32, ctx->d_rc_coef, ctx->d_rc_lam, ctx->d_gga, ctx->d_gga_v1,
+                  ctx->d_ion, ctx->d_qvec, ctx->d_atom_of_ion};
     for (void* p : mp)
         if (p) cudaFree(p);
     if (ctx->h_pin) cudaFreeHost(ctx->h_pin);
@@ -1960,6 +1995,10 @@ chfsi_status chfsi_set_basis(chfsi_ctx* ctx, const int32_t* miller, const double
     ctx->perm_identity = true;
     for (int g = 0; g < n; ++g)
         if (perm[g] != g) { ctx->perm_identity = false; break; }
+    ctx->miller_ctx.resize(3 * (size_t)n);
+    for (int i = 0; i < n; ++i)
+        for (int d = 0; d < 3; ++d) ctx->miller_ctx[3 * (size_t)i + d] = miller[3 * (size_t)perm[i] + d];
+    if (ctx->d_qvec) { cudaFree(ctx->d_qvec); ctx->d_qvec = nullptr; }
     std::vector<int> col_start, col_pos, pw_col(n), pw_zpos(n), xact;
     std::vector<double> kin(n);
     std::vector<char> xused(nx, 0);
@@ -2379,6 +2418,13 @@ chfsi_status chfsi_create_from_system(const chfsi_system* sys, const chfsi_confi
             return bail(st);
         if ((st = chfsi_set_augmentation(ctx, s.pos.data(), s.q_width))) return bail(st);
     }
+    {
+        // ions of the analytic local model, for forces
+        std::vector<double> rc(s.n_atoms, s.params.rc_loc);
+        if ((st = chfsi_set_ions(ctx, s.n_atoms, s.pos.data(), s.zion.data(), rc.data(),
+                                 s.params.kpt)))
+            return bail(st);
+    }
     // a usable V_eff before the first SCF step: V_loc alone
     if (cudaError_t e = cudaMemcpyAsync(ctx->d_veff_d, ctx->d_vloc, sizeof(double) * ctx->fng,
                                         cudaMemcpyDeviceToDevice, ctx->st))
@@ -2420,6 +2466,7 @@ chfsi_status chfsi_set_cell(chfsi_ctx* ctx, const double* lattice, double e_ewal
     cross(a + 6, a + 0, ctx->recip + 3);
     cross(a + 0, a + 3, ctx->recip + 6);
     for (int i = 0; i < 9; ++i) ctx->recip[i] *= tp;
+    std::memcpy(ctx->lattice, lattice, sizeof(ctx->lattice));
     ctx->e_ewald = e_ewald;
     ctx->n_atoms = n_atoms;
     return CHFSI_OK;
@@ -2733,9 +2780,17 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
         CK(cudaMemsetAsync(ctx->d_acc, 0, sizeof(double) * 8, st));
         launch_real_to_complex(ctx->d_rho_out, ctx->d_cgrid, ng, st);
         grid_fft3(ctx, ctx->d_cgrid, true);
+        if (ctx->xc == CHFSI_XC_PBE) gga_gradient(ctx);
         launch_hartree_gspace(ctx->d_cgrid, grid_recip(ctx), ctx->omega, ctx->d_acc + 0, st);
         launch_energy_terms(ctx->d_rho_out, ctx->d_veff_d, ctx->d_vloc, ng, dv, ctx->d_acc + 1,
                             ctx->d_acc + 2, st);
+        if (ctx->xc == CHFSI_XC_PBE) {
+            // E_xc of rho_out from the gradient formed above (the LDA sum is discarded)
+            CK(cudaMemsetAsync(ctx->d_acc + 1, 0, sizeof(double), st));
+            double2* g0 = ctx->d_gga;
+            launch_pbe_point(ctx->d_rho_out, g0, g0 + ng, g0 + 2 * ng, nullptr, ng, dv,
+                             ctx->d_acc + 1, false, st);
+        }
         CK(cudaGetLastError());
         double acc[3];
         CK(cudaMemcpyAsync(acc, ctx->d_acc, sizeof(acc), cudaMemcpyDeviceToHost, st));
@@ -2933,6 +2988,110 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
     r->status = status;
     if (r->eigenvalues) std::memcpy(r->eigenvalues, eig.data(), sizeof(double) * ctx->nb);
     return status;
+}
+
+extern "C" chfsi_status chfsi_set_xc(chfsi_ctx* ctx, int functional) {
+    if (!ctx) return CHFSI_ERR_BAD_INPUT;
+    if (functional != CHFSI_XC_LDA_PZ && functional != CHFSI_XC_PBE)
+        return ctx->fail(CHFSI_ERR_BAD_INPUT, "unknown exchange-correlation functional");
+    cudaSetDevice(ctx->device);
+    if (functional == CHFSI_XC_PBE) {
+        if (!ctx->d_gga) CK(dalloc(&ctx->d_gga, 3 * ctx->fng));
+        if (!ctx->d_gga_v1) CK(dalloc(&ctx->d_gga_v1, ctx->fng));
+    }
+    ctx->xc = functional;
+    return CHFSI_OK;
+}
+
+extern "C" chfsi_status chfsi_set_ions(chfsi_ctx* ctx, int n_atoms, const double* positions,
+                                       const double* zion, const double* rc_loc, const double* kpt) {
+    if (!ctx || n_atoms <= 0 || !positions || !zion || !rc_loc)
+        return CHFSI_ERR_BAD_INPUT;
+    if (ctx->np > 0 && ctx->nions > n_atoms)
+        return ctx->fail(CHFSI_ERR_BAD_INPUT, "more ions with projectors than atoms");
+    cudaSetDevice(ctx->device);
+    ctx->n_ion_atoms = n_atoms;
+    ctx->atom_pos.assign(positions, positions + 3 * (size_t)n_atoms);
+    ctx->atom_z.assign(zion, zion + n_atoms);
+    ctx->atom_rc.assign(rc_loc, rc_loc + n_atoms);
+    for (int d = 0; d < 3; ++d) ctx->ion_kpt[d] = kpt ? kpt[d] : 0.0;
+    if (ctx->d_ion) cudaFree(ctx->d_ion);
+    if (ctx->d_atom_of_ion) cudaFree(ctx->d_atom_of_ion);
+    ctx->d_ion = nullptr;
+    ctx->d_atom_of_ion = nullptr;
+    CK(dalloc(&ctx->d_ion, 8 * (size_t)n_atoms));
+    std::vector<double> h(5 * (size_t)n_atoms);
+    std::memcpy(h.data(), positions, sizeof(double) * 3 * n_atoms);
+    std::memcpy(h.data() + 3 * n_atoms, zion, sizeof(double) * n_atoms);
+    std::memcpy(h.data() + 4 * n_atoms, rc_loc, sizeof(double) * n_atoms);
+    CK(copy_sync(ctx->d_ion, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice, ctx->st));
+    if (ctx->nions > 0) {
+        std::vector<int> map(ctx->nions);
+        for (int i = 0; i < ctx->nions; ++i) map[i] = i;
+        CK(dalloc(&ctx->d_atom_of_ion, ctx->nions));
+        CK(copy_sync(ctx->d_atom_of_ion, map.data(), sizeof(int) * map.size(), cudaMemcpyHostToDevice,
+                     ctx->st));
+    }
+    if (ctx->d_qvec) { cudaFree(ctx->d_qvec); ctx->d_qvec = nullptr; }
+    return CHFSI_OK;
+}
+
+extern "C" chfsi_status chfsi_forces(chfsi_ctx* ctx, double* forces) {
+    if (!ctx || !forces) return CHFSI_ERR_BAD_INPUT;
+    if (ctx->n_ion_atoms == 0) return ctx->fail(CHFSI_ERR_BAD_INPUT, "ions not set (chfsi_set_ions)");
+    if (ctx->omega <= 0.0 || !ctx->basis_set || !ctx->psi_set)
+        return ctx->fail(CHFSI_ERR_BAD_INPUT, "context not fully initialised");
+    if (ctx->uspp)
+        return ctx->fail(CHFSI_ERR_NOT_IMPLEMENTED, "forces of ultrasoft cells are not built");
+    if (ctx->fng != ctx->ng)
+        return ctx->fail(CHFSI_ERR_NOT_IMPLEMENTED, "forces need the density grid equal to the FFT grid");
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->st;
+    const int na = ctx->n_ion_atoms, nb = ctx->nb, npw = ctx->n_pw, np = ctx->np;
+    double* d_pos = ctx->d_ion;
+    double* d_z = d_pos + 3 * na;
+    double* d_rc = d_z + na;
+    double* d_f = d_rc + na;
+    CK(cudaMemsetAsync(d_f, 0, sizeof(double) * 3 * na, st));
+    // local part from rho_out in G space
+    const size_t ng = ctx->fng;
+    launch_real_to_complex(ctx->d_rho_out, ctx->d_cgrid, ng, st);
+    grid_fft3(ctx, ctx->d_cgrid, true);
+    const int wave[3] = {ctx->nx, ctx->ny, ctx->nz};
+    launch_force_local(ctx->d_cgrid, grid_recip(ctx), wave, d_pos, d_z, d_rc, na, ctx->omega, d_f, st);
+    // non-local part: C = beta^H psi, B_a = beta^H (q_a psi)
+    if (np > 0) {
+        if (!ctx->d_qvec) {
+            std::vector<double> q(3 * (size_t)npw);
+            for (int i = 0; i < npw; ++i) {
+                const double m[3] = {ctx->miller_ctx[3 * (size_t)i] + ctx->ion_kpt[0],
+                                     ctx->miller_ctx[3 * (size_t)i + 1] + ctx->ion_kpt[1],
+                                     ctx->miller_ctx[3 * (size_t)i + 2] + ctx->ion_kpt[2]};
+                for (int d = 0; d < 3; ++d)
+                    q[(size_t)d * npw + i] = m[0] * ctx->recip[d] + m[1] * ctx->recip[3 + d] +
+                                             m[2] * ctx->recip[6 + d];
+            }
+            CK(dalloc(&ctx->d_qvec, q.size()));
+            CK(copy_sync(ctx->d_qvec, q.data(), sizeof(double) * q.size(), cudaMemcpyHostToDevice, st));
+        }
+        gemm_cn(ctx->d_beta, npw, ctx->d_psi, npw, np, nb, npw, ctx->d_part, ctx->d_cp, st);
+        for (int a = 0; a < 3; ++a) {
+            launch_scale_pw(ctx->d_psi, ctx->d_qvec + (size_t)a * npw, npw, nb, ctx->d_hpsi, st);
+            gemm_cn(ctx->d_beta, npw, ctx->d_hpsi, npw, np, nb, npw, ctx->d_part, ctx->d_cd, st);
+            launch_force_nl(ctx->d_cp, ctx->d_cd, nb, ctx->d_occ, ctx->d_poff, ctx->d_doff,
+                            ctx->d_dmat, ctx->nions, a, ctx->d_atom_of_ion, d_f, st);
+        }
+    }
+    CK(cudaGetLastError());
+    std::vector<double> f(3 * (size_t)na);
+    CK(copy_sync(f.data(), d_f, sizeof(double) * f.size(), cudaMemcpyDeviceToHost, st));
+    // ion-ion part
+    double lat[9];
+    for (int i = 0; i < 9; ++i) lat[i] = ctx->lattice[i];
+    std::vector<double> fe;
+    ewald_forces(lat, ctx->recip, ctx->atom_pos, ctx->atom_z, fe);
+    for (size_t i = 0; i < f.size(); ++i) forces[i] = f[i] + fe[i];
+    return CHFSI_OK;
 }
 
 extern "C" chfsi_status chfsi_get_density(chfsi_ctx* ctx, double* rho) {

@@ -1,6 +1,8 @@
 // Launch interfaces of the device kernels (host side).
 #pragma once
 
+#include <vector>
+
 #include <cuda_runtime.h>
 #include <cstddef>
 #include <cstdint>
@@ -90,6 +92,31 @@ struct GridRecip {
     double b[9];       // reciprocal lattice rows b1, b2, b3
 };
 void launch_real_to_complex(const double* r, double2* c, size_t n, cudaStream_t st);
+// ---- GGA (PBE) pieces, gga.cu
+// o_a = i G_a f(G) / N (digit-reversed density-grid layout)
+void launch_grad_gspace(const double2* f, const GridRecip& gr, double2* o0, double2* o1,
+                        double2* o2, cudaStream_t st);
+// pointwise PBE on rho and grad rho (real parts of g0..g2): exc_acc += E_xc;
+// with want_potential: v1 = de/drho, g_a <- 2 de/dsigma grad_a rho
+void launch_pbe_point(const double* rho, double2* g0, double2* g1, double2* g2, double* v1,
+                      size_t n, double dv, double* exc_acc, bool want_potential, cudaStream_t st);
+// o = sum_a i G_a h_a(G) / N
+void launch_div_gspace(const double2* h0, const double2* h1, const double2* h2,
+                       const GridRecip& gr, double2* o, cudaStream_t st);
+// veff = vloc + Re vh + v1 - Re div
+void launch_assemble_gga(const double* vloc, const double2* vh, const double* v1,
+                         const double2* div, double* veff, size_t n, cudaStream_t st);
+// ---- Hellmann-Feynman forces, forces.cu
+void launch_force_local(const double2* rhog, const GridRecip& gr, const int* wave_grid,
+                        const double* pos, const double* zion, const double* rc, int n_ions,
+                        double omega, double* force, cudaStream_t st);
+void launch_scale_pw(const double2* psi, const double* q, int npw, int nb, double2* out,
+                     cudaStream_t st);
+void launch_force_nl(const double2* C, const double2* B, int nb, const double* occ,
+                     const int* poff, const int* doff, const double2* dmat, int n_ions, int axis,
+                     const int* atom_of_ion, double* force, cudaStream_t st);
+void ewald_forces(const double* lattice, const double* recip, const std::vector<double>& pos,
+                  const std::vector<double>& z, std::vector<double>& f);
 // In G space (digit-reversed layout): c <- 4 pi c / (N^3 G^2), G = 0 -> 0;
 // eh_acc += 1/2 Omega 4 pi |c / N^3|^2 / G^2 (before scaling).
 void launch_hartree_gspace(double2* c, const GridRecip& gr, double omega, double* eh_acc,

@@ -114,7 +114,7 @@ static double ewald_energy(const std::vector<double>& pos, const std::vector<dou
     return e_real + e_recip + e_self + e_bg;
 }
 
-chfsi_status generate_system(const chfsi_synth_params& p, System& s) {
+chfsi_status generate_system(const chfsi_synth_params& p, System& s, const double* pos_override) {
     if (p.n_rep < 1 || p.a_conv <= 0 || p.ecut <= 0 || p.lmax < 0 || p.lmax > 1 ||
         p.n_shell < 0 || p.n_shell > 4)
         return CHFSI_ERR_BAD_INPUT;
@@ -156,6 +156,7 @@ chfsi_status generate_system(const chfsi_synth_params& p, System& s) {
                     s.zion.push_back(p.z_val);
                 }
     s.n_atoms = (int)s.zion.size();
+    if (pos_override) std::memcpy(s.pos.data(), pos_override, sizeof(double) * s.pos.size());
     s.n_elec = p.z_val * s.n_atoms;
     s.n_occ = (int)std::ceil(s.n_elec / 2.0 - 1e-9);
     s.n_bands = p.n_bands > 0 ? p.n_bands : (int)std::ceil(1.25 * s.n_occ - 1e-9);
@@ -415,6 +416,23 @@ chfsi_status chfsi_system_generate(const chfsi_synth_params* p, chfsi_system** o
     chfsi_status st;
     try {
         st = chfsi::generate_system(*p, *s);
+    } catch (const std::bad_alloc&) {
+        st = CHFSI_ERR_OUT_OF_MEMORY;
+    }
+    if (st != CHFSI_OK) { delete s; return st; }
+    *out = s;
+    return CHFSI_OK;
+}
+
+chfsi_status chfsi_system_generate_at(const chfsi_synth_params* p, const double* positions,
+                                      chfsi_system** out) {
+    if (!p || !out || !positions) return CHFSI_ERR_BAD_INPUT;
+    *out = nullptr;
+    chfsi_system* s = new (std::nothrow) chfsi_system();
+    if (!s) return CHFSI_ERR_OUT_OF_MEMORY;
+    chfsi_status st;
+    try {
+        st = chfsi::generate_system(*p, *s, positions);
     } catch (const std::bad_alloc&) {
         st = CHFSI_ERR_OUT_OF_MEMORY;
     }

@@ -29,7 +29,9 @@ struct System {
     std::vector<double> psi0;           // 2 x n_bands x n_pw
 };
 
-chfsi_status generate_system(const chfsi_synth_params& p, System& s);
+// pos_override: n_atoms x 3 Cartesian positions in place of the seeded lattice
+chfsi_status generate_system(const chfsi_synth_params& p, System& s,
+                             const double* pos_override = nullptr);
 int next_smooth235(int n);
 
 }  // namespace chfsi

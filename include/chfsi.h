@@ -148,6 +148,11 @@ typedef struct chfsi_system_info {
 
 chfsi_status chfsi_synth_defaults(int config_index, chfsi_synth_params* out);
 chfsi_status chfsi_system_generate(const chfsi_synth_params* p, chfsi_system** out);
+/* The same system with the atoms at the given Cartesian positions (n_atoms x
+ * 3, bohr) in place of the seeded jittered lattice (finite-difference
+ * forces, displaced geometries). */
+chfsi_status chfsi_system_generate_at(const chfsi_synth_params* p, const double* positions,
+                                      chfsi_system** out);
 void         chfsi_system_destroy(chfsi_system* s);
 chfsi_status chfsi_system_get_info(const chfsi_system* s, chfsi_system_info* out);
 /* Miller indices (n_pw x 3), sorted by (iy, ix) column then iz. */
@@ -308,6 +313,29 @@ chfsi_status chfsi_construct_density(chfsi_ctx* ctx, double* rho_out);
 chfsi_status chfsi_build_veff(chfsi_ctx* ctx, const double* rho, double* e2);
 /* Density of the last chfsi_construct_density / chfsi_scf_run step. */
 chfsi_status chfsi_get_density(chfsi_ctx* ctx, double* rho);
+
+/* Exchange-correlation functional of chfsi_build_veff and chfsi_scf_run:
+ * LDA (Perdew-Zunger 1981, the default) or the GGA PBE (Perdew, Burke,
+ * Ernzerhof 1996 with PW92 correlation), the functional of the reference's
+ * planned V_eff builder (plans/phase-2/PHASE_PLAN.md:90-95). */
+enum { CHFSI_XC_LDA_PZ = 0, CHFSI_XC_PBE = 1 };
+chfsi_status chfsi_set_xc(chfsi_ctx* ctx, int functional);
+
+/* Ions of the cell for forces: Cartesian positions (n_atoms x 3, bohr),
+ * valence charges and the local-pseudopotential widths of the analytic
+ * model v(G) = -4 pi Z/(Omega G^2) exp(-G^2 rc^2/4) that chfsi_set_vloc_g
+ * received summed over ions, and k (fractional) of the context's basis.
+ * Ions with projectors are the first n_ions of chfsi_set_projectors, in the
+ * same order.  Set by chfsi_create_from_system. */
+chfsi_status chfsi_set_ions(chfsi_ctx* ctx, int n_atoms, const double* positions,
+                            const double* zion, const double* rc_loc, const double* kpt);
+/* Hellmann-Feynman forces (Ha/bohr, n_atoms x 3) of the current density and
+ * wavefunctions (after chfsi_scf_run): local pseudopotential, non-local
+ * projectors and ion-ion Ewald terms; the forces output of the planned
+ * scf_run (PROJECT_ROOT_PLAN.md:957-1018).  Norm-conserving and local cells
+ * with equal density and wavefunction grids; CHFSI_ERR_NOT_IMPLEMENTED for
+ * ultrasoft ones (their augmentation and overlap terms are not built). */
+chfsi_status chfsi_forces(chfsi_ctx* ctx, double* forces);
 
 typedef struct chfsi_scf_params {
     int    ndeg;          /* Chebyshev degree                                   */

@@ -73,14 +73,17 @@ class UsppScf:
 
     def __init__(self, s):
         self.s = s
-        self.o = orc.Oracle.from_system(s)
+        beta = s.beta()  # one host copy shared by the oracle and the augmentation sums
+        self.o = orc.Oracle(s.ngrid, s.miller(), s.kinetic(), beta, s.proj_offsets(), s.dmat(),
+                            s.psi0(), s.occupations(), s.vloc_g(), s.omega, s.gmax, s.e_ewald,
+                            s.n_atoms)
         self.o.set_qmat(s.qmat())
         self.nw = tuple(s.ngrid)
         self.nf = tuple(s.ngrid_density)
         self.omega = s.omega
         self.width = s.q_width
         self.pos = s.positions().reshape(-1, 3)
-        self.beta = s.beta().reshape(s.n_proj, s.n_pw)
+        self.beta = beta.reshape(s.n_proj, s.n_pw)
         self.poff = s.proj_offsets()
         self.d0 = s.dmat()
         self.q = s.qmat()

@@ -29,8 +29,9 @@ def sys2(chfsi):
     return s
 
 
-@pytest.fixture(scope="module")
+@pytest.fixture
 def pair(chfsi, oracle, sys2):
+    # function scope: the oracle holds a 4.8 GB host copy of the projectors
     s = sys2
     ctx = chfsi.Context(s)
     o = oracle.Oracle(s.ngrid, s.miller(), s.kinetic(), s.beta(), s.proj_offsets(), s.dmat(),
@@ -41,7 +42,9 @@ def pair(chfsi, oracle, sys2):
     v = v + 0.05 * np.sin(np.arange(v.size) * 1e-3)
     ctx.set_veff(v)
     o.set_veff(v)
-    return ctx, o
+    yield ctx, o
+    o.close()
+    ctx.close()
 
 
 def rel(a, b):
@@ -83,7 +86,11 @@ def test_augmented_density_144(chfsi, sys2):
     ctx = chfsi.Context(s)
     ctx.set_occupations(occ)
     rho = ctx.construct_density()
-    ref, _ = uo.UsppScf(s).density(occ)
+    ctx.close()
+    u = uo.UsppScf(s)
+    ref, _ = u.density(occ)
+    u.o.close()
+    del u
     err = rel(rho, ref)
     print("216-atom cell augmented density on 144^3: relative error %.3e" % err)
     assert rho.size == 144 ** 3
