@@ -11,8 +11,9 @@ At N = 1 the line also carries the time-to-SCF of the 216-atom ultrasoft
 cell (n_pw 173,925, 576 bands, 1,728 projectors, 108^3 / 144^3 grids):
 FP64 + Pulay, mixed precision + Pulay and mixed precision + the learned
 mixer, each stopped at |dE| < 1e-6 Ha/atom with the occupied eigenvalues
-changing by less than 1e-7 Ha, and each compared with the FP64 run
-continued (untimed) to tight convergence.
+changing by less than 1e-6 Ha between iterations, and each compared with
+the FP64 run continued (untimed) for further iterations toward tight
+convergence.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -277,8 +278,8 @@ def run_ours(args):
         if not args.no_scf and world == 1:
             import learned_mixer
             net = learned_mixer.load(device=local)
-            mixed["time_to_scf"] = time_to_scf(chfsi, s, NDEG, local, net, max_iter=80,
-                                               tight_max_iter=80)
+            mixed["time_to_scf"] = time_to_scf(chfsi, s, NDEG, local, net, max_iter=100,
+                                               tight_max_iter=40)
 
     # ---- headline: time-to-SCF of the 216-atom ultrasoft cell (N = 1 only) ----
     scf216 = None
@@ -287,7 +288,7 @@ def run_ours(args):
         s2 = chfsi.SyntheticSystem(config_index=2)
         net = learned_mixer.load(device=local)
         scf216 = time_to_scf(chfsi, s2, 16, local, net, max_iter=args.scf_216_max_iter,
-                             tight_max_iter=60)
+                             tight_max_iter=30)
         scf216["workload"] = ("216-atom ultrasoft cell, a=30.78 bohr, Ecut 25 Ha, n_pw=%d, "
                               "grid 108^3 (density 144^3), %d bands, %d projectors, degree 16"
                               % (s2.n_pw, s2.n_bands, s2.n_proj))
@@ -322,7 +323,7 @@ def run_ours(args):
 
 # time-to-SCF stopping rule of every timed arm, and the tight FP64 reference
 SCF_TOL_PER_ATOM = 1e-6   # |dE| per atom (Ha)
-SCF_TOL_EIG = 1e-7        # change of the occupied eigenvalues between iterations (Ha)
+SCF_TOL_EIG = 1e-6        # change of the occupied eigenvalues between iterations (Ha)
 TIGHT_TOL_PER_ATOM = 1e-10
 TIGHT_TOL_EIG = 1e-9
 
@@ -355,10 +356,14 @@ def time_to_scf(chfsi, s, ndeg, device, net, max_iter, tight_max_iter):
     out = {"criterion": "|dE| < %g Ha/atom and occupied eigenvalues changing by < %g Ha "
                         "(Fermi-Dirac kT = 0.01 Ha; Pulay alpha 0.3, history 6)"
                         % (SCF_TOL_PER_ATOM, SCF_TOL_EIG),
-           "reference": "FP64 run continued to |dE| < %g Ha/atom and eigenvalue changes < %g Ha"
-                        % (TIGHT_TOL_PER_ATOM, TIGHT_TOL_EIG),
+           "reference": "FP64 run continued for up to %d more iterations toward |dE| < %g "
+                        "Ha/atom and eigenvalue changes < %g Ha" % (tight_max_iter,
+                                                                   TIGHT_TOL_PER_ATOM, TIGHT_TOL_EIG),
            "reference_converged": bool(tight["converged"]),
            "reference_extra_iterations": tight["n_iter"],
+           "reference_last_energy_change_per_atom_Ha":
+               float(abs(tight["energies"][-1] - tight["energies"][-2]) / s.n_atoms)
+               if len(tight["energies"]) > 1 else None,
            "arms": {}}
     f = res["fp64"]
     for name, r in res.items():
@@ -530,7 +535,7 @@ def main():
     ap.add_argument("--no-scf", action="store_true", help="skip every time-to-SCF comparison")
     ap.add_argument("--no-scf-216", action="store_true",
                     help="skip the 216-atom time-to-SCF comparison (about ten minutes)")
-    ap.add_argument("--scf-216-max-iter", type=int, default=120)
+    ap.add_argument("--scf-216-max-iter", type=int, default=150)
     ap.add_argument("--profile", choices=["local", "fp64", "mixed", "fp64-216", "mixed-216", "gemm"],
                     default=None,
                     help="a short fixed workload for ncu captures (no JSON line): two local "

@@ -780,7 +780,8 @@ chfsi_status rr_dev(chfsi_ctx* ctx, bool fp32_block) {
         count_launch();
         k_conj<<<grid_for((size_t)np * n), 256, 0, st>>>(ctx->d_cp, ctx->d_cq, (size_t)np * n);
     }
-    gemm_cn(ctx->d_psi, ctx->n_pw, ctx->d_hpsi, ctx->n_pw, n, n, ctx->n_pw, ctx->d_part, ctx->d_T1, st);
+    // psi^H H psi and psi^H psi are Hermitian: upper tiles only
+    gemm_cn_herm(ctx->d_psi, ctx->n_pw, ctx->d_hpsi, ctx->n_pw, n, ctx->n_pw, ctx->d_part, ctx->d_T1, st);
     if (nl_sub) {
         // H_sub += C^H D C
         count_launch();
@@ -789,7 +790,7 @@ chfsi_status rr_dev(chfsi_ctx* ctx, bool fp32_block) {
         gemm_tn(ctx->d_cq, n, ctx->d_cd, n, ctx->d_T1, n, n, n, np, 1.0, 1.0, st);
     }
     symmetrize(ctx->d_T1, ctx->d_H, n, st);
-    gemm_cn(ctx->d_psi, ctx->n_pw, ctx->d_psi, ctx->n_pw, n, n, ctx->n_pw, ctx->d_part, ctx->d_T1, st);
+    gemm_cn_herm(ctx->d_psi, ctx->n_pw, ctx->d_psi, ctx->n_pw, n, ctx->n_pw, ctx->d_part, ctx->d_T1, st);
     if (aug_s) {
         // S_sub = psi^H psi + C^H q C
         count_launch();
@@ -1503,7 +1504,8 @@ chfsi_status alloc_all(chfsi_ctx* ctx) {
     CK(dalloc(&ctx->d_dots, kPulayMax));
     // split-K partials: max over the GEMMs that use them
     // (any band count 1..nb may reach the projector GEMM through chfsi_apply_h)
-    size_t pe = splitk_partial_elems(ctx->nb, ctx->nb, ctx->n_pw);
+    size_t pe = std::max(splitk_partial_elems(ctx->nb, ctx->nb, ctx->n_pw),
+                         splitk_partial_elems_herm(ctx->nb, ctx->n_pw));
     if (ctx->np > 0)
         for (int n = 1; n <= nbx; ++n)
             pe = std::max(pe, splitk_partial_elems(ctx->np, n, ctx->n_pw));
@@ -2689,6 +2691,7 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
     int reverts = 0;
     bool have_prev = false, fell_back = false;
     int rises = 0;
+    bool restart_pulay = false;
     double r_prev = -1.0;
     std::vector<double> eig(ctx->nb), eig_prev(ctx->nb);
     bool have_eig = restart;
@@ -2912,7 +2915,13 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
         if (r->residuals) r->residuals[it - 1] = rnorm;
         if (learned && !fell_back) {
             rises = (r_prev >= 0.0 && rnorm > r_prev) ? rises + 1 : 0;
-            if (rises >= 2) fell_back = true;
+            if (rises >= 2) {
+                // Pulay takes over from the current input density with a fresh
+                // history: the learned steps' entries span a subspace that
+                // stalls the extrapolation (observed on the 216-atom cell)
+                fell_back = true;
+                restart_pulay = true;
+            }
         }
         r_prev = rnorm;
         if (learned) ring_push(ctx, ring, ctx->d_rho_out, ctx->d_rho_in);
@@ -2933,10 +2942,26 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
             for (float v : yh)
                 if (!std::isfinite(v)) {
                     fell_back = true;
+                    restart_pulay = true;
                     if (p->verbose)
                         std::fprintf(stderr, "scf %3d: learned mixer output not finite, Pulay from here\n", it);
                     break;
                 }
+        }
+        if (restart_pulay) {
+            // keep only the newest entry (rho_in, R): a linear-mixing step now,
+            // Pulay extrapolation over a new history from the next iteration
+            const int newest = (ps.head + ps.m - 1) % kPulayMax;
+            ps.head = newest;
+            ps.m = 1;
+            ps.M[0][0] = dd[nw];
+            for (int j = 0; j < kPulayMax; ++j) c[j] = 0.0;
+            c[0] = 1.0;
+            double* pr = ctx->d_hist + (size_t)newest * ng;
+            double* pres = ctx->d_hist + (size_t)(kPulayMax + newest) * ng;
+            CK(cudaMemcpyAsync(ctx->d_hist_ptrs, &pres, sizeof(double*), cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(ctx->d_hist_ptrs + kPulayMax, &pr, sizeof(double*), cudaMemcpyHostToDevice, st));
+            restart_pulay = false;
         }
         if (!learned || fell_back) {
             pulay_combine(ctx->d_hist_ptrs + kPulayMax, ctx->d_hist_ptrs, ps.m, c, p->alpha, ng,

@@ -42,12 +42,21 @@ constexpr int kDT = BM + 4;  // row stride (doubles) of M/N-contiguous planes
 // P[s][m][n] = sum_{k in chunk s} conj(A[m][k]) B[n][k]
 __global__ void __launch_bounds__(256, 2)
 k_zgemm_cn_dmma(const double2* __restrict__ A, int lda, const double2* __restrict__ B, int ldb,
-                int M, int N, int K, int kchunk, double2* __restrict__ part) {
+                int M, int N, int K, int kchunk, double2* __restrict__ part, int tri) {
     __shared__ double Ar[BM][kDS], Ai[BM][kDS], Br[BN][kDS], Bi[BN][kDS];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int gid = lane >> 2, tig = lane & 3;
     const int wm = warp & 1, wn = warp >> 1;
-    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    int tm = blockIdx.x, tn = blockIdx.y;
+    if (tri > 0) {
+        // Hermitian product: blockIdx.x enumerates the tile pairs tm <= tn of
+        // a tri x tri tile grid, row by row
+        int t = blockIdx.x, row = 0;
+        while (t >= tri - row) { t -= tri - row; ++row; }
+        tm = row;
+        tn = row + t;
+    }
+    const int m0 = tm * BM, n0 = tn * BN;
     const int kb = blockIdx.z * kchunk;
     const int ke = min(K, kb + kchunk);
     double cr[4][2][2], ci[4][2][2];
@@ -215,6 +224,26 @@ k_zgemm_tn_dmma(const double2* __restrict__ W, int ldw, const double2* __restric
     }
 }
 
+// Hermitian product from its upper tiles: out[m][n] = sum of partials where
+// tile(m) <= tile(n), out[n][m] = conj of it where tile(m) < tile(n)
+__global__ void k_reduce_herm(const double2* __restrict__ part, int splits, int N,
+                              double2* __restrict__ out) {
+    const size_t nn = (size_t)N * N;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nn;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const int m = (int)(i / N), n = (int)(i % N);
+        if (m / BM > n / BN) continue;
+        double2 s = make_double2(0.0, 0.0);
+        for (int t = 0; t < splits; ++t) {
+            const double2 v = part[(size_t)t * nn + i];
+            s.x += v.x;
+            s.y += v.y;
+        }
+        out[i] = s;
+        if (m / BM < n / BN) out[(size_t)n * N + m] = make_double2(s.x, -s.y);
+    }
+}
+
 __global__ void k_reduce_partials(const double2* __restrict__ part, int splits, size_t mn,
                                   double2* __restrict__ out) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < mn;
@@ -239,7 +268,10 @@ __global__ void k_reduce_partials(const double2* __restrict__ part, int splits, 
 // waves; psi^H psi of 576 bands (81 tiles) as 18 splits, 1,458 CTAs in 4.93
 // waves, not as 4 splits, 324 CTAs in 1.09 waves.
 int splitk_count(int M, int N, int K) {
-    const int tiles = ((M + BM - 1) / BM) * ((N + BN - 1) / BN);
+    return splitk_count_tiles(((M + BM - 1) / BM) * ((N + BN - 1) / BN), K);
+}
+
+int splitk_count_tiles(int tiles, int K) {
     const int max_splits = std::min(64, std::max(1, (K + 255) / 256));
     int best = 1;
     double best_eff = -1.0;
@@ -259,6 +291,11 @@ size_t splitk_partial_elems(int M, int N, int K) {
     return (size_t)splitk_count(M, N, K) * M * N;
 }
 
+size_t splitk_partial_elems_herm(int N, int K) {
+    const int tn = (N + BN - 1) / BN;
+    return (size_t)splitk_count_tiles(tn * (tn + 1) / 2, K) * N * N;
+}
+
 void gemm_cn(const double2* A, int lda, const double2* B, int ldb, int M, int N, int K,
              double2* part, double2* out, cudaStream_t st) {
     count_launch(2);
@@ -267,11 +304,31 @@ void gemm_cn(const double2* A, int lda, const double2* B, int ldb, int M, int N,
     kchunk = (kchunk + BK - 1) / BK * BK;
     const int used = (K + kchunk - 1) / kchunk;
     dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN, used);
-    k_zgemm_cn_dmma<<<grid, 256, 0, st>>>(A, lda, B, ldb, M, N, K, kchunk, part);
+    k_zgemm_cn_dmma<<<grid, 256, 0, st>>>(A, lda, B, ldb, M, N, K, kchunk, part, 0);
     const size_t mn = (size_t)M * N;
     int blocks = (int)((mn + 255) / 256);
     if (blocks > 148 * 8) blocks = 148 * 8;
     k_reduce_partials<<<blocks, 256, 0, st>>>(part, used, mn, out);
+}
+
+// C = conj(A) A'^T for a Hermitian result (A' = A, or A' = H A with H
+// Hermitian on the span): only the tiles on and above the diagonal are
+// computed (half the flops), the rest mirrored by conjugation.
+void gemm_cn_herm(const double2* A, int lda, const double2* B, int ldb, int N, int K,
+                  double2* part, double2* out, cudaStream_t st) {
+    count_launch(2);
+    const int tn = (N + BN - 1) / BN;
+    const int tiles = tn * (tn + 1) / 2;
+    const int splits = splitk_count_tiles(tiles, K);
+    int kchunk = (K + splits - 1) / splits;
+    kchunk = (kchunk + BK - 1) / BK * BK;
+    const int used = (K + kchunk - 1) / kchunk;
+    dim3 grid(tiles, 1, used);
+    k_zgemm_cn_dmma<<<grid, 256, 0, st>>>(A, lda, B, ldb, N, N, K, kchunk, part, tn);
+    const size_t nn = (size_t)N * N;
+    int blocks = (int)((nn + 255) / 256);
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    k_reduce_herm<<<blocks, 256, 0, st>>>(part, used, N, out);
 }
 
 void gemm_tn(const double2* W, int ldw, const double2* X, int ldx, double2* O, int ldo, int M,
@@ -297,7 +354,7 @@ void gemm_cn_capped(const double2* A, int lda, const double2* B, int ldb, int M,
     kchunk = (kchunk + BK - 1) / BK * BK;
     const int used = (K + kchunk - 1) / kchunk;
     dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN, used);
-    k_zgemm_cn_dmma<<<grid, 256, 0, st>>>(A, lda, B, ldb, M, N, K, kchunk, part);
+    k_zgemm_cn_dmma<<<grid, 256, 0, st>>>(A, lda, B, ldb, M, N, K, kchunk, part, 0);
     const size_t mn = (size_t)M * N;
     int blocks = (int)((mn + 255) / 256);
     if (blocks > 148 * 8) blocks = 148 * 8;

@@ -433,6 +433,7 @@ bool invert(std::vector<cplx>& a, int n) {
             }
         const cplx d = a[(size_t)col * n + col];
         for (int k = 0; k < n; ++k) { a[(size_t)col * n + k] /= d; inv[(size_t)col * n + k] /= d; }
+#pragma omp parallel for schedule(static) if (n > 256)
         for (int r = 0; r < n; ++r) {
             if (r == col) continue;
             const cplx f = a[(size_t)r * n + col];
@@ -889,7 +890,9 @@ void oracle_set_occ(OracleCtx* c, const double* occ) { c->occ.assign(occ, occ + 
 // Ultrasoft overlap: per-ion q blocks (layout of D).  Builds the Woodbury
 // factor M = q (1 + B q)^-1 with B = beta^H beta and the lower bound
 // s_min = 1 - max_i sum_j |(q B)_ij| of the spectrum of S.  Returns 0 or -6.
-int oracle_set_qmat(OracleCtx* c, const double* qmat) {
+// bmat: B = beta^H beta (n_proj x n_proj) when the caller has it (a BLAS
+// product on the host), else null and formed here.
+int oracle_set_qmat_b(OracleCtx* c, const double* qmat, const double* bmat) {
     const int np = c->n_proj;
     c->qmat.assign(c->dmat.size(), 0.0);
     if (np == 0) return -6;
@@ -900,13 +903,17 @@ int oracle_set_qmat(OracleCtx* c, const double* qmat) {
         for (int i = 0; i < ne; ++i)
             for (int j = 0; j < ne; ++j) Q[(size_t)(p0 + i) * np + p0 + j] = c->qmat[c->dmat_off[ion] + i * ne + j];
     }
+    if (bmat) {
+        std::memcpy(B.data(), bmat, sizeof(cplx) * B.size());
+    } else {
 #pragma omp parallel for schedule(dynamic, 1)
-    for (int p = 0; p < np; ++p)
-        for (int q = 0; q < np; ++q) {
-            cplx s = 0.0;
-            for (int g = 0; g < c->n_pw; ++g) s += std::conj(c->beta[(size_t)p * c->n_pw + g]) * c->beta[(size_t)q * c->n_pw + g];
-            B[(size_t)p * np + q] = s;
-        }
+        for (int p = 0; p < np; ++p)
+            for (int q = 0; q < np; ++q) {
+                cplx s = 0.0;
+                for (int g = 0; g < c->n_pw; ++g) s += std::conj(c->beta[(size_t)p * c->n_pw + g]) * c->beta[(size_t)q * c->n_pw + g];
+                B[(size_t)p * np + q] = s;
+            }
+    }
     for (int i = 0; i < np; ++i)
         for (int k = 0; k < np; ++k) {
             const cplx qik = Q[(size_t)i * np + k];
@@ -940,6 +947,7 @@ int oracle_set_qmat(OracleCtx* c, const double* qmat) {
     c->uspp = true;
     return 0;
 }
+int oracle_set_qmat(OracleCtx* c, const double* qmat) { return oracle_set_qmat_b(c, qmat, nullptr); }
 
 void oracle_apply_s(OracleCtx* c, const double* x, double* y, int nb) {
     apply_s(*c, reinterpret_cast<const cplx*>(x), reinterpret_cast<cplx*>(y), nb);

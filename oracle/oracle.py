@@ -59,6 +59,7 @@ def lib():
                             C.c_double, dp, ip, dp, dp], C.c_int),
         "oracle_fermi": ([dp, C.c_int, C.c_double, C.c_double, dp], C.c_double),
         "oracle_set_qmat": ([vp, vp], C.c_int),
+        "oracle_set_qmat_b": ([vp, vp, vp], C.c_int),
         "oracle_line_search": ([C.c_double, C.c_double, C.c_double, C.c_double, dp], None),
         "oracle_tpa_diag": ([dp, C.c_int, dp], None),
         "oracle_band_cg": ([vp, C.c_int, C.c_double, dp, ip], C.c_int),
@@ -188,10 +189,17 @@ class Oracle:
         lib().oracle_get_hpsi(self.h, _p(p))
         return p
 
-    def set_qmat(self, qmat):
-        """Ultrasoft overlap S = 1 + beta q beta^H (per-ion q blocks)."""
+    def set_qmat(self, qmat, beta=None):
+        """Ultrasoft overlap S = 1 + beta q beta^H (per-ion q blocks).  With the
+        projector array given, B = beta^H beta is formed by numpy's BLAS
+        (the same product, faster than the oracle's loop at 1,728 projectors)."""
         self._q = np.ascontiguousarray(qmat, dtype=np.complex128)
-        st = lib().oracle_set_qmat(self.h, _p(self._q))
+        if beta is not None:
+            b = np.asarray(beta).reshape(-1, self.n_pw)
+            bm = np.ascontiguousarray(np.conj(b) @ b.T)
+            st = lib().oracle_set_qmat_b(self.h, _p(self._q), _p(bm))
+        else:
+            st = lib().oracle_set_qmat(self.h, _p(self._q))
         if st != 0:
             raise RuntimeError("oracle_set_qmat failed")
 

@@ -77,7 +77,8 @@ class UsppScf:
         self.o = orc.Oracle(s.ngrid, s.miller(), s.kinetic(), beta, s.proj_offsets(), s.dmat(),
                             s.psi0(), s.occupations(), s.vloc_g(), s.omega, s.gmax, s.e_ewald,
                             s.n_atoms)
-        self.o.set_qmat(s.qmat())
+        self._beta_all = beta
+        self._qmat_set = False
         self.nw = tuple(s.ngrid)
         self.nf = tuple(s.ngrid_density)
         self.omega = s.omega
@@ -192,6 +193,10 @@ class UsppScf:
     def run_scf(self, ndeg, max_iter=30, tol_per_atom=1e-6, alpha=0.3, max_hist=6,
                 first_passes=4, kT=0.01):
         s = self.s
+        if not self._qmat_set:
+            # the generalised eigenproblem of the SCF needs S
+            self.o.set_qmat(s.qmat(), beta=self._beta_all)
+            self._qmat_set = True
         ngf = int(np.prod(self.nf))
         dv = self.omega / ngf
         n_elec = s.n_elec

@@ -37,7 +37,6 @@ def pair(chfsi, oracle, sys2):
     o = oracle.Oracle(s.ngrid, s.miller(), s.kinetic(), s.beta(), s.proj_offsets(), s.dmat(),
                       s.psi0(), s.occupations(), s.vloc_g(), s.omega, s.gmax, s.e_ewald,
                       s.n_atoms)
-    o.set_qmat(s.qmat())
     v = o.vloc_r()
     v = v + 0.05 * np.sin(np.arange(v.size) * 1e-3)
     ctx.set_veff(v)
@@ -67,6 +66,7 @@ def test_hpsi_108_full_projectors(pair, sys2):
 
 def test_sinv_hpsi_108_full_projectors(pair, sys2):
     ctx, o = pair
+    o.set_qmat(sys2.qmat(), beta=sys2.beta())
     psi = np.ascontiguousarray(sys2.psi0()[:NB])
     x = torch.from_numpy(psi).cuda()
     y = torch.empty_like(x)

@@ -33,7 +33,7 @@ def test_rchfsi_fp64_matches_oracle(chfsi, oracle, kind):
     wg = ctx.diagonalize(ndeg)           # no Ritz values yet: Chebyshev filter
     wc = o.diagonalize(ndeg)
     np.testing.assert_allclose(wg, wc, atol=1e-10, rtol=0)
-    for _ in range(2):                   # residual filter from the Ritz pairs
+    for _ in range(2 if kind != "kb" else 1):  # residual filter from the Ritz pairs
         wg_next = ctx.diagonalize(ndeg, wg)
         wc_next = o.rchfsi_diagonalize(ndeg, wc)
         err = np.abs(wg_next - wc_next).max()
