@@ -21,29 +21,59 @@ namespace chfsi {
 namespace {
 
 constexpr int BM = 64, BN = 64, BK = 16;
+constexpr int kStages = 3;
+// one CTA of 256 threads per SM (about 150 registers per thread, 120 KB of
+// shared memory): split-K counts fill waves of 148 CTAs
+constexpr int kCtasPerWave = 148;
 
-// ---- FP64 tensor-core (DMMA) versions: mma.sync m8n8k4 .f64, one warp
-// issues 256 FMAs per instruction.  Complex products as four real MMAs on
-// split (re, im) shared-memory planes.  Fragments (PTX m8n8k4 .f64): A row
-// (lane >> 2), col (lane & 3); B row (lane & 3), col (lane >> 2); C row
-// (lane >> 2), cols 2 (lane & 3) + {0, 1}.  CTA tile 64 x 64, 8 warps as
-// 2 (M) x 4 (N), warp tile 32 x 16 = 4 x 2 MMA tiles.
-// Not volatile: the MMA has no effect beyond its outputs, so the compiler may
-// interleave independent MMAs with the fragment loads.
+// ---- FP64 tensor-core (DMMA) versions: mma.sync m8n8k4 .f64.  Fragments
+// (PTX m8n8k4 .f64): A row (lane >> 2), col (lane & 3); B row (lane & 3), col
+// (lane >> 2); C row (lane >> 2), cols 2 (lane & 3) + {0, 1}.  CTA tile
+// 64 x 64, 8 warps as 2 (M) x 4 (N), warp tile 32 x 16 = 4 x 2 MMA tiles.
+// Complex products by Gauss's three-multiplication form (three real MMAs per
+// complex MAC instead of four):
+//   conj(a) b:  t1 = ar br, t2 = ai bi, t3 = (ar - ai)(br + bi);
+//               re = t1 + t2, im = t3 - t1 + t2
+//   a b:        t1 = ar br, t2 = ai bi, t3 = (ar + ai)(br + bi);
+//               re = t1 - t2, im = t3 - t1 - t2
+// Operand tiles stream global -> shared with cp.async (16-byte complex
+// elements, zero fill outside the matrix) through a 3-stage ring; each
+// fragment is one 128-bit shared load of a complex element (re and im
+// together).
 __device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
     asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
         : "+d"(d[0]), "+d"(d[1])
         : "d"(a), "d"(b));
 }
 
-constexpr int kDS = BK + 4;  // row stride (doubles) of K-contiguous planes
-constexpr int kDT = BM + 4;  // row stride (doubles) of M/N-contiguous planes
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// 16-byte async copy global -> shared; src_bytes 0 writes zeros
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, int src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_addr(dst)), "l"(src),
+                 "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// row strides (complex elements): K-contiguous tiles 20 = 4 mod 8, M/N-
+// contiguous tiles 66 = 2 mod 8, so that the 8 lanes of each quarter-warp
+// fragment load hit 8 different 16-byte bank groups
+constexpr int kSK = BK + 4;
+constexpr int kSM = BM + 2;
 
 // P[s][m][n] = sum_{k in chunk s} conj(A[m][k]) B[n][k]
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(256, 1)
 k_zgemm_cn_dmma(const double2* __restrict__ A, int lda, const double2* __restrict__ B, int ldb,
                 int M, int N, int K, int kchunk, double2* __restrict__ part, int tri) {
-    __shared__ double Ar[BM][kDS], Ai[BM][kDS], Br[BN][kDS], Bi[BN][kDS];
+    extern __shared__ __align__(16) double2 sm_cn[];
+    double2* As = sm_cn;                           // [kStages][BM][kSK]
+    double2* Bs = sm_cn + kStages * BM * kSK;      // [kStages][BN][kSK]
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int gid = lane >> 2, tig = lane & 3;
     const int wm = warp & 1, wn = warp >> 1;
@@ -59,68 +89,70 @@ k_zgemm_cn_dmma(const double2* __restrict__ A, int lda, const double2* __restric
     const int m0 = tm * BM, n0 = tn * BN;
     const int kb = blockIdx.z * kchunk;
     const int ke = min(K, kb + kchunk);
-    double cr[4][2][2], ci[4][2][2];
+    const int nsteps = ke > kb ? (ke - kb + BK - 1) / BK : 0;
+    // copy assignment: chunk c = threadIdx.x + 256 i (i < 4): row c / 16, col c % 16
+    auto load_stage = [&](int step, int slot) {
+        const int k0 = kb + step * BK;
+        double2* as = As + slot * BM * kSK;
+        double2* bs = Bs + slot * BN * kSK;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int c = threadIdx.x + 256 * i;
+            const int r = c >> 4, kk = c & 15;
+            const int k = k0 + kk;
+            const int am = m0 + r, bn = n0 + r;
+            const bool ka = k < ke;
+            const double2* srca = A + ((ka && am < M) ? (size_t)am * lda + k : 0);
+            const double2* srcb = B + ((ka && bn < N) ? (size_t)bn * ldb + k : 0);
+            cp_async16(as + r * kSK + kk, srca, (ka && am < M) ? 16 : 0);
+            cp_async16(bs + r * kSK + kk, srcb, (ka && bn < N) ? 16 : 0);
+        }
+    };
+    double t1[4][2][2], t2[4][2][2], t3[4][2][2];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 2; ++j) cr[i][j][0] = cr[i][j][1] = ci[i][j][0] = ci[i][j][1] = 0.0;
-    const int lr = threadIdx.x >> 2, lk = (threadIdx.x & 3) * 4;
-    const int am = m0 + lr, bn_ = n0 + lr;
-    const double2* ap = A + (size_t)am * lda;
-    const double2* bp = B + (size_t)bn_ * ldb;
-    double2 ra[4], rb[4];
-    auto fetch = [&](int k0) {
+        for (int j = 0; j < 2; ++j)
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const int k = k0 + lk + i;
-            ra[i] = (am < M && k < ke) ? ap[k] : make_double2(0.0, 0.0);
-            rb[i] = (bn_ < N && k < ke) ? bp[k] : make_double2(0.0, 0.0);
-        }
-    };
-    if (kb < ke) fetch(kb);
-    for (int k0 = kb; k0 < ke; k0 += BK) {
+            for (int e = 0; e < 2; ++e) t1[i][j][e] = t2[i][j][e] = t3[i][j][e] = 0.0;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            Ar[lr][lk + i] = ra[i].x; Ai[lr][lk + i] = ra[i].y;
-            Br[lr][lk + i] = rb[i].x; Bi[lr][lk + i] = rb[i].y;
-        }
+    for (int st = 0; st < kStages - 1; ++st) {
+        if (st < nsteps) load_stage(st, st);
+        cp_async_commit();
+    }
+    for (int step = 0; step < nsteps; ++step) {
+        cp_async_wait<kStages - 2>();
         __syncthreads();
-        if (k0 + BK < ke) fetch(k0 + BK);
+        // refill the slot consumed one step ago
+        const int nxt = step + kStages - 1;
+        if (nxt < nsteps) load_stage(nxt, nxt % kStages);
+        cp_async_commit();
+        const double2* as = As + (step % kStages) * BM * kSK;
+        const double2* bs = Bs + (step % kStages) * BN * kSK;
 #pragma unroll
         for (int kk = 0; kk < BK; kk += 4) {
-            double br[2], bi[2];
+            double br[2], bi[2], bs_[2];
 #pragma unroll
             for (int j = 0; j < 2; ++j) {
-                const int n = wn * 16 + j * 8 + gid;
-                br[j] = Br[n][kk + tig];
-                bi[j] = Bi[n][kk + tig];
+                const double2 v = bs[(wn * 16 + j * 8 + gid) * kSK + kk + tig];
+                br[j] = v.x;
+                bi[j] = v.y;
+                bs_[j] = v.x + v.y;
             }
-            double ar[4], ai[4];
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
-                const int m = wm * 32 + i * 8 + gid;
-                ar[i] = Ar[m][kk + tig];
-                ai[i] = Ai[m][kk + tig];
+                const double2 v = as[(wm * 32 + i * 8 + gid) * kSK + kk + tig];
+                const double ad = v.x - v.y;
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    dmma(t1[i][j], v.x, br[j]);
+                    dmma(t2[i][j], v.y, bi[j]);
+                    dmma(t3[i][j], ad, bs_[j]);
+                }
             }
-            // two rounds of 16 independent MMAs: each accumulator's second
-            // product comes 16 MMAs after its first
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 2; ++j) {
-                    dmma(cr[i][j], ar[i], br[j]);
-                    dmma(ci[i][j], ar[i], bi[j]);
-                }
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 2; ++j) {
-                    dmma(cr[i][j], ai[i], bi[j]);
-                    dmma(ci[i][j], -ai[i], br[j]);
-                }
         }
-        __syncthreads();
     }
+    cp_async_wait<0>();
     double2* pp = part + (size_t)blockIdx.z * M * N;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
@@ -131,78 +163,87 @@ k_zgemm_cn_dmma(const double2* __restrict__ A, int lda, const double2* __restric
 #pragma unroll
             for (int e = 0; e < 2; ++e) {
                 const int n = n0 + wn * 16 + j * 8 + 2 * tig + e;
-                if (n < N) pp[(size_t)m * N + n] = make_double2(cr[i][j][e], ci[i][j][e]);
+                if (n < N)
+                    pp[(size_t)m * N + n] = make_double2(t1[i][j][e] + t2[i][j][e],
+                                                         t3[i][j][e] - t1[i][j][e] + t2[i][j][e]);
             }
     }
 }
 
 // O[m][n] = alpha sum_k W[k][m] X[k][n] + beta O[m][n]
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(256, 1)
 k_zgemm_tn_dmma(const double2* __restrict__ W, int ldw, const double2* __restrict__ X, int ldx,
                 double2* O, int ldo, int M, int N, int K, double alpha, double beta) {
-    __shared__ double Wr[BK][kDT], Wi[BK][kDT], Xr[BK][kDT], Xi[BK][kDT];
+    extern __shared__ __align__(16) double2 sm_tn[];
+    double2* Ws = sm_tn;                           // [kStages][BK][kSM]
+    double2* Xs = sm_tn + kStages * BK * kSM;      // [kStages][BK][kSM]
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int gid = lane >> 2, tig = lane & 3;
     const int wm = warp & 1, wn = warp >> 1;
     const int n0 = blockIdx.x * BN, m0 = blockIdx.y * BM;
-    double cr[4][2][2], ci[4][2][2];
+    const int nsteps = (K + BK - 1) / BK;
+    // chunk c = threadIdx.x + 256 i (i < 4): k row c / 64, column c % 64
+    auto load_stage = [&](int step, int slot) {
+        const int k0 = step * BK;
+        double2* ws = Ws + slot * BK * kSM;
+        double2* xs = Xs + slot * BK * kSM;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int c = threadIdx.x + 256 * i;
+            const int r = c >> 6, col = c & 63;
+            const int k = k0 + r;
+            const int m = m0 + col, n = n0 + col;
+            const bool kw = k < K;
+            const double2* srcw = W + ((kw && m < M) ? (size_t)k * ldw + m : 0);
+            const double2* srcx = X + ((kw && n < N) ? (size_t)k * ldx + n : 0);
+            cp_async16(ws + r * kSM + col, srcw, (kw && m < M) ? 16 : 0);
+            cp_async16(xs + r * kSM + col, srcx, (kw && n < N) ? 16 : 0);
+        }
+    };
+    double t1[4][2][2], t2[4][2][2], t3[4][2][2];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 2; ++j) cr[i][j][0] = cr[i][j][1] = ci[i][j][0] = ci[i][j][1] = 0.0;
-    const int lk = threadIdx.x >> 4, lc = (threadIdx.x & 15) * 4;
-    double2 rw[4], rx[4];
-    auto fetch = [&](int k0) {
-        const int k = k0 + lk;
+        for (int j = 0; j < 2; ++j)
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const int m = m0 + lc + i, n = n0 + lc + i;
-            rw[i] = (k < K && m < M) ? W[(size_t)k * ldw + m] : make_double2(0.0, 0.0);
-            rx[i] = (k < K && n < N) ? X[(size_t)k * ldx + n] : make_double2(0.0, 0.0);
-        }
-    };
-    fetch(0);
-    for (int k0 = 0; k0 < K; k0 += BK) {
+            for (int e = 0; e < 2; ++e) t1[i][j][e] = t2[i][j][e] = t3[i][j][e] = 0.0;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            Wr[lk][lc + i] = rw[i].x; Wi[lk][lc + i] = rw[i].y;
-            Xr[lk][lc + i] = rx[i].x; Xi[lk][lc + i] = rx[i].y;
-        }
+    for (int st = 0; st < kStages - 1; ++st) {
+        if (st < nsteps) load_stage(st, st);
+        cp_async_commit();
+    }
+    for (int step = 0; step < nsteps; ++step) {
+        cp_async_wait<kStages - 2>();
         __syncthreads();
-        if (k0 + BK < K) fetch(k0 + BK);
+        const int nxt = step + kStages - 1;
+        if (nxt < nsteps) load_stage(nxt, nxt % kStages);
+        cp_async_commit();
+        const double2* ws = Ws + (step % kStages) * BK * kSM;
+        const double2* xs = Xs + (step % kStages) * BK * kSM;
 #pragma unroll
         for (int kk = 0; kk < BK; kk += 4) {
-            double xr[2], xi[2];
+            double xr[2], xi[2], xsum[2];
 #pragma unroll
             for (int j = 0; j < 2; ++j) {
-                const int n = wn * 16 + j * 8 + gid;
-                xr[j] = Xr[kk + tig][n];
-                xi[j] = Xi[kk + tig][n];
+                const double2 v = xs[(kk + tig) * kSM + wn * 16 + j * 8 + gid];
+                xr[j] = v.x;
+                xi[j] = v.y;
+                xsum[j] = v.x + v.y;
             }
-            double wr[4], wi[4];
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
-                const int m = wm * 32 + i * 8 + gid;
-                wr[i] = Wr[kk + tig][m];
-                wi[i] = Wi[kk + tig][m];
+                const double2 v = ws[(kk + tig) * kSM + wm * 32 + i * 8 + gid];
+                const double as_ = v.x + v.y;
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    dmma(t1[i][j], v.x, xr[j]);
+                    dmma(t2[i][j], v.y, xi[j]);
+                    dmma(t3[i][j], as_, xsum[j]);
+                }
             }
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 2; ++j) {
-                    dmma(cr[i][j], wr[i], xr[j]);
-                    dmma(ci[i][j], wr[i], xi[j]);
-                }
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 2; ++j) {
-                    dmma(cr[i][j], -wi[i], xi[j]);
-                    dmma(ci[i][j], wi[i], xr[j]);
-                }
         }
-        __syncthreads();
     }
+    cp_async_wait<0>();
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         const int m = m0 + wm * 32 + i * 8 + gid;
@@ -214,7 +255,9 @@ k_zgemm_tn_dmma(const double2* __restrict__ W, int ldw, const double2* __restric
                 const int n = n0 + wn * 16 + j * 8 + 2 * tig + e;
                 if (n >= N) continue;
                 double2* o = O + (size_t)m * ldo + n;
-                double2 r = make_double2(alpha * cr[i][j][e], alpha * ci[i][j][e]);
+                const double re = t1[i][j][e] - t2[i][j][e];
+                const double im = t3[i][j][e] - t1[i][j][e] - t2[i][j][e];
+                double2 r = make_double2(alpha * re, alpha * im);
                 if (beta != 0.0) {
                     r.x += beta * o->x;
                     r.y += beta * o->y;
@@ -222,6 +265,17 @@ k_zgemm_tn_dmma(const double2* __restrict__ W, int ldw, const double2* __restric
                 *o = r;
             }
     }
+}
+
+constexpr size_t kSmemCn = (size_t)kStages * (BM + BN) * kSK * sizeof(double2);
+constexpr size_t kSmemTn = (size_t)kStages * 2 * BK * kSM * sizeof(double2);
+
+void gemm_smem_setup() {
+    static bool done = false;
+    if (done) return;
+    cudaFuncSetAttribute(k_zgemm_cn_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemCn);
+    cudaFuncSetAttribute(k_zgemm_tn_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemTn);
+    done = true;
 }
 
 // Hermitian product from its upper tiles: out[m][n] = sum of partials where
@@ -260,13 +314,11 @@ __global__ void k_reduce_partials(const double2* __restrict__ part, int splits, 
 
 }  // namespace
 
-// Two CTAs of k_zgemm_cn_dmma fit an SM, so the grid runs in waves of 296.
+// One CTA of k_zgemm_cn_dmma fills an SM, so the grid runs in waves of 148.
 // The split count that fills the last wave best wins (a larger one only
 // when it fills it 2 % better), with at least 256 k per split and 64 splits
-// at most.  E.g. the 256-projector x 160-band product (12 tiles) runs as 49
-// splits, 588 CTAs in two full waves, not as 25 splits, 300 CTAs in 1.01
-// waves; psi^H psi of 576 bands (81 tiles) as 18 splits, 1,458 CTAs in 4.93
-// waves, not as 4 splits, 324 CTAs in 1.09 waves.
+// at most (e.g. 12 tiles of the 256-projector x 160-band product as 37
+// splits: 444 CTAs in three full waves).
 int splitk_count(int M, int N, int K) {
     return splitk_count_tiles(((M + BM - 1) / BM) * ((N + BN - 1) / BN), K);
 }
@@ -277,8 +329,8 @@ int splitk_count_tiles(int tiles, int K) {
     double best_eff = -1.0;
     for (int s = 1; s <= max_splits; ++s) {
         const long long ctas = (long long)tiles * s;
-        const long long waves = (ctas + 295) / 296;
-        const double eff = (double)ctas / (waves * 296.0);
+        const long long waves = (ctas + kCtasPerWave - 1) / kCtasPerWave;
+        const double eff = (double)ctas / (waves * (double)kCtasPerWave);
         if (eff > best_eff + 0.02) {
             best_eff = eff;
             best = s;
@@ -304,7 +356,8 @@ void gemm_cn(const double2* A, int lda, const double2* B, int ldb, int M, int N,
     kchunk = (kchunk + BK - 1) / BK * BK;
     const int used = (K + kchunk - 1) / kchunk;
     dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN, used);
-    k_zgemm_cn_dmma<<<grid, 256, 0, st>>>(A, lda, B, ldb, M, N, K, kchunk, part, 0);
+    gemm_smem_setup();
+    k_zgemm_cn_dmma<<<grid, 256, kSmemCn, st>>>(A, lda, B, ldb, M, N, K, kchunk, part, 0);
     const size_t mn = (size_t)M * N;
     int blocks = (int)((mn + 255) / 256);
     if (blocks > 148 * 8) blocks = 148 * 8;
@@ -324,7 +377,8 @@ void gemm_cn_herm(const double2* A, int lda, const double2* B, int ldb, int N, i
     kchunk = (kchunk + BK - 1) / BK * BK;
     const int used = (K + kchunk - 1) / kchunk;
     dim3 grid(tiles, 1, used);
-    k_zgemm_cn_dmma<<<grid, 256, 0, st>>>(A, lda, B, ldb, N, N, K, kchunk, part, tn);
+    gemm_smem_setup();
+    k_zgemm_cn_dmma<<<grid, 256, kSmemCn, st>>>(A, lda, B, ldb, N, N, K, kchunk, part, tn);
     const size_t nn = (size_t)N * N;
     int blocks = (int)((nn + 255) / 256);
     if (blocks > 148 * 8) blocks = 148 * 8;
@@ -335,7 +389,8 @@ void gemm_tn(const double2* W, int ldw, const double2* X, int ldx, double2* O, i
              int N, int K, double alpha, double beta, cudaStream_t st) {
     count_launch();
     dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
-    k_zgemm_tn_dmma<<<grid, 256, 0, st>>>(W, ldw, X, ldx, O, ldo, M, N, K, alpha, beta);
+    gemm_smem_setup();
+    k_zgemm_tn_dmma<<<grid, 256, kSmemTn, st>>>(W, ldw, X, ldx, O, ldo, M, N, K, alpha, beta);
 }
 
 }  // namespace chfsi
@@ -354,7 +409,8 @@ void gemm_cn_capped(const double2* A, int lda, const double2* B, int ldb, int M,
     kchunk = (kchunk + BK - 1) / BK * BK;
     const int used = (K + kchunk - 1) / kchunk;
     dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN, used);
-    k_zgemm_cn_dmma<<<grid, 256, 0, st>>>(A, lda, B, ldb, M, N, K, kchunk, part, 0);
+    gemm_smem_setup();
+    k_zgemm_cn_dmma<<<grid, 256, kSmemCn, st>>>(A, lda, B, ldb, M, N, K, kchunk, part, 0);
     const size_t mn = (size_t)M * N;
     int blocks = (int)((mn + 255) / 256);
     if (blocks > 148 * 8) blocks = 148 * 8;
