@@ -428,7 +428,7 @@ struct chfsi_ctx {
     AxisPlan ax{}, ay{}, az{};
     std::vector<int> dr[3];
     int* d_col_start = nullptr; int* d_col_pos = nullptr; int* d_pw_col = nullptr;
-    int* d_pw_zpos = nullptr; int* d_xact = nullptr; int* d_idr[3] = {nullptr, nullptr, nullptr};
+    int* d_pw_zpos = nullptr; int* d_xact = nullptr; int* d_colidx = nullptr; int* d_idr[3] = {nullptr, nullptr, nullptr};
     int* d_perm = nullptr; bool perm_identity = true;
     double2* d_twd = nullptr;  // twiddle tables x | y | z, FP64
     float2* d_twf = nullptr;   // same, FP32
@@ -1555,7 +1555,7 @@ void free_all(chfsi_ctx* ctx) {
                   ctx->d_cgv, ctx->d_cgc, ctx->d_cgov, ctx->d_cgpart, ctx->d_cgdot, ctx->d_cgG,
                   ctx->d_psi_save, ctx->d_rc_hx, ctx->d_rc_y, ctx->d_rc_r0, ctx->d_rc_r1,
                   ctx->d_rc_y32, ctx->d_rc_coef, ctx->d_rc_lam, ctx->d_gga, ctx->d_gga_v1,
-                  ctx->d_ion, ctx->d_qvec, ctx->d_atom_of_ion};
+                  ctx->d_ion, ctx->d_qvec, ctx->d_atom_of_ion, ctx->d_colidx};
     for (void* p : mp)
         if (p) cudaFree(p);
     if (ctx->h_pin) cudaFreeHost(ctx->h_pin);
@@ -2001,7 +2001,7 @@ chfsi_status chfsi_set_basis(chfsi_ctx* ctx, const int32_t* miller, const double
     for (int i = 0; i < n; ++i)
         for (int d = 0; d < 3; ++d) ctx->miller_ctx[3 * (size_t)i + d] = miller[3 * (size_t)perm[i] + d];
     if (ctx->d_qvec) { cudaFree(ctx->d_qvec); ctx->d_qvec = nullptr; }
-    std::vector<int> col_start, col_pos, pw_col(n), pw_zpos(n), xact;
+    std::vector<int> col_start, col_pos, pw_col(n), pw_zpos(n), xact, col_px, col_py;
     std::vector<double> kin(n);
     std::vector<char> xused(nx, 0);
     int last = -1;
@@ -2013,6 +2013,8 @@ chfsi_status chfsi_set_basis(chfsi_ctx* ctx, const int32_t* miller, const double
             const int px = ctx->dr[0][ix[g]], py = ctx->dr[1][iy[g]];
             // plane rows and elements are XOR-swizzled in shared memory
             col_pos.push_back(swz(py, ny) * (nx | 1) + swz(px, nx));
+            col_px.push_back(px);
+            col_py.push_back(py);
             xused[px] = 1;
             last = c;
         } else if (i > 0 && miller[3 * g + 2] == miller[3 * perm[i - 1] + 2]) {
@@ -2024,8 +2026,17 @@ chfsi_status chfsi_set_basis(chfsi_ctx* ctx, const int32_t* miller, const double
     }
     const int ncol = (int)col_start.size();
     col_start.push_back(n);
+    std::vector<int> line_of(nx, -1);
     for (int x = 0; x < nx; ++x)
-        if (xused[x]) xact.push_back(swz(x, nx));
+        if (xused[x]) {
+            line_of[x] = (int)xact.size();
+            xact.push_back(swz(x, nx));
+        }
+    // direct column I/O table of the compile-time plane kernel:
+    // colidx[line * ny + py] = column at (active x line, digit-reversed y)
+    std::vector<int> colidx(xact.size() * (size_t)ny, -1);
+    for (int c = 0; c < (int)col_px.size(); ++c)
+        colidx[(size_t)line_of[col_px[c]] * ny + col_py[c]] = c;
     double kmax = 0.0;
     for (int g = 0; g < n; ++g) kmax = std::max(kmax, kinetic[g]);
     // kinetic bound of the reference: 1/2 Gmax^2 (chebyshev.rs:232)
@@ -2033,12 +2044,16 @@ chfsi_status chfsi_set_basis(chfsi_ctx* ctx, const int32_t* miller, const double
     if (ctx->d_col_start) cudaFree(ctx->d_col_start);
     if (ctx->d_col_pos) cudaFree(ctx->d_col_pos);
     if (ctx->d_xact) cudaFree(ctx->d_xact);
+    if (ctx->d_colidx) cudaFree(ctx->d_colidx);
+    ctx->d_colidx = nullptr;
     if (ctx->d_work) cudaFree(ctx->d_work);
     ctx->d_col_start = ctx->d_col_pos = ctx->d_xact = nullptr;
     ctx->d_work = nullptr;
     CK(dalloc(&ctx->d_col_start, ncol + 1));
     CK(dalloc(&ctx->d_col_pos, ncol));
     CK(dalloc(&ctx->d_xact, xact.size()));
+    CK(dalloc(&ctx->d_colidx, colidx.size()));
+    CK(copy_sync(ctx->d_colidx, colidx.data(), sizeof(int) * colidx.size(), cudaMemcpyHostToDevice, ctx->st));
     CK(dalloc(&ctx->d_work, (size_t)(ctx->nb + 1) * nz * ncol));
     CK(copy_sync(ctx->d_col_start, col_start.data(), sizeof(int) * (ncol + 1), cudaMemcpyHostToDevice, ctx->st));
     CK(copy_sync(ctx->d_col_pos, col_pos.data(), sizeof(int) * ncol, cudaMemcpyHostToDevice, ctx->st));
@@ -2070,6 +2085,10 @@ chfsi_status chfsi_set_basis(chfsi_ctx* ctx, const int32_t* miller, const double
     g.lsz = nz | 1; g.lsx = nx | 1; g.nxact = (int)xact.size();
     g.col_start = ctx->d_col_start; g.col_pos = ctx->d_col_pos; g.pw_col = ctx->d_pw_col;
     g.pw_zpos = ctx->d_pw_zpos; g.xact = ctx->d_xact;
+    g.colidx = nx <= 256 ? ctx->d_colidx : nullptr;
+    for (int w = 0; w < 8; ++w) g.xbits[w] = 0u;
+    for (int x = 0; x < nx && x < 256; ++x)
+        if (xused[x]) g.xbits[x >> 5] |= 1u << (x & 31);
     g.ax = ctx->ax; g.ay = ctx->ay; g.az = ctx->az;
     if (planes_smem_bytes(g, sizeof(double2)) > 227 * 1024)
         return ctx->fail(CHFSI_ERR_BAD_INPUT, "xy plane does not fit in shared memory");

@@ -275,6 +275,136 @@ k_planes_vloc_p2(C* __restrict__ work, const double* __restrict__ veff, HGeom g)
     for (int c = threadIdx.x; c < g.ncol; c += blockDim.x) wp[c] = plane[g.col_pos[c]];
 }
 
+// ------------------------------- pass 2, compile-time plans, no zero fill
+// The compile-time pipeline with the plane's columns read and written in
+// place of the shared-memory scatter and gather: the first inverse y stage
+// of every active x line loads its inputs from the column array (zero where
+// (x, y) holds no column), the last forward y stage stores its outputs
+// straight to the columns, the first inverse x stage reads zero for x
+// positions without columns instead of loading them, and the last forward x
+// stage stores only the x positions the forward y stage reads.  No position
+// of the plane is ever read before this CTA writes it, so the plane is not
+// zeroed, and the shared-memory traffic per plane drops by about 30 %.
+template <typename C, int V, int R0, int R1>
+__global__ void __launch_bounds__(PlanesCfg<C, V>::threads, PlanesCfg<C, V>::min_blocks)
+k_planes_vloc_p3(C* __restrict__ work, const double* __restrict__ veff, HGeom g) {
+    constexpr int N = R0 * R1, LS = N | 1, T = R0 > R1 ? R0 : R1, PW = 32 / T;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* twx = reinterpret_cast<C*>(smem_raw);
+    C* twy = reinterpret_cast<C*>(smem_raw + align16<C>(N));
+    C* plane = reinterpret_cast<C*>(smem_raw + 2 * align16<C>(N));
+    int* xl = reinterpret_cast<int*>(plane + (size_t)N * LS);
+    const int z = blockIdx.x, b = blockIdx.y;
+    const int nxact = g.nxact;
+    copy_twiddles(twx, g.twd_x, g.twf_x, N);
+    copy_twiddles(twy, g.twd_y, g.twf_y, N);
+    for (int i = threadIdx.x; i < nxact; i += blockDim.x) xl[i] = g.xact[i];
+    __syncthreads();
+    C* wp = work + ((size_t)b * g.nz + z) * g.ncol;
+    const int lane = threadIdx.x & 31, gi = lane / T, li = lane - gi * T;
+    const bool ing = gi < PW;
+    const int groups = (blockDim.x >> 5) * PW, gid = (threadIdx.x >> 5) * PW + gi;
+    using R = typename RealOf<C>::type;
+    // y lines through the active x positions: inverse, inputs from the columns
+    for (int l0 = 0; l0 < nxact; l0 += groups) {
+        const int l = l0 + gid;
+        const bool act = ing && l < nxact;
+        C* line = plane + (act ? xl[l] : 0);
+        if (act && li < R0) {
+            const int* ci = g.colidx + (size_t)l * N + li * R1;
+            C x[R1];
+#pragma unroll
+            for (int j = 0; j < R1; ++j) {
+                const int c = __ldg(ci + j);
+                x[j] = c >= 0 ? wp[c] : czero<C>();
+            }
+            dft_r<R1, 1>(x);
+#pragma unroll
+            for (int m = 0; m < R1; ++m) line[swz(li * R1 + m, N) * LS] = x[m];
+        }
+        __syncwarp();
+        if (act && li < R1) {
+            C x[R0];
+            p2_load_span<R0, R1>(line, LS, li, x);
+            p2_span_inverse<R0>(x, li, twy);
+            p2_store_span<R0, R1>(line, LS, li, x);
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+    // x rows: inverse (x positions without columns read as zero), x V(r),
+    // forward (only x positions with columns stored)
+    const double* vz = veff + (size_t)z * N * N;
+    for (int y0 = 0; y0 < N; y0 += groups) {
+        const int y = y0 + gid;
+        const bool act = ing && y < N;
+        C* row = plane + (act ? swz(y, N) * LS : 0);
+        if (act && li < R0) {
+            C x[R1];
+#pragma unroll
+            for (int j = 0; j < R1; ++j) {
+                const int px = li * R1 + j;
+                const bool on = (g.xbits[px >> 5] >> (px & 31)) & 1u;
+                x[j] = on ? row[swz(px, N)] : czero<C>();
+            }
+            dft_r<R1, 1>(x);
+#pragma unroll
+            for (int m = 0; m < R1; ++m) row[swz(li * R1 + m, N)] = x[m];
+        }
+        __syncwarp();
+        if (act && li < R1) {
+            C x[R0];
+            p2_load_span<R0, R1>(row, 1, li, x);
+            p2_span_inverse<R0>(x, li, twx);
+            const double* vr = vz + (size_t)y * N + li;
+#pragma unroll
+            for (int m = 0; m < R0; ++m) x[m] = cscale(x[m], (R)vr[m * R1]);
+            p2_span_forward<R0>(x, li, twx);
+            p2_store_span<R0, R1>(row, 1, li, x);
+        }
+        __syncwarp();
+        if (act && li < R0) {
+            C x[R1];
+#pragma unroll
+            for (int j = 0; j < R1; ++j) x[j] = row[swz(li * R1 + j, N)];
+            dft_r<R1, -1>(x);
+#pragma unroll
+            for (int m = 0; m < R1; ++m) {
+                const int px = li * R1 + m;
+                if ((g.xbits[px >> 5] >> (px & 31)) & 1u) row[swz(px, N)] = x[m];
+            }
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+    // y lines forward, outputs to the columns
+    for (int l0 = 0; l0 < nxact; l0 += groups) {
+        const int l = l0 + gid;
+        const bool act = ing && l < nxact;
+        C* line = plane + (act ? xl[l] : 0);
+        if (act && li < R1) {
+            C x[R0];
+            p2_load_span<R0, R1>(line, LS, li, x);
+            p2_span_forward<R0>(x, li, twy);
+            p2_store_span<R0, R1>(line, LS, li, x);
+        }
+        __syncwarp();
+        if (act && li < R0) {
+            C x[R1];
+#pragma unroll
+            for (int j = 0; j < R1; ++j) x[j] = line[swz(li * R1 + j, N) * LS];
+            dft_r<R1, -1>(x);
+            const int* ci = g.colidx + (size_t)l * N + li * R1;
+#pragma unroll
+            for (int m = 0; m < R1; ++m) {
+                const int c = __ldg(ci + m);
+                if (c >= 0) wp[c] = x[m];
+            }
+        }
+        __syncwarp();
+    }
+}
+
 // ---------------------------------------------------------------- pass 3
 template <typename C, int MODE, int kColsPerBlock>
 __global__ void __launch_bounds__(256)
@@ -600,6 +730,11 @@ template <typename C, int V, int R0, int R1>
 void planes_vloc_p2(C* work, const double* veff, int nb, const HGeom& g, cudaStream_t st) {
     dim3 grid(g.nz, nb);
     size_t sm = planes_smem_bytes(g, sizeof(C));
+    if (g.colidx && R0 * R1 <= 256) {
+        allow_smem(k_planes_vloc_p3<C, V, R0, R1>, sm);
+        k_planes_vloc_p3<C, V, R0, R1><<<grid, PlanesCfg<C, V>::threads, sm, st>>>(work, veff, g);
+        return;
+    }
     allow_smem(k_planes_vloc_p2<C, V, R0, R1>, sm);
     k_planes_vloc_p2<C, V, R0, R1><<<grid, PlanesCfg<C, V>::threads, sm, st>>>(work, veff, g);
 }

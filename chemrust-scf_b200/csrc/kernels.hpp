@@ -35,6 +35,11 @@ struct HGeom {
     // xy-plane kernels with compile-time radices where the plan has one
     // (square planes, two radices); 0 = always the generic kernel
     int fixed_planes = 1;
+    // direct column I/O of the compile-time plane kernel: colidx[l * ny + py]
+    // = column at (active x line l, digit-reversed y position py) or -1;
+    // xbits: bit px set when digit-reversed x position px carries columns
+    const int* colidx = nullptr;
+    unsigned int xbits[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 };
 
 // Pass-3 epilogue: what to do with (H psi)_g once it is assembled.
