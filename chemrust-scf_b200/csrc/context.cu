@@ -2863,10 +2863,10 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
         }
         eig_prev = eig;
         const bool eig_ok = p->tol_eig <= 0.0 || deig < p->tol_eig;
-        // the FP32 filter leaves ~1e-7 Ha of noise in the eigenvalue changes:
-        // the switch to FP64 takes ten times the tolerance, the FP64 steps
-        // after it meet the tolerance itself
-        const bool eig_near = p->tol_eig <= 0.0 || deig < 10.0 * p->tol_eig;
+        // the mixed iterations' eigenvalue changes carry ~2e-7 Ha of FP32
+        // noise (measured on the 216-atom cell): the switch to FP64 takes
+        // twice the tolerance, the FP64 iterations after it the tolerance
+        const bool eig_near = p->tol_eig <= 0.0 || deig < 2.0 * p->tol_eig;
         if (ctx->mixed_active) ++r->n_iter_mixed;
         if (p->verbose && p->tol_eig > 0.0)
             std::fprintf(stderr, "scf %3d max |d eig_occ| %.3e\n", it, deig);
@@ -2887,7 +2887,8 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
                 ctx->mixed_active = false;
                 low_mixed = 0;
             }
-        } else if (ctx->mixed && de > 10.0 * sw && reverts < kMaxReverts) {
+        } else if (ctx->mixed && (de > 10.0 * sw || (p->tol_eig > 0.0 && deig > 10.0 * p->tol_eig)) &&
+                   reverts < kMaxReverts) {
             ctx->mixed_active = true;
             ++reverts;
             if (p->verbose) std::fprintf(stderr, "scf %3d: |dE| %.3e, back to mixed precision\n", it, de);

@@ -56,9 +56,100 @@ template <typename C> __host__ __device__ __forceinline__ size_t align16(size_t 
     return (n * sizeof(C) + 15) & ~(size_t)15;
 }
 
+// ---- two-radix line transforms with compile-time plans (N = R0 R1; DIF
+// stage 0: radix R0 with span R1; stage 1: radix R1 on blocks of R1
+// consecutive elements, all twiddles 1), used by the z-stick and plane passes
+// radix-R1 stage on block blk (elements blk R1 .. blk R1 + R1 - 1)
+template <int R0, int R1, int SIGN, typename C>
+__device__ __forceinline__ void p2_blocks(C* line, int es, int blk) {
+    constexpr int N = R0 * R1;
+    C x[R1];
+#pragma unroll
+    for (int j = 0; j < R1; ++j) x[j] = line[swz(blk * R1 + j, N) * es];
+    dft_r<R1, SIGN>(x);
+#pragma unroll
+    for (int m = 0; m < R1; ++m) line[swz(blk * R1 + m, N) * es] = x[m];
+}
+template <int R0, int R1, typename C>
+__device__ __forceinline__ void p2_load_span(const C* line, int es, int n1, C* x) {
+#pragma unroll
+    for (int j = 0; j < R0; ++j) x[j] = line[swz(n1 + j * R1, R0 * R1) * es];
+}
+template <int R0, int R1, typename C>
+__device__ __forceinline__ void p2_store_span(C* line, int es, int n1, const C* x) {
+#pragma unroll
+    for (int j = 0; j < R0; ++j) line[swz(n1 + j * R1, R0 * R1) * es] = x[j];
+}
+// DIT stage 0 on span n1: twiddle w^(n1 m), radix-R0 DFT (sign +1)
+template <int R0, typename C>
+__device__ __forceinline__ void p2_span_inverse(C* x, int n1, const C* tw) {
+#pragma unroll
+    for (int m = 1; m < R0; ++m) x[m] = cmul(tw[n1 * m], x[m]);
+    dft_r<R0, 1>(x);
+}
+// DIF stage 0 on span n1: radix-R0 DFT (sign -1), twiddle w^(-n1 m)
+template <int R0, typename C>
+__device__ __forceinline__ void p2_span_forward(C* x, int n1, const C* tw) {
+    dft_r<R0, -1>(x);
+#pragma unroll
+    for (int m = 1; m < R0; ++m) x[m] = cmulc(tw[n1 * m], x[m]);
+}
+// whole-line transforms by one lane group (lane i); every lane of the warp
+// calls them (act = false: idle)
+template <int R0, int R1, typename C>
+__device__ __forceinline__ void p2_line_inverse(C* line, bool act, int i, int es, const C* tw) {
+    if (act && i < R0) p2_blocks<R0, R1, 1>(line, es, i);
+    __syncwarp();
+    if (act && i < R1) {
+        C x[R0];
+        p2_load_span<R0, R1>(line, es, i, x);
+        p2_span_inverse<R0>(x, i, tw);
+        p2_store_span<R0, R1>(line, es, i, x);
+    }
+    __syncwarp();
+}
+template <int R0, int R1, typename C>
+__device__ __forceinline__ void p2_line_forward(C* line, bool act, int i, int es, const C* tw) {
+    if (act && i < R1) {
+        C x[R0];
+        p2_load_span<R0, R1>(line, es, i, x);
+        p2_span_forward<R0>(x, i, tw);
+        p2_store_span<R0, R1>(line, es, i, x);
+    }
+    __syncwarp();
+    if (act && i < R0) p2_blocks<R0, R1, -1>(line, es, i);
+    __syncwarp();
+}
+
 // ---------------------------------------------------------------- pass 1
-template <typename C, int kColsPerBlock>
-__global__ void __launch_bounds__(256)
+// z lines of a block of columns transformed by one lane group per line with
+// the compile-time two-radix plan (R0 > 0) or by the generic engine
+template <int R0, int R1, bool FWD, typename C>
+__device__ __forceinline__ void zlines_fft(C* lines, int nl, const HGeom& g, const C* tw) {
+    if constexpr (R0 > 0) {
+        constexpr int T = R0 > R1 ? R0 : R1, PW = 32 / T;
+        const int lane = threadIdx.x & 31, gi = lane / T, li = lane - gi * T;
+        const bool ing = gi < PW;
+        const int groups = (blockDim.x >> 5) * PW, gid = (threadIdx.x >> 5) * PW + gi;
+        for (int l0 = 0; l0 < nl; l0 += groups) {
+            const int l = l0 + gid;
+            const bool act = ing && l < nl;
+            C* line = lines + (act ? l * g.lsz : 0);
+            if (FWD) p2_line_forward<R0, R1>(line, act, li, 1, tw);
+            else p2_line_inverse<R0, R1>(line, act, li, 1, tw);
+        }
+        __syncthreads();
+    } else {
+        fft_lines_grouped<FWD>(lines, nl, LinesStrided{g.lsz}, 1, g.az, tw);
+    }
+}
+
+// 3 resident blocks per SM with the compile-time plans (their registers
+// allow it), 1 guaranteed with the generic engine
+template <int R0> struct ZCfg { static constexpr int min_blocks = R0 > 0 ? 3 : 1; };
+
+template <typename C, int kColsPerBlock, int R0, int R1>
+__global__ void __launch_bounds__(256, ZCfg<R0>::min_blocks)
 k_zsticks_inverse(const C* __restrict__ psi, int ldp, C* __restrict__ work, HGeom g) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* tw = reinterpret_cast<C*>(smem_raw);
@@ -75,7 +166,7 @@ k_zsticks_inverse(const C* __restrict__ psi, int ldp, C* __restrict__ work, HGeo
     for (int q = g0 + threadIdx.x; q < g1; q += blockDim.x)
         lines[(g.pw_col[q] - c0) * g.lsz + swz(g.pw_zpos[q], g.nz)] = pb[q];
     __syncthreads();
-    fft_lines_grouped<false>(lines, nl, LinesStrided{g.lsz}, 1, g.az, tw);
+    zlines_fft<R0, R1, false>(lines, nl, g, tw);
     C* wb = work + (size_t)b * g.nz * g.ncol;
     for (int u = threadIdx.x; u < g.nz * kColsPerBlock; u += blockDim.x) {
         const int z = u / kColsPerBlock, cl = u - z * kColsPerBlock;
@@ -148,68 +239,6 @@ k_planes_vloc(C* __restrict__ work, const double* __restrict__ veff, HGeom g) {
 // stage, the V(r) multiply and the first forward stage share registers:
 // lane n1 of a row's lane group holds the R0 elements n1 + m R1, which is
 // what those two stages read and write.
-
-// radix-R1 stage on block blk (elements blk R1 .. blk R1 + R1 - 1)
-template <int R0, int R1, int SIGN, typename C>
-__device__ __forceinline__ void p2_blocks(C* line, int es, int blk) {
-    constexpr int N = R0 * R1;
-    C x[R1];
-#pragma unroll
-    for (int j = 0; j < R1; ++j) x[j] = line[swz(blk * R1 + j, N) * es];
-    dft_r<R1, SIGN>(x);
-#pragma unroll
-    for (int m = 0; m < R1; ++m) line[swz(blk * R1 + m, N) * es] = x[m];
-}
-template <int R0, int R1, typename C>
-__device__ __forceinline__ void p2_load_span(const C* line, int es, int n1, C* x) {
-#pragma unroll
-    for (int j = 0; j < R0; ++j) x[j] = line[swz(n1 + j * R1, R0 * R1) * es];
-}
-template <int R0, int R1, typename C>
-__device__ __forceinline__ void p2_store_span(C* line, int es, int n1, const C* x) {
-#pragma unroll
-    for (int j = 0; j < R0; ++j) line[swz(n1 + j * R1, R0 * R1) * es] = x[j];
-}
-// DIT stage 0 on span n1: twiddle w^(n1 m), radix-R0 DFT (sign +1)
-template <int R0, typename C>
-__device__ __forceinline__ void p2_span_inverse(C* x, int n1, const C* tw) {
-#pragma unroll
-    for (int m = 1; m < R0; ++m) x[m] = cmul(tw[n1 * m], x[m]);
-    dft_r<R0, 1>(x);
-}
-// DIF stage 0 on span n1: radix-R0 DFT (sign -1), twiddle w^(-n1 m)
-template <int R0, typename C>
-__device__ __forceinline__ void p2_span_forward(C* x, int n1, const C* tw) {
-    dft_r<R0, -1>(x);
-#pragma unroll
-    for (int m = 1; m < R0; ++m) x[m] = cmulc(tw[n1 * m], x[m]);
-}
-// whole-line transforms by one lane group (lane i); every lane of the warp
-// calls them (act = false: idle)
-template <int R0, int R1, typename C>
-__device__ __forceinline__ void p2_line_inverse(C* line, bool act, int i, int es, const C* tw) {
-    if (act && i < R0) p2_blocks<R0, R1, 1>(line, es, i);
-    __syncwarp();
-    if (act && i < R1) {
-        C x[R0];
-        p2_load_span<R0, R1>(line, es, i, x);
-        p2_span_inverse<R0>(x, i, tw);
-        p2_store_span<R0, R1>(line, es, i, x);
-    }
-    __syncwarp();
-}
-template <int R0, int R1, typename C>
-__device__ __forceinline__ void p2_line_forward(C* line, bool act, int i, int es, const C* tw) {
-    if (act && i < R1) {
-        C x[R0];
-        p2_load_span<R0, R1>(line, es, i, x);
-        p2_span_forward<R0>(x, i, tw);
-        p2_store_span<R0, R1>(line, es, i, x);
-    }
-    __syncwarp();
-    if (act && i < R0) p2_blocks<R0, R1, -1>(line, es, i);
-    __syncwarp();
-}
 
 // Square planes (nx = ny = R0 R1, both axes on the same plan); shared memory
 // layout and launch shape as k_planes_vloc.
@@ -406,8 +435,8 @@ k_planes_vloc_p3(C* __restrict__ work, const double* __restrict__ veff, HGeom g)
 }
 
 // ---------------------------------------------------------------- pass 3
-template <typename C, int MODE, int kColsPerBlock>
-__global__ void __launch_bounds__(256)
+template <typename C, int MODE, int kColsPerBlock, int R0, int R1>
+__global__ void __launch_bounds__(256, ZCfg<R0>::min_blocks)
 k_zsticks_forward(const C* __restrict__ work, const C* __restrict__ psi, int ldp, C* out, int ldo,
                   HGeom g, Epilogue e) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -426,7 +455,7 @@ k_zsticks_forward(const C* __restrict__ work, const C* __restrict__ psi, int ldp
         lines[cl * g.lsz + swz(z, g.nz)] = cl < nl ? wb[(size_t)z * g.ncol + c0 + cl] : czero<C>();
     }
     __syncthreads();
-    fft_lines_grouped<true>(lines, nl, LinesStrided{g.lsz}, 1, g.az, tw);
+    zlines_fft<R0, R1, true>(lines, nl, g, tw);
     const int g0 = g.col_start[c0], g1 = g.col_start[c1];
     const C* pb = psi + (size_t)b * ldp;
     C* ob = out + (size_t)b * ldo;
@@ -693,12 +722,26 @@ int grid_for(size_t n, int threads) {
 }  // namespace
 
 // ------------------------------------------------------------------ launchers
-template <typename C, int COLS>
-void zsticks_inverse_cols(const C* psi, int ldp, C* work, int nb, const HGeom& g, cudaStream_t st) {
+template <typename C, int COLS, int R0, int R1>
+void zsticks_inverse_launch(const C* psi, int ldp, C* work, int nb, const HGeom& g, cudaStream_t st) {
     dim3 grid((g.ncol + COLS - 1) / COLS, nb);
     size_t sm = align16<C>(g.nz) + (size_t)COLS * g.lsz * sizeof(C);
-    allow_smem(k_zsticks_inverse<C, COLS>, sm);
-    k_zsticks_inverse<C, COLS><<<grid, 256, sm, st>>>(psi, ldp, work, g);
+    allow_smem(k_zsticks_inverse<C, COLS, R0, R1>, sm);
+    k_zsticks_inverse<C, COLS, R0, R1><<<grid, 256, sm, st>>>(psi, ldp, work, g);
+}
+
+// two-radix z plans with compile-time kernels (the xy-plane list)
+#define CHFSI_ZPLANS(X) X(9, 8) X(12, 9) X(8, 5) X(12, 12) X(8, 8) X(8, 6)
+
+template <typename C, int COLS>
+void zsticks_inverse_cols(const C* psi, int ldp, C* work, int nb, const HGeom& g, cudaStream_t st) {
+    const int key = g.az.nst == 2 ? g.az.r[0] * 100 + g.az.r[1] : 0;
+    switch (key) {
+#define CHFSI_ZI(A, B) case A * 100 + B: zsticks_inverse_launch<C, COLS, A, B>(psi, ldp, work, nb, g, st); return;
+        CHFSI_ZPLANS(CHFSI_ZI)
+#undef CHFSI_ZI
+    default: zsticks_inverse_launch<C, COLS, 0, 0>(psi, ldp, work, nb, g, st);
+    }
 }
 
 template <typename C>
@@ -784,28 +827,35 @@ void launch_planes_vloc(C* work, const double* veff, int nb, const HGeom& g, cud
     }
 }
 
+template <typename C, int MODE, int COLS, int R0, int R1>
+void zsticks_forward_launch(const C* work, const C* psi, int ldp, C* out, int ldo, int nb,
+                            const HGeom& g, const Epilogue& e, cudaStream_t st) {
+    dim3 grid((g.ncol + COLS - 1) / COLS, nb);
+    size_t sm = align16<C>(g.nz) + (size_t)COLS * g.lsz * sizeof(C);
+    allow_smem(k_zsticks_forward<C, MODE, COLS, R0, R1>, sm);
+    k_zsticks_forward<C, MODE, COLS, R0, R1><<<grid, 256, sm, st>>>(work, psi, ldp, out, ldo, g, e);
+}
+
+template <typename C, int COLS, int R0, int R1>
+void zsticks_forward_modes(const C* work, const C* psi, int ldp, C* out, int ldo, int nb,
+                           const HGeom& g, const Epilogue& e, cudaStream_t st) {
+    switch (e.mode) {
+    case kEpiApply: zsticks_forward_launch<C, kEpiApply, COLS, R0, R1>(work, psi, ldp, out, ldo, nb, g, e, st); break;
+    case kEpiChebFirst: zsticks_forward_launch<C, kEpiChebFirst, COLS, R0, R1>(work, psi, ldp, out, ldo, nb, g, e, st); break;
+    case kEpiResid: zsticks_forward_launch<C, kEpiResid, COLS, R0, R1>(work, psi, ldp, out, ldo, nb, g, e, st); break;
+    default: zsticks_forward_launch<C, kEpiCheb, COLS, R0, R1>(work, psi, ldp, out, ldo, nb, g, e, st); break;
+    }
+}
+
 template <typename C, int COLS>
 void zsticks_forward_cols(const C* work, const C* psi, int ldp, C* out, int ldo, int nb,
                           const HGeom& g, const Epilogue& e, cudaStream_t st) {
-    dim3 grid((g.ncol + COLS - 1) / COLS, nb);
-    size_t sm = align16<C>(g.nz) + (size_t)COLS * g.lsz * sizeof(C);
-    switch (e.mode) {
-    case kEpiApply:
-        allow_smem(k_zsticks_forward<C, kEpiApply, COLS>, sm);
-        k_zsticks_forward<C, kEpiApply, COLS><<<grid, 256, sm, st>>>(work, psi, ldp, out, ldo, g, e);
-        break;
-    case kEpiChebFirst:
-        allow_smem(k_zsticks_forward<C, kEpiChebFirst, COLS>, sm);
-        k_zsticks_forward<C, kEpiChebFirst, COLS><<<grid, 256, sm, st>>>(work, psi, ldp, out, ldo, g, e);
-        break;
-    case kEpiResid:
-        allow_smem(k_zsticks_forward<C, kEpiResid, COLS>, sm);
-        k_zsticks_forward<C, kEpiResid, COLS><<<grid, 256, sm, st>>>(work, psi, ldp, out, ldo, g, e);
-        break;
-    default:
-        allow_smem(k_zsticks_forward<C, kEpiCheb, COLS>, sm);
-        k_zsticks_forward<C, kEpiCheb, COLS><<<grid, 256, sm, st>>>(work, psi, ldp, out, ldo, g, e);
-        break;
+    const int key = g.az.nst == 2 ? g.az.r[0] * 100 + g.az.r[1] : 0;
+    switch (key) {
+#define CHFSI_ZF(A, B) case A * 100 + B: zsticks_forward_modes<C, COLS, A, B>(work, psi, ldp, out, ldo, nb, g, e, st); return;
+        CHFSI_ZPLANS(CHFSI_ZF)
+#undef CHFSI_ZF
+    default: zsticks_forward_modes<C, COLS, 0, 0>(work, psi, ldp, out, ldo, nb, g, e, st);
     }
 }
 

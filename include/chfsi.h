@@ -362,7 +362,8 @@ typedef struct chfsi_scf_params {
                              (f > 0.01) to change by less than this (Ha) from the
                              previous iteration; mixed runs switch to FP64 only after
                              two mixed iterations with |dE| below the switch and
-                             eigenvalue changes below 10 x tol_eig                   */
+                             eigenvalue changes below 2 x tol_eig; an FP64 iteration
+                             with changes above 10 x tol_eig returns to mixed         */
 } chfsi_scf_params;
 
 /* Density mixers of chfsi_scf_run.  PULAY: Pulay/DIIS over (rho_in,
