@@ -11,9 +11,10 @@ At N = 1 the line also carries the time-to-SCF of the 216-atom ultrasoft
 cell (n_pw 173,925, 576 bands, 1,728 projectors, 108^3 / 144^3 grids):
 FP64 + Pulay, mixed precision + Pulay and mixed precision + the learned
 mixer, each stopped at |dE| < 1e-6 Ha/atom with the occupied eigenvalues
-changing by less than 1e-6 Ha between iterations, and each compared with
-the FP64 run continued (untimed) for further iterations toward tight
-convergence.
+changing by less than 1e-7 Ha between FP64 iterations (on this slowly
+converging metallic cell the remaining error is several times the last
+change), and each compared with the FP64 run continued (untimed) for
+further iterations toward tight convergence.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -288,11 +289,15 @@ def run_ours(args):
         s2 = chfsi.SyntheticSystem(config_index=2)
         net = learned_mixer.load(device=local)
         scf216 = time_to_scf(chfsi, s2, 16, local, net, max_iter=args.scf_216_max_iter,
-                             tight_max_iter=30)
+                             tight_max_iter=20)
         scf216["workload"] = ("216-atom ultrasoft cell, a=30.78 bohr, Ecut 25 Ha, n_pw=%d, "
                               "grid 108^3 (density 144^3), %d bands, %d projectors, degree 16"
                               % (s2.n_pw, s2.n_bands, s2.n_proj))
         del s2
+
+    batched = None
+    if world == 1 and not args.no_batch:
+        batched = batched_passes(chfsi, local)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -313,6 +318,7 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "mixed_precision": mixed,
             "time_to_scf_216atom": scf216,
+            "batched": batched,
         }
         print(json.dumps(line))
     if dist:
@@ -323,7 +329,8 @@ def run_ours(args):
 
 # time-to-SCF stopping rule of every timed arm, and the tight FP64 reference
 SCF_TOL_PER_ATOM = 1e-6   # |dE| per atom (Ha)
-SCF_TOL_EIG = 1e-6        # change of the occupied eigenvalues between iterations (Ha)
+SCF_TOL_EIG = 1e-7        # change of the occupied eigenvalues between iterations (Ha)
+FP64_SWITCH_EIG = 1e-6    # mixed arms: FP64 filter once the changes fall below this
 TIGHT_TOL_PER_ATOM = 1e-10
 TIGHT_TOL_EIG = 1e-9
 
@@ -347,15 +354,18 @@ def time_to_scf(chfsi, s, ndeg, device, net, max_iter, tight_max_iter):
             ctx.set_mixer(net)
         res[name] = ctx.run_scf(ndeg, tol_per_atom=SCF_TOL_PER_ATOM, tol_eig=SCF_TOL_EIG,
                                 max_iter=max_iter, kT=0.01, mixer=mode,
-                                fp64_switch_per_atom=SCF_TOL_PER_ATOM)
+                                fp64_switch_per_atom=SCF_TOL_PER_ATOM,
+                                fp64_switch_eig=FP64_SWITCH_EIG)
         if name == "fp64":
             tight = ctx.run_scf(ndeg, tol_per_atom=TIGHT_TOL_PER_ATOM, tol_eig=TIGHT_TOL_EIG,
                                 max_iter=tight_max_iter, kT=0.01, restart=True)
         ctx.close()
     n_occ = s.n_occ
     out = {"criterion": "|dE| < %g Ha/atom and occupied eigenvalues changing by < %g Ha "
-                        "(Fermi-Dirac kT = 0.01 Ha; Pulay alpha 0.3, history 6)"
-                        % (SCF_TOL_PER_ATOM, SCF_TOL_EIG),
+                        "on an FP64 iteration (Fermi-Dirac kT = 0.01 Ha; Pulay alpha 0.3, "
+                        "history 6); mixed arms filter in FP64 once two mixed iterations "
+                        "change the eigenvalues by < %g Ha"
+                        % (SCF_TOL_PER_ATOM, SCF_TOL_EIG, FP64_SWITCH_EIG),
            "reference": "FP64 run continued for up to %d more iterations toward |dE| < %g "
                         "Ha/atom and eigenvalue changes < %g Ha" % (tight_max_iter,
                                                                    TIGHT_TOL_PER_ATOM, TIGHT_TOL_EIG),
@@ -380,6 +390,73 @@ def time_to_scf(chfsi, s, ndeg, device, net, max_iter, tight_max_iter):
         if name != "fp64":
             a["speedup_vs_fp64"] = round(f["seconds"] / r["seconds"], 3) if r["seconds"] > 0 else None
         out["arms"][name] = a
+    return out
+
+
+# batched passes: the 8-atom cell on a 4x4x4 Monkhorst-Pack mesh (64
+# k-points) and 32 seeded cells of 8, 16, 27 or 64 atoms at the 8-atom cell's
+# density (Z = 4, Ecut 15 Ha, 1.25 x the occupied bands)
+BATCH_KINDS = [(0, 1, 8), (2, 2, 2), (1, 3, 1), (0, 2, 8)]  # (lattice, n_rep, atoms per cell)
+BATCH_DEG = 12
+
+
+def batch_systems(chfsi):
+    import numpy as np
+    out = []
+    mp = [(i - 2.5) / 4.0 for i in range(1, 5)]
+    for kx in mp:
+        for ky in mp:
+            for kz in mp:
+                out.append(chfsi.SyntheticSystem(config_index=0, kpt=(kx, ky, kz)))
+    rng = np.random.default_rng(2024)
+    vol = 10.26 ** 3 / 8.0
+    for i in range(32):
+        lattice, n_rep, per = BATCH_KINDS[int(rng.integers(0, len(BATCH_KINDS)))]
+        out.append(chfsi.SyntheticSystem(config_index=0, lattice=lattice, n_rep=n_rep,
+                                         a_conv=(per * vol) ** (1.0 / 3.0), seed=100 + i,
+                                         ngrid=(0, 0, 0), n_bands=0))
+    return out
+
+
+def batched_passes(chfsi, device, reps=3):
+    """One mixed-precision pass (degree-12 FP32 filter + FP64 Rayleigh-Ritz)
+    of all 96 members: replayed as one CUDA graph, and context by context;
+    host wall time per pass including the eigenvalue read-back."""
+    import numpy as np
+    systems = batch_systems(chfsi)
+    ctxs, eigs = [], []
+    for s in systems:
+        c = chfsi.Context(s, device=device, precision=chfsi.PREC_MIXED)
+        c.build_v_eff(np.full(c.ng_density, s.n_elec / s.omega))
+        w = c.diagonalize(BATCH_DEG)
+        w = c.diagonalize(BATCH_DEG, w)
+        ctxs.append(c)
+        eigs.append(w)
+    b = chfsi.Batch(ctxs)
+    nodes = b.capture(BATCH_DEG)
+    b.run()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        eigs = b.run()
+    t_graph = (time.perf_counter() - t0) / reps
+    for i, c in enumerate(ctxs):
+        eigs[i] = c.diagonalize(BATCH_DEG, eigs[i])
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        for i, c in enumerate(ctxs):
+            eigs[i] = c.diagonalize(BATCH_DEG, eigs[i])
+    t_seq = (time.perf_counter() - t0) / reps
+    n_pw = [s.n_pw for s in systems]
+    out = {"workload": "64 k-points of the 8-atom cell (4x4x4 Monkhorst-Pack) + 32 cells of "
+                       "8/16/27/64 atoms; one degree-%d mixed-precision pass of each" % BATCH_DEG,
+           "members": len(systems), "bands": int(sum(s.n_bands for s in systems)),
+           "n_pw_min": int(min(n_pw)), "n_pw_max": int(max(n_pw)),
+           "graph_nodes": int(nodes), "graph_ms_per_pass": round(t_graph * 1e3, 2),
+           "sequential_ms_per_pass": round(t_seq * 1e3, 2),
+           "speedup": round(t_seq / t_graph, 3)}
+    b.close()
+    for c in ctxs:
+        c.close()
     return out
 
 
@@ -536,6 +613,8 @@ def main():
     ap.add_argument("--no-scf-216", action="store_true",
                     help="skip the 216-atom time-to-SCF comparison (about ten minutes)")
     ap.add_argument("--scf-216-max-iter", type=int, default=150)
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip the batched-pass comparison (64 k-points + 32 cells)")
     ap.add_argument("--profile", choices=["local", "fp64", "mixed", "fp64-216", "mixed-216", "gemm"],
                     default=None,
                     help="a short fixed workload for ncu captures (no JSON line): two local "

@@ -121,7 +121,8 @@ class ScfParams(C.Structure):
                 ("alpha", C.c_double), ("max_hist", C.c_int), ("first_passes", C.c_int),
                 ("kT", C.c_double), ("fp64_switch_per_atom", C.c_double),
                 ("mixer", C.c_int), ("cg_steps", C.c_int), ("trace", C.POINTER(C.c_double)),
-                ("verbose", C.c_int), ("restart", C.c_int), ("tol_eig", C.c_double)]
+                ("verbose", C.c_int), ("restart", C.c_int), ("tol_eig", C.c_double),
+                ("fp64_switch_eig", C.c_double)]
 
 
 class ScfResult(C.Structure):
@@ -723,15 +724,16 @@ class Context:
     def run_scf(self, ndeg, tol_per_atom=1e-6, max_iter=30, alpha=0.3, max_hist=6,
                 first_passes=4, kT=0.01, fp64_switch_per_atom=1e-4, raise_not_converged=False,
                 mixer=MIXER_PULAY, trace=False, cg_steps=0, verbose=False, tol_eig=0.0,
-                restart=False):
+                restart=False, fp64_switch_eig=0.0):
         """Full SCF; mixer is MIXER_PULAY or, after set_mixer(), MIXER_LEARNED /
-        MIXER_LEARNED_PULAY.  tol_eig > 0 adds the occupied-eigenvalue change test;
+        MIXER_LEARNED_PULAY.  tol_eig > 0 adds the occupied-eigenvalue change test
+        (mixed runs switch to FP64 below max(2 tol_eig, fp64_switch_eig));
         restart=True continues from this context's last state.  trace=True also
         returns rho_in and rho_out of every iteration (n_iter x N^3 each) as
         'trace_in' / 'trace_out'."""
         p = ScfParams(ndeg, max_iter, tol_per_atom, alpha, max_hist, first_passes, kT,
                       fp64_switch_per_atom, mixer, cg_steps, None, int(verbose), int(restart),
-                      tol_eig)
+                      tol_eig, fp64_switch_eig)
         tr = None
         if trace:
             tr = np.zeros((max_iter, 2, self.ng_density))

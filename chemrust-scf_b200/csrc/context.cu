@@ -487,6 +487,7 @@ struct chfsi_ctx {
     double s_min = 1.0;
     double2* d_qmat = nullptr;   // per-ion q blocks (layout of D)
     double2* d_sinvT = nullptr;  // M^T, M = q (1 + B q)^-1, S^-1 = 1 - beta M beta^H
+    double2* d_bmatT = nullptr;  // B^T = conj(B), B = beta^H beta
     double2* d_cq = nullptr;     // n_proj x n_bands scratch
     double2* d_sx = nullptr;     // n_bands x n_pw scratch
     // mixed precision (FP32 filter, tcgen05 BF16x3 GEMMs)
@@ -584,7 +585,7 @@ struct ResidStep {
 
 chfsi_status apply_h_dev(chfsi_ctx* ctx, const double2* psi, double2* out, int nb, int mode,
                          double* norm_acc, int plain_band = -1, double2* plain_out = nullptr,
-                         const ResidStep* rs = nullptr) {
+                         const ResidStep* rs = nullptr, bool with_nl = true) {
     Epilogue e{};
     e.mode = mode;
     e.plain_band = plain_band;
@@ -595,7 +596,7 @@ chfsi_status apply_h_dev(chfsi_ctx* ctx, const double2* psi, double2* out, int n
     e.nl = nullptr;
     e.norm_acc = norm_acc;
     e.inv_n = 1.0 / (double)ctx->ng;
-    if (ctx->np > 0) {
+    if (ctx->np > 0 && with_nl) {
         // C = beta^H psi, C <- D C, nl = beta C  (chebyshev.rs:416-500)
         gemm_cn(ctx->d_beta, ctx->n_pw, psi, ctx->n_pw, ctx->np, nb, ctx->n_pw, ctx->d_part,
                 ctx->d_cp, ctx->st);
@@ -615,9 +616,37 @@ chfsi_status apply_h_dev(chfsi_ctx* ctx, const double2* psi, double2* out, int n
     return CHFSI_OK;
 }
 
+// S^-1 H x of the generalised (ultrasoft) problem as d_hpsi - d_sx:
+//   H x = H_loc x + beta G,  G = D C,  C = beta^H x,
+//   S^-1 = 1 - beta M beta^H,  M = q (1 + B q)^-1,  B = beta^H beta,
+//   S^-1 H x = H_loc x - beta F,  F = M (E + B G) - G,  E = beta^H (H_loc x),
+// so one application takes two n_pw-long projections (C, E) and one
+// expansion (beta F); B G and M (.) are n_proj-sized products.  d_hpsi gets
+// H_loc x for ncols columns, d_sx gets beta F for the first nout of them;
+// d_cd keeps G (ld ncols).
+chfsi_status sinv_h_parts(chfsi_ctx* ctx, const double2* x, int ncols, int nout) {
+    cudaStream_t st = ctx->st;
+    const int np = ctx->np, npw = ctx->n_pw;
+    gemm_cn(ctx->d_beta, npw, x, npw, np, ncols, npw, ctx->d_part, ctx->d_cp, st);
+    count_launch();
+    k_apply_dmat<<<grid_for((size_t)np * ncols), 256, 0, st>>>(
+        ctx->d_cp, ctx->d_cd, np, ncols, ctx->d_proj_ion, ctx->d_poff, ctx->d_doff, ctx->d_dmat);
+    chfsi_status s = apply_h_dev(ctx, x, ctx->d_hpsi, ncols, kEpiApply, nullptr, -1, nullptr,
+                                 nullptr, false);
+    if (s) return s;
+    gemm_cn(ctx->d_beta, npw, ctx->d_hpsi, npw, np, ncols, npw, ctx->d_part, ctx->d_cp, st);
+    gemm_tn(ctx->d_bmatT, np, ctx->d_cd, ncols, ctx->d_cp, ncols, np, ncols, np, 1.0, 1.0, st);
+    CK(cudaMemcpyAsync(ctx->d_cq, ctx->d_cd, sizeof(double2) * (size_t)np * ncols,
+                       cudaMemcpyDeviceToDevice, st));
+    gemm_tn(ctx->d_sinvT, np, ctx->d_cp, ncols, ctx->d_cq, ncols, np, ncols, np, 1.0, -1.0, st);
+    gemm_tn(ctx->d_cq, ncols, ctx->d_beta, npw, ctx->d_sx, npw, nout, npw, np, 1.0, 0.0, st);
+    CK(cudaGetLastError());
+    return CHFSI_OK;
+}
+
 // One filter operator application: H x, or S^-1 H x for the generalised
-// (ultrasoft) problem, where S^-1 = 1 - beta M beta^H is applied to H x by
-// three GEMMs and the recurrence epilogue runs in k_cheb_combine.
+// (ultrasoft) problem (sinv_h_parts), with the recurrence epilogue in
+// k_cheb_combine.
 // lz_col: row nb of x holds the carried Lanczos vector v; H v goes to d_lz_f
 // (the H of the generalised problem's pencil, without S^-1, like the
 // separate Lanczos run).
@@ -627,17 +656,17 @@ chfsi_status apply_op_dev(chfsi_ctx* ctx, const double2* x, double2* out, int nb
         if (!lz_col) return apply_h_dev(ctx, x, out, nb, mode, norm_acc);
         return apply_h_dev(ctx, x, out, nb + 1, mode, norm_acc, nb, ctx->d_lz_f);
     }
-    chfsi_status s = apply_h_dev(ctx, x, ctx->d_hpsi, nb + (lz_col ? 1 : 0), kEpiApply, nullptr);
+    const int ncols = nb + (lz_col ? 1 : 0);
+    chfsi_status s = sinv_h_parts(ctx, x, ncols, nb);
     if (s) return s;
-    if (lz_col)
-        CK(cudaMemcpyAsync(ctx->d_lz_f, ctx->d_hpsi + (size_t)nb * ctx->n_pw,
-                           sizeof(double2) * ctx->n_pw, cudaMemcpyDeviceToDevice, ctx->st));
     cudaStream_t st = ctx->st;
-    gemm_cn(ctx->d_beta, ctx->n_pw, ctx->d_hpsi, ctx->n_pw, ctx->np, nb, ctx->n_pw, ctx->d_part,
-            ctx->d_cp, st);
-    gemm_tn(ctx->d_sinvT, ctx->np, ctx->d_cp, nb, ctx->d_cq, nb, ctx->np, nb, ctx->np, 1.0, 0.0, st);
-    gemm_tn(ctx->d_cq, nb, ctx->d_beta, ctx->n_pw, ctx->d_sx, ctx->n_pw, nb, ctx->n_pw, ctx->np, 1.0,
-            0.0, st);
+    if (lz_col) {
+        // H v = H_loc v + beta G_v
+        CK(cudaMemcpyAsync(ctx->d_lz_f, ctx->d_hpsi + (size_t)nb * ctx->n_pw,
+                           sizeof(double2) * ctx->n_pw, cudaMemcpyDeviceToDevice, st));
+        gemm_tn(ctx->d_cd + nb, ncols, ctx->d_beta, ctx->n_pw, ctx->d_lz_f, ctx->n_pw, 1,
+                ctx->n_pw, ctx->np, 1.0, 1.0, st);
+    }
     const size_t n = (size_t)nb * ctx->n_pw;
     count_launch();
     k_cheb_combine<double2><<<grid_for(n), 256, 0, st>>>(ctx->d_hpsi, ctx->d_sx, x, out, n, ctx->d_coef,
@@ -912,22 +941,43 @@ chfsi_status apply_h_dev32(chfsi_ctx* ctx, const float2* psi, float2* out, int n
     return CHFSI_OK;
 }
 
-// S^-1 H x for the FP32 filter of the generalised problem: H x (FP32 local
-// pass), C = beta^H Hx (tcgen05), M C (FP64), beta (M C) (tcgen05, FP32
-// out), then the recurrence epilogue in k_cheb_combine<float2>.
+// S^-1 H x for the FP32 filter of the generalised problem as
+// d_hpsi32 - d_nl32, in the form of sinv_h_parts: C = beta^H x and
+// E = beta^H (H_loc x) on tcgen05, F = M (E + B G) - G in FP64, beta F on
+// tcgen05 (FP32 out).
+chfsi_status sinv_h_parts32(chfsi_ctx* ctx, const float2* x, int nb) {
+    cudaStream_t st = ctx->st;
+    const int np = ctx->np, npw = ctx->n_pw;
+    tc_pack<float2>(x, npw, nb, npw, false, kSrcPlain, ctx->tp_psi_b, st);
+    CK(tc_gemm(ctx->tp_beta_a, ctx->tp_psi_b, np, nb, npw, kTcOutPartial, ctx->d_cp, nb,
+               ctx->d_tc_part, ctx->d_tc_err, st));
+    count_launch();
+    k_apply_dmat<<<grid_for((size_t)np * nb), 256, 0, st>>>(
+        ctx->d_cp, ctx->d_cd, np, nb, ctx->d_proj_ion, ctx->d_poff, ctx->d_doff, ctx->d_dmat);
+    chfsi_status s = apply_h_dev32(ctx, x, ctx->d_hpsi32, nb, kEpiApply, nullptr, true);
+    if (s) return s;
+    tc_pack<float2>(ctx->d_hpsi32, npw, nb, npw, false, kSrcPlain, ctx->tp_psi_b, st);
+    CK(tc_gemm(ctx->tp_beta_a, ctx->tp_psi_b, np, nb, npw, kTcOutPartial, ctx->d_cp, nb,
+               ctx->d_tc_part, ctx->d_tc_err, st));
+    gemm_tn(ctx->d_bmatT, np, ctx->d_cd, nb, ctx->d_cp, nb, np, nb, np, 1.0, 1.0, st);
+    CK(cudaMemcpyAsync(ctx->d_cq, ctx->d_cd, sizeof(double2) * (size_t)np * nb,
+                       cudaMemcpyDeviceToDevice, st));
+    gemm_tn(ctx->d_sinvT, np, ctx->d_cp, nb, ctx->d_cq, nb, np, nb, np, 1.0, -1.0, st);
+    tc_pack<double2>(ctx->d_cq, nb, nb, np, true, kSrcConjT, ctx->tp_small_a, st);
+    CK(tc_gemm(ctx->tp_small_a, ctx->tp_betaT_b, nb, npw, np, kTcOutComplexF32, ctx->d_nl32, npw,
+               nullptr, ctx->d_tc_err, st));
+    CK(cudaGetLastError());
+    return CHFSI_OK;
+}
+
+// S^-1 H x for the FP32 filter of the generalised problem (sinv_h_parts32),
+// then the recurrence epilogue in k_cheb_combine<float2>.
 chfsi_status apply_op_dev32(chfsi_ctx* ctx, const float2* x, float2* out, int nb, int mode,
                             double* norm_acc) {
     if (!ctx->uspp || mode == kEpiApply) return apply_h_dev32(ctx, x, out, nb, mode, norm_acc);
-    chfsi_status s = apply_h_dev32(ctx, x, ctx->d_hpsi32, nb, kEpiApply, nullptr);
+    chfsi_status s = sinv_h_parts32(ctx, x, nb);
     if (s) return s;
     cudaStream_t st = ctx->st;
-    tc_pack<float2>(ctx->d_hpsi32, ctx->n_pw, nb, ctx->n_pw, false, kSrcPlain, ctx->tp_psi_b, st);
-    CK(tc_gemm(ctx->tp_beta_a, ctx->tp_psi_b, ctx->np, nb, ctx->n_pw, kTcOutPartial, ctx->d_cp, nb,
-               ctx->d_tc_part, ctx->d_tc_err, st));
-    gemm_tn(ctx->d_sinvT, ctx->np, ctx->d_cp, nb, ctx->d_cq, nb, ctx->np, nb, ctx->np, 1.0, 0.0, st);
-    tc_pack<double2>(ctx->d_cq, nb, nb, ctx->np, true, kSrcConjT, ctx->tp_small_a, st);
-    CK(tc_gemm(ctx->tp_small_a, ctx->tp_betaT_b, nb, ctx->n_pw, ctx->np, kTcOutComplexF32,
-               ctx->d_nl32, ctx->n_pw, nullptr, ctx->d_tc_err, st));
     const size_t n = (size_t)nb * ctx->n_pw;
     count_launch();
     k_cheb_combine<float2><<<grid_for(n), 256, 0, st>>>(ctx->d_hpsi32, ctx->d_nl32, x, out, n,
@@ -1012,14 +1062,9 @@ chfsi_status alloc_rchfsi(chfsi_ctx* ctx, bool fp32) {
 chfsi_status rc_step64(chfsi_ctx* ctx, const double2* x, double2* out, const ResidStep& rs) {
     const int nb = ctx->nb;
     if (!ctx->uspp) return apply_h_dev(ctx, x, out, nb, kEpiResid, nullptr, -1, nullptr, &rs);
-    chfsi_status s = apply_h_dev(ctx, x, ctx->d_hpsi, nb, kEpiApply, nullptr);
+    chfsi_status s = sinv_h_parts(ctx, x, nb, nb);
     if (s) return s;
     cudaStream_t st = ctx->st;
-    gemm_cn(ctx->d_beta, ctx->n_pw, ctx->d_hpsi, ctx->n_pw, ctx->np, nb, ctx->n_pw, ctx->d_part,
-            ctx->d_cp, st);
-    gemm_tn(ctx->d_sinvT, ctx->np, ctx->d_cp, nb, ctx->d_cq, nb, ctx->np, nb, ctx->np, 1.0, 0.0, st);
-    gemm_tn(ctx->d_cq, nb, ctx->d_beta, ctx->n_pw, ctx->d_sx, ctx->n_pw, nb, ctx->n_pw, ctx->np, 1.0,
-            0.0, st);
     const size_t n = (size_t)nb * ctx->n_pw;
     count_launch();
     k_cheb_combine<double2><<<grid_for(n), 256, 0, st>>>(
@@ -1032,16 +1077,9 @@ chfsi_status rc_step64(chfsi_ctx* ctx, const double2* x, double2* out, const Res
 chfsi_status rc_step32(chfsi_ctx* ctx, const float2* x, float2* out, const ResidStep& rs) {
     const int nb = ctx->nb;
     if (!ctx->uspp) return apply_h_dev32(ctx, x, out, nb, kEpiResid, nullptr, false, &rs);
-    chfsi_status s = apply_h_dev32(ctx, x, ctx->d_hpsi32, nb, kEpiApply, nullptr);
+    chfsi_status s = sinv_h_parts32(ctx, x, nb);
     if (s) return s;
     cudaStream_t st = ctx->st;
-    tc_pack<float2>(ctx->d_hpsi32, ctx->n_pw, nb, ctx->n_pw, false, kSrcPlain, ctx->tp_psi_b, st);
-    CK(tc_gemm(ctx->tp_beta_a, ctx->tp_psi_b, ctx->np, nb, ctx->n_pw, kTcOutPartial, ctx->d_cp, nb,
-               ctx->d_tc_part, ctx->d_tc_err, st));
-    gemm_tn(ctx->d_sinvT, ctx->np, ctx->d_cp, nb, ctx->d_cq, nb, ctx->np, nb, ctx->np, 1.0, 0.0, st);
-    tc_pack<double2>(ctx->d_cq, nb, nb, ctx->np, true, kSrcConjT, ctx->tp_small_a, st);
-    CK(tc_gemm(ctx->tp_small_a, ctx->tp_betaT_b, nb, ctx->n_pw, ctx->np, kTcOutComplexF32,
-               ctx->d_nl32, ctx->n_pw, nullptr, ctx->d_tc_err, st));
     const size_t n = (size_t)nb * ctx->n_pw;
     count_launch();
     k_cheb_combine<float2><<<grid_for(n), 256, 0, st>>>(
@@ -1555,7 +1593,7 @@ void free_all(chfsi_ctx* ctx) {
                   ctx->d_cgv, ctx->d_cgc, ctx->d_cgov, ctx->d_cgpart, ctx->d_cgdot, ctx->d_cgG,
                   ctx->d_psi_save, ctx->d_rc_hx, ctx->d_rc_y, ctx->d_rc_r0, ctx->d_rc_r1,
                   ctx->d_rc_y32, ctx->d_rc_coef, ctx->d_rc_lam, ctx->d_gga, ctx->d_gga_v1,
-                  ctx->d_ion, ctx->d_qvec, ctx->d_atom_of_ion, ctx->d_colidx};
+                  ctx->d_ion, ctx->d_qvec, ctx->d_atom_of_ion, ctx->d_colidx, ctx->d_bmatT};
     for (void* p : mp)
         if (p) cudaFree(p);
     if (ctx->h_pin) cudaFreeHost(ctx->h_pin);
@@ -2175,6 +2213,12 @@ chfsi_status chfsi_set_qmat(chfsi_ctx* ctx, const chfsi_c128* qmat) {
     gemm_cn(ctx->d_beta, ctx->n_pw, ctx->d_beta, ctx->n_pw, np, np, ctx->n_pw, part, dB, ctx->st);
     std::vector<std::complex<double>> B((size_t)np * np), Q((size_t)np * np, 0.0);
     cudaError_t e = cudaMemcpyAsync(B.data(), dB, B.size() * sizeof(double2), cudaMemcpyDeviceToHost, ctx->st);
+    if (e == cudaSuccess && !ctx->d_bmatT) e = dalloc(&ctx->d_bmatT, (size_t)np * np);
+    if (e == cudaSuccess) {
+        count_launch();
+        k_conj<<<grid_for((size_t)np * np), 256, 0, ctx->st>>>(dB, ctx->d_bmatT, (size_t)np * np);
+        e = cudaGetLastError();
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->st);
     cudaFree(part);
     cudaFree(dB);
@@ -2319,15 +2363,9 @@ chfsi_status chfsi_apply_sinv_h(chfsi_ctx* ctx, const chfsi_c128* psi_dev, chfsi
     if (!ctx->uspp) {
         s = apply_h_dev(ctx, x, out, nb, kEpiApply, nullptr);
     } else {
-        s = apply_h_dev(ctx, x, ctx->d_hpsi, nb, kEpiApply, nullptr);
+        s = sinv_h_parts(ctx, x, nb, nb);
         if (s) return s;
         cudaStream_t st = ctx->st;
-        gemm_cn(ctx->d_beta, ctx->n_pw, ctx->d_hpsi, ctx->n_pw, ctx->np, nb, ctx->n_pw,
-                ctx->d_part, ctx->d_cp, st);
-        gemm_tn(ctx->d_sinvT, ctx->np, ctx->d_cp, nb, ctx->d_cq, nb, ctx->np, nb, ctx->np, 1.0,
-                0.0, st);
-        gemm_tn(ctx->d_cq, nb, ctx->d_beta, ctx->n_pw, ctx->d_sx, ctx->n_pw, nb, ctx->n_pw,
-                ctx->np, 1.0, 0.0, st);
         const size_t n = (size_t)nb * ctx->n_pw;
         count_launch();
         k_cheb_combine<double2><<<grid_for(n), 256, 0, st>>>(ctx->d_hpsi, ctx->d_sx, x, out, n,
@@ -2712,6 +2750,8 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
     int rises = 0;
     bool restart_pulay = false;
     double r_prev = -1.0;
+    constexpr int kStallWindow = 5;
+    std::vector<double> rhist;
     std::vector<double> eig(ctx->nb), eig_prev(ctx->nb);
     bool have_eig = restart;
     if (restart)
@@ -2864,9 +2904,10 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
         eig_prev = eig;
         const bool eig_ok = p->tol_eig <= 0.0 || deig < p->tol_eig;
         // the mixed iterations' eigenvalue changes carry ~2e-7 Ha of FP32
-        // noise (measured on the 216-atom cell): the switch to FP64 takes
-        // twice the tolerance, the FP64 iterations after it the tolerance
-        const bool eig_near = p->tol_eig <= 0.0 || deig < 2.0 * p->tol_eig;
+        // noise (measured on the 216-atom cell): the switch to FP64 takes at
+        // least twice the tolerance, the FP64 iterations after it the tolerance
+        const double sw_eig = std::max(2.0 * p->tol_eig, p->fp64_switch_eig);
+        const bool eig_near = p->tol_eig <= 0.0 || deig < sw_eig;
         if (ctx->mixed_active) ++r->n_iter_mixed;
         if (p->verbose && p->tol_eig > 0.0)
             std::fprintf(stderr, "scf %3d max |d eig_occ| %.3e\n", it, deig);
@@ -2887,7 +2928,7 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
                 ctx->mixed_active = false;
                 low_mixed = 0;
             }
-        } else if (ctx->mixed && (de > 10.0 * sw || (p->tol_eig > 0.0 && deig > 10.0 * p->tol_eig)) &&
+        } else if (ctx->mixed && (de > 10.0 * sw || (p->tol_eig > 0.0 && deig > 10.0 * sw_eig)) &&
                    reverts < kMaxReverts) {
             ctx->mixed_active = true;
             ++reverts;
@@ -2933,9 +2974,23 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
         // learned mixers: two rises in a row hand the run to Pulay
         const double rnorm = std::sqrt(std::max(0.0, dd[nw]) * dv);
         if (r->residuals) r->residuals[it - 1] = rnorm;
+        rhist.push_back(rnorm);
         if (learned && !fell_back) {
             rises = (r_prev >= 0.0 && rnorm > r_prev) ? rises + 1 : 0;
-            if (rises >= 2) {
+            // a learned run that stalls (the best residual of the last five
+            // iterations is not below half the best before them) is handed
+            // over as well: the network's steps stop helping near convergence
+            bool stalled = false;
+            const int nh = (int)rhist.size();
+            if (nh >= kStallWindow + 5) {
+                const double recent = *std::min_element(rhist.end() - kStallWindow, rhist.end());
+                const double before = *std::min_element(rhist.begin(), rhist.end() - kStallWindow);
+                stalled = recent > 0.5 * before;
+            }
+            if (rises >= 2 || stalled) {
+                if (p->verbose)
+                    std::fprintf(stderr, "scf %3d: learned mixer %s, Pulay from here\n", it,
+                                 rises >= 2 ? "residual rose twice" : "stalled");
                 // Pulay takes over from the current input density with a fresh
                 // history: the learned steps' entries span a subspace that
                 // stalls the extrapolation (observed on the 216-atom cell)

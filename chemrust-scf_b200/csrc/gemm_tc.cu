@@ -11,11 +11,19 @@
 // FP32 level with BF16 tensor-core throughput.
 //
 // Kernel structure (one CTA per 128 x BN output tile and K range):
-//   warp 0 lane 0: TMA producer, 4-stage ring of {A 128x64, B BNx64} bf16
-//                  tiles with 128-byte swizzle, mbarrier complete_tx
-//   warp 1 lane 0: MMA issuer, 4 x tcgen05.mma (M128 x N BN x K16) per
-//                  stage, tcgen05.commit frees the stage
+//   warp 0 lane 0: TMA producer, 3-stage ring; a stage holds all six
+//                  operand tiles of one 32-wide K slice, {A1, A2, A3}
+//                  128x32 and {B1, B2, B3} BNx32 bf16 with 64-byte swizzle,
+//                  one mbarrier complete_tx for the six loads
+//   warp 1 lane 0: MMA issuer, 6 products x 2 tcgen05.mma (M128 x N BN x
+//                  K16) per stage, tcgen05.commit frees the stage; the five
+//                  small products accumulate in a second TMEM accumulator
+//                  (FP32 rounding of each small term against its own sum,
+//                  not against the leading product's)
 //   all 4 warps  : epilogue, tcgen05.ld 32 lanes x 16 columns per step
+// Every plane is loaded once per K slice and feeds the products that use it
+// (A1 and B1 three times, A2 and B2 twice): half the shared-memory fill of
+// one {A, B} pair per product, 60-72 KB per 12 MMAs.
 // Every wait is bounded in time (%globaltimer) and in iterations; on timeout
 // the kernel records the failure in an error word, stops issuing work, waits
 // (again bounded) for the TMA loads and MMAs it has already issued, frees its
@@ -37,8 +45,9 @@ namespace chfsi {
 namespace {
 
 constexpr int kBM = 128;
-constexpr int kBK = 64;          // one 128-byte swizzle atom of bf16
-constexpr int kStages = 4;
+constexpr int kBK = 64;          // K padding and K-split granule (bf16 elements)
+constexpr int kSK = 32;          // K width of one stage: one 64-byte swizzle row of bf16
+constexpr int kStages = 3;
 constexpr int kThreads = 128;
 // hard cap on polls of one wait, whatever the clock says
 constexpr long long kSpinLimit = 1LL << 30;
@@ -99,15 +108,15 @@ __device__ __forceinline__ void tma_load_2d(void* smem_dst, const CUtensorMap* m
         : "memory");
 }
 
-// K-major, 128-byte swizzled operand tile: rows of 64 bf16 (128 B), 8-row
-// groups 1024 B apart (SBO), start address advanced 32 B per K=16 step.
-__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
+// K-major, 64-byte swizzled operand tile: rows of 32 bf16 (64 B), 8-row
+// groups 512 B apart (SBO), start address advanced 32 B per K=16 step.
+__device__ __forceinline__ uint64_t umma_desc_sw64(uint32_t saddr) {
     uint64_t d = 0;
     d |= (uint64_t)((saddr >> 4) & 0x3FFF);
-    d |= (uint64_t)1 << 16;                 // leading byte offset (unused for SW128 K-major)
-    d |= (uint64_t)(1024 >> 4) << 32;        // stride byte offset
+    d |= (uint64_t)1 << 16;                 // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t)(512 >> 4) << 32;         // stride byte offset
     d |= (uint64_t)1 << 46;                  // descriptor version (sm_100)
-    d |= (uint64_t)2 << 61;                  // 128-byte swizzle
+    d |= (uint64_t)4 << 61;                  // 64-byte swizzle
     return d;
 }
 
@@ -157,13 +166,12 @@ k_umma_split3(const __grid_constant__ TcMaps maps, int M2, int N, int bn, int kt
               int ktiles_per_split, void* out, long long ldo, int* err,
               unsigned long long wait_ns, int no_loads) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    // 1024-byte aligned stage ring
+    // 1024-byte aligned stage ring: stage s = [A1 A2 A3 B1 B2 B3]
     unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    const int a_bytes = kBM * kBK * 2;
-    const int b_bytes = bn * kBK * 2;
-    unsigned char* sa = base;
-    unsigned char* sb = base + kStages * a_bytes;
-    uint64_t* full = (uint64_t*)(sb + kStages * b_bytes);
+    const int a_bytes = kBM * kSK * 2;
+    const int b_bytes = bn * kSK * 2;
+    const int stage_bytes = 3 * (a_bytes + b_bytes);
+    uint64_t* full = (uint64_t*)(base + kStages * stage_bytes);
     uint64_t* empty = full + kStages;
     uint64_t* done = empty + kStages;
     uint32_t* tmem_slot = (uint32_t*)(done + 1);
@@ -171,15 +179,22 @@ k_umma_split3(const __grid_constant__ TcMaps maps, int M2, int N, int bn, int kt
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * bn;
+    // K slices of kSK columns: ktiles_* count kBK-wide tiles
     const int kt0 = blockIdx.z * ktiles_per_split;
     const int kt1 = min(ktiles_total, kt0 + ktiles_per_split);
     const int nk = kt1 - kt0;
-    const int iters = 6 * (nk > 0 ? nk : 0);
+    const int iters = (kBK / kSK) * (nk > 0 ? nk : 0);
+    const int ks0 = (kBK / kSK) * kt0;
     // (a plane, b plane) pairs, smallest terms first
     const int pa[6] = {2, 1, 0, 1, 0, 0};
     const int pb[6] = {0, 1, 2, 0, 1, 0};
-    int ncols = 32;
-    while (ncols < bn) ncols <<= 1;
+    // two accumulators of acc_cols TMEM columns each: the five small
+    // products sum in the second, the leading product (1,1) in the first,
+    // so that no small term is rounded against the large running sum; the
+    // epilogue adds the two
+    int acc_cols = 32;
+    while (acc_cols < bn) acc_cols <<= 1;
+    const int ncols = 2 * acc_cols;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; ++s) {
@@ -215,11 +230,15 @@ k_umma_split3(const __grid_constant__ TcMaps maps, int M2, int N, int bn, int kt
                 break;
             }
             if (*(volatile int*)abort_flag) { aborted = true; break; }
-            const int t = it / nk, kk = it - t * nk;
-            const int kx = (kt0 + kk) * kBK;
-            mbar_expect_tx(&full[s], a_bytes + b_bytes);
-            tma_load_2d(sa + s * a_bytes, &maps.a[pa[t]], &full[s], kx, m0);
-            tma_load_2d(sb + s * b_bytes, &maps.b[pb[t]], &full[s], kx, n0);
+            const int kx = (ks0 + it) * kSK;
+            unsigned char* st_base = base + (size_t)s * stage_bytes;
+            mbar_expect_tx(&full[s], stage_bytes);
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+                tma_load_2d(st_base + i * a_bytes, &maps.a[i], &full[s], kx, m0);
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+                tma_load_2d(st_base + 3 * a_bytes + i * b_bytes, &maps.b[i], &full[s], kx, n0);
             ++issued;
         }
         if (aborted) {
@@ -245,11 +264,18 @@ k_umma_split3(const __grid_constant__ TcMaps maps, int M2, int N, int bn, int kt
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint64_t da = umma_desc_sw128(smem_u32(sa + s * a_bytes));
-            const uint64_t db = umma_desc_sw128(smem_u32(sb + s * b_bytes));
+            const uint32_t st_addr = smem_u32(base + (size_t)s * stage_bytes);
 #pragma unroll
-            for (int k = 0; k < kBK / 16; ++k)
-                umma_bf16(tmem, da + 2 * k, db + 2 * k, idesc, (it > 0 || k > 0) ? 1u : 0u);
+            for (int t = 0; t < 6; ++t) {
+                const uint64_t da = umma_desc_sw64(st_addr + pa[t] * a_bytes);
+                const uint64_t db = umma_desc_sw64(st_addr + 3 * a_bytes + pb[t] * b_bytes);
+                const bool lead = t == 5;
+                const uint32_t acc = lead ? tmem : tmem + (uint32_t)acc_cols;
+#pragma unroll
+                for (int k = 0; k < kSK / 16; ++k)
+                    umma_bf16(acc, da + 2 * k, db + 2 * k, idesc,
+                              (it > 0 || (!lead && t > 0) || k > 0) ? 1u : 0u);
+            }
             umma_commit(&empty[s]);
         }
         (void)ok;
@@ -271,7 +297,13 @@ k_umma_split3(const __grid_constant__ TcMaps maps, int M2, int N, int bn, int kt
     for (int c0 = 0; c0 < bn; c0 += 16) {
         uint32_t r[16];
         if (have) {
-            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, r);
+            uint32_t rs[16];
+            const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+            tmem_ld16(ta, r);
+            tmem_ld16(ta + (uint32_t)acc_cols, rs);
+#pragma unroll
+            for (int j = 0; j < 16; ++j)
+                r[j] = __float_as_uint(__uint_as_float(r[j]) + __uint_as_float(rs[j]));
         } else {
 #pragma unroll
             for (int j = 0; j < 16; ++j) r[j] = 0u;
@@ -397,10 +429,10 @@ bool make_map(CUtensorMap* m, const void* ptr, int rows, int kp, int box_rows) {
     if (!enc || rows < box_rows) return false;
     cuuint64_t dims[2] = {(cuuint64_t)kp, (cuuint64_t)rows};
     cuuint64_t strides[1] = {(cuuint64_t)kp * 2};
-    cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)box_rows};
+    cuuint32_t box[2] = {(cuuint32_t)kSK, (cuuint32_t)box_rows};
     cuuint32_t es[2] = {1, 1};
     CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr), dims, strides,
-                     box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                     box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;
 }
@@ -413,7 +445,7 @@ int pick_bn(int n) {
 }
 
 size_t smem_bytes(int bn) {
-    return 1024 + (size_t)kStages * (kBM * kBK * 2 + bn * kBK * 2) + (2 * kStages + 1) * 8 + 16;
+    return 1024 + (size_t)kStages * 3 * (kBM * kSK * 2 + bn * kSK * 2) + (2 * kStages + 1) * 8 + 16;
 }
 
 int grid_for(long long n) {

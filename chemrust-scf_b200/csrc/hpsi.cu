@@ -80,40 +80,85 @@ __device__ __forceinline__ void p2_store_span(C* line, int es, int n1, const C* 
 #pragma unroll
     for (int j = 0; j < R0; ++j) line[swz(n1 + j * R1, R0 * R1) * es] = x[j];
 }
+// Span twiddles in the order the lanes of a group read them:
+// twm[(m - 1) R1 + n1] = w^(n1 m), w = exp(2 pi i / (R0 R1)).  For a fixed m
+// the lanes n1 = 0 .. R1 - 1 read consecutive entries (no bank conflicts;
+// the table w^j indexed by n1 m puts lanes on the same bank group whenever m
+// shares a factor with 8).
+__device__ __forceinline__ double2 tw_entry(const double2* twd, const float2*, int j, double2) {
+    return twd[j];
+}
+__device__ __forceinline__ float2 tw_entry(const double2*, const float2* twf, int j, float2) {
+    return twf[j];
+}
+template <int R0, int R1, typename C>
+__device__ __forceinline__ void p2_twiddles(C* twm, const double2* twd, const float2* twf) {
+    for (int i = threadIdx.x; i < (R0 - 1) * R1; i += blockDim.x) {
+        const int m = i / R1 + 1, n1 = i - (m - 1) * R1;
+        twm[i] = tw_entry(twd, twf, n1 * m, C{});
+    }
+}
+// Lane -> (group, index in group) of the two-radix line transforms with T
+// lanes per line and PW lines per warp.  Indices 0-7 of every group fill
+// whole 8-lane phases (one line per phase), the higher indices follow
+// packed: the 16-byte shared-memory accesses of a phase then fall on one
+// line, whose XOR-swizzled elements span all eight bank groups.
+template <int T, int PW>
+__device__ __forceinline__ void p2_lane(int lane, int& gi, int& li) {
+    if constexpr (T <= 8) {
+        gi = lane / T;
+        li = lane - gi * T;
+    } else {
+        if (lane < PW * 8) {
+            gi = lane >> 3;
+            li = lane & 7;
+        } else {
+            const int r = lane - PW * 8;
+            gi = r / (T - 8);
+            li = 8 + (r - gi * (T - 8));
+        }
+    }
+}
+// Span twiddle w^(n1 m) from the table w^j (TWM false) or from the
+// lane-ordered table of p2_twiddles (TWM true)
+template <int R1, bool TWM, typename C>
+__device__ __forceinline__ C span_tw(const C* tw, int n1, int m) {
+    return TWM ? tw[(m - 1) * R1 + n1] : tw[n1 * m];
+}
 // DIT stage 0 on span n1: twiddle w^(n1 m), radix-R0 DFT (sign +1)
-template <int R0, typename C>
+template <int R0, int R1, bool TWM, typename C>
 __device__ __forceinline__ void p2_span_inverse(C* x, int n1, const C* tw) {
 #pragma unroll
-    for (int m = 1; m < R0; ++m) x[m] = cmul(tw[n1 * m], x[m]);
+    for (int m = 1; m < R0; ++m) x[m] = cmul(span_tw<R1, TWM>(tw, n1, m), x[m]);
     dft_r<R0, 1>(x);
 }
 // DIF stage 0 on span n1: radix-R0 DFT (sign -1), twiddle w^(-n1 m)
-template <int R0, typename C>
+template <int R0, int R1, bool TWM, typename C>
 __device__ __forceinline__ void p2_span_forward(C* x, int n1, const C* tw) {
     dft_r<R0, -1>(x);
 #pragma unroll
-    for (int m = 1; m < R0; ++m) x[m] = cmulc(tw[n1 * m], x[m]);
+    for (int m = 1; m < R0; ++m) x[m] = cmulc(span_tw<R1, TWM>(tw, n1, m), x[m]);
 }
 // whole-line transforms by one lane group (lane i); every lane of the warp
 // calls them (act = false: idle)
-template <int R0, int R1, typename C>
+template <int R0, int R1, bool TWM, typename C>
 __device__ __forceinline__ void p2_line_inverse(C* line, bool act, int i, int es, const C* tw) {
     if (act && i < R0) p2_blocks<R0, R1, 1>(line, es, i);
     __syncwarp();
     if (act && i < R1) {
         C x[R0];
         p2_load_span<R0, R1>(line, es, i, x);
-        p2_span_inverse<R0>(x, i, tw);
+        p2_span_inverse<R0, R1, TWM>(x, i, tw);
         p2_store_span<R0, R1>(line, es, i, x);
     }
     __syncwarp();
 }
-template <int R0, int R1, typename C>
+template <int R0, int R1, bool TWM, typename C>
 __device__ __forceinline__ void p2_line_forward(C* line, bool act, int i, int es, const C* tw) {
     if (act && i < R1) {
         C x[R0];
         p2_load_span<R0, R1>(line, es, i, x);
-        p2_span_forward<R0>(x, i, tw);
+        p2_span_forward<R0, R1, TWM>(x, i, tw);
         p2_store_span<R0, R1>(line, es, i, x);
     }
     __syncwarp();
@@ -135,8 +180,8 @@ __device__ __forceinline__ void zlines_fft(C* lines, int nl, const HGeom& g, con
             const int l = l0 + gid;
             const bool act = ing && l < nl;
             C* line = lines + (act ? l * g.lsz : 0);
-            if (FWD) p2_line_forward<R0, R1>(line, act, li, 1, tw);
-            else p2_line_inverse<R0, R1>(line, act, li, 1, tw);
+            if (FWD) p2_line_forward<R0, R1, false>(line, act, li, 1, tw);
+            else p2_line_inverse<R0, R1, false>(line, act, li, 1, tw);
         }
         __syncthreads();
     } else {
@@ -253,22 +298,24 @@ k_planes_vloc_p2(C* __restrict__ work, const double* __restrict__ veff, HGeom g)
     int* xl = reinterpret_cast<int*>(plane + (size_t)N * LS);
     const int z = blockIdx.x, b = blockIdx.y;
     const int nxact = g.nxact;
-    copy_twiddles(twx, g.twd_x, g.twf_x, N);
-    copy_twiddles(twy, g.twd_y, g.twf_y, N);
+    p2_twiddles<R0, R1, C>(twx, g.twd_x, g.twf_x);
+    p2_twiddles<R0, R1, C>(twy, g.twd_y, g.twf_y);
     for (int i = threadIdx.x; i < nxact; i += blockDim.x) xl[i] = g.xact[i];
     for (int i = threadIdx.x; i < N * LS; i += blockDim.x) plane[i] = czero<C>();
     __syncthreads();
     C* wp = work + ((size_t)b * g.nz + z) * g.ncol;
     for (int c = threadIdx.x; c < g.ncol; c += blockDim.x) plane[g.col_pos[c]] = wp[c];
     __syncthreads();
-    const int lane = threadIdx.x & 31, gi = lane / T, li = lane - gi * T;
+    const int lane = threadIdx.x & 31;
+    int gi, li;
+    p2_lane<T, PW>(lane, gi, li);
     const bool ing = gi < PW;
     const int groups = (blockDim.x >> 5) * PW, gid = (threadIdx.x >> 5) * PW + gi;
     // y lines through the active x positions
     for (int l0 = 0; l0 < nxact; l0 += groups) {
         const int l = l0 + gid;
         const bool act = ing && l < nxact;
-        p2_line_inverse<R0, R1>(plane + (act ? xl[l] : 0), act, li, LS, twy);
+        p2_line_inverse<R0, R1, true>(plane + (act ? xl[l] : 0), act, li, LS, twy);
     }
     __syncthreads();
     // x rows: inverse, x V(r), forward
@@ -283,11 +330,11 @@ k_planes_vloc_p2(C* __restrict__ work, const double* __restrict__ veff, HGeom g)
         if (act && li < R1) {
             C x[R0];
             p2_load_span<R0, R1>(row, 1, li, x);
-            p2_span_inverse<R0>(x, li, twx);
+            p2_span_inverse<R0, R1, true>(x, li, twx);
             const double* vr = vz + (size_t)y * N + li;
 #pragma unroll
             for (int m = 0; m < R0; ++m) x[m] = cscale(x[m], (R)vr[m * R1]);
-            p2_span_forward<R0>(x, li, twx);
+            p2_span_forward<R0, R1, true>(x, li, twx);
             p2_store_span<R0, R1>(row, 1, li, x);
         }
         __syncwarp();
@@ -298,7 +345,7 @@ k_planes_vloc_p2(C* __restrict__ work, const double* __restrict__ veff, HGeom g)
     for (int l0 = 0; l0 < nxact; l0 += groups) {
         const int l = l0 + gid;
         const bool act = ing && l < nxact;
-        p2_line_forward<R0, R1>(plane + (act ? xl[l] : 0), act, li, LS, twy);
+        p2_line_forward<R0, R1, true>(plane + (act ? xl[l] : 0), act, li, LS, twy);
     }
     __syncthreads();
     for (int c = threadIdx.x; c < g.ncol; c += blockDim.x) wp[c] = plane[g.col_pos[c]];
@@ -325,12 +372,14 @@ k_planes_vloc_p3(C* __restrict__ work, const double* __restrict__ veff, HGeom g)
     int* xl = reinterpret_cast<int*>(plane + (size_t)N * LS);
     const int z = blockIdx.x, b = blockIdx.y;
     const int nxact = g.nxact;
-    copy_twiddles(twx, g.twd_x, g.twf_x, N);
-    copy_twiddles(twy, g.twd_y, g.twf_y, N);
+    p2_twiddles<R0, R1, C>(twx, g.twd_x, g.twf_x);
+    p2_twiddles<R0, R1, C>(twy, g.twd_y, g.twf_y);
     for (int i = threadIdx.x; i < nxact; i += blockDim.x) xl[i] = g.xact[i];
     __syncthreads();
     C* wp = work + ((size_t)b * g.nz + z) * g.ncol;
-    const int lane = threadIdx.x & 31, gi = lane / T, li = lane - gi * T;
+    const int lane = threadIdx.x & 31;
+    int gi, li;
+    p2_lane<T, PW>(lane, gi, li);
     const bool ing = gi < PW;
     const int groups = (blockDim.x >> 5) * PW, gid = (threadIdx.x >> 5) * PW + gi;
     using R = typename RealOf<C>::type;
@@ -355,7 +404,7 @@ k_planes_vloc_p3(C* __restrict__ work, const double* __restrict__ veff, HGeom g)
         if (act && li < R1) {
             C x[R0];
             p2_load_span<R0, R1>(line, LS, li, x);
-            p2_span_inverse<R0>(x, li, twy);
+            p2_span_inverse<R0, R1, true>(x, li, twy);
             p2_store_span<R0, R1>(line, LS, li, x);
         }
         __syncwarp();
@@ -384,11 +433,11 @@ k_planes_vloc_p3(C* __restrict__ work, const double* __restrict__ veff, HGeom g)
         if (act && li < R1) {
             C x[R0];
             p2_load_span<R0, R1>(row, 1, li, x);
-            p2_span_inverse<R0>(x, li, twx);
+            p2_span_inverse<R0, R1, true>(x, li, twx);
             const double* vr = vz + (size_t)y * N + li;
 #pragma unroll
             for (int m = 0; m < R0; ++m) x[m] = cscale(x[m], (R)vr[m * R1]);
-            p2_span_forward<R0>(x, li, twx);
+            p2_span_forward<R0, R1, true>(x, li, twx);
             p2_store_span<R0, R1>(row, 1, li, x);
         }
         __syncwarp();
@@ -414,7 +463,7 @@ k_planes_vloc_p3(C* __restrict__ work, const double* __restrict__ veff, HGeom g)
         if (act && li < R1) {
             C x[R0];
             p2_load_span<R0, R1>(line, LS, li, x);
-            p2_span_forward<R0>(x, li, twy);
+            p2_span_forward<R0, R1, true>(x, li, twy);
             p2_store_span<R0, R1>(line, LS, li, x);
         }
         __syncwarp();

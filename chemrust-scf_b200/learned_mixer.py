@@ -36,15 +36,29 @@ CELL_KINDS = [(0, 1, 8), (2, 2, 2), (1, 3, 1), (0, 2, 8), (0, 3, 8)]
 VOLUME_PER_ATOM = 10.26 ** 3 / 8.0  # the 8-atom diamond cell's density
 
 
-def cell_params(seed, kinds=(0, 1, 2, 3), weights=(0.4, 0.3, 0.2, 0.1), jitter=0.3, ecut=15.0):
-    """Seeded random cell: 8-64 atoms, Z in {1..6}, fixed atomic density."""
+# dilute cells: 64 atoms at 1.5-3.375x the volume per atom (edges of 23.5 to
+# 30.78 bohr, the 216-atom cell's), so that the lowest |G| shells of the large
+# cells (shells 8 and 9) occur in training
+DILUTE_RANGE = (1.5, 3.375)
+DILUTE_KIND = 3
+
+
+def cell_params(seed, kinds=(0, 1, 2, 3), weights=(0.4, 0.3, 0.2, 0.1), jitter=0.3, ecut=15.0,
+                dilute_frac=0.0):
+    """Seeded random cell: 8-64 atoms, Z in {1..6}, the 8-atom diamond cell's
+    atomic density, or with probability dilute_frac a 64-atom cell with a
+    volume per atom DILUTE_RANGE times larger."""
     rng = np.random.default_rng(seed)
     k = kinds[rng.choice(len(kinds), p=np.asarray(weights) / np.sum(weights))]
+    vol = VOLUME_PER_ATOM
+    if dilute_frac > 0.0 and rng.uniform() < dilute_frac:
+        k = DILUTE_KIND
+        vol *= rng.uniform(*DILUTE_RANGE)
     lattice, n_rep, per_conv = CELL_KINDS[k]
     p = chfsi.SynthParams()
     chfsi._check(chfsi.lib().chfsi_synth_defaults(0, chfsi.C.byref(p)))
     p.lattice, p.n_rep = lattice, n_rep
-    p.a_conv = (per_conv * VOLUME_PER_ATOM) ** (1.0 / 3.0)
+    p.a_conv = (per_conv * vol) ** (1.0 / 3.0)
     p.jitter = jitter
     p.z_val = float(rng.integers(1, 7))
     p.ecut = ecut
@@ -55,11 +69,11 @@ def cell_params(seed, kinds=(0, 1, 2, 3), weights=(0.4, 0.3, 0.2, 0.1), jitter=0
     return p
 
 
-def trajectories(seed, ndeg=12, max_iter=60, tol=1e-8):
+def trajectories(seed, ndeg=12, max_iter=60, tol=1e-8, dilute_frac=0.0):
     """Two trajectories of one cell: Pulay with a random alpha (also gives the
     converged density rho*) and linear mixing with a random alpha."""
     rng = np.random.default_rng(seed + 1_000_003)
-    s = chfsi.SyntheticSystem(cell_params(seed))
+    s = chfsi.SyntheticSystem(cell_params(seed, dilute_frac=dilute_frac))
     ctx = chfsi.Context(s)
     r = ctx.run_scf(ndeg, tol_per_atom=tol, max_iter=max_iter, kT=0.01,
                     alpha=float(rng.uniform(0.1, 0.5)), trace=True)
@@ -74,11 +88,11 @@ def trajectories(seed, ndeg=12, max_iter=60, tol=1e-8):
     return s, ctx, [(a, b, star) for a, b in out]
 
 
-def on_policy_samples(mixer, seed, ndeg=12, max_iter=60, tol=1e-8):
+def on_policy_samples(mixer, seed, ndeg=12, max_iter=60, tol=1e-8, dilute_frac=0.0):
     """Samples from the network's own trajectories (learned-preconditioned
     Pulay and pure learned mixing), so that training sees the states the
     network itself produces."""
-    s = chfsi.SyntheticSystem(cell_params(seed))
+    s = chfsi.SyntheticSystem(cell_params(seed, dilute_frac=dilute_frac))
     out = []
     for mode in (chfsi.MIXER_LEARNED_PULAY, chfsi.MIXER_LEARNED):
         ctx = chfsi.Context(s)
@@ -89,11 +103,11 @@ def on_policy_samples(mixer, seed, ndeg=12, max_iter=60, tol=1e-8):
     return out
 
 
-def dataset(seeds, log=print):
+def dataset(seeds, log=print, dilute_frac=0.0):
     X, T = [], []
     t0 = time.time()
     for i, sd in enumerate(seeds):
-        s, ctx, trs = trajectories(sd)
+        s, ctx, trs = trajectories(sd, dilute_frac=dilute_frac)
         for rin, rout, star in trs:
             x, t = ctx.mixer_samples(rin, rout, star)
             X.append(x)
@@ -114,13 +128,13 @@ def load(path=WEIGHTS, device=0):
 
 
 def train(n_cells=300, epochs=150, batch=256, lr=1e-3, seed=0, out=WEIGHTS, dagger_cells=0,
-          log=print):
+          log=print, dilute_frac=0.0):
     """Off-policy data (Pulay and linear-mixing trajectories), Adam at lr then
     lr/10; optionally one on-policy round on dagger_cells further cells."""
     seeds = list(range(10_000 + seed, 10_000 + seed + n_cells))
     log("generating trajectories on %d cells" % n_cells)
     t0 = time.time()
-    X, T = dataset(seeds, log)
+    X, T = dataset(seeds, log, dilute_frac)
     gen_s = time.time() - t0
     log("%d samples; training" % len(X))
     m = chfsi.Mixer(seed=seed)
@@ -129,14 +143,15 @@ def train(n_cells=300, epochs=150, batch=256, lr=1e-3, seed=0, out=WEIGHTS, dagg
     l2 = m.train(X, T, epochs=max(1, epochs // 2), batch=batch, lr=lr * 0.1, seed=seed + 1)
     train_s = time.time() - t0
     log("loss %.4f -> %.4f -> %.4f in %.1f s" % (l1[0], l1[-1], l2[-1], train_s))
-    meta = {"cells": n_cells, "samples": int(len(X)), "epochs": epochs, "batch": batch, "lr": lr,
+    meta = {"cells": n_cells, "dilute_frac": dilute_frac, "samples": int(len(X)), "epochs": epochs,
+            "batch": batch, "lr": lr,
             "loss_first": float(l1[0]), "loss_last": float(l2[-1]),
             "generate_seconds": gen_s, "train_seconds": train_s}
     if dagger_cells:
         t0 = time.time()
         Xd, Td = [], []
         for sd in range(50_000 + seed, 50_000 + seed + dagger_cells):
-            for x, t in on_policy_samples(m, sd):
+            for x, t in on_policy_samples(m, sd, dilute_frac=dilute_frac):
                 Xd.append(x)
                 Td.append(t)
         X = np.concatenate([X] + Xd)
@@ -185,6 +200,8 @@ def main():
     a.add_argument("--seed", type=int, default=0)
     a.add_argument("--out", default=WEIGHTS)
     a.add_argument("--dagger-cells", type=int, default=0)
+    a.add_argument("--dilute-frac", type=float, default=0.0,
+                   help="share of training cells with a larger volume per atom")
     b = sub.add_parser("evaluate")
     b.add_argument("--weights", default=WEIGHTS)
     b.add_argument("--cells", type=int, default=8)
@@ -193,7 +210,8 @@ def main():
     b.add_argument("--kinds", default="0,1,2,3", help="cell kinds (4 = 216 atoms)")
     args = ap.parse_args()
     if args.cmd == "train":
-        train(args.cells, args.epochs, args.batch, args.lr, args.seed, args.out, args.dagger_cells)
+        train(args.cells, args.epochs, args.batch, args.lr, args.seed, args.out, args.dagger_cells,
+              dilute_frac=args.dilute_frac)
     else:
         m = load(args.weights)
         kinds = tuple(int(k) for k in args.kinds.split(","))

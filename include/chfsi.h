@@ -362,8 +362,12 @@ typedef struct chfsi_scf_params {
                              (f > 0.01) to change by less than this (Ha) from the
                              previous iteration; mixed runs switch to FP64 only after
                              two mixed iterations with |dE| below the switch and
-                             eigenvalue changes below 2 x tol_eig; an FP64 iteration
-                             with changes above 10 x tol_eig returns to mixed         */
+                             eigenvalue changes below the eigenvalue switch; an FP64
+                             iteration with changes above 10 x that switch returns
+                             to mixed                                                 */
+    double fp64_switch_eig; /* eigenvalue switch of mixed runs: max(this, 2 x tol_eig)
+                               (the mixed iterations' eigenvalue changes carry FP32
+                               noise of ~2e-7 Ha on the 216-atom cell)               */
 } chfsi_scf_params;
 
 /* Density mixers of chfsi_scf_run.  PULAY: Pulay/DIIS over (rho_in,
@@ -373,7 +377,9 @@ typedef struct chfsi_scf_params {
  * LEARNED_PULAY: Pulay extrapolation with the MLP's a_s as per-shell
  * preconditioner in place of alpha.  Both learned modes fall back to plain
  * Pulay for the rest of the run once the residual norm rises two steps in a
- * row (the Pulay history is kept up to date throughout). */
+ * row, once the smallest residual of the last five iterations is not below
+ * half the smallest before them (a stall), or once the network's output is
+ * not finite; Pulay then starts a fresh history from the current density. */
 #define CHFSI_MIXER_PULAY 0
 #define CHFSI_MIXER_LEARNED 1
 #define CHFSI_MIXER_LEARNED_PULAY 2

@@ -102,3 +102,23 @@ def test_non_finite_learned_mixer_falls_back_to_pulay(chfsi):
     plain = chfsi.Context(s).run_scf(12, tol_per_atom=1e-6, max_iter=40, kT=0.01)
     # after the first (fallen-back) step the run is plain Pulay
     assert abs(r["e_total"] - plain["e_total"]) / s.n_atoms < 1e-6
+
+
+def test_stalled_learned_mixer_hands_over_to_pulay(chfsi):
+    # a network with all weights zero outputs a_s = b_s = 0: the learned
+    # steps leave the density where it is, the residual stops falling, and
+    # the stall rule (or the rise rule) hands the run to Pulay
+    s = chfsi.SyntheticSystem(config_index=0)
+    m = chfsi.Mixer(device=0, seed=1)
+    p = m.get_params()
+    p[:] = 0.0
+    m.set_params(p)
+    ctx = chfsi.Context(s)
+    ctx.set_mixer(m)
+    r = ctx.run_scf(12, tol_per_atom=1e-6, max_iter=60, kT=0.01,
+                    mixer=chfsi.MIXER_LEARNED_PULAY)
+    assert r["fell_back"]
+    assert r["converged"]
+    assert r["n_iter_learned"] <= 12
+    plain = chfsi.Context(s).run_scf(12, tol_per_atom=1e-6, max_iter=60, kT=0.01)
+    assert abs(r["e_total"] - plain["e_total"]) / s.n_atoms < 1e-6
