@@ -45,9 +45,9 @@ CONFIG_INDEX = 1
 METRIC = "H|psi> band-applies/s (ChFSI iteration: degree-16 Chebyshev filter + Rayleigh-Ritz)"
 UNIT = "band-applies/s"
 # DRAM bytes (read + write) per band of one local H|psi> launch (the three
-# FFT-pass kernels, 160 bands: 1,148,613,376 bytes), from the ncu capture
-# summarised in profiles/local_hpsi_cfg1_traffic.md
-TRAFFIC_PER_BAND = 1148613376 / 160
+# FFT-pass kernels, 160 bands: 1,151,111,424 bytes), from an ncu capture of
+# dram__bytes_read.sum + dram__bytes_write.sum of those kernels
+TRAFFIC_PER_BAND = 1151111424 / 160
 
 
 def peaks():

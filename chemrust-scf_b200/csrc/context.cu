@@ -2750,7 +2750,7 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
     int rises = 0;
     bool restart_pulay = false;
     double r_prev = -1.0;
-    constexpr int kStallWindow = 5;
+    constexpr int kStallWindow = 10;
     std::vector<double> rhist;
     std::vector<double> eig(ctx->nb), eig_prev(ctx->nb);
     bool have_eig = restart;
@@ -2977,12 +2977,12 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
         rhist.push_back(rnorm);
         if (learned && !fell_back) {
             rises = (r_prev >= 0.0 && rnorm > r_prev) ? rises + 1 : 0;
-            // a learned run that stalls (the best residual of the last five
+            // a learned run that stalls (the best residual of the last ten
             // iterations is not below half the best before them) is handed
             // over as well: the network's steps stop helping near convergence
             bool stalled = false;
             const int nh = (int)rhist.size();
-            if (nh >= kStallWindow + 5) {
+            if (nh >= kStallWindow + 3) {
                 const double recent = *std::min_element(rhist.end() - kStallWindow, rhist.end());
                 const double before = *std::min_element(rhist.begin(), rhist.end() - kStallWindow);
                 stalled = recent > 0.5 * before;

@@ -377,7 +377,7 @@ typedef struct chfsi_scf_params {
  * LEARNED_PULAY: Pulay extrapolation with the MLP's a_s as per-shell
  * preconditioner in place of alpha.  Both learned modes fall back to plain
  * Pulay for the rest of the run once the residual norm rises two steps in a
- * row, once the smallest residual of the last five iterations is not below
+ * row, once the smallest residual of the last ten iterations is not below
  * half the smallest before them (a stall), or once the network's output is
  * not finite; Pulay then starts a fresh history from the current density. */
 #define CHFSI_MIXER_PULAY 0
