@@ -179,6 +179,10 @@ def lib():
         "chfsi_get_stream": [vp, C.POINTER(vp)],
         "chfsi_zgemm_cn": [vp, C.c_int, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp],
         "chfsi_zgemm_cn_bf16x3": [vp, C.c_int, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp],
+        "chfsi_zgemm_cn_bf16x3_shape": [vp, C.c_int, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp,
+                                        vp, C.c_int],
+        "chfsi_get_tc_shapes": [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)],
+        "chfsi_set_tc_shapes": [vp, C.c_int, C.c_int],
         "chfsi_zgemm_cn_noalloc": [vp, C.c_int, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp],
         "chfsi_chebyshev_filter": [vp, C.c_int, dp, C.c_int],
         "chfsi_rayleigh_ritz": [vp, dp],
@@ -364,10 +368,19 @@ def hegv_dev(h_dev, s_dev, n, v_dev, stream=0):
     return w
 
 
-def zgemm_cn_bf16x3(a_dev, lda, b_dev, ldb, m, n, k, c_dev, stream=0):
-    """Same product on tcgen05 tensor cores, BF16 3-way split, FP32 accumulation."""
-    _check(lib().chfsi_zgemm_cn_bf16x3(C.c_void_p(a_dev), lda, C.c_void_p(b_dev), ldb, m, n, k,
-                                       C.c_void_p(c_dev), C.c_void_p(stream)))
+TC_SHAPES = 3
+
+
+def zgemm_cn_bf16x3(a_dev, lda, b_dev, ldb, m, n, k, c_dev, stream=0, shape=None):
+    """Same product on tcgen05 tensor cores, BF16 3-way split, FP32 accumulation;
+    shape (0..TC_SHAPES-1) picks the kernel's launch shape."""
+    if shape is None:
+        _check(lib().chfsi_zgemm_cn_bf16x3(C.c_void_p(a_dev), lda, C.c_void_p(b_dev), ldb, m, n,
+                                           k, C.c_void_p(c_dev), C.c_void_p(stream)))
+    else:
+        _check(lib().chfsi_zgemm_cn_bf16x3_shape(C.c_void_p(a_dev), lda, C.c_void_p(b_dev), ldb,
+                                                 m, n, k, C.c_void_p(c_dev), C.c_void_p(stream),
+                                                 shape))
 
 
 def inject_fault(what, arg=0):
@@ -769,6 +782,15 @@ class Context:
 
     def set_launch_config(self, choice):
         self._c(lib().chfsi_set_launch_config(self.handle, choice))
+
+    def tc_shapes(self):
+        """Launch shapes of the projection and expansion tcgen05 GEMMs (-1: not tuned yet)."""
+        a, b = C.c_int(), C.c_int()
+        self._c(lib().chfsi_get_tc_shapes(self.handle, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def set_tc_shapes(self, projection, expansion):
+        self._c(lib().chfsi_set_tc_shapes(self.handle, projection, expansion))
 
     def band_cg(self, max_steps, tol=1e-10):
         """Band-by-band CG refinement; returns (band energies, steps, n_converged)."""

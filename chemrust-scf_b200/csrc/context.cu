@@ -22,6 +22,9 @@
 #include "system.hpp"
 
 #include <algorithm>
+#include <array>
+#include <map>
+#include <mutex>
 #include <atomic>
 #include <cmath>
 #include <complex>
@@ -501,6 +504,9 @@ struct chfsi_ctx {
     TcPlanes tp_beta_a, tp_betaT_b, tp_psi_b, tp_small_a;
     float* d_tc_part = nullptr; int* d_tc_err = nullptr;
     bool beta_planes_ready = false;
+    // tcgen05 launch shapes of the projection and the expansion (-1: time
+    // them at the first mixed filter)
+    int tc_shape[2] = {-1, -1};
     bool last_pass_fp32 = false;  // the last filter ran in FP32
     int last_sweeps = 0;          // Jacobi sweeps of the last Rayleigh-Ritz
     // density grid: density, potentials, mixing and augmentation live here.
@@ -899,6 +905,97 @@ chfsi_status alloc_mixed(chfsi_ctx* ctx, int ncol) {
     return CHFSI_OK;
 }
 
+static_assert(CHFSI_TC_SHAPES == kTcVariantCount, "tcgen05 shape count");
+
+// The context's launch shape of the projection (which 0) or the expansion
+// (which 1) tcgen05 GEMM; shape 0 until the autotuner has run.
+int tc_shape(const chfsi_ctx* ctx, int which) {
+    return ctx->tc_shape[which] < 0 ? 0 : ctx->tc_shape[which];
+}
+
+// Autotuner of the projector GEMMs: every launch shape of the tcgen05 kernel
+// on this context's projection (n_proj x n_b x n_pw) and expansion
+// (n_b x n_pw x n_proj), one warm-up and two timed launches each (CUDA events
+// on the context stream); the fastest is kept.  The operands are the packed
+// projector planes and whatever the band planes hold (the timing does not
+// depend on values); the outputs land in scratch the filter overwrites.
+// Skipped while the stream is being captured (shape 0 then).
+// Choices are kept per device and size class (which GEMM, M, N, K), so every
+// context of one size uses the same shape and gives the same numbers.
+std::mutex g_tc_shape_mu;
+std::map<std::array<int, 5>, int> g_tc_shape_cache;
+
+chfsi_status tune_tc_shapes(chfsi_ctx* ctx) {
+    if (ctx->tc_shape[0] >= 0 && ctx->tc_shape[1] >= 0) return CHFSI_OK;
+    const int np = ctx->np, nb = ctx->nb, npw = ctx->n_pw;
+    const std::array<int, 5> key[2] = {{ctx->device, 0, np, nb, npw}, {ctx->device, 1, nb, npw, np}};
+    {
+        std::lock_guard<std::mutex> lk(g_tc_shape_mu);
+        for (int which = 0; which < 2; ++which) {
+            auto it = g_tc_shape_cache.find(key[which]);
+            if (ctx->tc_shape[which] < 0 && it != g_tc_shape_cache.end())
+                ctx->tc_shape[which] = it->second;
+        }
+    }
+    if (ctx->tc_shape[0] >= 0 && ctx->tc_shape[1] >= 0) return CHFSI_OK;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(ctx->st, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return CHFSI_OK;
+    cudaStream_t st = ctx->st;
+    // band-side operands as the filter packs them (their planes may not have
+    // been packed yet: zero-filled planes of the right shape time the same)
+    TcPlanes psi_b = ctx->tp_psi_b, small_a = ctx->tp_small_a;
+    psi_b.rows = nb;
+    psi_b.kp = tc_kpad(npw);
+    small_a.rows = 2 * nb;
+    small_a.kp = tc_kpad(np);
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    cudaError_t e = cudaSuccess;
+    int tuned[2] = {ctx->tc_shape[0], ctx->tc_shape[1]};
+    for (int which = 0; which < 2 && e == cudaSuccess; ++which) {
+        if (tuned[which] >= 0) continue;
+        float best = 1e30f;
+        int best_v = 0;
+        for (int v = 0; v < kTcVariantCount && e == cudaSuccess; ++v) {
+            auto run = [&]() {
+                return which == 0
+                           ? tc_gemm(ctx->tp_beta_a, psi_b, np, nb, npw, kTcOutPartial,
+                                     ctx->d_cp, nb, ctx->d_tc_part, ctx->d_tc_err, st, v)
+                           : tc_gemm(small_a, ctx->tp_betaT_b, nb, npw, np,
+                                     kTcOutComplexF32, ctx->d_nl32, npw, nullptr, ctx->d_tc_err,
+                                     st, v);
+            };
+            e = run();
+            if (e == cudaSuccess) e = cudaEventRecord(e0, st);
+            for (int r = 0; r < 2 && e == cudaSuccess; ++r) e = run();
+            if (e == cudaSuccess) e = cudaEventRecord(e1, st);
+            if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+            float ms = 0.f;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+            if (e == cudaSuccess && ms < best) { best = ms; best_v = v; }
+        }
+        tuned[which] = best_v;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    CK(e);
+    int herr = 0;
+    CK(copy_sync(&herr, ctx->d_tc_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (herr) {
+        // a timed-out launch makes the timings meaningless: tune again later
+        CK(cudaMemsetAsync(ctx->d_tc_err, 0, 4 * sizeof(int), st));
+        return ctx->fail(CHFSI_ERR_TIMEOUT, "tensor-core GEMM pipeline wait timed out");
+    }
+    std::lock_guard<std::mutex> lk(g_tc_shape_mu);
+    for (int which = 0; which < 2; ++which) {
+        ctx->tc_shape[which] = tuned[which];
+        g_tc_shape_cache.emplace(key[which], tuned[which]);
+    }
+    return CHFSI_OK;
+}
+
 chfsi_status pack_beta_planes(chfsi_ctx* ctx) {
     if (!ctx->mixed || ctx->np == 0) return CHFSI_OK;
     // beta^H psi: A operand = beta rows (doubled); back-projection: B operand = beta^T
@@ -906,7 +1003,7 @@ chfsi_status pack_beta_planes(chfsi_ctx* ctx) {
     tc_pack<double2>(ctx->d_beta, ctx->n_pw, ctx->n_pw, ctx->np, false, kSrcT, ctx->tp_betaT_b, ctx->st);
     CK(cudaGetLastError());
     ctx->beta_planes_ready = true;
-    return CHFSI_OK;
+    return tune_tc_shapes(ctx);
 }
 
 chfsi_status apply_h_dev32(chfsi_ctx* ctx, const float2* psi, float2* out, int nb, int mode,
@@ -925,13 +1022,13 @@ chfsi_status apply_h_dev32(chfsi_ctx* ctx, const float2* psi, float2* out, int n
         // C = beta^H psi (tcgen05), C <- D C (FP64), nl = beta C (tcgen05, FP32 out)
         tc_pack<float2>(psi, ctx->n_pw, nb, ctx->n_pw, false, kSrcPlain, ctx->tp_psi_b, st);
         CK(tc_gemm(ctx->tp_beta_a, ctx->tp_psi_b, ctx->np, nb, ctx->n_pw, kTcOutPartial, ctx->d_cp,
-                   nb, ctx->d_tc_part, ctx->d_tc_err, st));
+                   nb, ctx->d_tc_part, ctx->d_tc_err, st, tc_shape(ctx, 0)));
         count_launch();
         k_apply_dmat<<<grid_for((size_t)ctx->np * nb), 256, 0, st>>>(
             ctx->d_cp, ctx->d_cd, ctx->np, nb, ctx->d_proj_ion, ctx->d_poff, ctx->d_doff, ctx->d_dmat);
         tc_pack<double2>(ctx->d_cd, nb, nb, ctx->np, true, kSrcConjT, ctx->tp_small_a, st);
         CK(tc_gemm(ctx->tp_small_a, ctx->tp_betaT_b, nb, ctx->n_pw, ctx->np, kTcOutComplexF32,
-                   ctx->d_nl32, ctx->n_pw, nullptr, ctx->d_tc_err, st));
+                   ctx->d_nl32, ctx->n_pw, nullptr, ctx->d_tc_err, st, tc_shape(ctx, 1)));
         e.nl = ctx->d_nl32;
     }
     launch_zsticks_inverse<float2>(psi, ctx->n_pw, ctx->d_work32, nb, ctx->geo, st);
@@ -950,7 +1047,7 @@ chfsi_status sinv_h_parts32(chfsi_ctx* ctx, const float2* x, int nb) {
     const int np = ctx->np, npw = ctx->n_pw;
     tc_pack<float2>(x, npw, nb, npw, false, kSrcPlain, ctx->tp_psi_b, st);
     CK(tc_gemm(ctx->tp_beta_a, ctx->tp_psi_b, np, nb, npw, kTcOutPartial, ctx->d_cp, nb,
-               ctx->d_tc_part, ctx->d_tc_err, st));
+               ctx->d_tc_part, ctx->d_tc_err, st, tc_shape(ctx, 0)));
     count_launch();
     k_apply_dmat<<<grid_for((size_t)np * nb), 256, 0, st>>>(
         ctx->d_cp, ctx->d_cd, np, nb, ctx->d_proj_ion, ctx->d_poff, ctx->d_doff, ctx->d_dmat);
@@ -958,14 +1055,14 @@ chfsi_status sinv_h_parts32(chfsi_ctx* ctx, const float2* x, int nb) {
     if (s) return s;
     tc_pack<float2>(ctx->d_hpsi32, npw, nb, npw, false, kSrcPlain, ctx->tp_psi_b, st);
     CK(tc_gemm(ctx->tp_beta_a, ctx->tp_psi_b, np, nb, npw, kTcOutPartial, ctx->d_cp, nb,
-               ctx->d_tc_part, ctx->d_tc_err, st));
+               ctx->d_tc_part, ctx->d_tc_err, st, tc_shape(ctx, 0)));
     gemm_tn(ctx->d_bmatT, np, ctx->d_cd, nb, ctx->d_cp, nb, np, nb, np, 1.0, 1.0, st);
     CK(cudaMemcpyAsync(ctx->d_cq, ctx->d_cd, sizeof(double2) * (size_t)np * nb,
                        cudaMemcpyDeviceToDevice, st));
     gemm_tn(ctx->d_sinvT, np, ctx->d_cp, nb, ctx->d_cq, nb, np, nb, np, 1.0, -1.0, st);
     tc_pack<double2>(ctx->d_cq, nb, nb, np, true, kSrcConjT, ctx->tp_small_a, st);
     CK(tc_gemm(ctx->tp_small_a, ctx->tp_betaT_b, nb, npw, np, kTcOutComplexF32, ctx->d_nl32, npw,
-               nullptr, ctx->d_tc_err, st));
+               nullptr, ctx->d_tc_err, st, tc_shape(ctx, 1)));
     CK(cudaGetLastError());
     return CHFSI_OK;
 }
@@ -989,8 +1086,9 @@ chfsi_status apply_op_dev32(chfsi_ctx* ctx, const float2* x, float2* out, int nb
 
 chfsi_status filter_dev32(chfsi_ctx* ctx, int ndeg, const double* eig_dev, int n_eig) {
     if (ndeg < 0 || ndeg > ctx->max_deg) return ctx->fail(CHFSI_ERR_BAD_INPUT, "ndeg out of range");
-    if (ctx->np > 0 && !ctx->beta_planes_ready) {
-        chfsi_status s = pack_beta_planes(ctx);
+    if (ctx->np > 0) {
+        chfsi_status s = ctx->beta_planes_ready ? CHFSI_OK : pack_beta_planes(ctx);
+        if (!s) s = tune_tc_shapes(ctx);
         if (s) return s;
     }
     chfsi_status s = compute_bounds(ctx, eig_dev, n_eig);
@@ -1096,6 +1194,7 @@ chfsi_status filter_rchfsi(chfsi_ctx* ctx, int ndeg, const double* eig_dev, int 
     chfsi_status s = alloc_rchfsi(ctx, fp32);
     if (s) return s;
     if (fp32 && np > 0 && !ctx->beta_planes_ready && (s = pack_beta_planes(ctx))) return s;
+    if (fp32 && np > 0 && (s = tune_tc_shapes(ctx))) return s;
     if ((s = compute_bounds(ctx, eig_dev, n_eig))) return s;
     cudaStream_t st = ctx->st;
     const size_t n = (size_t)nb * npw;
@@ -1171,9 +1270,14 @@ chfsi_status filter_rchfsi(chfsi_ctx* ctx, int ndeg, const double* eig_dev, int 
 // cut at lambda_max / 3, where the deepest states grow by ~1e9 over degree
 // 16 relative to the cut: FP32 rounding of the weakly amplified top bands
 // would swamp them, so such passes always run in FP64.
+// The residual form runs the FP32 passes of a mixed-precision context (where
+// it keeps the filtered block's error proportional to the Ritz residuals) and
+// every pass of an FP64 context; the FP64 passes of a mixed context (the
+// passes that confirm convergence) run the reference's Chebyshev filter.
 chfsi_status filter_any(chfsi_ctx* ctx, int ndeg, const double* eig_dev, int n_eig) {
     ctx->last_pass_fp32 = ctx->mixed_active && eig_dev != nullptr && n_eig > 0;
-    if (ctx->cfg.filter_form == CHFSI_FILTER_RESIDUAL && eig_dev && n_eig == ctx->nb && ndeg >= 1) {
+    if (ctx->cfg.filter_form == CHFSI_FILTER_RESIDUAL && (ctx->last_pass_fp32 || !ctx->mixed) &&
+        eig_dev && n_eig == ctx->nb && ndeg >= 1) {
         ctx->d_psi32 = nullptr;  // the Rayleigh-Ritz gets the full H psi in FP64
         return filter_rchfsi(ctx, ndeg, eig_dev, n_eig, ctx->last_pass_fp32);
     }
@@ -2920,7 +3024,11 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
         // the switch threshold (a single one falls below it by chance where
         // the energy turns); an FP64 iteration whose |dE| is still ten times
         // above it hands the run back to mixed precision (at most kMaxReverts
-        // times, so the two can never alternate for ever)
+        // times, so the two can never alternate for ever).  Eigenvalue changes
+        // do not hand a run back: the first FP64 iterations move the
+        // eigenvalues by up to ~1e-4 Ha while the density relaxes from the
+        // mixed-precision iterate (its FP32 rounding, ~1e-7 relative in the
+        // density, shifts V_eff), which is the work the FP64 iterations do.
         const double sw = std::max(p->fp64_switch_per_atom, p->tol_per_atom);
         if (ctx->mixed_active) {
             low_mixed = de < sw && eig_near ? low_mixed + 1 : 0;
@@ -2928,7 +3036,7 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
                 ctx->mixed_active = false;
                 low_mixed = 0;
             }
-        } else if (ctx->mixed && (de > 10.0 * sw || (p->tol_eig > 0.0 && deig > 10.0 * sw_eig)) &&
+        } else if (ctx->mixed && de > 10.0 * sw &&
                    reverts < kMaxReverts) {
             ctx->mixed_active = true;
             ++reverts;
@@ -3466,6 +3574,24 @@ extern "C" chfsi_status chfsi_autotune(chfsi_ctx* ctx, int* choice, float* times
     return CHFSI_OK;
 }
 
+extern "C" chfsi_status chfsi_get_tc_shapes(chfsi_ctx* ctx, int* projection, int* expansion) {
+    if (!ctx || !projection || !expansion) return CHFSI_ERR_BAD_INPUT;
+    *projection = ctx->tc_shape[0];
+    *expansion = ctx->tc_shape[1];
+    return CHFSI_OK;
+}
+
+extern "C" chfsi_status chfsi_set_tc_shapes(chfsi_ctx* ctx, int projection, int expansion) {
+    if (!ctx || projection < -1 || projection >= kTcVariantCount || expansion < -1 ||
+        expansion >= kTcVariantCount) {
+        set_last_error("chfsi_set_tc_shapes: shape outside -1..CHFSI_TC_SHAPES-1");
+        return CHFSI_ERR_BAD_INPUT;
+    }
+    ctx->tc_shape[0] = projection;
+    ctx->tc_shape[1] = expansion;
+    return CHFSI_OK;
+}
+
 extern "C" chfsi_status chfsi_set_launch_config(chfsi_ctx* ctx, int choice) {
     if (!ctx || choice < 0 || choice >= kLaunchConfigs) return CHFSI_ERR_BAD_INPUT;
     apply_launch_config(ctx, choice);
@@ -3580,9 +3706,20 @@ extern "C" chfsi_status chfsi_zgemm_cn(const chfsi_c128* a_dev, int lda, const c
 extern "C" chfsi_status chfsi_zgemm_cn_bf16x3(const chfsi_c128* a_dev, int lda,
                                               const chfsi_c128* b_dev, int ldb, int m, int n,
                                               int k, chfsi_c128* c_dev, void* stream) {
+    return chfsi_zgemm_cn_bf16x3_shape(a_dev, lda, b_dev, ldb, m, n, k, c_dev, stream, 0);
+}
+
+extern "C" chfsi_status chfsi_zgemm_cn_bf16x3_shape(const chfsi_c128* a_dev, int lda,
+                                                    const chfsi_c128* b_dev, int ldb, int m,
+                                                    int n, int k, chfsi_c128* c_dev, void* stream,
+                                                    int shape) {
     if (!a_dev || !b_dev || !c_dev || m <= 0 || n <= 0 || k <= 0 || lda < k || ldb < k ||
         k > kGemmMaxK) {
         g_last_error = "chfsi_zgemm_cn_bf16x3: null pointer, size outside 1..2^30 or lda/ldb < k";
+        return CHFSI_ERR_BAD_INPUT;
+    }
+    if (shape < 0 || shape >= kTcVariantCount) {
+        g_last_error = "chfsi_zgemm_cn_bf16x3_shape: shape outside 0..CHFSI_TC_SHAPES-1";
         return CHFSI_ERR_BAD_INPUT;
     }
     cudaStream_t st = (cudaStream_t)stream;
@@ -3605,7 +3742,7 @@ extern "C" chfsi_status chfsi_zgemm_cn_bf16x3(const chfsi_c128* a_dev, int lda,
     float* part = (float*)(buf + 3 * (na + nbe) * 2 + 256);
     tc_pack<double2>(reinterpret_cast<const double2*>(a_dev), lda, m, k, true, kSrcPlain, pa, st);
     tc_pack<double2>(reinterpret_cast<const double2*>(b_dev), ldb, n, k, false, kSrcPlain, pb, st);
-    e = tc_gemm(pa, pb, m, n, k, kTcOutPartial, c_dev, n, part, err, st);
+    e = tc_gemm(pa, pb, m, n, k, kTcOutPartial, c_dev, n, part, err, st, shape);
     int herr = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st);
     cudaFreeAsync(buf, st);

@@ -46,8 +46,12 @@ namespace {
 
 constexpr int kBM = 128;
 constexpr int kBK = 64;          // K padding and K-split granule (bf16 elements)
-constexpr int kSK = 32;          // K width of one stage: one 64-byte swizzle row of bf16
-constexpr int kStages = 3;
+// Stage shapes: SK = 32 (one 64-byte swizzle row of bf16 per tile row, 3
+// stages, BN up to 256) or SK = 64 (128-byte swizzle, 2 stages, BN up to 160);
+// both hold the six plane tiles of one K slice per stage.
+template <int SK> struct TcStage {
+    static constexpr int stages = SK == 32 ? 3 : 2;
+};
 constexpr int kThreads = 128;
 // hard cap on polls of one wait, whatever the clock says
 constexpr long long kSpinLimit = 1LL << 30;
@@ -108,15 +112,17 @@ __device__ __forceinline__ void tma_load_2d(void* smem_dst, const CUtensorMap* m
         : "memory");
 }
 
-// K-major, 64-byte swizzled operand tile: rows of 32 bf16 (64 B), 8-row
-// groups 512 B apart (SBO), start address advanced 32 B per K=16 step.
-__device__ __forceinline__ uint64_t umma_desc_sw64(uint32_t saddr) {
+// K-major swizzled operand tile: rows of SK bf16 (SK = 32: 64 B rows, 64-byte
+// swizzle, 8-row groups 512 B apart; SK = 64: 128 B rows, 128-byte swizzle,
+// 8-row groups 1024 B apart), start address advanced 32 B per K=16 step.
+template <int SK>
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
     uint64_t d = 0;
     d |= (uint64_t)((saddr >> 4) & 0x3FFF);
-    d |= (uint64_t)1 << 16;                 // leading byte offset (unused for swizzled K-major)
-    d |= (uint64_t)(512 >> 4) << 32;         // stride byte offset
+    d |= (uint64_t)1 << 16;                  // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t)((8 * SK * 2) >> 4) << 32;  // stride byte offset: 8 rows
     d |= (uint64_t)1 << 46;                  // descriptor version (sm_100)
-    d |= (uint64_t)4 << 61;                  // 64-byte swizzle
+    d |= (uint64_t)(SK == 32 ? 4 : 2) << 61; // 64-byte or 128-byte swizzle
     return d;
 }
 
@@ -160,11 +166,13 @@ struct TcMaps {
 // out modes
 enum { kOutPartialF32 = 0, kOutComplexF32 = 1, kOutComplexF64 = 2 };
 
-template <int MODE>
+template <int MODE, int SK>
 __global__ void __launch_bounds__(kThreads, 1)
 k_umma_split3(const __grid_constant__ TcMaps maps, int M2, int N, int bn, int ktiles_total,
               int ktiles_per_split, void* out, long long ldo, int* err,
               unsigned long long wait_ns, int no_loads) {
+    constexpr int kSK = SK;
+    constexpr int kStages = TcStage<SK>::stages;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     // 1024-byte aligned stage ring: stage s = [A1 A2 A3 B1 B2 B3]
     unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -267,8 +275,8 @@ k_umma_split3(const __grid_constant__ TcMaps maps, int M2, int N, int bn, int kt
             const uint32_t st_addr = smem_u32(base + (size_t)s * stage_bytes);
 #pragma unroll
             for (int t = 0; t < 6; ++t) {
-                const uint64_t da = umma_desc_sw64(st_addr + pa[t] * a_bytes);
-                const uint64_t db = umma_desc_sw64(st_addr + 3 * a_bytes + pb[t] * b_bytes);
+                const uint64_t da = umma_desc<SK>(st_addr + pa[t] * a_bytes);
+                const uint64_t db = umma_desc<SK>(st_addr + 3 * a_bytes + pb[t] * b_bytes);
                 const bool lead = t == 5;
                 const uint32_t acc = lead ? tmem : tmem + (uint32_t)acc_cols;
 #pragma unroll
@@ -424,28 +432,35 @@ PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
     return fn;
 }
 
-bool make_map(CUtensorMap* m, const void* ptr, int rows, int kp, int box_rows) {
+bool make_map(CUtensorMap* m, const void* ptr, int rows, int kp, int box_rows, int sk) {
     auto enc = get_encode();
     if (!enc || rows < box_rows) return false;
     cuuint64_t dims[2] = {(cuuint64_t)kp, (cuuint64_t)rows};
     cuuint64_t strides[1] = {(cuuint64_t)kp * 2};
-    cuuint32_t box[2] = {(cuuint32_t)kSK, (cuuint32_t)box_rows};
+    cuuint32_t box[2] = {(cuuint32_t)sk, (cuuint32_t)box_rows};
     cuuint32_t es[2] = {1, 1};
     CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr), dims, strides,
-                     box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+                     box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     sk == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B,
                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;
 }
 
-int pick_bn(int n) {
-    const int tiles = (n + 255) / 256;
+// Launch shapes the autotuner chooses from: stage K width and the largest
+// N tile (the N tiles of a product are balanced below that cap).
+struct TcVariant { int sk; int bn_cap; };
+constexpr TcVariant kTcVariants[kTcVariantCount] = {{32, 256}, {32, 128}, {64, 160}};
+
+int pick_bn(int n, int cap) {
+    const int tiles = (n + cap - 1) / cap;
     int bn = (n + tiles - 1) / tiles;
     bn = (bn + 15) / 16 * 16;
-    return bn < 16 ? 16 : (bn > 256 ? 256 : bn);
+    return bn < 16 ? 16 : (bn > cap ? cap : bn);
 }
 
-size_t smem_bytes(int bn) {
-    return 1024 + (size_t)kStages * 3 * (kBM * kSK * 2 + bn * kSK * 2) + (2 * kStages + 1) * 8 + 16;
+size_t smem_bytes(int bn, int sk) {
+    const int stages = sk == 32 ? TcStage<32>::stages : TcStage<64>::stages;
+    return 1024 + (size_t)stages * 3 * (kBM * sk * 2 + bn * sk * 2) + (2 * stages + 1) * 8 + 16;
 }
 
 int grid_for(long long n) {
@@ -483,8 +498,13 @@ int tc_splits(int tiles, int ktiles) {
 size_t tc_partial_floats(int M, int N, int K) {
     const int kp = tc_kpad(K);
     const int ktiles = kp / kBK;
-    const int mt = (2 * M + kBM - 1) / kBM, nt = (N + pick_bn(N) - 1) / pick_bn(N);
-    return (size_t)tc_splits(mt * nt, ktiles) * 2 * M * N;
+    const int mt = (2 * M + kBM - 1) / kBM;
+    size_t most = 0;
+    for (const TcVariant& v : kTcVariants) {
+        const int bn = pick_bn(N, v.bn_cap), nt = (N + bn - 1) / bn;
+        most = std::max(most, (size_t)tc_splits(mt * nt, ktiles) * 2 * M * N);
+    }
+    return most;
 }
 
 template <typename CIn>
@@ -513,20 +533,23 @@ void tc_pack(const CIn* x, long long ldx, int rows, int K, bool doubled, int src
 }
 
 int tc_rows_alloc(int rows, bool a_operand, int n_for_b) {
-    const int box = a_operand ? kBM : pick_bn(n_for_b);
+    // the largest TMA box of any variant (variant 0 has the largest N tiles)
+    const int box = a_operand ? kBM : pick_bn(n_for_b, kTcVariants[0].bn_cap);
     return rows < box ? box : rows;
 }
 
 cudaError_t tc_gemm(const TcPlanes& a, const TcPlanes& b, int M, int N, int K, int out_mode,
-                    void* out, long long ldo, float* part, int* err, cudaStream_t st) {
+                    void* out, long long ldo, float* part, int* err, cudaStream_t st, int variant) {
     if (a.kp != tc_kpad(K) || b.kp != a.kp || a.rows != 2 * M || b.rows != N)
         return cudaErrorInvalidValue;
-    const int bn = pick_bn(N);
+    if (variant < 0 || variant >= kTcVariantCount) return cudaErrorInvalidValue;
+    const TcVariant var = kTcVariants[variant];
+    const int bn = pick_bn(N, var.bn_cap);
     if (a.rows_alloc < kBM || b.rows_alloc < bn) return cudaErrorInvalidValue;
     TcMaps maps;
     for (int i = 0; i < 3; ++i) {
-        if (!make_map(&maps.a[i], a.p[i], a.rows_alloc, a.kp, kBM)) return cudaErrorInvalidValue;
-        if (!make_map(&maps.b[i], b.p[i], b.rows_alloc, b.kp, bn)) return cudaErrorInvalidValue;
+        if (!make_map(&maps.a[i], a.p[i], a.rows_alloc, a.kp, kBM, var.sk)) return cudaErrorInvalidValue;
+        if (!make_map(&maps.b[i], b.p[i], b.rows_alloc, b.kp, bn, var.sk)) return cudaErrorInvalidValue;
     }
     const int ktiles = a.kp / kBK;
     const int mt = (2 * M + kBM - 1) / kBM, nt = (N + bn - 1) / bn;
@@ -535,7 +558,7 @@ cudaError_t tc_gemm(const TcPlanes& a, const TcPlanes& b, int M, int N, int K, i
     const int kps = (ktiles + splits - 1) / splits;
     splits = (ktiles + kps - 1) / kps;
     dim3 grid(mt, nt, splits);
-    const size_t sm = smem_bytes(bn);
+    const size_t sm = smem_bytes(bn, var.sk);
     int no_loads = 0;
     unsigned long long wait_ns = kWaitNs;
     for (int left = g_inject_no_loads.load(); left > 0; left = g_inject_no_loads.load())
@@ -545,22 +568,23 @@ cudaError_t tc_gemm(const TcPlanes& a, const TcPlanes& b, int M, int N, int K, i
             break;
         }
     count_launch();
+    auto launch = [&](auto kernel, void* dst, long long ld) {
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        kernel<<<grid, kThreads, sm, st>>>(maps, 2 * M, N, bn, ktiles, kps, dst, ld, err, wait_ns,
+                                           no_loads);
+    };
+    const bool s64 = var.sk == 64;
     if (out_mode == kTcOutPartial) {
-        cudaFuncSetAttribute(k_umma_split3<kOutPartialF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k_umma_split3<kOutPartialF32><<<grid, kThreads, sm, st>>>(maps, 2 * M, N, bn, ktiles, kps,
-                                                                  part, N, err, wait_ns, no_loads);
+        if (s64) launch(k_umma_split3<kOutPartialF32, 64>, part, N);
+        else launch(k_umma_split3<kOutPartialF32, 32>, part, N);
         count_launch();
         k_reduce_tc<<<grid_for((long long)M * N), 256, 0, st>>>(part, splits, M, N, (double2*)out);
     } else if (out_mode == kTcOutComplexF32) {
-        cudaFuncSetAttribute(k_umma_split3<kOutComplexF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k_umma_split3<kOutComplexF32><<<grid, kThreads, sm, st>>>(maps, 2 * M, N, bn, ktiles, kps,
-                                                                  out, ldo, err, wait_ns,
-                                                                  no_loads);
+        if (s64) launch(k_umma_split3<kOutComplexF32, 64>, out, ldo);
+        else launch(k_umma_split3<kOutComplexF32, 32>, out, ldo);
     } else {
-        cudaFuncSetAttribute(k_umma_split3<kOutComplexF64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k_umma_split3<kOutComplexF64><<<grid, kThreads, sm, st>>>(maps, 2 * M, N, bn, ktiles, kps,
-                                                                  out, ldo, err, wait_ns,
-                                                                  no_loads);
+        if (s64) launch(k_umma_split3<kOutComplexF64, 64>, out, ldo);
+        else launch(k_umma_split3<kOutComplexF64, 32>, out, ldo);
     }
     return cudaGetLastError();
 }

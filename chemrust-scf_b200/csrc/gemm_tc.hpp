@@ -40,7 +40,11 @@ void tc_pack(const CIn* x, long long ldx, int rows, int K, bool doubled, int src
 // error word is set, nothing is left in flight).
 void tc_inject_no_loads(int launches);
 
+// Launch shapes of the autotuner (stage K width, largest N tile):
+// 0: K 32, N <= 256; 1: K 32, N <= 128; 2: K 64, N <= 160.
+constexpr int kTcVariantCount = 3;
 cudaError_t tc_gemm(const TcPlanes& a, const TcPlanes& b, int M, int N, int K, int out_mode,
-                    void* out, long long ldo, float* part, int* err, cudaStream_t st);
+                    void* out, long long ldo, float* part, int* err, cudaStream_t st,
+                    int variant = 0);
 
 }  // namespace chfsi

@@ -93,7 +93,9 @@ enum {
  * the Ritz pairs with the Woodbury S^-1 as approximate inverse: the same
  * span in exact arithmetic, and in the mixed-precision mode an FP32/BF16x3
  * filter whose error falls with the residual instead of stalling at FP32
- * rounding.  The norm guard does not apply to the residual recurrence. */
+ * rounding.  The norm guard does not apply to the residual recurrence.  In a
+ * mixed-precision context the FP64 passes (first pass, convergence checks)
+ * keep the Chebyshev form. */
 enum { CHFSI_FILTER_CHEBYSHEV = 0, CHFSI_FILTER_RESIDUAL = 1 };
 
 /* ------------------------------------------------------------------------ */
@@ -295,6 +297,19 @@ chfsi_status chfsi_zgemm_cn_noalloc(const chfsi_c128* a_dev, int lda, const chfs
  * with FP32 accumulation (the mixed-precision filter's projector GEMM). */
 chfsi_status chfsi_zgemm_cn_bf16x3(const chfsi_c128* a_dev, int lda, const chfsi_c128* b_dev,
                                    int ldb, int m, int n, int k, chfsi_c128* c_dev, void* stream);
+/* The same with an explicit launch shape of the tcgen05 kernel:
+ * 0: stages of K 32 (64-byte swizzle, 3 stages), N tiles up to 256;
+ * 1: K 32, N tiles up to 128; 2: K 64 (128-byte swizzle, 2 stages), N up to 160. */
+#define CHFSI_TC_SHAPES 3
+chfsi_status chfsi_zgemm_cn_bf16x3_shape(const chfsi_c128* a_dev, int lda, const chfsi_c128* b_dev,
+                                         int ldb, int m, int n, int k, chfsi_c128* c_dev,
+                                         void* stream, int shape);
+/* Launch shapes of a mixed-precision context's two projector GEMMs
+ * (projection beta^H x, expansion beta F).  The context times every shape on
+ * its own sizes at its first mixed-precision filter (outside stream capture)
+ * and keeps the fastest; chfsi_set_tc_shapes fixes them instead (-1: tune). */
+chfsi_status chfsi_get_tc_shapes(chfsi_ctx* ctx, int* projection, int* expansion);
+chfsi_status chfsi_set_tc_shapes(chfsi_ctx* ctx, int projection, int expansion);
 
 
 /* ------------------------------------------------------------------------ */
@@ -362,12 +377,11 @@ typedef struct chfsi_scf_params {
                              (f > 0.01) to change by less than this (Ha) from the
                              previous iteration; mixed runs switch to FP64 only after
                              two mixed iterations with |dE| below the switch and
-                             eigenvalue changes below the eigenvalue switch; an FP64
-                             iteration with changes above 10 x that switch returns
-                             to mixed                                                 */
+                             eigenvalue changes below the eigenvalue switch          */
     double fp64_switch_eig; /* eigenvalue switch of mixed runs: max(this, 2 x tol_eig)
-                               (the mixed iterations' eigenvalue changes carry FP32
-                               noise of ~2e-7 Ha on the 216-atom cell)               */
+                               (on the 216-atom cell the mixed iterations' eigenvalue
+                               changes level off at 1-3e-6 Ha: FP32 rounding of the
+                               filtered bands, ~1e-7 relative in the density)        */
 } chfsi_scf_params;
 
 /* Density mixers of chfsi_scf_run.  PULAY: Pulay/DIIS over (rho_in,

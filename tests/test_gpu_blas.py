@@ -44,27 +44,28 @@ def test_zgemm_cn_matches_numpy(chfsi, m, n, k):
     assert np.abs(out - ref).max() <= 1e-12 * np.abs(ref).max() * max(1.0, np.sqrt(k / 100))
 
 
-def run_bf16x3(chfsi, A, B):
+def run_bf16x3(chfsi, A, B, shape=None):
     m, k = A.shape
     n = B.shape[0]
     a = torch.from_numpy(np.ascontiguousarray(A)).cuda()
     b = torch.from_numpy(np.ascontiguousarray(B)).cuda()
     c = torch.zeros((m, n), dtype=torch.complex128, device="cuda")
     chfsi.zgemm_cn_bf16x3(a.data_ptr(), k, b.data_ptr(), k, m, n, k, c.data_ptr(),
-                          torch.cuda.current_stream().cuda_stream)
+                          torch.cuda.current_stream().cuda_stream, shape=shape)
     return c.cpu().numpy()
 
 
+@pytest.mark.parametrize("shape", [0, 1, 2])
 @pytest.mark.parametrize("m,n,k", [(20, 20, 2945), (160, 160, 37073), (256, 160, 37073),
-                                   (65, 130, 1000), (1, 7, 300)])
-def test_tcgen05_bf16x3_matches_fp64(chfsi, m, n, k):
+                                   (65, 130, 1000), (1, 7, 300), (40, 300, 500)])
+def test_tcgen05_bf16x3_matches_fp64(chfsi, m, n, k, shape):
     """BF16 3-way split on tcgen05: error at the FP32 level (bound 1e-6 relative
     to the product of norms)."""
     rng = np.random.default_rng(m * 7 + n + k)
     A = rng.standard_normal((m, k)) + 1j * rng.standard_normal((m, k))
     B = rng.standard_normal((n, k)) + 1j * rng.standard_normal((n, k))
     ref = np.conj(A) @ B.T
-    out = run_bf16x3(chfsi, A, B)
+    out = run_bf16x3(chfsi, A, B, shape)
     scale = np.sqrt(k) * 2.0  # typical |C| for unit-variance entries
     assert np.abs(out - ref).max() < 1e-6 * scale * 10
 

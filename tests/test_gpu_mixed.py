@@ -75,3 +75,28 @@ def test_scf_does_not_depend_on_earlier_contexts(chfsi, oracle, sys0):
     del a, b
     e = c.run_scf(12, max_iter=3, kT=0.01)["energies"]
     np.testing.assert_allclose(e, ref, rtol=0, atol=1e-8)
+
+
+def test_tc_shapes_tuned_per_size_class_and_results_close(chfsi):
+    # the projector GEMMs' launch shapes are timed at the first mixed filter
+    # of a size class and shared by every context of that size; a forced
+    # shape gives the same eigenvalues to the FP32-filter level
+    s = chfsi.SyntheticSystem(config_index=0, n_shell=1, lmax=1, rc_proj=[1.2, 0, 0, 0],
+                              d_min=0.5, d_max=2.0)
+    ctxs = [chfsi.Context(s, precision=chfsi.PREC_MIXED) for _ in range(2)]
+    shapes = [c.tc_shapes() for c in ctxs]
+    assert all(0 <= a < chfsi.TC_SHAPES and 0 <= b < chfsi.TC_SHAPES for a, b in shapes)
+    assert shapes[0] == shapes[1]
+    ws = []
+    for forced in (None, (0, 0), (2, 1)):
+        c = chfsi.Context(s, precision=chfsi.PREC_MIXED)
+        if forced:
+            c.set_tc_shapes(*forced)
+        v = c.get_vloc()
+        c.set_veff(v)
+        w = c.diagonalize(8)
+        for _ in range(3):
+            w = c.diagonalize(8, w)
+        ws.append(w)
+    for w in ws[1:]:
+        np.testing.assert_allclose(w, ws[0], atol=1e-7, rtol=0)
