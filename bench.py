@@ -336,6 +336,12 @@ SCF_TOL_PER_ATOM = 1e-6   # |dE| per atom (Ha)
 # FP64 iterations then need ~30 iterations to move the density to the FP64
 # fixed point.
 SCF_TOL_EIG = {"64": 1e-7, "216": 1e-6}
+# filter form of each arm: the mixed + Pulay arm's FP32 passes run R-ChFSI;
+# the learned arm keeps the plain FP32 filter (with R-ChFSI the Pulay
+# continuation after the learned mixer's hand-over stalled at density residuals
+# of 2-5e-5 on the 216-atom cell in two runs)
+FILTER_FORM = {"fp64": lambda c: c.FILTER_CHEBYSHEV, "mixed": lambda c: c.FILTER_RESIDUAL,
+               "mixed_learned": lambda c: c.FILTER_CHEBYSHEV}
 TIGHT_TOL_PER_ATOM = 1e-10
 TIGHT_TOL_EIG = 1e-9
 
@@ -354,8 +360,7 @@ def time_to_scf(chfsi, s, ndeg, device, net, max_iter, tight_max_iter, cell):
     for name, prec, mode in arms:
         t0 = time.time()
         ctx = chfsi.Context(s, device=device, precision=prec,
-                            filter_form=chfsi.FILTER_RESIDUAL if prec == chfsi.PREC_MIXED
-                            else chfsi.FILTER_CHEBYSHEV)
+                            filter_form=FILTER_FORM[name](chfsi))
         setup[name] = time.time() - t0
         if mode != chfsi.MIXER_PULAY:
             ctx.set_mixer(net)
@@ -369,9 +374,10 @@ def time_to_scf(chfsi, s, ndeg, device, net, max_iter, tight_max_iter, cell):
     n_occ = s.n_occ
     out = {"criterion": "|dE| < %g Ha/atom and occupied eigenvalues changing by < %g Ha "
                         "on an FP64 iteration (Fermi-Dirac kT = 0.01 Ha; Pulay alpha 0.3, "
-                        "history 6); mixed arms (R-ChFSI FP32 filter, BF16x3 projector "
-                        "GEMMs, FP64 Rayleigh-Ritz) filter in FP64 once two mixed iterations "
-                        "change the eigenvalues by < %g Ha"
+                        "history 6); mixed arms (FP32 filter, BF16x3 projector GEMMs, FP64 "
+                        "Rayleigh-Ritz; R-ChFSI form in the mixed + Pulay arm) filter in "
+                        "FP64 once two mixed iterations change the eigenvalues by < %g Ha "
+                        "or those changes level off"
                         % (SCF_TOL_PER_ATOM, SCF_TOL_EIG[cell], 2 * SCF_TOL_EIG[cell]),
            "reference": "FP64 run continued for up to %d more iterations toward |dE| < %g "
                         "Ha/atom and eigenvalue changes < %g Ha" % (tight_max_iter,

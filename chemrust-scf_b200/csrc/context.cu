@@ -2848,6 +2848,7 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
     if (learned && (s = alloc_mix(ctx))) return s;
     MixRing ring;
     int low_mixed = 0;  // mixed iterations in a row with |dE| below the switch
+    std::vector<double> mixed_deig;  // eigenvalue changes of the mixed iterations
     constexpr int kMaxReverts = 3;
     int reverts = 0;
     bool have_prev = false, fell_back = false;
@@ -3029,12 +3030,30 @@ extern "C" chfsi_status chfsi_scf_run(chfsi_ctx* ctx, const chfsi_scf_params* p,
         // eigenvalues by up to ~1e-4 Ha while the density relaxes from the
         // mixed-precision iterate (its FP32 rounding, ~1e-7 relative in the
         // density, shifts V_eff), which is the work the FP64 iterations do.
+        // The mixed iterations' eigenvalue changes level off at the FP32
+        // filter's floor: once the best change of the last eight mixed
+        // iterations is below three times the switch but not below half the
+        // best of the mixed iterations before them (a plateau), the eigenvalue
+        // test of the switch counts as met.
         const double sw = std::max(p->fp64_switch_per_atom, p->tol_per_atom);
         if (ctx->mixed_active) {
-            low_mixed = de < sw && eig_near ? low_mixed + 1 : 0;
+            if (p->tol_eig > 0.0 && it > 1) mixed_deig.push_back(deig);
+            bool plateau = false;
+            const int nm = (int)mixed_deig.size();
+            if (nm >= 12) {
+                const double recent = *std::min_element(mixed_deig.end() - 8, mixed_deig.end());
+                const double before = *std::min_element(mixed_deig.begin(), mixed_deig.end() - 8);
+                plateau = recent < 3.0 * sw_eig && recent > 0.5 * before;
+            }
+            low_mixed = de < sw && (eig_near || plateau) ? low_mixed + 1 : 0;
             if (low_mixed >= 2) {
+                if (p->verbose)
+                    std::fprintf(stderr, "scf %3d: FP64 filter from here (%s)\n", it,
+                                 eig_near ? "eigenvalue changes below the switch"
+                                          : "mixed eigenvalue changes level off");
                 ctx->mixed_active = false;
                 low_mixed = 0;
+                mixed_deig.clear();
             }
         } else if (ctx->mixed && de > 10.0 * sw &&
                    reverts < kMaxReverts) {

@@ -377,7 +377,10 @@ typedef struct chfsi_scf_params {
                              (f > 0.01) to change by less than this (Ha) from the
                              previous iteration; mixed runs switch to FP64 only after
                              two mixed iterations with |dE| below the switch and
-                             eigenvalue changes below the eigenvalue switch          */
+                             eigenvalue changes below the eigenvalue switch, or
+                             levelled off below three times it (the best of the
+                             last eight mixed iterations not below half the best
+                             before them)                                           */
     double fp64_switch_eig; /* eigenvalue switch of mixed runs: max(this, 2 x tol_eig)
                                (on the 216-atom cell the mixed iterations' eigenvalue
                                changes level off at 1-3e-6 Ha: FP32 rounding of the
