@@ -483,6 +483,186 @@ k_planes_vloc_p3(C* __restrict__ work, const double* __restrict__ veff, HGeom g)
     }
 }
 
+// ------------------------- pass 2, FP32, two bands per CTA (compile-time plans)
+// The pipeline of k_planes_vloc_p3 for the FP32 filter with the same plane
+// position of bands 2p and 2p + 1 in one 16-byte shared-memory element: every
+// shared access is a 16-byte access in 8-lane phases, the case the lane
+// mapping and lane-ordered twiddles make conflict-free (8-byte elements in
+// 16-lane phases put two lines on the same bank groups), and each twiddle and
+// V(r) load serves both bands.  An odd last band runs alone (its partner
+// loads repeat it and are not stored).
+__device__ __forceinline__ float4 pair4(float2 a, float2 b) { return make_float4(a.x, a.y, b.x, b.y); }
+__device__ __forceinline__ float2 lo2(float4 v) { return make_float2(v.x, v.y); }
+__device__ __forceinline__ float2 hi2(float4 v) { return make_float2(v.z, v.w); }
+
+template <int V, int R0, int R1>
+__global__ void __launch_bounds__(PlanesCfg<double2, V>::threads, PlanesCfg<double2, V>::min_blocks)
+k_planes_vloc_p3x2(float2* __restrict__ work, const double* __restrict__ veff, int nb, HGeom g) {
+    constexpr int N = R0 * R1, LS = N | 1, T = R0 > R1 ? R0 : R1, PW = 32 / T;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* twx = reinterpret_cast<float2*>(smem_raw);
+    float2* twy = reinterpret_cast<float2*>(smem_raw + align16<float2>(N));
+    float4* plane = reinterpret_cast<float4*>(smem_raw + 2 * align16<float2>(N));
+    int* xl = reinterpret_cast<int*>(plane + (size_t)N * LS);
+    const int z = blockIdx.x, b0 = 2 * blockIdx.y;
+    const bool two = b0 + 1 < nb;
+    const int nxact = g.nxact;
+    p2_twiddles<R0, R1, float2>(twx, g.twd_x, g.twf_x);
+    p2_twiddles<R0, R1, float2>(twy, g.twd_y, g.twf_y);
+    for (int i = threadIdx.x; i < nxact; i += blockDim.x) xl[i] = g.xact[i];
+    __syncthreads();
+    float2* wa = work + ((size_t)b0 * g.nz + z) * g.ncol;
+    float2* wb = two ? work + ((size_t)(b0 + 1) * g.nz + z) * g.ncol : wa;
+    const int lane = threadIdx.x & 31;
+    int gi, li;
+    p2_lane<T, PW>(lane, gi, li);
+    const bool ing = gi < PW;
+    const int groups = (blockDim.x >> 5) * PW, gid = (threadIdx.x >> 5) * PW + gi;
+    const float2 zero = make_float2(0.f, 0.f);
+    // y lines through the active x positions: inverse, inputs from the columns
+    for (int l0 = 0; l0 < nxact; l0 += groups) {
+        const int l = l0 + gid;
+        const bool act = ing && l < nxact;
+        float4* line = plane + (act ? xl[l] : 0);
+        if (act && li < R0) {
+            const int* ci = g.colidx + (size_t)l * N + li * R1;
+            float2 xa[R1], xb[R1];
+#pragma unroll
+            for (int j = 0; j < R1; ++j) {
+                const int c = __ldg(ci + j);
+                xa[j] = c >= 0 ? wa[c] : zero;
+                xb[j] = c >= 0 ? wb[c] : zero;
+            }
+            dft_r<R1, 1>(xa);
+            dft_r<R1, 1>(xb);
+#pragma unroll
+            for (int m = 0; m < R1; ++m) line[swz(li * R1 + m, N) * LS] = pair4(xa[m], xb[m]);
+        }
+        __syncwarp();
+        if (act && li < R1) {
+            float2 xa[R0], xb[R0];
+#pragma unroll
+            for (int j = 0; j < R0; ++j) {
+                const float4 v = line[swz(li + j * R1, N) * LS];
+                xa[j] = lo2(v);
+                xb[j] = hi2(v);
+            }
+            p2_span_inverse<R0, R1, true>(xa, li, twy);
+            p2_span_inverse<R0, R1, true>(xb, li, twy);
+#pragma unroll
+            for (int j = 0; j < R0; ++j) line[swz(li + j * R1, N) * LS] = pair4(xa[j], xb[j]);
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+    // x rows: inverse (x positions without columns read as zero), x V(r),
+    // forward (only x positions with columns stored)
+    const double* vz = veff + (size_t)z * N * N;
+    for (int y0 = 0; y0 < N; y0 += groups) {
+        const int y = y0 + gid;
+        const bool act = ing && y < N;
+        float4* row = plane + (act ? swz(y, N) * LS : 0);
+        if (act && li < R0) {
+            float2 xa[R1], xb[R1];
+#pragma unroll
+            for (int j = 0; j < R1; ++j) {
+                const int px = li * R1 + j;
+                const bool on = (g.xbits[px >> 5] >> (px & 31)) & 1u;
+                const float4 v = on ? row[swz(px, N)] : make_float4(0.f, 0.f, 0.f, 0.f);
+                xa[j] = lo2(v);
+                xb[j] = hi2(v);
+            }
+            dft_r<R1, 1>(xa);
+            dft_r<R1, 1>(xb);
+#pragma unroll
+            for (int m = 0; m < R1; ++m) row[swz(li * R1 + m, N)] = pair4(xa[m], xb[m]);
+        }
+        __syncwarp();
+        if (act && li < R1) {
+            float2 xa[R0], xb[R0];
+#pragma unroll
+            for (int j = 0; j < R0; ++j) {
+                const float4 v = row[swz(li + j * R1, N)];
+                xa[j] = lo2(v);
+                xb[j] = hi2(v);
+            }
+            p2_span_inverse<R0, R1, true>(xa, li, twx);
+            p2_span_inverse<R0, R1, true>(xb, li, twx);
+            const double* vr = vz + (size_t)y * N + li;
+#pragma unroll
+            for (int m = 0; m < R0; ++m) {
+                const float s = (float)vr[m * R1];
+                xa[m] = cscale(xa[m], s);
+                xb[m] = cscale(xb[m], s);
+            }
+            p2_span_forward<R0, R1, true>(xa, li, twx);
+            p2_span_forward<R0, R1, true>(xb, li, twx);
+#pragma unroll
+            for (int j = 0; j < R0; ++j) row[swz(li + j * R1, N)] = pair4(xa[j], xb[j]);
+        }
+        __syncwarp();
+        if (act && li < R0) {
+            float2 xa[R1], xb[R1];
+#pragma unroll
+            for (int j = 0; j < R1; ++j) {
+                const float4 v = row[swz(li * R1 + j, N)];
+                xa[j] = lo2(v);
+                xb[j] = hi2(v);
+            }
+            dft_r<R1, -1>(xa);
+            dft_r<R1, -1>(xb);
+#pragma unroll
+            for (int m = 0; m < R1; ++m) {
+                const int px = li * R1 + m;
+                if ((g.xbits[px >> 5] >> (px & 31)) & 1u) row[swz(px, N)] = pair4(xa[m], xb[m]);
+            }
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+    // y lines forward, outputs to the columns
+    for (int l0 = 0; l0 < nxact; l0 += groups) {
+        const int l = l0 + gid;
+        const bool act = ing && l < nxact;
+        float4* line = plane + (act ? xl[l] : 0);
+        if (act && li < R1) {
+            float2 xa[R0], xb[R0];
+#pragma unroll
+            for (int j = 0; j < R0; ++j) {
+                const float4 v = line[swz(li + j * R1, N) * LS];
+                xa[j] = lo2(v);
+                xb[j] = hi2(v);
+            }
+            p2_span_forward<R0, R1, true>(xa, li, twy);
+            p2_span_forward<R0, R1, true>(xb, li, twy);
+#pragma unroll
+            for (int j = 0; j < R0; ++j) line[swz(li + j * R1, N) * LS] = pair4(xa[j], xb[j]);
+        }
+        __syncwarp();
+        if (act && li < R0) {
+            float2 xa[R1], xb[R1];
+#pragma unroll
+            for (int j = 0; j < R1; ++j) {
+                const float4 v = line[swz(li * R1 + j, N) * LS];
+                xa[j] = lo2(v);
+                xb[j] = hi2(v);
+            }
+            dft_r<R1, -1>(xa);
+            dft_r<R1, -1>(xb);
+            const int* ci = g.colidx + (size_t)l * N + li * R1;
+#pragma unroll
+            for (int m = 0; m < R1; ++m) {
+                const int c = __ldg(ci + m);
+                if (c >= 0) {
+                    wa[c] = xa[m];
+                    if (two) wb[c] = xb[m];
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
 // ---------------------------------------------------------------- pass 3
 template <typename C, int MODE, int kColsPerBlock, int R0, int R1>
 __global__ void __launch_bounds__(256, ZCfg<R0>::min_blocks)
@@ -822,6 +1002,20 @@ template <typename C, int V, int R0, int R1>
 void planes_vloc_p2(C* work, const double* veff, int nb, const HGeom& g, cudaStream_t st) {
     dim3 grid(g.nz, nb);
     size_t sm = planes_smem_bytes(g, sizeof(C));
+    if constexpr (sizeof(C) == 8) {
+        // FP32: two bands per CTA in 16-byte elements, where two such CTAs
+        // still fit one SM's shared memory (planes up to 80 x 80)
+        const size_t sm2 = 2 * align16<float2>(R0 * R1) +
+                           (size_t)R0 * R1 * ((R0 * R1) | 1) * sizeof(float4) +
+                           (size_t)g.nxact * sizeof(int);
+        if (g.colidx && R0 * R1 <= 256 && sm2 <= 112 * 1024) {
+            dim3 grid2(g.nz, (nb + 1) / 2);
+            allow_smem(k_planes_vloc_p3x2<V, R0, R1>, sm2);
+            k_planes_vloc_p3x2<V, R0, R1><<<grid2, PlanesCfg<double2, V>::threads, sm2, st>>>(
+                reinterpret_cast<float2*>(work), veff, nb, g);
+            return;
+        }
+    }
     if (g.colidx && R0 * R1 <= 256) {
         allow_smem(k_planes_vloc_p3<C, V, R0, R1>, sm);
         k_planes_vloc_p3<C, V, R0, R1><<<grid, PlanesCfg<C, V>::threads, sm, st>>>(work, veff, g);

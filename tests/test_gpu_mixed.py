@@ -20,7 +20,14 @@ def sys1s(chfsi):
     return chfsi.SyntheticSystem(config_index=1, n_bands=132)
 
 
-@pytest.mark.parametrize("which,ndeg,passes", [("sys0", 12, 3), ("sys1s", 16, 2)])
+@pytest.fixture(scope="module")
+def sys0odd(chfsi):
+    # odd band count: the FP32 plane pass runs two bands per CTA, the last alone
+    return chfsi.SyntheticSystem(config_index=0, n_bands=21)
+
+
+@pytest.mark.parametrize("which,ndeg,passes", [("sys0", 12, 3), ("sys1s", 16, 2),
+                                               ("sys0odd", 12, 3)])
 def test_mixed_diagonalize_close_to_fp64(chfsi, oracle, which, ndeg, passes, request):
     s = request.getfixturevalue(which)
     ctx = chfsi.Context(s, precision=chfsi.PREC_MIXED)
