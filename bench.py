@@ -278,8 +278,8 @@ def run_ours(args):
         if not args.no_scf and world == 1:
             import learned_mixer
             net = learned_mixer.load(device=local)
-            mixed["time_to_scf"] = time_to_scf(chfsi, s, NDEG, local, net, max_iter=100,
-                                               tight_max_iter=40, cell="64")
+            mixed["time_to_scf"] = guarded(time_to_scf, chfsi, s, NDEG, local, net, max_iter=100,
+                                           tight_max_iter=40, cell="64")
 
     # ---- headline: time-to-SCF of the 216-atom ultrasoft cell (N = 1 only) ----
     scf216 = None
@@ -287,8 +287,8 @@ def run_ours(args):
         import learned_mixer
         s2 = chfsi.SyntheticSystem(config_index=2)
         net = learned_mixer.load(device=local)
-        scf216 = time_to_scf(chfsi, s2, 16, local, net, max_iter=args.scf_216_max_iter,
-                             tight_max_iter=20, cell="216")
+        scf216 = guarded(time_to_scf, chfsi, s2, 16, local, net, max_iter=args.scf_216_max_iter,
+                         tight_max_iter=20, cell="216")
         scf216["workload"] = ("216-atom ultrasoft cell, a=30.78 bohr, Ecut 25 Ha, n_pw=%d, "
                               "grid 108^3 (density 144^3), %d bands, %d projectors, degree 16"
                               % (s2.n_pw, s2.n_bands, s2.n_proj))
@@ -296,11 +296,11 @@ def run_ours(args):
 
     batched = None
     if world == 1 and not args.no_batch:
-        batched = batched_passes(chfsi, local)
+        batched = guarded(batched_passes, chfsi, local)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(steps=2)
+        cpu = guarded(cpu_baseline, steps=2)
 
     if rank == 0:
         line = {
@@ -324,6 +324,17 @@ def run_ours(args):
         dist.barrier()
         dist.destroy_process_group()
     ctx.close()
+
+
+def guarded(fn, *a, **kw):
+    """Run one of the line's optional blocks (single-process only); a failure
+    is reported in the block instead of losing the whole JSON line."""
+    try:
+        return fn(*a, **kw)
+    except Exception as e:  # the headline value and e2e are already measured
+        import traceback
+        traceback.print_exc()
+        return {"error": "%s: %s" % (type(e).__name__, e)}
 
 
 # time-to-SCF stopping rule of every timed arm, and the tight FP64 reference
