@@ -39,6 +39,7 @@
 #include <atomic>
 #include <cstring>
 #include <mutex>
+#include <unordered_map>
 
 namespace chfsi {
 
@@ -451,6 +452,63 @@ bool make_map(CUtensorMap* m, const void* ptr, int rows, int kp, int box_rows, i
 struct TcVariant { int sk; int bn_cap; };
 constexpr TcVariant kTcVariants[kTcVariantCount] = {{32, 256}, {32, 128}, {64, 160}};
 
+// Tensor maps are a pure function of (address, rows, K padding, box rows,
+// stage K width); the planes of a context live as long as the context, so
+// their maps are encoded once and reused.  The cache is cleared when it grows
+// past kMapCacheMax entries (one-off operands of chfsi_zgemm_cn_bf16x3).
+struct MapKey {
+    const void* ptr;
+    int rows, kp, box, sk;
+    bool operator==(const MapKey& o) const {
+        return ptr == o.ptr && rows == o.rows && kp == o.kp && box == o.box && sk == o.sk;
+    }
+};
+struct MapKeyHash {
+    size_t operator()(const MapKey& k) const {
+        size_t h = std::hash<const void*>()(k.ptr);
+        for (int v : {k.rows, k.kp, k.box, k.sk}) h = h * 1000003u ^ std::hash<int>()(v);
+        return h;
+    }
+};
+constexpr size_t kMapCacheMax = 256;
+std::mutex g_map_mu;
+std::unordered_map<MapKey, CUtensorMap, MapKeyHash> g_map_cache;
+
+bool cached_map(CUtensorMap* m, const void* ptr, int rows, int kp, int box_rows, int sk) {
+    const MapKey key{ptr, rows, kp, box_rows, sk};
+    {
+        std::lock_guard<std::mutex> lk(g_map_mu);
+        auto it = g_map_cache.find(key);
+        if (it != g_map_cache.end()) {
+            *m = it->second;
+            return true;
+        }
+    }
+    if (!make_map(m, ptr, rows, kp, box_rows, sk)) return false;
+    std::lock_guard<std::mutex> lk(g_map_mu);
+    if (g_map_cache.size() >= kMapCacheMax) g_map_cache.clear();
+    g_map_cache.emplace(key, *m);
+    return true;
+}
+
+// Dynamic shared memory limit of a kernel, raised on a device only when a
+// launch needs more than it was last set to.
+std::mutex g_attr_mu;
+std::unordered_map<const void*, int> g_attr_smem[64];
+
+cudaError_t ensure_smem(const void* kernel, int bytes) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    std::lock_guard<std::mutex> lk(g_attr_mu);
+    int& have = g_attr_smem[dev][kernel];
+    if (have >= bytes) return cudaSuccess;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) have = bytes;
+    return e;
+}
+
 int pick_bn(int n, int cap) {
     const int tiles = (n + cap - 1) / cap;
     int bn = (n + tiles - 1) / tiles;
@@ -548,8 +606,8 @@ cudaError_t tc_gemm(const TcPlanes& a, const TcPlanes& b, int M, int N, int K, i
     if (a.rows_alloc < kBM || b.rows_alloc < bn) return cudaErrorInvalidValue;
     TcMaps maps;
     for (int i = 0; i < 3; ++i) {
-        if (!make_map(&maps.a[i], a.p[i], a.rows_alloc, a.kp, kBM, var.sk)) return cudaErrorInvalidValue;
-        if (!make_map(&maps.b[i], b.p[i], b.rows_alloc, b.kp, bn, var.sk)) return cudaErrorInvalidValue;
+        if (!cached_map(&maps.a[i], a.p[i], a.rows_alloc, a.kp, kBM, var.sk)) return cudaErrorInvalidValue;
+        if (!cached_map(&maps.b[i], b.p[i], b.rows_alloc, b.kp, bn, var.sk)) return cudaErrorInvalidValue;
     }
     const int ktiles = a.kp / kBK;
     const int mt = (2 * M + kBM - 1) / kBM, nt = (N + bn - 1) / bn;
@@ -569,7 +627,7 @@ cudaError_t tc_gemm(const TcPlanes& a, const TcPlanes& b, int M, int N, int K, i
         }
     count_launch();
     auto launch = [&](auto kernel, void* dst, long long ld) {
-        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        ensure_smem((const void*)kernel, (int)sm);
         kernel<<<grid, kThreads, sm, st>>>(maps, 2 * M, N, bn, ktiles, kps, dst, ld, err, wait_ns,
                                            no_loads);
     };
