@@ -18,8 +18,13 @@ needs every band: it follows the reference's planned Row/Column design
 The math of steps 2, 4 and 5 goes through an `ops` object: `DeviceOps` uses
 the library's own FP64 tensor-path GEMMs (chfsi_zgemm_cn / chfsi_zgemm_tn)
 and its Cholesky + Jacobi eigensolver (chfsi_hegv_dev) on CUDA tensors, the
-collectives are NCCL.  Ultrasoft cells (S_sub with the projector term) are
-not split this way; the generalised problem runs per cell.
+collectives are NCCL.
+
+For the ultrasoft overlap S = 1 + beta q beta^H the subspace overlap is
+S_sub = psi^H psi + C^H q C with C = beta^H psi: step 2 also forms the
+partial C_r = beta_r^H psi_r over the rank's plane waves, step 3 sums it
+with the two n_b^2 matrices (one all-reduce), and C^H q C is formed on every
+rank after the sum (it is not a sum of per-rank terms).
 """
 import numpy as np
 
@@ -111,9 +116,28 @@ def _all_to_all(x_blocks, recv_rows, send_cols, recv_cols, dist):
     return torch.cat(rows, dim=0)
 
 
-def rayleigh_ritz_bandsplit(psi_blk, hpsi_blk, nb, npw, rank, world, dist, ops):
+def qmat_dense(qblocks, proj_offsets):
+    """The block-diagonal n_proj x n_proj q from its per-ion blocks (the
+    layout of chfsi_set_qmat)."""
+    off = np.asarray(proj_offsets)
+    n = int(off[-1])
+    q = np.zeros((n, n), dtype=np.complex128)
+    k = 0
+    for i in range(len(off) - 1):
+        a, b = int(off[i]), int(off[i + 1])
+        ne = b - a
+        q[a:b, a:b] = np.asarray(qblocks[k:k + ne * ne]).reshape(ne, ne)
+        k += ne * ne
+    return q
+
+
+def rayleigh_ritz_bandsplit(psi_blk, hpsi_blk, nb, npw, rank, world, dist, ops, beta_pw=None,
+                            qmat=None):
     """Steps 1-6 for this rank's band block (torch complex128 tensors,
-    nb_r x npw).  Returns (new band block, eigenvalues of all bands)."""
+    nb_r x npw).  For the ultrasoft overlap, beta_pw is this rank's
+    plane-wave slice of the projectors (n_proj x its plane waves) and qmat
+    the dense n_proj x n_proj q (torch tensors).  Returns (new band block,
+    eigenvalues of all bands)."""
     import torch
     bands = split_counts(nb, world)
     pws = split_counts(npw, world)
@@ -123,11 +147,21 @@ def rayleigh_ritz_bandsplit(psi_blk, hpsi_blk, nb, npw, rank, world, dist, ops):
     # 2. partial subspace matrices over this rank's plane waves
     s = ops.gemm_cn(p, p)
     h = ops.gemm_cn(p, hp)
+    c = ops.gemm_cn(beta_pw, p) if beta_pw is not None else None
     # 3. sum over ranks
     if world > 1:
-        both = torch.view_as_real(torch.stack([s, h])).contiguous()
-        dist.all_reduce(both)
-        s, h = torch.view_as_complex(both)[0], torch.view_as_complex(both)[1]
+        mats = [s, h] + ([c] if c is not None else [])
+        flat = torch.cat([torch.view_as_real(m).reshape(-1) for m in mats])
+        dist.all_reduce(flat)
+        parts = torch.split(flat, [m.numel() * 2 for m in mats])
+        mats = [torch.view_as_complex(x.reshape(*m.shape, 2)) for x, m in zip(parts, mats)]
+        s, h = mats[0], mats[1]
+        if c is not None:
+            c = mats[2]
+    if c is not None:
+        # S_sub = psi^H psi + C^H q C: conj(C^T) (q C)
+        qc = qmat @ c
+        s = s + ops.gemm_cn(c.T.contiguous(), qc.T.contiguous())
     # 4. the small eigenproblem, redundant on every rank
     w, v = ops.hegv(h, s)
     # 5. rotation of this rank's plane-wave slice
