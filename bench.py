@@ -13,7 +13,10 @@ FP64 + Pulay, mixed precision + Pulay and mixed precision + the learned
 mixer, each stopped at |dE| < 1e-6 Ha/atom with the occupied eigenvalues
 changing by less than 1e-6 Ha between FP64 iterations, and each compared
 with the FP64 run continued (untimed) for further iterations toward tight
-convergence.
+convergence (about nine minutes), and the batched pass of 96 members (64
+k-points of the 8-atom cell and 32 cells of 8-64 atoms) as one CUDA graph
+against member by member.  --no-scf-216 and --no-batch skip those blocks; a
+block that fails reports its error in the line instead of losing it.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
