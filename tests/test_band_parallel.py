@@ -159,3 +159,14 @@ def test_two_rank_bandsplit_matches_one_process(uspp):
     ov = np.abs(np.sum(np.conj(sp) * psi_ref, axis=1))
     np.testing.assert_allclose(ov, 1.0, atol=1e-9)
     np.testing.assert_allclose(np.conj(psi) @ sp.T, np.eye(s.n_bands), atol=1e-10)
+
+
+def test_qmat_dense_layout():
+    # per-ion blocks in chfsi_set_qmat order -> block-diagonal matrix
+    off = np.array([0, 2, 5])
+    blocks = np.concatenate([np.arange(4) + 1j, np.arange(9) * 2.0 + 0j])
+    q = bp.qmat_dense(blocks, off)
+    assert q.shape == (5, 5)
+    np.testing.assert_array_equal(q[:2, :2], (np.arange(4) + 1j).reshape(2, 2))
+    np.testing.assert_array_equal(q[2:, 2:], (np.arange(9) * 2.0).reshape(3, 3))
+    assert not q[:2, 2:].any() and not q[2:, :2].any()

@@ -89,3 +89,27 @@ def test_shell_index_g0_and_symmetry():
     s = mo.shell_index(ngrid, recip).reshape(8, 12, 10)
     assert s[0, 0, 0] == 255
     assert (s[1:, 1:, 1:] == s[1:, 1:, 1:][::-1, ::-1, ::-1]).all()  # |G| = |-G|
+
+
+def test_training_cells_reproducible_and_dilute_cells_reach_large_edges():
+    # cell_params without dilute cells keeps the seeds' historical draws (the
+    # shipped weights were trained on them); dilute cells are 64-atom cells
+    # whose edge reaches the 216-atom cell's 30.78 bohr
+    import sys
+    import os
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "..", "chemrust-scf_b200"))
+    import learned_mixer as lm
+    a = [(p.lattice, p.n_rep, round(p.a_conv, 6), p.z_val)
+         for p in (lm.cell_params(sd) for sd in range(10_000, 10_040))]
+    b = [(p.lattice, p.n_rep, round(p.a_conv, 6), p.z_val)
+         for p in (lm.cell_params(sd, dilute_frac=0.0) for sd in range(10_000, 10_040))]
+    assert a == b
+    edges = []
+    for sd in range(20_000, 20_200):
+        p = lm.cell_params(sd, dilute_frac=0.3)
+        edge = p.a_conv * p.n_rep
+        if edge > 21.0:  # larger than the densest 64-atom cell (20.52 bohr)
+            assert (p.lattice, p.n_rep) == lm.CELL_KINDS[lm.DILUTE_KIND][:2]
+            edges.append(edge)
+    assert 30 <= len(edges) <= 90
+    assert max(edges) <= 30.78 + 1e-6 and min(edges) >= 20.52 * 1.5 ** (1 / 3) - 1e-6
