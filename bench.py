@@ -349,7 +349,7 @@ SCF_TOL_PER_ATOM = 1e-6   # |dE| per atom (Ha)
 # 216-atom cell's mixed iterations level off at changes of 1-3e-6 Ha and the
 # FP64 iterations then need ~30 iterations to move the density to the FP64
 # fixed point.
-SCF_TOL_EIG = {"64": 1e-7, "216": 1e-6}
+SCF_TOL_EIG = {"64": 1e-6, "216": 1e-6}
 # filter form of each arm: the mixed + Pulay arm's FP32 passes run R-ChFSI;
 # the learned arm keeps the plain FP32 filter (with R-ChFSI the Pulay
 # continuation after the learned mixer's hand-over stalled at density residuals
